@@ -1,0 +1,364 @@
+"""Benchmark of the MD step hot path: 1,048,576-atom Lennard-Jones argon, NVE, float32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one velocity-Verlet step of the whole system: the drift with the on-GPU reuse
+check, the neighbor rebuild behind its device flag, and the forces with the second half kick.
+Workload (synthetic, seeded): a 64^3-cell FCC lattice (4 sites per cell) in L = 36.77 nm
+(rho = 21.1 per nm^3) with Gaussian jitter 0.02 nm, sigma 0.34 nm, epsilon 0.996 kJ/mol, mass
+39.948 Da, cutoff 1.0 nm, skin 0.1 nm, dt 0.004 ps, Maxwell-Boltzmann velocities at 120 K.
+The working set (positions, velocities, forces, neighbor list of about 0.4 GB) is larger than
+the 126 MB L2, so no flush is needed between steps.
+
+Prints one JSON line (rank 0). With N > 1 each rank runs its own replica (the path does not
+shard: replicas only); ``value`` is the atom-steps of all ranks over the slowest rank's time.
+``--impl reference`` times the oracle port of the reference's algorithm on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ATOMS_PER_SIDE_CELLS = 64
+LENGTH = 36.77
+SIGMA, EPSILON, MASS, CUTOFF, SKIN, TIMESTEP, TEMPERATURE = 0.34, 0.996, 39.948, 1.0, 0.1, 0.004, 120.0
+WORKLOAD = "LJ argon NVE, 1,048,576 atoms (64^3-cell FCC, L=36.77 nm, rho=21.1/nm^3), fp32"
+METRIC = "atom-steps/s, 1M-atom LJ fp32 NVE"
+# Algorithmic traffic of the force kernel per atom and launch: read x (12 B) and v (12 B),
+# write F (12 B) and v (12 B), and the neighbor indices a half list needs, 58.8 x 4 B.
+FORCE_BYTES_PER_ATOM = 48 + 58.8 * 4
+# The step's algorithmic cost per atom-step: 307 B (state 72 B + 235 B indices) and
+# 44.2 in-cutoff half pairs x 26 flop.
+STEP_BYTES_PER_ATOM = 307.0
+STEP_FLOPS_PER_ATOM = 44.2 * 26
+
+
+def load_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        peaks = json.loads(path.read_text())
+        return {"hbm_gbs": float(peaks["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.process = None
+
+    def __enter__(self):
+        try:
+            self.process = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL,
+            )
+        except OSError:
+            self.process = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.process is not None:
+            time.sleep(0.25)
+            self.process.terminate()
+            self.process.wait(timeout=10)
+
+    def summary(self) -> dict:
+        self.file.seek(0)
+        rows = [line.split(",") for line in self.file.read().strip().splitlines() if line]
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        clocks = [float(r[1]) for r in rows if len(r) > 2 and r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({name for r in rows for name, value in zip(names, r[5:9])
+                          if "Active" in value and "Not" not in value})
+        return {
+            "sm_mhz": statistics.median(clocks) if clocks else None,
+            "sm_max_mhz": float(rows[0][2]) if rows[0][2].strip().replace(".", "").isdigit() else None,
+            "reasons": reasons,
+            "samples": len(rows),
+        }
+
+
+def build_system(torch, device, seed: int):
+    from nabladyn_b200 import lattice, md, potential
+
+    positions, cell = lattice.fcc(ATOMS_PER_SIDE_CELLS, LENGTH, 0.02, seed)
+    n = positions.shape[0]
+    dtype = torch.float32
+    model = potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64, device=device),
+        sigma=torch.tensor([SIGMA], dtype=dtype, device=device),
+        epsilon=torch.tensor([EPSILON], dtype=dtype, device=device),
+        cutoff=CUTOFF,
+    )
+    masses = torch.full((n,), MASS, dtype=dtype, device=device)
+    velocities = md.maxwell_boltzmann(masses, TEMPERATURE, seed=seed)
+    host = {
+        "positions": torch.tensor(positions, dtype=dtype).pin_memory(),
+        "velocities": velocities.cpu().pin_memory(),
+    }
+    x = host["positions"].to(device)
+    box = torch.tensor(cell, dtype=dtype, device=device)
+    simulation = md.nve(model, x, velocities, masses, box, timestep=TIMESTEP, skin=SKIN)
+    return simulation, host, n
+
+
+def cpu_port_rate(steps: int = 3, cells: int = 24) -> dict:
+    """The oracle port of the reference's step on the host: pairs by the C restatement of the
+    neighbor operator, LJ and velocity Verlet in float64 numpy, one thread.
+
+    Sample: a cells^3-cell FCC block of the same density (4 cells^3 atoms), ``steps`` steps,
+    the pairs rebuilt every step (the port keeps no list between steps).
+    """
+    from nabladyn_b200 import lattice
+    from oracle import lj
+    from oracle import neighbors as on
+
+    length = LENGTH * cells / ATOMS_PER_SIDE_CELLS
+    positions, cell = lattice.fcc(cells, length, 0.02, seed=1)
+    n = positions.shape[0]
+    rng = np.random.default_rng(1)
+    velocities = rng.normal(0.0, math.sqrt(0.00831446261815324 * TEMPERATURE / MASS), (n, 3))
+    x = on.wrap(positions, cell)
+    first, second, _ = on.pairs(x, cell, CUTOFF)
+    _, forces, _ = lj.energy_force_virial(x, cell, first, second, [SIGMA], [EPSILON], CUTOFF)
+    start = time.perf_counter()
+    for _ in range(steps):
+        velocities += 0.5 * TIMESTEP * forces / MASS
+        x = on.wrap(x + TIMESTEP * velocities, cell)
+        first, second, _ = on.pairs(x, cell, CUTOFF)
+        _, forces, _ = lj.energy_force_virial(x, cell, first, second, [SIGMA], [EPSILON], CUTOFF)
+        velocities += 0.5 * TIMESTEP * forces / MASS
+    elapsed = time.perf_counter() - start
+    return {
+        "value": n * steps / elapsed,
+        "unit": "atom-steps/s",
+        "cores": 1,
+        "kind": "port",
+        "sample": f"{steps} NVE steps of a {cells}^3-cell FCC block ({n} atoms, same density) "
+                  "by the oracle port (C neighbor restatement + float64 numpy LJ/Verlet)",
+        "seconds": elapsed,
+    }
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    # Each bench step is one port step of the sample; warm-up steps run untimed.
+    cpu_port_rate(steps=max(1, args.warmup), cells=12)
+    baseline = cpu_port_rate(steps=min(steps, 5), cells=24)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": baseline["value"],
+        "unit": "atom-steps/s",
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * baseline["seconds"] / min(steps, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": baseline["sample"]},
+        "cpu_baseline": baseline,
+        "e2e": {"value": baseline["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(value: float) -> float:
+        if world == 1:
+            return value
+        tensor = torch.tensor([value], dtype=torch.float64, device=device)
+        dist.all_reduce(tensor, op=dist.ReduceOp.MAX)
+        return float(tensor)
+
+    simulation, host, n = build_system(torch, device, seed=2024 + rank)
+    engine = simulation._engine
+    stream = torch.cuda.current_stream(device)
+    simulation.run(max(3, args.warmup))
+    torch.cuda.synchronize(device)
+
+    # value: K steps replayed from the captured graphs, timed by CUDA events.
+    rebuilds_before = simulation._rebuild_count
+    barrier()
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        simulation.run(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+    barrier()
+    elapsed_ms = max_over_ranks(start.elapsed_time(end))
+    rebuilds = simulation._rebuild_count - rebuilds_before
+    value = world * n * args.steps / (elapsed_ms / 1e3)
+
+    # Roofline of the dominant kernel: the same steps run eagerly, each phase between events.
+    phases = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    for events in phases:
+        events[0].record(stream)
+        for phase in range(3):
+            engine.step_phase(phase, False)
+            events[phase + 1].record(stream)
+    torch.cuda.synchronize(device)
+    phase_ms = [sum(e[p].elapsed_time(e[p + 1]) for e in phases) / args.steps for p in range(3)]
+    peaks = load_peaks()
+    force_bytes = FORCE_BYTES_PER_ATOM * n
+    achieved = force_bytes / (phase_ms[2] / 1e3) / 1e9
+    step_roof_s = STEP_BYTES_PER_ATOM / (peaks["hbm_gbs"] * 1e9)
+    traffic = None
+    traffic_file = ROOT / "profiles" / "force_kernel_traffic.json"
+    if traffic_file.exists():
+        traffic = json.loads(traffic_file.read_text()).get("bytes_per_launch_1m")
+
+    # e2e: the public API with host buffers: per call, the frame from pinned host memory,
+    # set_frame, run(chunk), state(), and the frame back into pinned host memory.
+    chunk = 100
+    calls = max(1, args.steps // chunk)
+    back = {name: torch.empty((n, 3), dtype=torch.float32).pin_memory()
+            for name in ("positions", "velocities", "forces")}
+    back_images = torch.empty((n, 3), dtype=torch.int64).pin_memory()
+    staged = {name: torch.empty((n, 3), dtype=torch.float32, device=device)
+              for name in ("positions", "velocities")}
+    barrier()
+    torch.cuda.synchronize(device)
+    e2e_start, e2e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_start.record(stream)
+    for _ in range(calls):
+        staged["positions"].copy_(host["positions"], non_blocking=True)
+        staged["velocities"].copy_(host["velocities"], non_blocking=True)
+        simulation.set_frame(staged["positions"], staged["velocities"])
+        simulation.run(chunk)
+        state = simulation.state()
+        back["positions"].copy_(state.positions, non_blocking=True)
+        back["velocities"].copy_(state.velocities, non_blocking=True)
+        back["forces"].copy_(state.forces, non_blocking=True)
+        back_images.copy_(state.images, non_blocking=True)
+    e2e_end.record(stream)
+    torch.cuda.synchronize(device)
+    e2e_ms = max_over_ranks(e2e_start.elapsed_time(e2e_end))
+    e2e_value = world * n * chunk * calls / (e2e_ms / 1e3)
+    h2d = 2 * n * 3 * 4 / chunk
+    d2h = (3 * n * 3 * 4 + n * 3 * 8) / chunk
+
+    cpu = cpu_port_rate() if (rank == 0 and world == 1) else None
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "atom-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": WORKLOAD,
+                "atoms_per_replica": n,
+                "ensemble": "NVE",
+                "timestep_ps": TIMESTEP,
+                "skin_nm": SKIN,
+                "parallelism": f"replicas x{world}",
+                "l2": "working set > L2 (126 MB); no flush",
+                "rebuilds_in_timed_steps": rebuilds,
+            },
+            "roofline": {
+                "kernel": "force_kernel (forces, second half kick, float64 tail)",
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peaks["hbm_gbs"],
+                "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"],
+                "peak_source": peaks["source"],
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": force_bytes,
+                "avg_launch_ms": phase_ms[2],
+            },
+            "phases_ms": {"drift": phase_ms[0], "rebuild_gated": phase_ms[1],
+                          "forces": phase_ms[2]},
+            "step_roofline": {
+                "bytes_per_atom_step": STEP_BYTES_PER_ATOM,
+                "flops_per_atom_step": STEP_FLOPS_PER_ATOM,
+                "t_roof_ps": step_roof_s * 1e12,
+                "frac": (value / world) * step_roof_s,
+            },
+            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps_per_call": chunk},
+            "gpu_launches": engine.step_launches * args.steps,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=1000)
+    parser.add_argument("--warmup", type=int, default=10)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,244 @@
+/*
+ * nabladyn_b200: the C-ABI of the B200 MD step hot path.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream (cudaStream_t passed
+ * as nd_stream_t), launches its kernels on that stream and returns ND_OK or an error code;
+ * nd_last_error() gives the calling thread's last message. No entry point allocates device
+ * memory, synchronizes the device or reads device memory on the host, so every call can be
+ * captured in a CUDA Graph. Callers own every buffer.
+ *
+ * Data errors (a cell too small, a non-finite coordinate, more pairs than the capacity) are
+ * not call errors: they are bits of a device status word, decoded by the host when it reads
+ * the status, exactly as in the reference's neighbor operator.
+ */
+#ifndef NABLADYN_B200_H
+#define NABLADYN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ND_OK 0
+#define ND_EINVAL 1 /* an argument is out of range; nothing was launched */
+#define ND_ECUDA 2  /* the CUDA runtime reported an error */
+
+#define ND_FLOAT32 0
+#define ND_FLOAT64 1
+
+/* Status bits of status[0]; they latch until the list is allocated again. */
+#define ND_STATUS_INVALID_CELL 1
+#define ND_STATUS_NON_FINITE 2
+#define ND_STATUS_OVERFLOW 8
+
+typedef void* nd_stream_t; /* a cudaStream_t */
+
+/* The calling thread's message for its last failed call. */
+const char* nd_last_error(void);
+
+/* The ABI version of this header: 1. */
+int nd_abi_version(void);
+
+/* ------------------------------------------------------------------------------------------
+ * The neighbor operator.
+ *
+ * Replaces the torch.library namespace nabladyn_neighbors of the reference
+ * (src/nabladyn/neighbors/csrc/ops.cpp:11-41, ops.h:12-89). The 15 buffers keep the
+ * reference's order and meaning; the host allocates them as
+ * src/nabladyn/neighbors/_neighbor_list.py:229-254 does (scan_temp sized by
+ * nd_neighbors_scan_temp_bytes). Positions and cell are [N, 3] and [3] of one dtype, with
+ * positions wrapped into [0, L).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct nd_neighbor_buffers {
+    int32_t* dims;           /* [3] bins per axis */
+    void* widths;            /* [3] bin widths, the positions' dtype */
+    int32_t* atom_bin;       /* [N] */
+    int32_t* bin_counts;     /* [B + 1], zero between builds */
+    int32_t* bin_offsets;    /* [B + 1] */
+    int64_t num_bin_slots;   /* B + 1 */
+    int32_t* unordered_ids;  /* [N] */
+    int32_t* sorted_ids;     /* [N] */
+    void* sorted_positions;  /* [N, 3], the positions' dtype */
+    uint8_t* scan_temp;      /* scratch of the scans */
+    int64_t scan_temp_bytes; /* its size */
+    int32_t* pair_counts;    /* [N] */
+    int32_t* pair_offsets;   /* [N] */
+    int32_t* pair_total;     /* [1] */
+    int32_t* status;         /* [2]: flags, pairs needed */
+    int32_t* pairs;          /* [2, C] */
+    int64_t capacity;        /* C */
+    int32_t* bits;           /* [N * ceil(N / 32)] on the all-pairs path, else NULL */
+    int64_t bits_numel;      /* 0 on the grid path */
+} nd_neighbor_buffers;
+
+/* The update's own buffers (src/nabladyn/neighbors/_neighbor_list.py:43-56, 265-272). */
+typedef struct nd_reuse_buffers {
+    void* reference_positions; /* [N, 3]: the frame of the last build */
+    void* reference_cell;      /* [3] */
+    const int32_t* limits;     /* [3]: the first grid's bins per axis */
+    void* reuse;               /* [4]: threshold^2, then the scale per axis */
+    int32_t* rebuild;          /* [1] */
+    int32_t* rebuild_count;    /* [1] */
+} nd_reuse_buffers;
+
+/* scan_temp_bytes(Tensor reference, int items) -> int
+ * (src/nabladyn/neighbors/csrc/runtime/entry_points.cu:284-301): the scratch bytes of a scan
+ * over `items` int32 values. */
+int nd_neighbors_scan_temp_bytes(int64_t items, int64_t* bytes);
+
+/* count_first_frame(positions, cell, radius, <15 buffers>)
+ * (src/nabladyn/neighbors/csrc/runtime/entry_points.cu:303-352): the grid and each atom's pair
+ * count, so the host can size the pairs. */
+int nd_neighbors_count_first_frame(int dtype, const void* positions, const void* cell,
+                                   int64_t num_atoms, double radius,
+                                   const nd_neighbor_buffers* buffers, nd_stream_t stream);
+
+/* fill_first_frame(positions, cell, radius, <15 buffers>)
+ * (src/nabladyn/neighbors/csrc/runtime/entry_points.cu:354-399): the pairs, into the capacity
+ * the host chose, then the total, the overflow check and the padding. */
+int nd_neighbors_fill_first_frame(int dtype, const void* positions, const void* cell,
+                                  int64_t num_atoms, double radius,
+                                  const nd_neighbor_buffers* buffers, nd_stream_t stream);
+
+/* update(positions, cell, cutoff, radius, reference_positions, reference_cell, limits, reuse,
+ *        rebuild, rebuild_count, <15 buffers>)
+ * (src/nabladyn/neighbors/csrc/runtime/entry_points.cu:401-508): check the cell, decide reuse
+ * on the GPU, rebuild behind the device flag and store the new reference frame. */
+int nd_neighbors_update(int dtype, const void* positions, const void* cell, int64_t num_atoms,
+                        double cutoff, double radius, const nd_reuse_buffers* reuse,
+                        const nd_neighbor_buffers* buffers, nd_stream_t stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Lennard-Jones over a [2, C] pair index.
+ *
+ * Replaces, for the Lennard-Jones model, the torch.func evaluation
+ * quantity.energy_force_virial(model)(positions, cell, pairs)
+ * (src/nabladyn/quantity.py:160-184 over src/nabladyn/potential/_lennard_jones/_potential.py:
+ * 209-234): E, F = -dE/dx and W = -dE/dstrain in one pass, plus dE/dsigma and dE/depsilon
+ * per type-pair row when sigma_grad is given. energy, virial and the gradients are float64.
+ * With a strain, every pair vector is deformed by (I + strain) first and F, W are the
+ * derivatives of that strained energy (src/nabladyn/space.py:51-64).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct nd_lj_pairs_args {
+    int dtype;
+    const void* positions;    /* [N, 3], wrapped into [0, L) */
+    const void* cell;         /* [3] */
+    int64_t num_atoms;        /* N */
+    const int32_t* pairs;     /* [2, C] */
+    int64_t capacity;         /* C */
+    const int32_t* atom_types; /* [N] in [0, T); ignored when T == 1 */
+    int32_t num_types;        /* T, 1..8 */
+    const void* sigma;        /* [T(T+1)/2] */
+    const void* epsilon;      /* [T(T+1)/2] */
+    double cutoff;
+    const void* strain;       /* [3, 3] strain, row-major; NULL for none */
+    double* energy;           /* [1] out */
+    void* forces;             /* [N, 3] out */
+    double* virial;           /* [3, 3] out */
+    double* sigma_grad;       /* [T(T+1)/2] out, or NULL */
+    double* epsilon_grad;     /* [T(T+1)/2] out, or NULL */
+} nd_lj_pairs_args;
+
+int nd_lj_energy_force_virial(const nd_lj_pairs_args* args, nd_stream_t stream);
+
+/* ------------------------------------------------------------------------------------------
+ * The MD engine: velocity-Verlet (NVE) and Nose-Hoover chain (NVT) steps of a Lennard-Jones
+ * system with the neighbor rebuild decided on the GPU.
+ *
+ * Replaces the step the reference assembles from three compiled programs around the neighbor
+ * operator and captures in a CUDA Graph (src/nabladyn/md/_simulation.py:316-364,
+ * src/nabladyn/md/_ensembles/_nve.py:39-58, _nvt.py:88-129, _verlet.py:8-31, _chain.py:36-83).
+ * Per-atom state lives in cell order (sorted by cell, then atom id, at each rebuild); `ids`
+ * maps a slot to the caller's atom. T is the system's dtype; positions are [N, 4] (x, y, z,
+ * type). The caller allocates every buffer; nd_md_partial_slots gives the size of partials.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct nd_md_system {
+    int dtype;
+    int64_t num_atoms;
+    int32_t num_types;       /* 1..8; types ride in positions[:, 3] */
+    int32_t small;           /* 1: one tile holds the whole system, minimum image per pair */
+    int32_t dims[3];         /* cells per axis (>= 3 each unless small) */
+    int32_t bricks_x;        /* bricks per row of cells along x */
+    int32_t width;           /* neighbor-list slots per atom */
+    int32_t tile_capacity;   /* atoms per brick tile, at most */
+    double cell[3];          /* orthorhombic cell lengths, fixed */
+    double widths[3];        /* cell widths, L / dims, rounded to T */
+    double cutoff;           /* LJ cutoff r_c */
+    double radius;           /* list radius R = r_c + skin */
+    double timestep;         /* dt */
+    double threshold_squared; /* reuse while every |x - x_ref|^2 is below this */
+    void* positions;         /* [N, 4] T */
+    void* velocities;        /* [N, 3] T */
+    void* forces;            /* [N, 3] T */
+    void* inverse_masses;    /* [N] T */
+    void* masses;            /* [N] T */
+    int64_t* images;         /* [N, 3] */
+    int32_t* ids;            /* [N] */
+    void* reference_positions; /* [N, 4] T */
+    void* shadow_positions;  /* the permutation's copies of the seven arrays above */
+    void* shadow_velocities;
+    void* shadow_forces;
+    void* shadow_inverse_masses;
+    void* shadow_masses;
+    int64_t* shadow_images;
+    int32_t* shadow_ids;
+    int32_t* cell_counts;    /* [cells + 1], zero between rebuilds */
+    int32_t* cell_offsets;   /* [cells + 1] */
+    int32_t* atom_cell;      /* [N] */
+    int32_t* slots;          /* [N] */
+    int32_t* unordered;      /* [N] */
+    int32_t* order;          /* [N] */
+    void* scan_temp;         /* nd_neighbors_scan_temp_bytes(cells + 1) bytes */
+    uint16_t* neighbors;     /* [ceil(N / 32) * 32 * width] */
+    int32_t* neighbor_counts; /* [N] */
+    int32_t* rebuild;        /* [1] */
+    int32_t* rebuild_count;  /* [1] */
+    int32_t* status;         /* [4]: flags, most neighbors needed, largest tile needed, largest tile built */
+    double* partials;        /* [nd_md_partial_slots] */
+    uint32_t* ticket;        /* [1], zero */
+    double* totals;          /* [16]: E, K, W xx yy zz xy xz yz; then K of nd_md_kinetic */
+    double* thermostat;      /* [24] float64 chain block */
+    const void* sigma;       /* [T(T+1)/2] T */
+    const void* epsilon;     /* [T(T+1)/2] T */
+} nd_md_system;
+
+/* Loads a frame in the caller's order: positions [N, 3] wrapped into [0, L), velocities,
+ * masses [N], images [N, 3] int64, types [N] int32 (NULL for one type). */
+int nd_md_import(const nd_md_system* system, const void* positions, const void* velocities,
+                 const void* masses, const int64_t* images, const int32_t* types,
+                 nd_stream_t stream);
+
+/* Wraps, re-sorts, permutes the state and builds the neighbor list, unconditionally. */
+int nd_md_rebuild(const nd_md_system* system, nd_stream_t stream);
+
+/* Forces and energy (and the virial) at the current positions; totals[0], totals[2..7]. */
+int nd_md_forces(const nd_md_system* system, int virial, nd_stream_t stream);
+
+/* One step: [NVT: chain half step] half kick, drift, reuse check; the rebuild behind the
+ * device flag; forces, half kick, [NVT: K and the closing chain half step]. */
+int nd_md_step(const nd_md_system* system, int thermostat, int virial, nd_stream_t stream);
+
+/* One phase of nd_md_step: 0 the drift and reuse check, 1 the gated rebuild, 2 the forces with
+ * the second half kick and the tail; -1 all three. Running 0, 1, 2 in order is one step. */
+int nd_md_step_phase(const nd_md_system* system, int phase, int thermostat, int virial,
+                     nd_stream_t stream);
+
+/* The number of kernels one nd_md_step launches. */
+int nd_md_step_launches(const nd_md_system* system, int64_t* launches);
+
+/* Writes the frame in the caller's order; any output may be NULL. */
+int nd_md_export(const nd_md_system* system, void* positions, void* velocities, void* forces,
+                 int64_t* images, int thermostat, nd_stream_t stream);
+
+/* K of the current velocities in float64, into totals[9]. */
+int nd_md_kinetic(const nd_md_system* system, int thermostat, nd_stream_t stream);
+
+/* The float64 slots the partials buffer needs. */
+int nd_md_partial_slots(const nd_md_system* system, int64_t* slots);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NABLADYN_B200_H */

@@ -1,0 +1,1402 @@
+// The MD engine: velocity-Verlet / Nose-Hoover steps of a Lennard-Jones system, with the
+// neighbor rebuild decided on the GPU, in a handful of kernels per step.
+//
+// It replaces, for one simulation, the reference's step of three compiled programs around the
+// neighbor operator (src/nabladyn/md/_simulation.py:316-364): programs[0] (chain half step,
+// half kick, drift, wrap), NeighborList._update_wrapped, programs[1] (LJ E/F by torch.func
+// and the second half kick, plus K for NVT) and programs[2] (the closing chain half step).
+//
+// Layout in HBM. The engine keeps every per-atom array in "cell order": the order of the last
+// rebuild, atoms sorted by cell and by atom id within a cell, so a cell's atoms are one
+// contiguous range. A rebuild re-sorts and permutes the state (positions, velocities, forces,
+// masses, images, ids, types); `ids` maps a slot back to the caller's atom. Positions are
+// [N] x (x, y, z, type) vectors, 16 B in float32, so one load fetches an atom. Between rebuilds
+// positions are NOT wrapped: an atom keeps the image it was binned in, which keeps every
+// precomputed cell image valid; a rebuild wraps them and counts the crossings.
+//
+// Bricks and tiles. Cells of at least the list radius are grouped along x into bricks of a few
+// cells. One CTA per brick stages the brick's 3 x 3 rows of neighbor cells (x extended by one
+// cell each way) into shared memory, each cell already shifted by its periodic image, with
+// coalesced 16-B loads. The neighbor list is a full list (both directions, no atomics) of
+// uint16 tile-local indices, interleaved by warps of 32 cell-order slots:
+//     entry (i, k) lives at ((i / 32) * width + k) * 32 + i % 32.
+// The force kernel re-stages the same tile from the current positions and reads every
+// neighbor from shared memory, so the only per-pair global traffic is the 2-B index.
+//
+// Small boxes (fewer than three cells on an axis) use one tile holding the whole system and
+// the minimum image per pair, as the reference's all-pairs path does.
+//
+// Reductions. Pair arithmetic is in the system's dtype; each block reduces its energy,
+// kinetic energy and virial in float64 into its own slot, and the last block to finish sums
+// the slots in a fixed order (deterministic totals) and runs the scalar tail: the Nose-Hoover
+// closing half step in float64 (src/nabladyn/md/_ensembles/_chain.py:36-83).
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <type_traits>
+
+#include "common.cuh"
+#include "geometry.cuh"
+#include "scan.cuh"
+
+namespace nd {
+
+template <typename T>
+struct alignas(4 * sizeof(T)) Pos4
+{
+    T x, y, z, w;
+};
+
+constexpr int kMDThreads = 128;
+constexpr int kMaxBrickCells = 14;                  // home cells per brick, at most
+constexpr int kMaxRowCells = kMaxBrickCells + 2;    // tile cells per row
+constexpr int kTileCells = 9 * kMaxRowCells;        // tile cells, at most
+constexpr int kReduced = 8;                         // E, K, W xx yy zz xy xz yz
+
+// Offsets into the float64 thermostat block.
+enum Thermo : int
+{
+    kChainA = 0,      // q[3], p[3] after the last closing half step
+    kKineticA = 6,    // carried K after the last closing half step
+    kChainB = 7,      // q[3], p[3] after this step's opening half step
+    kKineticB = 13,   // carried K after the opening
+    kPendingScale = 14,  // the closing factor not yet applied to the stored velocities
+    kOpenScale = 15,  // this step's opening factor
+    kChainMass = 16,  // Q[3]
+    kThermalEnergy = 19,  // kT
+    kDegrees = 20,    // g = 3N - 3
+    kTimestep = 21,
+    kThermoSize = 24,
+};
+
+// The device view of one system, built from nd_md_system.
+template <typename T>
+struct System
+{
+    Pos4<T>* pos;
+    T* vel;
+    T* force;
+    T* inv_mass;
+    T* mass;
+    long long* images;
+    index_t* ids;
+    Pos4<T>* ref_pos;
+    Pos4<T>* pos_b;
+    T* vel_b;
+    T* force_b;
+    T* inv_mass_b;
+    T* mass_b;
+    long long* images_b;
+    index_t* ids_b;
+    index_t* cell_counts;
+    index_t* cell_offsets;
+    index_t* atom_cell;
+    index_t* slot;
+    index_t* unordered;
+    index_t* order;
+    void* scan_temp;
+    std::uint16_t* nbr;
+    index_t* nbr_count;
+    index_t* rebuild;
+    index_t* rebuild_count;
+    index_t* status;
+    double* partials;
+    unsigned* ticket;
+    double* totals;
+    double* thermo;
+    const T* sigma;
+    const T* epsilon;
+    index_t n;
+    index_t dims[3];
+    T length[3];
+    T widths[3];
+    index_t bricks_x;
+    index_t num_bricks;
+    index_t width;
+    index_t tile_cap;
+    int small;
+    int num_types;
+    T dt;
+    T half_dt;
+    T threshold_squared;
+    T radius_squared;
+    T cutoff_squared;
+};
+
+// ---------------------------------------------------------------------------------------
+// Lennard-Jones parameters of a type pair, prepared once per block.
+
+template <typename T>
+struct PairParams
+{
+    T s2;     // sigma^2
+    T e4;     // 4 eps
+    T e24;    // 24 eps
+    T shift;  // u(r_c)
+};
+
+template <typename T>
+__device__ __forceinline__ PairParams<T> pair_params(T sigma, T epsilon, T cutoff_squared)
+{
+    PairParams<T> p;
+    p.s2 = sigma * sigma;
+    p.e4 = T(4) * epsilon;
+    p.e24 = T(24) * epsilon;
+    const T q = p.s2 / cutoff_squared;
+    const T q6 = q * q * q;
+    p.shift = p.e4 * (q6 * q6 - q6);
+    return p;
+}
+
+__device__ __forceinline__ float fast_reciprocal(float x)
+{
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ double fast_reciprocal(double x)
+{
+    return 1.0 / x;
+}
+
+__device__ __forceinline__ int type_pair_row(int a, int b, int num_types)
+{
+    const int low = a < b ? a : b;
+    const int high = a < b ? b : a;
+    return low * (2 * num_types - low - 1) / 2 + high;
+}
+
+// ---------------------------------------------------------------------------------------
+// Tiles.
+
+// The geometry of one brick's tile in shared memory. Row r = 3 (dz + 1) + (dy + 1) holds the
+// tile cells c = 0 .. cells_per_row - 1 at x = x0 - 1 + c. start[r * cells_per_row + c] is
+// the tile slot of the cell's first atom (the last entry is the tile size), first[...] the
+// cell's first cell-order slot.
+struct TileShape
+{
+    int cells_per_row;
+    int size;
+    int home_first;  // cell-order slots [home_first, home_end) are the brick's centers
+    int home_end;
+};
+
+template <typename T>
+__device__ __forceinline__ TileShape stage_brick(
+    const System<T>& s,
+    int brick,
+    const Pos4<T>* __restrict__ positions,
+    Pos4<T>* tile,
+    int* start,
+    int* first
+)
+{
+    const int nx = s.dims[0], ny = s.dims[1], nz = s.dims[2];
+    const int bx = brick % s.bricks_x;
+    const int y = (brick / s.bricks_x) % ny;
+    const int z = brick / (s.bricks_x * ny);
+    const int x0 = bx * nx / s.bricks_x;
+    const int x1 = (bx + 1) * nx / s.bricks_x;
+    const int per_row = x1 - x0 + 2;
+    const int cells = 9 * per_row;
+    // Per tile cell: its cell-order range.
+    for (int t = threadIdx.x; t < cells; t += blockDim.x)
+    {
+        const int r = t / per_row, c = t % per_row;
+        int cx = x0 - 1 + c, cy = y + r % 3 - 1, cz = z + r / 3 - 1;
+        cx = cx < 0 ? cx + nx : (cx >= nx ? cx - nx : cx);
+        cy = cy < 0 ? cy + ny : (cy >= ny ? cy - ny : cy);
+        cz = cz < 0 ? cz + nz : (cz >= nz ? cz - nz : cz);
+        const int cell = cx + nx * (cy + ny * cz);
+        const int begin = s.cell_offsets[cell];
+        first[t] = begin;
+        start[t] = s.cell_offsets[cell + 1] - begin;  // the count, scanned below
+    }
+    __syncthreads();
+    // Exclusive scan of the counts by the first warp.
+    if (threadIdx.x < kWarp)
+    {
+        int carry = 0;
+        for (int base = 0; base < cells; base += kWarp)
+        {
+            const int t = base + threadIdx.x;
+            const int count = t < cells ? start[t] : 0;
+            int inclusive = count;
+#pragma unroll
+            for (int offset = 1; offset < kWarp; offset *= 2)
+            {
+                const int up = __shfl_up_sync(kFullMask, inclusive, offset);
+                inclusive += threadIdx.x >= offset ? up : 0;
+            }
+            if (t < cells)
+            {
+                start[t] = carry + inclusive - count;
+            }
+            carry += __shfl_sync(kFullMask, inclusive, kWarp - 1);
+        }
+        if (threadIdx.x == 0)
+        {
+            start[cells] = carry;
+        }
+    }
+    __syncthreads();
+    TileShape shape;
+    shape.cells_per_row = per_row;
+    shape.size = start[cells];
+    const int home_row = 4 * per_row;
+    shape.home_first = first[home_row + 1];
+    shape.home_end = first[home_row + per_row - 2] + (start[home_row + per_row - 1] -
+                                                      start[home_row + per_row - 2]);
+    if (shape.size > s.tile_cap)
+    {
+        return shape;  // the caller flags the overflow; nothing is staged
+    }
+    // Copy, one warp per tile cell, each cell shifted by its image.
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    for (int t = warp; t < cells; t += blockDim.x / kWarp)
+    {
+        const int r = t / per_row, c = t % per_row;
+        const int cx = x0 - 1 + c, cy = y + r % 3 - 1, cz = z + r / 3 - 1;
+        const T sx = cx < 0 ? -s.length[0] : (cx >= nx ? s.length[0] : T(0));
+        const T sy = cy < 0 ? -s.length[1] : (cy >= ny ? s.length[1] : T(0));
+        const T sz = cz < 0 ? -s.length[2] : (cz >= nz ? s.length[2] : T(0));
+        const int begin = first[t];
+        const int dst = start[t];
+        const int count = start[t + 1] - dst;
+        for (int k = lane; k < count; k += kWarp)
+        {
+            Pos4<T> p = positions[begin + k];
+            p.x += sx;
+            p.y += sy;
+            p.z += sz;
+            tile[dst + k] = p;
+        }
+    }
+    __syncthreads();
+    return shape;
+}
+
+// The tile cell (in the home row) of a center and its tile slot.
+__device__ __forceinline__ int home_cell(const TileShape& shape, const int* first, int center)
+{
+    const int home_row = 4 * shape.cells_per_row;
+    int c = 1;
+    while (c + 1 < shape.cells_per_row - 1 && center >= first[home_row + c + 1])
+    {
+        ++c;
+    }
+    return c;
+}
+
+__device__ __forceinline__ std::int64_t list_slot(int center, int k, int width)
+{
+    return ((static_cast<std::int64_t>(center) >> 5) * width + k) * kWarp + (center & 31);
+}
+
+__device__ __forceinline__ void flag_overflow(index_t* status, int word, int needed)
+{
+    atomicOr(status, kOverflow);
+    atomicMax(status + word, needed);
+}
+
+// ---------------------------------------------------------------------------------------
+// The list build, one CTA per brick (grid) or per 128 centers (small box).
+
+template <typename T>
+__global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int gated)
+{
+    if (gated && !rebuilding(s.rebuild, s.status))
+    {
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
+    __shared__ int start[kTileCells + 1];
+    __shared__ int first[kTileCells];
+    const T r2max = s.radius_squared;
+    if (s.small)
+    {
+        // The whole system, unshifted; the minimum image per candidate.
+        for (int k = threadIdx.x; k < s.n; k += blockDim.x)
+        {
+            tile[k] = s.pos[k];
+        }
+        __syncthreads();
+        const int center = blockIdx.x * blockDim.x + threadIdx.x;
+        if (center >= s.n)
+        {
+            return;
+        }
+        const Pos4<T> c = tile[center];
+        int count = 0;
+        for (int k = 0; k < s.n; ++k)
+        {
+            if (k == center)
+            {
+                continue;
+            }
+            const Pos4<T> p = tile[k];
+            const T dx = min_image(c.x, p.x, s.length[0]);
+            const T dy = min_image(c.y, p.y, s.length[1]);
+            const T dz = min_image(c.z, p.z, s.length[2]);
+            if (squared_norm(dx, dy, dz) < r2max)
+            {
+                if (count < s.width)
+                {
+                    s.nbr[list_slot(center, count, s.width)] = static_cast<std::uint16_t>(k);
+                }
+                ++count;
+            }
+        }
+        s.nbr_count[center] = count;
+        if (count > s.width)
+        {
+            flag_overflow(s.status, 1, count);
+        }
+        return;
+    }
+    const TileShape shape = stage_brick(s, blockIdx.x, s.pos, tile, start, first);
+    if (threadIdx.x == 0)
+    {
+        atomicMax(s.status + 3, shape.size);  // the largest tile of this build, for sizing
+    }
+    if (shape.size > s.tile_cap)
+    {
+        if (threadIdx.x == 0)
+        {
+            flag_overflow(s.status, 2, shape.size);
+        }
+        return;
+    }
+    const int per_row = shape.cells_per_row;
+    for (int center = shape.home_first + threadIdx.x; center < shape.home_end;
+         center += blockDim.x)
+    {
+        const int c = home_cell(shape, first, center);
+        const int self = start[4 * per_row + c] + (center - first[4 * per_row + c]);
+        const Pos4<T> me = tile[self];
+        int count = 0;
+        for (int r = 0; r < 9; ++r)
+        {
+            const int begin = start[r * per_row + c - 1];
+            const int end = start[r * per_row + c + 2];
+            for (int k = begin; k < end; ++k)
+            {
+                if (k == self)
+                {
+                    continue;
+                }
+                const Pos4<T> p = tile[k];
+                if (squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max)
+                {
+                    if (count < s.width)
+                    {
+                        s.nbr[list_slot(center, count, s.width)] = static_cast<std::uint16_t>(k);
+                    }
+                    ++count;
+                }
+            }
+        }
+        s.nbr_count[center] = count;
+        if (count > s.width)
+        {
+            flag_overflow(s.status, 1, count);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Forces, the second half kick and the step's reductions.
+
+enum ForceMode : int
+{
+    kForceOnly = 0,  // F and E (and W): a first frame or a panel
+    kKick = 1,       // also v += dt/2 F / m, and K in float64
+};
+
+template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
+__device__ __forceinline__ void force_center(
+    const System<T>& s,
+    const Pos4<T>* __restrict__ tile,
+    const PairParams<T>* __restrict__ params,
+    int center,
+    int self,
+    double* sums
+)
+{
+    const Pos4<T> me = tile[self];
+    const int count = s.nbr_count[center];
+    const int count_used = count < s.width ? count : s.width;
+    T fx = 0, fy = 0, fz = 0, energy = 0;
+    T w[6] = {0, 0, 0, 0, 0, 0};
+    PairParams<T> pp = params[0];
+    const std::uint16_t* list = s.nbr + list_slot(center, 0, s.width);
+    for (int k = 0; k < count_used; ++k)
+    {
+        const Pos4<T> p = tile[list[static_cast<std::int64_t>(k) * kWarp]];
+        T dx, dy, dz;
+        if (kSmall)
+        {
+            dx = min_image(me.x, p.x, s.length[0]);
+            dy = min_image(me.y, p.y, s.length[1]);
+            dz = min_image(me.z, p.z, s.length[2]);
+        }
+        else
+        {
+            dx = me.x - p.x;
+            dy = me.y - p.y;
+            dz = me.z - p.z;
+        }
+        const T r2 = squared_norm(dx, dy, dz);
+        if (r2 < s.cutoff_squared)
+        {
+            if (kMulti)
+            {
+                pp = params[type_pair_row(static_cast<int>(me.w), static_cast<int>(p.w),
+                                          s.num_types)];
+            }
+            const T inv_r2 = fast_reciprocal(r2);
+            const T q = pp.s2 * inv_r2;
+            const T p6 = q * q * q;
+            const T fs = pp.e24 * inv_r2 * (p6 * (T(2) * p6 - T(1)));
+            energy += pp.e4 * (p6 * (p6 - T(1))) - pp.shift;
+            fx = fma(fs, dx, fx);
+            fy = fma(fs, dy, fy);
+            fz = fma(fs, dz, fz);
+            if (kVirial)
+            {
+                w[0] = fma(fs * dx, dx, w[0]);
+                w[1] = fma(fs * dy, dy, w[1]);
+                w[2] = fma(fs * dz, dz, w[2]);
+                w[3] = fma(fs * dx, dy, w[3]);
+                w[4] = fma(fs * dx, dz, w[4]);
+                w[5] = fma(fs * dy, dz, w[5]);
+            }
+        }
+    }
+    // Each pair is listed from both ends: half of the energy and virial per end.
+    sums[0] += 0.5 * double(energy);
+    if (kVirial)
+    {
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+        {
+            sums[2 + k] += 0.5 * double(w[k]);
+        }
+    }
+    T* f = s.force + 3LL * center;
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = fz;
+    if (kKickStep)
+    {
+        const T scale = s.half_dt * s.inv_mass[center];
+        T* v = s.vel + 3LL * center;
+        const T vx = fma(scale, fx, v[0]);
+        const T vy = fma(scale, fy, v[1]);
+        const T vz = fma(scale, fz, v[2]);
+        v[0] = vx;
+        v[1] = vy;
+        v[2] = vz;
+        if (kThermostat)
+        {
+            sums[1] += 0.5 * double(s.mass[center]) *
+                       (double(vx) * vx + double(vy) * vy + double(vz) * vz);
+        }
+    }
+}
+
+// The Nose-Hoover chain of three, advanced by half a step against the kinetic energy K
+// (Martyna, Tuckerman, Tobias and Klein 1996; src/nabladyn/md/_ensembles/_chain.py:36-83).
+// Returns the velocity scale; q and p advance in place and K is scaled.
+__device__ inline double chain_half_step(double& kinetic, double* q, double* p, const double* mass,
+                                         double degrees, double kT, double dt)
+{
+    const double quarter = 0.25 * dt, eighth = 0.125 * dt;
+    auto driving = [&](int k, double energy) {
+        return k == 0 ? 2.0 * energy - degrees * kT : p[k - 1] * p[k - 1] / mass[k - 1] - kT;
+    };
+    double damping[2];
+    for (int k = 2; k >= 0; --k)
+    {
+        if (k == 2)
+        {
+            p[k] = p[k] + quarter * driving(k, kinetic);
+        }
+        else
+        {
+            const double kick = quarter * driving(k, kinetic);
+            p[k] = damping[k] * (damping[k] * p[k] + kick);
+        }
+        if (k > 0)
+        {
+            damping[k - 1] = exp(-eighth * p[k] / mass[k]);
+        }
+    }
+    const double factor = exp(-0.5 * dt * p[0] / mass[0]);
+    double scaled = kinetic * (factor * factor);
+    for (int k = 0; k < 3; ++k)
+    {
+        q[k] = q[k] + 0.5 * dt * p[k] / mass[k];
+    }
+    for (int k = 0; k < 3; ++k)
+    {
+        if (k == 2)
+        {
+            p[k] = p[k] + quarter * driving(k, scaled);
+        }
+        else
+        {
+            const double kick = quarter * driving(k, scaled);
+            p[k] = damping[k] * (damping[k] * p[k] + kick);
+        }
+    }
+    kinetic = scaled;
+    return factor;
+}
+
+// Block sums -> the block's slot; the last block reduces the slots in a fixed order, stores
+// the totals and runs the scalar tail.
+template <bool kThermostat, bool kStep>
+__device__ __forceinline__ void reduce_and_tail(double* sums, double* partials, unsigned* ticket,
+                                                double* totals, double* thermo, index_t* rebuild)
+// totals: the kReduced float64 outputs this kernel owns.
+{
+    __shared__ double warp_sums[kReduced][kMDThreads / kWarp];
+    __shared__ bool last;
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+#pragma unroll
+    for (int k = 0; k < kReduced; ++k)
+    {
+        const double v = warp_sum(sums[k]);
+        if (lane == 0)
+        {
+            warp_sums[k][warp] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kReduced)
+    {
+        double v = 0;
+        for (int w = 0; w < kMDThreads / kWarp; ++w)
+        {
+            v += warp_sums[threadIdx.x][w];
+        }
+        partials[static_cast<std::int64_t>(blockIdx.x) * kReduced + threadIdx.x] = v;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last)
+    {
+        return;
+    }
+    __threadfence();
+    // Fixed-order sums over the blocks: thread t takes blocks t, t + 128, ...
+    double mine[kReduced];
+#pragma unroll
+    for (int k = 0; k < kReduced; ++k)
+    {
+        mine[k] = 0;
+    }
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    {
+#pragma unroll
+        for (int k = 0; k < kReduced; ++k)
+        {
+            mine[k] += __ldcg(partials + static_cast<std::int64_t>(b) * kReduced + k);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kReduced; ++k)
+    {
+        const double v = warp_sum(mine[k]);
+        if (lane == 0)
+        {
+            warp_sums[k][warp] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double total[kReduced];
+        for (int k = 0; k < kReduced; ++k)
+        {
+            total[k] = 0;
+            for (int w = 0; w < kMDThreads / kWarp; ++w)
+            {
+                total[k] += warp_sums[k][w];
+            }
+            totals[k] = total[k];
+        }
+        *ticket = 0;
+        if (kStep)
+        {
+            rebuild[0] = 0;  // the next step's check starts clean
+        }
+        if (kThermostat)
+        {
+            // The closing half step against this step's K; its factor is applied to the stored
+            // velocities by the next drift (or when the frame is read).
+            double kinetic = total[1];
+            double q[3], p[3];
+            for (int k = 0; k < 3; ++k)
+            {
+                q[k] = thermo[kChainB + k];
+                p[k] = thermo[kChainB + 3 + k];
+            }
+            const double factor = chain_half_step(kinetic, q, p, thermo + kChainMass,
+                                                  thermo[kDegrees], thermo[kThermalEnergy],
+                                                  thermo[kTimestep]);
+            for (int k = 0; k < 3; ++k)
+            {
+                thermo[kChainA + k] = q[k];
+                thermo[kChainA + 3 + k] = p[k];
+            }
+            thermo[kKineticA] = kinetic;
+            thermo[kPendingScale] = factor;
+        }
+    }
+}
+
+template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
+__global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
+    __shared__ int start[kTileCells + 1];
+    __shared__ int first[kTileCells];
+    __shared__ PairParams<T> params[36];
+    const int rows = s.num_types * (s.num_types + 1) / 2;
+    for (int k = threadIdx.x; k < rows; k += blockDim.x)
+    {
+        params[k] = pair_params(s.sigma[k], s.epsilon[k], s.cutoff_squared);
+    }
+    double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (kSmall)
+    {
+        for (int k = threadIdx.x; k < s.n; k += blockDim.x)
+        {
+            tile[k] = s.pos[k];
+        }
+        __syncthreads();
+        const int center = blockIdx.x * blockDim.x + threadIdx.x;
+        if (center < s.n)
+        {
+            force_center<T, true, kMulti, kVirial, kKickStep, kThermostat>(s, tile, params, center,
+                                                                          center, sums);
+        }
+    }
+    else
+    {
+        const TileShape shape = stage_brick(s, blockIdx.x, s.pos, tile, start, first);
+        if (shape.size <= s.tile_cap)
+        {
+            const int per_row = shape.cells_per_row;
+            for (int center = shape.home_first + threadIdx.x; center < shape.home_end;
+                 center += blockDim.x)
+            {
+                const int c = home_cell(shape, first, center);
+                const int self = start[4 * per_row + c] + (center - first[4 * per_row + c]);
+                force_center<T, false, kMulti, kVirial, kKickStep, kThermostat>(
+                    s, tile, params, center, self, sums);
+            }
+        }
+        else if (threadIdx.x == 0)
+        {
+            flag_overflow(s.status, 2, shape.size);
+        }
+    }
+    reduce_and_tail<kThermostat, kKickStep>(sums, s.partials, s.ticket, s.totals, s.thermo,
+                                            s.rebuild);
+}
+
+// ---------------------------------------------------------------------------------------
+// The first half of a step: the deferred thermostat scales, the half kick, the drift, the
+// finiteness check and the reuse check, per atom.
+
+template <typename T, bool kThermostat>
+__global__ void drift_kernel(System<T> s)
+{
+    __shared__ T scales[2];
+    if (kThermostat)
+    {
+        // Every block advances the chain's opening half step from the same inputs; block 0
+        // stores it. The closing factor of the previous step is applied first, as there.
+        if (threadIdx.x == 0)
+        {
+            const double* th = s.thermo;
+            double kinetic = th[kKineticA];
+            double q[3], p[3];
+            for (int k = 0; k < 3; ++k)
+            {
+                q[k] = th[kChainA + k];
+                p[k] = th[kChainA + 3 + k];
+            }
+            const double factor = chain_half_step(kinetic, q, p, th + kChainMass, th[kDegrees],
+                                                  th[kThermalEnergy], th[kTimestep]);
+            scales[0] = static_cast<T>(th[kPendingScale]);
+            scales[1] = static_cast<T>(factor);
+            if (blockIdx.x == 0)
+            {
+                double* out = s.thermo;
+                for (int k = 0; k < 3; ++k)
+                {
+                    out[kChainB + k] = q[k];
+                    out[kChainB + 3 + k] = p[k];
+                }
+                out[kKineticB] = kinetic;
+                out[kOpenScale] = factor;
+            }
+        }
+        __syncthreads();
+    }
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= s.n)
+    {
+        return;
+    }
+    T* v = s.vel + 3 * i;
+    const T* f = s.force + 3 * i;
+    const T kick = s.half_dt * s.inv_mass[i];
+    T vx = v[0], vy = v[1], vz = v[2];
+    if (kThermostat)
+    {
+        vx = (vx * scales[0]) * scales[1];
+        vy = (vy * scales[0]) * scales[1];
+        vz = (vz * scales[0]) * scales[1];
+    }
+    vx = fma(kick, f[0], vx);
+    vy = fma(kick, f[1], vy);
+    vz = fma(kick, f[2], vz);
+    Pos4<T> p = s.pos[i];
+    p.x = fma(s.dt, vx, p.x);
+    p.y = fma(s.dt, vy, p.y);
+    p.z = fma(s.dt, vz, p.z);
+    v[0] = vx;
+    v[1] = vy;
+    v[2] = vz;
+    s.pos[i] = p;
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
+    {
+        atomicOr(s.status, kNonFinite);
+        return;
+    }
+    const Pos4<T> r = s.ref_pos[i];
+    if (squared_norm(p.x - r.x, p.y - r.y, p.z - r.z) >= s.threshold_squared)
+    {
+        s.rebuild[0] = 1;  // every writer stores the same value
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// The rebuild: wrap, bin, sort by cell and id, permute the state, build the list.
+
+template <typename T>
+__global__ void wrap_and_bin_kernel(System<T> s, int gated)
+{
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= s.n || (gated && !rebuilding(s.rebuild, s.status)))
+    {
+        return;
+    }
+    Pos4<T> p = s.pos[i];
+    long long cx, cy, cz;
+    p.x = wrap_axis(p.x, s.length[0], cx);
+    p.y = wrap_axis(p.y, s.length[1], cy);
+    p.z = wrap_axis(p.z, s.length[2], cz);
+    if (cx | cy | cz)
+    {
+        long long* image = s.images + 3 * i;
+        image[0] += cx;
+        image[1] += cy;
+        image[2] += cz;
+    }
+    s.pos[i] = p;
+    if (s.small)
+    {
+        s.ref_pos[i] = p;
+        return;
+    }
+    const index_t nx = s.dims[0], ny = s.dims[1], nz = s.dims[2];
+    const index_t cell = axis_bin(p.x, s.widths[0], nx) +
+                         nx * (axis_bin(p.y, s.widths[1], ny) + ny * axis_bin(p.z, s.widths[2], nz));
+    s.atom_cell[i] = cell;
+    s.slot[i] = atomicAdd(s.cell_counts + cell, 1);
+}
+
+template <typename T>
+__global__ void place_kernel(System<T> s, int gated)
+{
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= s.n || (gated && !rebuilding(s.rebuild, s.status)))
+    {
+        return;
+    }
+    const index_t cell = s.atom_cell[i];
+    s.unordered[s.cell_offsets[cell] + s.slot[i]] = static_cast<index_t>(i);
+    s.cell_counts[cell] = 0;
+}
+
+// One warp per cell: rank each atom by its id among the cell's atoms; order[new] = old slot.
+template <typename T>
+__global__ void order_kernel(System<T> s, std::int64_t num_cells, int gated)
+{
+    const std::int64_t cell =
+        (static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
+    const int lane = threadIdx.x % kWarp;
+    if (cell >= num_cells || (gated && !rebuilding(s.rebuild, s.status)))
+    {
+        return;
+    }
+    const index_t begin = s.cell_offsets[cell];
+    const index_t count = s.cell_offsets[cell + 1] - begin;
+    for (index_t mine = 0; mine < count; mine += kWarp)
+    {
+        const bool active = mine + lane < count;
+        const index_t old = active ? s.unordered[begin + mine + lane] : 0;
+        const index_t id = active ? s.ids[old] : 0;
+        index_t rank = 0;
+        for (index_t base = 0; base < count; base += kWarp)
+        {
+            const index_t other =
+                base + lane < count ? s.ids[s.unordered[begin + base + lane]] : 0x7fffffff;
+            const int valid = count - base < kWarp ? count - base : kWarp;
+            for (int t = 0; t < valid; ++t)
+            {
+                rank += __shfl_sync(kFullMask, other, t) < id;
+            }
+        }
+        if (active)
+        {
+            s.order[begin + rank] = old;
+        }
+    }
+}
+
+template <typename T>
+__global__ void permute_kernel(System<T> s, int gated)
+{
+    const std::int64_t k = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= s.n || (gated && !rebuilding(s.rebuild, s.status)))
+    {
+        return;
+    }
+    const index_t old = s.order[k];
+    s.pos_b[k] = s.pos[old];
+    for (int a = 0; a < 3; ++a)
+    {
+        s.vel_b[3 * k + a] = s.vel[3LL * old + a];
+        s.force_b[3 * k + a] = s.force[3LL * old + a];
+        s.images_b[3 * k + a] = s.images[3LL * old + a];
+    }
+    s.inv_mass_b[k] = s.inv_mass[old];
+    s.mass_b[k] = s.mass[old];
+    s.ids_b[k] = s.ids[old];
+}
+
+template <typename T>
+__global__ void commit_kernel(System<T> s, int gated)
+{
+    const std::int64_t k = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= s.n || (gated && !rebuilding(s.rebuild, s.status)))
+    {
+        return;
+    }
+    if (k == 0)
+    {
+        ++s.rebuild_count[0];
+    }
+    if (s.small)
+    {
+        return;  // the wrap stored the reference already; the order is unchanged
+    }
+    const Pos4<T> p = s.pos_b[k];
+    s.pos[k] = p;
+    s.ref_pos[k] = p;
+    for (int a = 0; a < 3; ++a)
+    {
+        s.vel[3 * k + a] = s.vel_b[3 * k + a];
+        s.force[3 * k + a] = s.force_b[3 * k + a];
+        s.images[3 * k + a] = s.images_b[3 * k + a];
+    }
+    s.inv_mass[k] = s.inv_mass_b[k];
+    s.mass[k] = s.mass_b[k];
+    s.ids[k] = s.ids_b[k];
+}
+
+// ---------------------------------------------------------------------------------------
+// Import and export in the caller's atom order.
+
+template <typename T>
+__global__ void import_kernel(System<T> s, const T* __restrict__ positions,
+                              const T* __restrict__ velocities, const T* __restrict__ masses,
+                              const long long* __restrict__ images,
+                              const index_t* __restrict__ types)
+{
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= s.n)
+    {
+        return;
+    }
+    Pos4<T> p;
+    p.x = positions[3 * i];
+    p.y = positions[3 * i + 1];
+    p.z = positions[3 * i + 2];
+    p.w = types != nullptr ? static_cast<T>(types[i]) : T(0);
+    s.pos[i] = p;
+    for (int a = 0; a < 3; ++a)
+    {
+        s.vel[3 * i + a] = velocities[3 * i + a];
+        s.force[3 * i + a] = T(0);
+        s.images[3 * i + a] = images[3 * i + a];
+    }
+    s.mass[i] = masses[i];
+    s.inv_mass[i] = T(1) / masses[i];
+    s.ids[i] = static_cast<index_t>(i);
+}
+
+// Writes the frame in the caller's order: positions wrapped into [0, L) with the crossings
+// added to the images, velocities with the pending thermostat scale applied, forces.
+template <typename T>
+__global__ void export_kernel(System<T> s, T* __restrict__ positions, T* __restrict__ velocities,
+                              T* __restrict__ forces, long long* __restrict__ images,
+                              int thermostat)
+{
+    const std::int64_t k = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= s.n)
+    {
+        return;
+    }
+    const index_t i = s.ids[k];
+    const Pos4<T> p = s.pos[k];
+    long long c[3];
+    const T w[3] = {wrap_axis(p.x, s.length[0], c[0]), wrap_axis(p.y, s.length[1], c[1]),
+                    wrap_axis(p.z, s.length[2], c[2])};
+    const T scale = thermostat ? static_cast<T>(s.thermo[kPendingScale]) : T(1);
+    for (int a = 0; a < 3; ++a)
+    {
+        if (positions)
+        {
+            positions[3LL * i + a] = w[a];
+        }
+        if (images)
+        {
+            images[3LL * i + a] = s.images[3 * k + a] + c[a];
+        }
+        if (velocities)
+        {
+            velocities[3LL * i + a] = thermostat ? s.vel[3 * k + a] * scale : s.vel[3 * k + a];
+        }
+        if (forces)
+        {
+            forces[3LL * i + a] = s.force[3 * k + a];
+        }
+    }
+}
+
+// K = sum m v^2 / 2 of the stored velocities times the pending scale, in float64, into
+// totals[1]; deterministic: per-block slots, fixed-order final sum by the last block.
+template <typename T>
+__global__ void __launch_bounds__(kMDThreads) kinetic_kernel(System<T> s, int thermostat)
+{
+    double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const std::int64_t k = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < s.n)
+    {
+        const double scale = thermostat ? double(static_cast<T>(s.thermo[kPendingScale])) : 1.0;
+        double v2 = 0;
+        for (int a = 0; a < 3; ++a)
+        {
+            const double v = thermostat ? double(s.vel[3 * k + a] * static_cast<T>(scale))
+                                        : double(s.vel[3 * k + a]);
+            v2 += v * v;
+        }
+        sums[1] = 0.5 * double(s.mass[k]) * v2;
+    }
+    reduce_and_tail<false, false>(sums, s.partials, s.ticket, s.totals + kReduced, s.thermo,
+                                  s.rebuild);
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side.
+
+template <typename T>
+System<T> view(const nd_md_system* m)
+{
+    System<T> s;
+    s.pos = static_cast<Pos4<T>*>(m->positions);
+    s.vel = static_cast<T*>(m->velocities);
+    s.force = static_cast<T*>(m->forces);
+    s.inv_mass = static_cast<T*>(m->inverse_masses);
+    s.mass = static_cast<T*>(m->masses);
+    s.images = reinterpret_cast<long long*>(m->images);
+    s.ids = m->ids;
+    s.ref_pos = static_cast<Pos4<T>*>(m->reference_positions);
+    s.pos_b = static_cast<Pos4<T>*>(m->shadow_positions);
+    s.vel_b = static_cast<T*>(m->shadow_velocities);
+    s.force_b = static_cast<T*>(m->shadow_forces);
+    s.inv_mass_b = static_cast<T*>(m->shadow_inverse_masses);
+    s.mass_b = static_cast<T*>(m->shadow_masses);
+    s.images_b = reinterpret_cast<long long*>(m->shadow_images);
+    s.ids_b = m->shadow_ids;
+    s.cell_counts = m->cell_counts;
+    s.cell_offsets = m->cell_offsets;
+    s.atom_cell = m->atom_cell;
+    s.slot = m->slots;
+    s.unordered = m->unordered;
+    s.order = m->order;
+    s.scan_temp = m->scan_temp;
+    s.nbr = m->neighbors;
+    s.nbr_count = m->neighbor_counts;
+    s.rebuild = m->rebuild;
+    s.rebuild_count = m->rebuild_count;
+    s.status = m->status;
+    s.partials = m->partials;
+    s.ticket = m->ticket;
+    s.totals = m->totals;
+    s.thermo = m->thermostat;
+    s.sigma = static_cast<const T*>(m->sigma);
+    s.epsilon = static_cast<const T*>(m->epsilon);
+    s.n = static_cast<index_t>(m->num_atoms);
+    for (int a = 0; a < 3; ++a)
+    {
+        s.dims[a] = m->dims[a];
+        s.length[a] = static_cast<T>(m->cell[a]);
+        s.widths[a] = static_cast<T>(m->widths[a]);
+    }
+    s.bricks_x = m->bricks_x;
+    s.small = m->small;
+    s.num_bricks = s.small ? static_cast<index_t>((m->num_atoms + kMDThreads - 1) / kMDThreads)
+                           : m->bricks_x * m->dims[1] * m->dims[2];
+    s.width = m->width;
+    s.tile_cap = m->tile_capacity;
+    s.num_types = m->num_types;
+    s.dt = static_cast<T>(m->timestep);
+    s.half_dt = static_cast<T>(0.5 * m->timestep);
+    s.threshold_squared = static_cast<T>(m->threshold_squared);
+    s.radius_squared = static_cast<T>(m->radius) * static_cast<T>(m->radius);
+    s.cutoff_squared = static_cast<T>(m->cutoff) * static_cast<T>(m->cutoff);
+    return s;
+}
+
+template <typename T>
+std::size_t tile_bytes(const System<T>& s)
+{
+    return static_cast<std::size_t>(s.small ? s.n : s.tile_cap) * sizeof(Pos4<T>);
+}
+
+// Raises a kernel's dynamic shared-memory limit when a launch needs more than any before; the
+// first launch of every kernel happens outside graph capture (allocation, warm-up).
+template <typename Kernel>
+cudaError_t allow_shared(Kernel kernel, std::size_t bytes, std::size_t& granted)
+{
+    if (bytes <= granted || bytes <= 48 * 1024)
+    {
+        return cudaSuccess;
+    }
+    const cudaError_t rc = cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (rc == cudaSuccess)
+    {
+        granted = bytes;
+    }
+    return rc;
+}
+
+template <typename T>
+int launch_build(const System<T>& s, int gated, cudaStream_t stream)
+{
+    const std::size_t bytes = tile_bytes(s);
+    static std::size_t granted = 0;
+    ND_CUDA_TRY(allow_shared(build_list_kernel<T>, bytes, granted));
+    build_list_kernel<T><<<s.num_bricks, kMDThreads, bytes, stream>>>(s, gated);
+    ND_LAUNCH_CHECK();
+    return ND_OK;
+}
+
+template <typename T>
+int launch_rebuild(const System<T>& s, std::int64_t num_cells, int gated, cudaStream_t stream)
+{
+    const unsigned atoms = blocks_for(s.n);
+    wrap_and_bin_kernel<T><<<atoms, kThreads, 0, stream>>>(s, gated);
+    ND_LAUNCH_CHECK();
+    const index_t* gate = gated ? s.rebuild : nullptr;
+    if (!s.small)
+    {
+        ND_CUDA_TRY(scan_exclusive(s.cell_counts, s.cell_offsets, num_cells + 1, s.scan_temp,
+                                   gate, s.status, stream));
+        place_kernel<T><<<atoms, kThreads, 0, stream>>>(s, gated);
+        ND_LAUNCH_CHECK();
+        order_kernel<T><<<blocks_for(num_cells * kWarp), kThreads, 0, stream>>>(s, num_cells,
+                                                                               gated);
+        ND_LAUNCH_CHECK();
+        permute_kernel<T><<<atoms, kThreads, 0, stream>>>(s, gated);
+        ND_LAUNCH_CHECK();
+    }
+    commit_kernel<T><<<atoms, kThreads, 0, stream>>>(s, gated);
+    ND_LAUNCH_CHECK();
+    return launch_build(s, gated, stream);
+}
+
+template <typename T, bool kVirial, bool kKickStep, bool kThermostat>
+int launch_force_variant(const System<T>& s, cudaStream_t stream)
+{
+    const std::size_t bytes = tile_bytes(s);
+    const bool multi = s.num_types > 1;
+#define ND_FORCE_CASE(SMALL, MULTI)                                                         \
+    if (s.small == SMALL && multi == MULTI)                                                 \
+    {                                                                                       \
+        auto kernel = force_kernel<T, SMALL, MULTI, kVirial, kKickStep, kThermostat>;       \
+        static std::size_t granted = 0;                                                     \
+        ND_CUDA_TRY(allow_shared(kernel, bytes, granted));                                  \
+        kernel<<<s.num_bricks, kMDThreads, bytes, stream>>>(s);                             \
+        ND_LAUNCH_CHECK();                                                                  \
+        return ND_OK;                                                                       \
+    }
+    ND_FORCE_CASE(1, true)
+    ND_FORCE_CASE(1, false)
+    ND_FORCE_CASE(0, true)
+    ND_FORCE_CASE(0, false)
+#undef ND_FORCE_CASE
+    return ND_OK;
+}
+
+template <typename T>
+int launch_forces(const System<T>& s, int virial, cudaStream_t stream)
+{
+    return virial ? launch_force_variant<T, true, false, false>(s, stream)
+                  : launch_force_variant<T, false, false, false>(s, stream);
+}
+
+// The three phases of a step: 0 the drift with the reuse check, 1 the gated rebuild, 2 the
+// forces with the second half kick and the tail. -1 runs all three.
+template <typename T>
+int launch_step(const System<T>& s, std::int64_t num_cells, int thermostat, int virial,
+                int phase, cudaStream_t stream)
+{
+    if (phase < 0 || phase == 0)
+    {
+        const unsigned atoms = blocks_for(s.n);
+        if (thermostat)
+        {
+            drift_kernel<T, true><<<atoms, kThreads, 0, stream>>>(s);
+        }
+        else
+        {
+            drift_kernel<T, false><<<atoms, kThreads, 0, stream>>>(s);
+        }
+        ND_LAUNCH_CHECK();
+    }
+    if (phase < 0 || phase == 1)
+    {
+        const int rc = launch_rebuild(s, num_cells, 1, stream);
+        if (rc != ND_OK)
+        {
+            return rc;
+        }
+    }
+    if (phase < 0 || phase == 2)
+    {
+        if (thermostat)
+        {
+            return virial ? launch_force_variant<T, true, true, true>(s, stream)
+                          : launch_force_variant<T, false, true, true>(s, stream);
+        }
+        return virial ? launch_force_variant<T, true, true, false>(s, stream)
+                      : launch_force_variant<T, false, true, false>(s, stream);
+    }
+    return ND_OK;
+}
+
+// The kernels one step launches, as launch_step issues them.
+std::int64_t step_launches(const nd_md_system* m)
+{
+    const std::int64_t cells = static_cast<std::int64_t>(m->dims[0]) * m->dims[1] * m->dims[2];
+    std::int64_t rebuild = 3;  // wrap_and_bin, commit, build_list
+    if (!m->small)
+    {
+        rebuild += (scan_tiles(cells + 1) <= 1 ? 1 : 3) + 3;  // scan, place, order, permute
+    }
+    return 1 + rebuild + 1;  // drift, rebuild, forces
+}
+
+int check_system(const nd_md_system* m)
+{
+    ND_REQUIRE(m != nullptr, "the system is null");
+    ND_REQUIRE(m->dtype == ND_FLOAT32 || m->dtype == ND_FLOAT64,
+               "the system must be float32 or float64");
+    ND_REQUIRE(m->num_atoms >= 2 && m->num_atoms <= INT32_MAX, "N must be in [2, 2**31)");
+    ND_REQUIRE(m->num_types >= 1 && m->num_types <= 8, "1 to 8 atom types are supported");
+    ND_REQUIRE(m->width >= 1, "the list width must be positive");
+    const std::size_t pos_bytes = m->dtype == ND_FLOAT32 ? 16 : 32;
+    if (m->small)
+    {
+        ND_REQUIRE(m->num_atoms <= 65535, "a small-box system holds at most 65535 atoms");
+        ND_REQUIRE(static_cast<std::size_t>(m->num_atoms) * pos_bytes <= 200 * 1024,
+                   "a small-box system must fit one shared-memory tile");
+    }
+    else
+    {
+        ND_REQUIRE(m->dims[0] >= 3 && m->dims[1] >= 3 && m->dims[2] >= 3,
+                   "the cell grid needs three or more cells per axis");
+        ND_REQUIRE(m->bricks_x >= 1 && m->bricks_x <= m->dims[0], "bricks_x out of range");
+        ND_REQUIRE((m->dims[0] + m->bricks_x - 1) / m->bricks_x <= kMaxBrickCells,
+                   "a brick spans too many cells");
+        ND_REQUIRE(m->tile_capacity >= 1 && m->tile_capacity <= 65535 &&
+                       static_cast<std::size_t>(m->tile_capacity) * pos_bytes <= 200 * 1024,
+                   "the tile capacity must fit shared memory and uint16 indices");
+    }
+    return ND_OK;
+}
+
+}  // namespace nd
+
+// ---------------------------------------------------------------------------------------
+// C-ABI.
+
+#define ND_MD_DISPATCH(m, call)                                                 \
+    ((m)->dtype == ND_FLOAT32 ? [&] { auto s = nd::view<float>(m); return call; }() \
+                              : [&] { auto s = nd::view<double>(m); return call; }())
+
+extern "C" {
+
+int nd_md_import(const nd_md_system* system, const void* positions, const void* velocities,
+                 const void* masses, const int64_t* images, const int32_t* types,
+                 nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    ND_REQUIRE(positions && velocities && masses && images, "a frame pointer is null");
+    auto st = static_cast<cudaStream_t>(stream);
+    return ND_MD_DISPATCH(system, ([&] {
+        using T = std::remove_pointer_t<decltype(s.vel)>;
+        nd::import_kernel<T><<<nd::blocks_for(s.n), nd::kThreads, 0, st>>>(
+            s, static_cast<const T*>(positions), static_cast<const T*>(velocities),
+            static_cast<const T*>(masses), reinterpret_cast<const long long*>(images),
+            system->num_types > 1 ? types : nullptr);
+        ND_LAUNCH_CHECK();
+        return ND_OK;
+    }()));
+}
+
+int nd_md_rebuild(const nd_md_system* system, nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    const std::int64_t cells =
+        static_cast<std::int64_t>(system->dims[0]) * system->dims[1] * system->dims[2];
+    return ND_MD_DISPATCH(system, nd::launch_rebuild(s, cells, 0, st));
+}
+
+int nd_md_forces(const nd_md_system* system, int virial, nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    return ND_MD_DISPATCH(system, nd::launch_forces(s, virial, st));
+}
+
+int nd_md_step(const nd_md_system* system, int thermostat, int virial, nd_stream_t stream)
+{
+    return nd_md_step_phase(system, -1, thermostat, virial, stream);
+}
+
+int nd_md_step_phase(const nd_md_system* system, int phase, int thermostat, int virial,
+                     nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    ND_REQUIRE(phase >= -1 && phase <= 2, "the phase must be -1 (all), 0, 1 or 2");
+    auto st = static_cast<cudaStream_t>(stream);
+    const std::int64_t cells =
+        static_cast<std::int64_t>(system->dims[0]) * system->dims[1] * system->dims[2];
+    return ND_MD_DISPATCH(system, nd::launch_step(s, cells, thermostat, virial, phase, st));
+}
+
+int nd_md_step_launches(const nd_md_system* system, int64_t* launches)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    ND_REQUIRE(launches != nullptr, "launches is null");
+    *launches = nd::step_launches(system);
+    return ND_OK;
+}
+
+int nd_md_export(const nd_md_system* system, void* positions, void* velocities, void* forces,
+                 int64_t* images, int thermostat, nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    return ND_MD_DISPATCH(system, ([&] {
+        using T = std::remove_pointer_t<decltype(s.vel)>;
+        nd::export_kernel<T><<<nd::blocks_for(s.n), nd::kThreads, 0, st>>>(
+            s, static_cast<T*>(positions), static_cast<T*>(velocities), static_cast<T*>(forces),
+            reinterpret_cast<long long*>(images), thermostat);
+        ND_LAUNCH_CHECK();
+        return ND_OK;
+    }()));
+}
+
+int nd_md_kinetic(const nd_md_system* system, int thermostat, nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    return ND_MD_DISPATCH(system, ([&] {
+        using T = std::remove_pointer_t<decltype(s.vel)>;
+        nd::kinetic_kernel<T><<<nd::blocks_for(s.n, nd::kMDThreads), nd::kMDThreads, 0, st>>>(
+            s, thermostat);
+        ND_LAUNCH_CHECK();
+        return ND_OK;
+    }()));
+}
+
+int nd_md_partial_slots(const nd_md_system* system, int64_t* slots)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    ND_REQUIRE(slots != nullptr, "slots is null");
+    const std::int64_t bricks =
+        system->small ? (system->num_atoms + nd::kMDThreads - 1) / nd::kMDThreads
+                      : static_cast<std::int64_t>(system->bricks_x) * system->dims[1] *
+                            system->dims[2];
+    const std::int64_t atoms = (system->num_atoms + nd::kMDThreads - 1) / nd::kMDThreads;
+    *slots = (bricks > atoms ? bricks : atoms) * nd::kReduced;
+    return ND_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+"""Generate the golden fixtures of tests/golden from the reference itself, on CPU.
+
+Run in a container where the reference is mounted (default /root/reference; override with
+NABLADYN_REFERENCE): ``python tests/golden/make_golden.py``. It imports the reference's Python
+package and evaluates its own code on CPU tensors; the GPU box never runs this script, it only
+reads the .npz files written here.
+
+Fixtures:
+* argon_512.npz — the reference's example frame (examples/data/argon_512.npz) with the
+  reference's E/F/W in float64 and float32 over every pair (i < j; the model masks by the
+  cutoff, so no neighbor list is involved) and the documented known answers
+  (examples/README.md:55-56): 29,014 pairs within 1.1 nm, 21,398 within 1.0 nm, capacity
+  36,268, E = -2,526.17 kJ/mol, max |F| = 386.06 kJ/mol/nm.
+* argon_512_md.npz — 20 NVE and 20 NVT steps of that frame, float64 and float32, made by the
+  reference's own ensemble halves (src/nabladyn/md/_ensembles/_nve.py, _nvt.py, _chain.py) in
+  the order Simulation._capture runs them (src/nabladyn/md/_simulation.py:331-348), with the
+  all-pairs index standing in for the neighbor list.
+* lj_frames_4.npz — four frames of examples/data/lj_frames.npz (216 atoms, two types) with the
+  file's labels and the reference's float64 E/F/W for the generating rows.
+"""
+
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+REFERENCE = Path(os.environ.get("NABLADYN_REFERENCE", "/root/reference"))
+OUT = Path(__file__).resolve().parent
+sys.path.insert(0, str(REFERENCE / "src"))
+
+from nabladyn import potential, quantity, space  # noqa: E402
+from nabladyn.md._ensembles._nve import NVE  # noqa: E402
+from nabladyn.md._ensembles._nvt import NVT  # noqa: E402
+from nabladyn.md._state import _Frame  # noqa: E402
+from nabladyn.neighbors import NeighborPairs  # noqa: E402
+from nabladyn.observables import kinetic_energy  # noqa: E402
+
+SIGMA, EPSILON, MASS, CUTOFF = 0.34, 0.996, 39.948, 1.0
+
+
+def all_pairs(n: int) -> torch.Tensor:
+    i, j = torch.triu_indices(n, n, offset=1)
+    return torch.stack([i, j]).to(torch.int32)
+
+
+def argon_model(n: int, dtype):
+    return potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64),
+        sigma=torch.tensor([SIGMA], dtype=dtype),
+        epsilon=torch.tensor([EPSILON], dtype=dtype),
+        cutoff=CUTOFF,
+    )
+
+
+def argon() -> None:
+    frame = np.load(REFERENCE / "examples" / "data" / "argon_512.npz")
+    out = {name: frame[name] for name in frame.files}
+    n = frame["positions"].shape[0]
+    index = all_pairs(n)
+    for dtype, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
+        positions = torch.tensor(frame["positions"], dtype=dtype)
+        cell = torch.tensor(frame["cell"], dtype=dtype)
+        model = argon_model(n, dtype)
+        pairs = NeighborPairs(index, n, CUTOFF)
+        energy, forces, virial = quantity.energy_force_virial(model)(positions, cell, pairs)
+        out[f"energy_{tag}"] = energy.detach().numpy()
+        out[f"forces_{tag}"] = forces.detach().numpy()
+        out[f"virial_{tag}"] = virial.detach().numpy()
+    # Counts by float64 distance, the documented known answers.
+    positions = torch.tensor(frame["positions"], dtype=torch.float64)
+    cell = torch.tensor(frame["cell"], dtype=torch.float64)
+    wrapped, _ = space.wrap(positions, cell)
+    r = space._displacement_wrapped(wrapped[index[0].long()], wrapped[index[1].long()], cell).norm(dim=-1)
+    out["pairs_within_1_1"] = np.int64((r < 1.1).sum())
+    out["pairs_within_1_0"] = np.int64((r < 1.0).sum())
+    out["documented"] = np.array([29014, 21398, 36268, -2526.17, 386.06])
+    np.savez_compressed(OUT / "argon_512.npz", **out)
+
+
+def trajectory(dtype, ensemble_name: str, steps: int, record=(1, 5, 20)):
+    frame_data = np.load(REFERENCE / "examples" / "data" / "argon_512.npz")
+    n = frame_data["positions"].shape[0]
+    positions = torch.tensor(frame_data["positions"], dtype=dtype)
+    velocities = torch.tensor(frame_data["velocities"], dtype=dtype)
+    cell = torch.tensor(frame_data["cell"], dtype=dtype)
+    masses = torch.full((n,), MASS, dtype=dtype)
+    model = argon_model(n, dtype)
+    pairs = NeighborPairs(all_pairs(n), n, CUTOFF)
+    # Simulation.__init__ (src/nabladyn/md/_simulation.py:171-192).
+    positions, crossings = space.wrap(positions, cell)
+    velocities = velocities - (masses[:, None] * velocities).sum(dim=0) / masses.sum()
+    evaluate = quantity.energy_force_virial(model._energy_wrapped)
+    with torch.no_grad():
+        energy, forces, virial = evaluate(positions, cell, pairs)
+    frame = _Frame(positions, velocities.clone(), forces, energy, virial, cell, crossings)
+    start = {"positions": positions.numpy().copy(), "velocities": velocities.numpy().copy(),
+             "energy": energy.detach().numpy().copy()}
+    if ensemble_name == "NVE":
+        ensemble = NVE(0.004, masses, frame)
+    else:
+        ensemble = NVT(0.004, masses, frame, temperature=120.0, timescale=0.1, chain=None)
+    step_eval = quantity.energy_and_force(model._energy_wrapped)
+    records = {}
+    with torch.no_grad():
+        for step in range(1, steps + 1):
+            ensemble.first_half(frame)
+            energy, forces = step_eval(frame.positions, frame.cell, pairs)
+            frame.energy.copy_(energy)
+            frame.forces.copy_(forces)
+            ensemble.second_half(frame)
+            if ensemble.closing is not None:
+                ensemble.closing(frame)
+            if step in record:
+                entry = {
+                    "positions": frame.positions.numpy().copy(),
+                    "velocities": frame.velocities.numpy().copy(),
+                    "forces": frame.forces.numpy().copy(),
+                    "images": frame.images.numpy().copy(),
+                    "energy": frame.energy.numpy().copy(),
+                    "kinetic": kinetic_energy(frame.velocities, masses).double().numpy().copy(),
+                }
+                if ensemble_name == "NVT":
+                    entry["chain_positions"] = ensemble._positions.numpy().copy()
+                    entry["chain_momenta"] = ensemble._momenta.numpy().copy()
+                records[step] = entry
+    return start, records
+
+
+def md() -> None:
+    out = {}
+    for dtype, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
+        for name in ("NVE", "NVT"):
+            start, records = trajectory(dtype, name, 20)
+            out[f"{name}_{tag}_start_positions"] = start["positions"]
+            out[f"{name}_{tag}_start_velocities"] = start["velocities"]
+            for step, entry in records.items():
+                for key, value in entry.items():
+                    out[f"{name}_{tag}_{step}_{key}"] = value
+    np.savez_compressed(OUT / "argon_512_md.npz", **out)
+
+
+def lj_frames() -> None:
+    data = np.load(REFERENCE / "examples" / "data" / "lj_frames.npz")
+    chosen = [0, 99, 150, 299]
+    out = {
+        "positions": data["positions"][chosen],
+        "cells": data["cells"][chosen],
+        "energy": data["energy"][chosen],
+        "forces": data["forces"][chosen],
+        "virial": data["virial"][chosen],
+        "atom_types": data["atom_types"],
+        "sigma": data["sigma"],
+        "epsilon": data["epsilon"],
+        "cutoff": data["cutoff"],
+    }
+    n = data["atom_types"].shape[0]
+    model = potential.lennard_jones(
+        atom_types=torch.tensor(data["atom_types"]),
+        sigma=torch.tensor(data["sigma"]),
+        epsilon=torch.tensor(data["epsilon"]),
+        cutoff=float(data["cutoff"]),
+    )
+    pairs = NeighborPairs(all_pairs(n), n, float(data["cutoff"]))
+    energies, forces, virials = [], [], []
+    for k in range(len(chosen)):
+        e, f, w = quantity.energy_force_virial(model)(
+            torch.tensor(out["positions"][k]), torch.tensor(out["cells"][k]), pairs,
+        )
+        energies.append(e.detach().numpy())
+        forces.append(f.detach().numpy())
+        virials.append(w.detach().numpy())
+    out["reference_energy"] = np.array(energies)
+    out["reference_forces"] = np.array(forces)
+    out["reference_virial"] = np.array(virials)
+    np.savez_compressed(OUT / "lj_frames_4.npz", **out)
+
+
+if __name__ == "__main__":
+    torch.set_num_threads(os.cpu_count() or 1)
+    argon()
+    md()
+    lj_frames()
+    print("wrote", sorted(p.name for p in OUT.glob("*.npz")))

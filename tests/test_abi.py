@@ -1,0 +1,89 @@
+"""The C-ABI library loads, exports every declared symbol and rejects bad arguments (CPU)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+import torch
+
+from nabladyn_b200 import _native
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "nabladyn_b200.h"
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nd_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    library = _native.lib()
+    names = declared_functions()
+    assert "nd_md_step" in names and "nd_neighbors_update" in names
+    for name in names:
+        assert hasattr(library, name), name
+    assert set(names) == set(_native.EXPORTED)
+    assert library.nd_abi_version() == 1
+
+
+def test_scan_temp_bytes_and_argument_errors():
+    library = _native.lib()
+    value = ctypes.c_int64(0)
+    assert library.nd_neighbors_scan_temp_bytes(100, ctypes.byref(value)) == _native.ND_OK
+    assert value.value > 0
+    assert library.nd_neighbors_scan_temp_bytes(0, ctypes.byref(value)) == _native.ND_EINVAL
+    assert b"int32" in library.nd_last_error()
+
+
+def test_lj_rejects_null_arguments():
+    library = _native.lib()
+    args = _native.LJPairsArgs(dtype=0, num_atoms=10, capacity=4, num_types=1, cutoff=1.0)
+    assert library.nd_lj_energy_force_virial(ctypes.byref(args), None) == _native.ND_EINVAL
+    assert b"null" in library.nd_last_error()
+    args.dtype = 7
+    assert library.nd_lj_energy_force_virial(ctypes.byref(args), None) == _native.ND_EINVAL
+
+
+def test_md_rejects_small_box_too_large():
+    library = _native.lib()
+    system = _native.MDSystem(dtype=0, num_atoms=100000, num_types=1, small=1, width=8)
+    slots = ctypes.c_int64(0)
+    assert library.nd_md_partial_slots(ctypes.byref(system), ctypes.byref(slots)) == _native.ND_EINVAL
+    system.num_atoms = 500
+    assert library.nd_md_partial_slots(ctypes.byref(system), ctypes.byref(slots)) == _native.ND_OK
+    assert slots.value == 4 * 8
+
+
+def test_neighbor_schemas_match_the_reference():
+    """src/nabladyn/neighbors/csrc/ops.cpp:11-41, byte for byte."""
+    ops = _native.neighbor_ops()
+    buffers = (
+        "Tensor(a!) dims, Tensor(b!) widths, Tensor(c!) atom_bin, Tensor(d!) bin_counts, "
+        "Tensor(e!) bin_offsets, Tensor(f!) unordered_ids, Tensor(g!) sorted_ids, "
+        "Tensor(h!) sorted_positions, Tensor(i!) scan_temp, Tensor(j!) pair_counts, "
+        "Tensor(k!) pair_offsets, Tensor(l!) pair_total, Tensor(m!) status, Tensor(n!) pairs, "
+        "Tensor(t!) bits"
+    )
+    expected = {
+        "scan_temp_bytes": "nabladyn_neighbors::scan_temp_bytes(Tensor reference, int items) -> int",
+        "count_first_frame": "nabladyn_neighbors::count_first_frame(Tensor positions, Tensor cell, "
+        f"float radius, {buffers}) -> ()",
+        "fill_first_frame": "nabladyn_neighbors::fill_first_frame(Tensor positions, Tensor cell, "
+        f"float radius, {buffers}) -> ()",
+        "update": "nabladyn_neighbors::update(Tensor positions, Tensor cell, float cutoff, "
+        "float radius, Tensor(o!) reference_positions, Tensor(p!) reference_cell, Tensor limits, "
+        "Tensor(q!) reuse, Tensor(r!) rebuild, Tensor(s!) rebuild_count, "
+        f"{buffers}) -> ()",
+    }
+    for name, schema in expected.items():
+        assert str(getattr(ops, name).default._schema) == schema
+    assert ops.scan_temp_bytes(torch.zeros(1), 5000) == 8
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(_native, "_lib", None)
+    monkeypatch.setattr(_native, "CORE_PATH", tmp_path / "libnabladyn_b200.so")
+    with pytest.raises(RuntimeError, match="not built"):
+        _native.lib()
