@@ -195,6 +195,57 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_reference_cuda(args) -> None:
+    """The reference's own GPU path on this B200: its md.nve (Inductor programs around its
+    CUDA neighbor operator, one CUDA Graph per step), installed in baseline/_ref. Not a driver
+    arm: it prints the reference's atom-steps/s for the same workload, for comparison."""
+    import torch
+
+    sys.path.insert(0, str(ROOT / "baseline" / "_ref"))
+    from nabladyn import md, potential  # the reference package
+
+    from nabladyn_b200 import lattice
+
+    device = torch.device("cuda", 0)
+    positions, cell = lattice.fcc(ATOMS_PER_SIDE_CELLS, LENGTH, 0.02, 2024)
+    n = positions.shape[0]
+    dtype = torch.float32
+    model = potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64, device=device),
+        sigma=torch.tensor([SIGMA], dtype=dtype, device=device),
+        epsilon=torch.tensor([EPSILON], dtype=dtype, device=device),
+        cutoff=CUTOFF,
+    )
+    masses = torch.full((n,), MASS, dtype=dtype, device=device)
+    velocities = md.maxwell_boltzmann(masses, TEMPERATURE, seed=2024)
+    setup = time.perf_counter()
+    simulation = md.nve(model, torch.tensor(positions, dtype=dtype, device=device), velocities,
+                        masses, torch.tensor(cell, dtype=dtype, device=device),
+                        timestep=TIMESTEP, skin=SKIN)
+    setup = time.perf_counter() - setup
+    simulation.run(max(3, args.warmup))
+    torch.cuda.synchronize(device)
+    rebuilds = simulation._neighbors._rebuild_count
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    simulation.run(args.steps)
+    end.record()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end)
+    print(json.dumps({
+        "impl": "reference-cuda",
+        "metric": METRIC,
+        "value": n * args.steps / (ms / 1e3),
+        "unit": "atom-steps/s",
+        "ms_per_step": ms / args.steps,
+        "steps": args.steps,
+        "setup_s": setup,
+        "rebuilds_in_timed_steps": simulation._neighbors._rebuild_count - rebuilds,
+        "pair_capacity": simulation._neighbors.pair_capacity,
+        "config": {"workload": WORKLOAD},
+    }), flush=True)
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -350,12 +401,14 @@ def main() -> None:
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=1000)
     parser.add_argument("--warmup", type=int, default=10)
-    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--impl", choices=("ours", "reference", "reference-cuda"), default="ours")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "reference-cuda":
+        run_reference_cuda(args)
     else:
         run_ours(args)
 

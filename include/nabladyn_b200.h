@@ -160,7 +160,7 @@ typedef struct nd_md_system {
     int32_t small;           /* 1: one tile holds the whole system, minimum image per pair */
     int32_t dims[3];         /* cells per axis (>= 3 each unless small) */
     int32_t bricks_x;        /* bricks per row of cells along x */
-    int32_t width;           /* neighbor-list slots per atom */
+    int32_t width;           /* neighbor-list slots per atom, a multiple of 8 */
     int32_t tile_capacity;   /* atoms per brick tile, at most */
     double cell[3];          /* orthorhombic cell lengths, fixed */
     double widths[3];        /* cell widths, L / dims, rounded to T */

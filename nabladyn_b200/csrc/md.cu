@@ -291,10 +291,77 @@ __device__ __forceinline__ int home_cell(const TileShape& shape, const int* firs
     return c;
 }
 
-__device__ __forceinline__ std::int64_t list_slot(int center, int k, int width)
+// The list stores each center's entries in chunks of kChunk uint16 indices, one 16-B word per
+// chunk, interleaved by warps of 32 cell-order slots: chunk c of center i is word
+// ((i / 32) * (width / kChunk) + c) * 32 + i % 32. A lane reads 8 neighbors with one load and
+// a warp reads 512 contiguous bytes; a partial last chunk is padded with the center itself.
+constexpr int kChunk = 8;
+
+__device__ __forceinline__ std::int64_t chunk_index(int center, int chunk, int width)
 {
-    return ((static_cast<std::int64_t>(center) >> 5) * width + k) * kWarp + (center & 31);
+    return ((static_cast<std::int64_t>(center) >> 5) * (width / kChunk) + chunk) * kWarp +
+           (center & 31);
 }
+
+// Collects one center's entries in registers and stores them a chunk at a time.
+struct ListWriter
+{
+    uint4* chunks;
+    int width;
+    int center;
+    unsigned long long pad;
+    unsigned long long lo;
+    unsigned long long hi;
+    int count;
+
+    __device__ __forceinline__ ListWriter(std::uint16_t* list, int width_, int center_,
+                                          unsigned self)
+        : chunks(reinterpret_cast<uint4*>(list)), width(width_), center(center_),
+          pad(0x0001000100010001ull * self), lo(pad), hi(pad), count(0)
+    {
+    }
+
+    __device__ __forceinline__ void add(unsigned index)
+    {
+        if (count < width)
+        {
+            const int r = count & (kChunk - 1);
+            const unsigned long long value = index;
+            const int shift = 16 * (r & 3);
+            if (r < 4)
+            {
+                lo = (lo & ~(0xffffull << shift)) | (value << shift);
+            }
+            else
+            {
+                hi = (hi & ~(0xffffull << shift)) | (value << shift);
+            }
+            if (r == kChunk - 1)
+            {
+                store(count / kChunk);
+            }
+        }
+        ++count;
+    }
+
+    __device__ __forceinline__ void store(int chunk)
+    {
+        chunks[chunk_index(center, chunk, width)] =
+            make_uint4(static_cast<unsigned>(lo), static_cast<unsigned>(lo >> 32),
+                       static_cast<unsigned>(hi), static_cast<unsigned>(hi >> 32));
+        lo = pad;
+        hi = pad;
+    }
+
+    __device__ __forceinline__ void finish()
+    {
+        const int stored = count < width ? count : width;
+        if (stored % kChunk != 0)
+        {
+            store(stored / kChunk);
+        }
+    }
+};
 
 __device__ __forceinline__ void flag_overflow(index_t* status, int word, int needed)
 {
@@ -331,7 +398,7 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             return;
         }
         const Pos4<T> c = tile[center];
-        int count = 0;
+        ListWriter list(s.nbr, s.width, center, center);
         for (int k = 0; k < s.n; ++k)
         {
             if (k == center)
@@ -344,17 +411,14 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             const T dz = min_image(c.z, p.z, s.length[2]);
             if (squared_norm(dx, dy, dz) < r2max)
             {
-                if (count < s.width)
-                {
-                    s.nbr[list_slot(center, count, s.width)] = static_cast<std::uint16_t>(k);
-                }
-                ++count;
+                list.add(k);
             }
         }
-        s.nbr_count[center] = count;
-        if (count > s.width)
+        list.finish();
+        s.nbr_count[center] = list.count;
+        if (list.count > s.width)
         {
-            flag_overflow(s.status, 1, count);
+            flag_overflow(s.status, 1, list.count);
         }
         return;
     }
@@ -378,7 +442,7 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
         const int c = home_cell(shape, first, center);
         const int self = start[4 * per_row + c] + (center - first[4 * per_row + c]);
         const Pos4<T> me = tile[self];
-        int count = 0;
+        ListWriter list(s.nbr, s.width, center, self);
         for (int r = 0; r < 9; ++r)
         {
             const int begin = start[r * per_row + c - 1];
@@ -392,18 +456,15 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
                 const Pos4<T> p = tile[k];
                 if (squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max)
                 {
-                    if (count < s.width)
-                    {
-                        s.nbr[list_slot(center, count, s.width)] = static_cast<std::uint16_t>(k);
-                    }
-                    ++count;
+                    list.add(k);
                 }
             }
         }
-        s.nbr_count[center] = count;
-        if (count > s.width)
+        list.finish();
+        s.nbr_count[center] = list.count;
+        if (list.count > s.width)
         {
-            flag_overflow(s.status, 1, count);
+            flag_overflow(s.status, 1, list.count);
         }
     }
 }
@@ -433,10 +494,26 @@ __device__ __forceinline__ void force_center(
     T fx = 0, fy = 0, fz = 0, energy = 0;
     T w[6] = {0, 0, 0, 0, 0, 0};
     PairParams<T> pp = params[0];
-    const std::uint16_t* list = s.nbr + list_slot(center, 0, s.width);
-    for (int k = 0; k < count_used; ++k)
+    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
+    const int num_chunks = (count_used + kChunk - 1) / kChunk;
+    // One 16-B word holds 8 neighbors; the next word is in flight while these are computed.
+    uint4 next = num_chunks > 0 ? chunks[0] : make_uint4(0, 0, 0, 0);
+    for (int chunk = 0; chunk < num_chunks; ++chunk)
     {
-        const Pos4<T> p = tile[list[static_cast<std::int64_t>(k) * kWarp]];
+        const uint4 word = next;
+        if (chunk + 1 < num_chunks)
+        {
+            next = chunks[static_cast<std::int64_t>(chunk + 1) * kWarp];
+        }
+        const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+        for (int r = 0; r < kChunk; ++r)
+        {
+        if (chunk * kChunk + r >= count_used)
+        {
+            break;
+        }
+        const Pos4<T> p = tile[(packed[r / 2] >> (16 * (r % 2))) & 0xffffu];
         T dx, dy, dz;
         if (kSmall)
         {
@@ -475,6 +552,7 @@ __device__ __forceinline__ void force_center(
                 w[4] = fma(fs * dx, dz, w[4]);
                 w[5] = fma(fs * dy, dz, w[5]);
             }
+        }
         }
     }
     // Each pair is listed from both ends: half of the energy and virial per end.
@@ -1235,7 +1313,7 @@ int check_system(const nd_md_system* m)
                "the system must be float32 or float64");
     ND_REQUIRE(m->num_atoms >= 2 && m->num_atoms <= INT32_MAX, "N must be in [2, 2**31)");
     ND_REQUIRE(m->num_types >= 1 && m->num_types <= 8, "1 to 8 atom types are supported");
-    ND_REQUIRE(m->width >= 1, "the list width must be positive");
+    ND_REQUIRE(m->width >= 8 && m->width % 8 == 0, "the list width must be a positive multiple of 8");
     const std::size_t pos_bytes = m->dtype == ND_FLOAT32 ? 16 : 32;
     if (m->small)
     {

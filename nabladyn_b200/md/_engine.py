@@ -133,8 +133,8 @@ class Engine:
         s.radius = self.radius
         s.timestep = float(timestep)
         s.threshold_squared = float(threshold)
-        # The sizing build: one slot per atom, the largest tile shared memory allows.
-        self._size_list(width=1, tile_capacity=self.tile_limit)
+        # The sizing build: one chunk per atom, the largest tile shared memory allows.
+        self._size_list(width=8, tile_capacity=self.tile_limit)
         slots = torch.empty(1, dtype=torch.int64)
         call("nd_md_partial_slots", s, _native.ctypes.cast(slots.data_ptr(), _native.c_int64_p))
         t["partials"] = torch.zeros(int(slots), **doubles)

@@ -176,6 +176,7 @@ def test_c_abi_count_and_fill(cuda):
         "pair_total": torch.zeros(1, **ints),
         "status": torch.zeros(2, **ints),
     }
+    t["pairs"] = torch.empty((2, 1), **ints)  # sized after the count, as allocate does
     buffers = _native.NeighborBuffers(
         **{k: v.data_ptr() for k, v in t.items()},
         num_bin_slots=bins + 1, scan_temp_bytes=scan.value, capacity=1, bits=None, bits_numel=0,
