@@ -109,6 +109,24 @@ int nd_neighbors_update(int dtype, const void* positions, const void* cell, int6
                         double cutoff, double radius, const nd_reuse_buffers* reuse,
                         const nd_neighbor_buffers* buffers, nd_stream_t stream);
 
+/* Builds one frame's pair list, as count_first_frame then fill_first_frame would, without
+ * allocating: for callers that cannot call cudaMalloc (code inside another framework's graph
+ * capture or memory pool, hosts that forbid allocation, fixed memory maps). It has no
+ * counterpart in the reference. Every intermediate buffer lives in one file-scope device array
+ * of about 1.3 MB that each GPU loading this library holds until the process exits; the caller
+ * passes only the inputs and the outputs: positions [N, 3] wrapped into [0, L) and cell [3]
+ * (device), the grid dims[3] and bin widths[3] (host values, as allocate chooses them), and
+ * pairs [2, capacity], pair_total [1], status [2] (device). Limits: N <= 16384 and at most
+ * 16384 bins; with at most three bins per axis (the all-pairs path) N <= 2048; larger inputs
+ * return ND_EINVAL. The first call on a device looks up the array's address with
+ * cudaGetSymbolAddress, so make it before any stream capture. Every call shares the array and
+ * leaves the last call's contents in it: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialized by the caller. */
+int nd_neighbors_build_no_alloc(int dtype, const void* positions, const void* cell,
+                                int64_t num_atoms, double radius, const int32_t* dims,
+                                const double* widths, int32_t* pairs, int64_t capacity,
+                                int32_t* pair_total, int32_t* status, nd_stream_t stream);
+
 /* ------------------------------------------------------------------------------------------
  * Lennard-Jones over a [2, C] pair index.
  *

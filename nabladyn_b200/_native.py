@@ -156,6 +156,11 @@ _SIGNATURES = {
         ctypes.c_double, ctypes.POINTER(ReuseBuffers), ctypes.POINTER(NeighborBuffers),
         ctypes.c_void_p,
     ],
+    "nd_neighbors_build_no_alloc": [
+        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p,
+    ],
     "nd_lj_energy_force_virial": [ctypes.POINTER(LJPairsArgs), ctypes.c_void_p],
     "nd_md_import": [
         ctypes.POINTER(MDSystem), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

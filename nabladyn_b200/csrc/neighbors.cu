@@ -831,3 +831,165 @@ int nd_neighbors_update(int dtype, const void* positions, const void* cell,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// The pair build without allocation.
+//
+// Some callers cannot call cudaMalloc at all: code running inside another framework's CUDA
+// Graph capture or memory pool, plugins whose host forbids allocation, or embedded drivers
+// with a fixed memory map. For them, nd_neighbors_build_no_alloc builds one frame's pair list
+// with every intermediate buffer (bins, sorted ids and positions, counts, offsets, scan tiles,
+// the all-pairs bit rows) in one file-scope device array of fixed size, kNoAllocBytes, which
+// every GPU that loads this library holds until the process exits. The caller passes only
+// the positions, the cell and the outputs.
+
+namespace nd {
+
+constexpr std::int64_t kNoAllocMaxAtoms = 16384;
+constexpr std::int64_t kNoAllocMaxBins = 16384;
+constexpr std::int64_t kNoAllocMaxAllPairsAtoms = 2048;
+
+constexpr std::int64_t round_up_256(std::int64_t bytes)
+{
+    return (bytes + 255) / 256 * 256;
+}
+
+// The layout of the array, in bytes from its start.
+struct NoAllocLayout
+{
+    static constexpr std::int64_t dims = 0;
+    static constexpr std::int64_t widths = 256;  // three doubles at most
+    static constexpr std::int64_t atom_bin = 512;
+    static constexpr std::int64_t bin_counts = atom_bin + round_up_256(4 * kNoAllocMaxAtoms);
+    static constexpr std::int64_t bin_offsets = bin_counts + round_up_256(4 * (kNoAllocMaxBins + 1));
+    static constexpr std::int64_t unordered_ids =
+        bin_offsets + round_up_256(4 * (kNoAllocMaxBins + 1));
+    static constexpr std::int64_t sorted_ids = unordered_ids + round_up_256(4 * kNoAllocMaxAtoms);
+    static constexpr std::int64_t sorted_positions =
+        sorted_ids + round_up_256(4 * kNoAllocMaxAtoms);
+    static constexpr std::int64_t pair_counts =
+        sorted_positions + round_up_256(3 * 8 * kNoAllocMaxAtoms);
+    static constexpr std::int64_t pair_offsets = pair_counts + round_up_256(4 * kNoAllocMaxAtoms);
+    static constexpr std::int64_t scan_temp = pair_offsets + round_up_256(4 * kNoAllocMaxAtoms);
+    static constexpr std::int64_t bits =
+        scan_temp + round_up_256((kNoAllocMaxAtoms + 1 + kTileItems - 1) / kTileItems * 4 + 16);
+    static constexpr std::int64_t size =
+        bits + round_up_256(4 * kNoAllocMaxAllPairsAtoms * ((kNoAllocMaxAllPairsAtoms + 31) / 32));
+};
+
+constexpr std::int64_t kNoAllocBytes = NoAllocLayout::size;
+
+// The scratch itself. In host code this name is only a stand-in for the symbol: its device
+// address comes from cudaGetSymbolAddress, per device.
+static __device__ __align__(256) unsigned char no_alloc_scratch[kNoAllocBytes];
+
+template <typename T>
+__global__ void store_grid_kernel(index_t* dims, T* widths, int nx, int ny, int nz, double wx,
+                                  double wy, double wz)
+{
+    dims[0] = nx;
+    dims[1] = ny;
+    dims[2] = nz;
+    widths[0] = static_cast<T>(wx);
+    widths[1] = static_cast<T>(wy);
+    widths[2] = static_cast<T>(wz);
+}
+
+// The array's device address on the current device, looked up once per device.
+int no_alloc_scratch_address(unsigned char** address)
+{
+    constexpr int kMaxDevices = 64;
+    static unsigned char* addresses[kMaxDevices] = {};
+    int device = 0;
+    ND_CUDA_TRY(cudaGetDevice(&device));
+    ND_REQUIRE(device >= 0 && device < kMaxDevices, "the device index is out of range");
+    if (addresses[device] == nullptr)
+    {
+        void* found = nullptr;
+        ND_CUDA_TRY(cudaGetSymbolAddress(&found, no_alloc_scratch));
+        addresses[device] = static_cast<unsigned char*>(found);
+    }
+    *address = addresses[device];
+    return ND_OK;
+}
+
+template <typename T>
+int build_no_alloc(const void* positions, const void* cell, std::int64_t n, double radius,
+                   const std::int32_t* dims, const double* widths, std::int32_t* pairs,
+                   std::int64_t capacity, std::int32_t* pair_total, std::int32_t* status,
+                   cudaStream_t stream)
+{
+    unsigned char* base = nullptr;
+    const int found = no_alloc_scratch_address(&base);
+    if (found != ND_OK)
+    {
+        return found;
+    }
+    const std::int64_t bins = static_cast<std::int64_t>(dims[0]) * dims[1] * dims[2];
+    const bool all_pairs = dims[0] <= 3 && dims[1] <= 3 && dims[2] <= 3;
+    nd_neighbor_buffers b{};
+    b.dims = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::dims);
+    b.widths = base + NoAllocLayout::widths;
+    b.atom_bin = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::atom_bin);
+    b.bin_counts = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::bin_counts);
+    b.bin_offsets = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::bin_offsets);
+    b.num_bin_slots = bins + 1;
+    b.unordered_ids = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::unordered_ids);
+    b.sorted_ids = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::sorted_ids);
+    b.sorted_positions = base + NoAllocLayout::sorted_positions;
+    b.scan_temp = base + NoAllocLayout::scan_temp;
+    b.scan_temp_bytes = NoAllocLayout::bits - NoAllocLayout::scan_temp;
+    b.pair_counts = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::pair_counts);
+    b.pair_offsets = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::pair_offsets);
+    b.pair_total = pair_total;
+    b.status = status;
+    b.pairs = pairs;
+    b.capacity = capacity;
+    b.bits = all_pairs ? reinterpret_cast<std::int32_t*>(base + NoAllocLayout::bits) : nullptr;
+    b.bits_numel = all_pairs ? n * bit_words(n) : 0;
+    // What must start at zero: the bin counts (a build returns them to zero, but an earlier
+    // call may have stopped short), the outputs' total and status.
+    ND_CUDA_TRY(cudaMemsetAsync(b.bin_counts, 0, sizeof(std::int32_t) * (bins + 1), stream));
+    ND_CUDA_TRY(cudaMemsetAsync(pair_total, 0, sizeof(std::int32_t), stream));
+    ND_CUDA_TRY(cudaMemsetAsync(status, 0, 2 * sizeof(std::int32_t), stream));
+    store_grid_kernel<T><<<1, 1, 0, stream>>>(b.dims, static_cast<T*>(b.widths), dims[0], dims[1],
+                                              dims[2], widths[0], widths[1], widths[2]);
+    ND_LAUNCH_CHECK();
+    const int counted = count_first_frame<T>(positions, cell, n, radius, &b, stream);
+    if (counted != ND_OK)
+    {
+        return counted;
+    }
+    const List list{&b, nullptr};
+    return launch_fill<T>(static_cast<const T*>(cell), n, radius, list, stream);
+}
+
+}  // namespace nd
+
+extern "C" int nd_neighbors_build_no_alloc(int dtype, const void* positions, const void* cell,
+                                           int64_t num_atoms, double radius,
+                                           const int32_t* dims, const double* widths,
+                                           int32_t* pairs, int64_t capacity,
+                                           int32_t* pair_total, int32_t* status,
+                                           nd_stream_t stream)
+{
+    ND_REQUIRE(dtype == ND_FLOAT32 || dtype == ND_FLOAT64, "positions must be float32 or float64");
+    ND_REQUIRE(positions && cell && dims && widths && pairs && pair_total && status,
+               "a required pointer is null");
+    ND_REQUIRE(num_atoms >= 1 && num_atoms <= nd::kNoAllocMaxAtoms,
+               "nd_neighbors_build_no_alloc takes at most 16384 atoms");
+    ND_REQUIRE(dims[0] >= 1 && dims[1] >= 1 && dims[2] >= 1, "dims must be positive");
+    const std::int64_t bins = static_cast<std::int64_t>(dims[0]) * dims[1] * dims[2];
+    ND_REQUIRE(bins <= nd::kNoAllocMaxBins, "nd_neighbors_build_no_alloc takes at most 16384 bins");
+    const bool all_pairs = dims[0] <= 3 && dims[1] <= 3 && dims[2] <= 3;
+    ND_REQUIRE(!all_pairs || num_atoms <= nd::kNoAllocMaxAllPairsAtoms,
+               "with at most three bins per axis nd_neighbors_build_no_alloc takes at most 2048 "
+               "atoms");
+    ND_REQUIRE(capacity >= 1 && capacity <= INT32_MAX, "pairs must be [2, C] with int32 C");
+    auto s = static_cast<cudaStream_t>(stream);
+    return dtype == ND_FLOAT32
+               ? nd::build_no_alloc<float>(positions, cell, num_atoms, radius, dims, widths, pairs,
+                                           capacity, pair_total, status, s)
+               : nd::build_no_alloc<double>(positions, cell, num_atoms, radius, dims, widths,
+                                            pairs, capacity, pair_total, status, s);
+}
