@@ -213,8 +213,7 @@ typedef struct nd_md_system {
     int32_t* rebuild;        /* [1] */
     int32_t* rebuild_count;  /* [1] */
     int32_t* status;         /* [4]: flags, most neighbors needed, largest tile needed, largest tile built */
-    double* partials;        /* [nd_md_partial_slots] */
-    uint32_t* ticket;        /* [1], zero */
+    double* partials;        /* [nd_md_partial_slots]: per-block float64 sums */
     double* totals;          /* [16]: E, K, W xx yy zz xy xz yz; then K of nd_md_kinetic */
     double* thermostat;      /* [24] float64 chain block */
     const void* sigma;       /* [T(T+1)/2] T */

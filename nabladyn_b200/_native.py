@@ -131,7 +131,6 @@ class MDSystem(ctypes.Structure):
         ("rebuild_count", ctypes.c_void_p),
         ("status", ctypes.c_void_p),
         ("partials", ctypes.c_void_p),
-        ("ticket", ctypes.c_void_p),
         ("totals", ctypes.c_void_p),
         ("thermostat", ctypes.c_void_p),
         ("sigma", ctypes.c_void_p),

@@ -49,7 +49,8 @@ struct alignas(4 * sizeof(T)) Pos4
     T x, y, z, w;
 };
 
-constexpr int kMDThreads = 128;
+constexpr int kMDThreads = 256;
+constexpr int kWarpsPerBlock = kMDThreads / kWarp;
 constexpr int kMaxBrickCells = 14;                  // home cells per brick, at most
 constexpr int kMaxRowCells = kMaxBrickCells + 2;    // tile cells per row
 constexpr int kTileCells = 9 * kMaxRowCells;        // tile cells, at most
@@ -103,7 +104,6 @@ struct System
     index_t* rebuild_count;
     index_t* status;
     double* partials;
-    unsigned* ticket;
     double* totals;
     double* thermo;
     const T* sigma;
@@ -116,6 +116,7 @@ struct System
     index_t num_bricks;
     index_t width;
     index_t tile_cap;
+    index_t sentinel;  // the tile slot of the far-away atom that pads partial list chunks
     int small;
     int num_types;
     T dt;
@@ -170,7 +171,77 @@ __device__ __forceinline__ int type_pair_row(int a, int b, int num_types)
 }
 
 // ---------------------------------------------------------------------------------------
+// Bulk asynchronous copies into shared memory, completed on an mbarrier (sm_90+ PTX).
+
+constexpr index_t kStageTimeout = 16;  // status bit: a tile copy did not complete in time
+constexpr int kWaitLimit = 1 << 22;    // mbarrier polls before a copy counts as lost
+
+__device__ __forceinline__ unsigned shared_address(const void* pointer)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(pointer));
+}
+
+__device__ __forceinline__ void barrier_init(std::uint64_t* barrier)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_address(barrier)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void barrier_expect_bytes(std::uint64_t* barrier, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                     shared_address(barrier)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Copies `bytes` (a multiple of 16, both addresses 16-B aligned) from global memory of this
+// GPU into this CTA's shared memory; completion counts on the barrier. No multicast.
+__device__ __forceinline__ void bulk_load(void* destination, const void* source, unsigned bytes,
+                                          std::uint64_t* barrier)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(shared_address(destination)),
+        "l"(source), "r"(bytes), "r"(shared_address(barrier))
+        : "memory");
+}
+
+__device__ __forceinline__ bool barrier_try_wait(std::uint64_t* barrier, unsigned phase)
+{
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(shared_address(barrier)), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+// Waits for phase 0 of the barrier, at most kWaitLimit polls; false when it gave up.
+__device__ __forceinline__ bool barrier_wait_bounded(std::uint64_t* barrier)
+{
+    for (int poll = 0; poll < kWaitLimit; ++poll)
+    {
+        if (barrier_try_wait(barrier, 0))
+        {
+            return true;
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------
 // Tiles.
+
+// The sentinel: an atom so far away that every distance to it fails the cutoff, yet stays
+// finite in float32 (1e18 nm squared is 3e36), so its masked force is an exact zero.
+template <typename T>
+__device__ __forceinline__ Pos4<T> far_atom()
+{
+    return Pos4<T>{T(1e18), T(1e18), T(1e18), T(0)};
+}
 
 // The geometry of one brick's tile in shared memory. Row r = 3 (dz + 1) + (dy + 1) holds the
 // tile cells c = 0 .. cells_per_row - 1 at x = x0 - 1 + c. start[r * cells_per_row + c] is
@@ -184,6 +255,10 @@ struct TileShape
     int home_end;
 };
 
+// Stages one brick's tile. The tile cells of a row are consecutive cells of the cell order
+// (apart from a wrap along x), so each maximal run of cells whose atoms are adjacent in memory
+// is one bulk copy, issued by the first warp; every thread then waits on the barrier, and the
+// cells across a periodic boundary get their image shift in shared memory.
 template <typename T>
 __device__ __forceinline__ TileShape stage_brick(
     const System<T>& s,
@@ -194,6 +269,7 @@ __device__ __forceinline__ TileShape stage_brick(
     int* first
 )
 {
+    __shared__ std::uint64_t copied;
     const int nx = s.dims[0], ny = s.dims[1], nz = s.dims[2];
     const int bx = brick % s.bricks_x;
     const int y = (brick / s.bricks_x) % ny;
@@ -202,6 +278,11 @@ __device__ __forceinline__ TileShape stage_brick(
     const int x1 = (bx + 1) * nx / s.bricks_x;
     const int per_row = x1 - x0 + 2;
     const int cells = 9 * per_row;
+    if (threadIdx.x == 0)
+    {
+        tile[s.sentinel] = far_atom<T>();
+        barrier_init(&copied);
+    }
     // Per tile cell: its cell-order range.
     for (int t = threadIdx.x; t < cells; t += blockDim.x)
     {
@@ -216,20 +297,21 @@ __device__ __forceinline__ TileShape stage_brick(
         start[t] = s.cell_offsets[cell + 1] - begin;  // the count, scanned below
     }
     __syncthreads();
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     // Exclusive scan of the counts by the first warp.
-    if (threadIdx.x < kWarp)
+    if (warp == 0)
     {
         int carry = 0;
         for (int base = 0; base < cells; base += kWarp)
         {
-            const int t = base + threadIdx.x;
+            const int t = base + lane;
             const int count = t < cells ? start[t] : 0;
             int inclusive = count;
 #pragma unroll
             for (int offset = 1; offset < kWarp; offset *= 2)
             {
                 const int up = __shfl_up_sync(kFullMask, inclusive, offset);
-                inclusive += threadIdx.x >= offset ? up : 0;
+                inclusive += lane >= offset ? up : 0;
             }
             if (t < cells)
             {
@@ -237,7 +319,7 @@ __device__ __forceinline__ TileShape stage_brick(
             }
             carry += __shfl_sync(kFullMask, inclusive, kWarp - 1);
         }
-        if (threadIdx.x == 0)
+        if (lane == 0)
         {
             start[cells] = carry;
         }
@@ -254,47 +336,71 @@ __device__ __forceinline__ TileShape stage_brick(
     {
         return shape;  // the caller flags the overflow; nothing is staged
     }
-    // Copy, one warp per tile cell, each cell shifted by its image.
-    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    for (int t = warp; t < cells; t += blockDim.x / kWarp)
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            barrier_expect_bytes(&copied, static_cast<unsigned>(shape.size * sizeof(Pos4<T>)));
+        }
+        __syncwarp();
+        // A run starts at a cell whose atoms do not follow the previous cell's in memory.
+        auto follows = [&](int t) { return first[t] == first[t - 1] + (start[t] - start[t - 1]); };
+        for (int base = 0; base < cells; base += kWarp)
+        {
+            const int t = base + lane;
+            if (t < cells && (t == 0 || !follows(t)))
+            {
+                int end = t + 1;
+                while (end < cells && follows(end))
+                {
+                    ++end;
+                }
+                const unsigned bytes = (start[end] - start[t]) * sizeof(Pos4<T>);
+                if (bytes > 0)
+                {
+                    bulk_load(tile + start[t], positions + first[t], bytes, &copied);
+                }
+            }
+        }
+    }
+    // One decision for the whole block, so every thread takes the same path below.
+    if (!__syncthreads_and(barrier_wait_bounded(&copied)))
+    {
+        // Lost copies: flag it, give them one more bounded wait, and compute nothing.
+        if (threadIdx.x == 0)
+        {
+            atomicOr(s.status, kStageTimeout);
+        }
+        barrier_wait_bounded(&copied);
+        shape.size = s.tile_cap + 1;
+        return shape;
+    }
+    // The image shifts of cells across a periodic boundary, one warp per such cell.
+    for (int t = warp; t < cells; t += kWarpsPerBlock)
     {
         const int r = t / per_row, c = t % per_row;
         const int cx = x0 - 1 + c, cy = y + r % 3 - 1, cz = z + r / 3 - 1;
         const T sx = cx < 0 ? -s.length[0] : (cx >= nx ? s.length[0] : T(0));
         const T sy = cy < 0 ? -s.length[1] : (cy >= ny ? s.length[1] : T(0));
         const T sz = cz < 0 ? -s.length[2] : (cz >= nz ? s.length[2] : T(0));
-        const int begin = first[t];
-        const int dst = start[t];
-        const int count = start[t + 1] - dst;
-        for (int k = lane; k < count; k += kWarp)
+        if (sx != T(0) || sy != T(0) || sz != T(0))
         {
-            Pos4<T> p = positions[begin + k];
-            p.x += sx;
-            p.y += sy;
-            p.z += sz;
-            tile[dst + k] = p;
+            for (int k = start[t] + lane; k < start[t + 1]; k += kWarp)
+            {
+                tile[k].x += sx;
+                tile[k].y += sy;
+                tile[k].z += sz;
+            }
         }
     }
     __syncthreads();
     return shape;
 }
 
-// The tile cell (in the home row) of a center and its tile slot.
-__device__ __forceinline__ int home_cell(const TileShape& shape, const int* first, int center)
-{
-    const int home_row = 4 * shape.cells_per_row;
-    int c = 1;
-    while (c + 1 < shape.cells_per_row - 1 && center >= first[home_row + c + 1])
-    {
-        ++c;
-    }
-    return c;
-}
-
 // The list stores each center's entries in chunks of kChunk uint16 indices, one 16-B word per
 // chunk, interleaved by warps of 32 cell-order slots: chunk c of center i is word
 // ((i / 32) * (width / kChunk) + c) * 32 + i % 32. A lane reads 8 neighbors with one load and
-// a warp reads 512 contiguous bytes; a partial last chunk is padded with the center itself.
+// a warp reads 512 contiguous bytes; a partial last chunk is padded with the sentinel.
 constexpr int kChunk = 8;
 
 __device__ __forceinline__ std::int64_t chunk_index(int center, int chunk, int width)
@@ -303,7 +409,8 @@ __device__ __forceinline__ std::int64_t chunk_index(int center, int chunk, int w
            (center & 31);
 }
 
-// Collects one center's entries in registers and stores them a chunk at a time.
+// Collects one center's entries in registers and stores them a chunk at a time; unused slots
+// of a chunk hold `pad`, the sentinel.
 struct ListWriter
 {
     uint4* chunks;
@@ -315,9 +422,9 @@ struct ListWriter
     int count;
 
     __device__ __forceinline__ ListWriter(std::uint16_t* list, int width_, int center_,
-                                          unsigned self)
+                                          unsigned pad_index)
         : chunks(reinterpret_cast<uint4*>(list)), width(width_), center(center_),
-          pad(0x0001000100010001ull * self), lo(pad), hi(pad), count(0)
+          pad(0x0001000100010001ull * pad_index), lo(pad), hi(pad), count(0)
     {
     }
 
@@ -392,13 +499,14 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             tile[k] = s.pos[k];
         }
         __syncthreads();
+        (void)first;
         const int center = blockIdx.x * blockDim.x + threadIdx.x;
         if (center >= s.n)
         {
             return;
         }
         const Pos4<T> c = tile[center];
-        ListWriter list(s.nbr, s.width, center, center);
+        ListWriter list(s.nbr, s.width, center, s.sentinel);
         for (int k = 0; k < s.n; ++k)
         {
             if (k == center)
@@ -435,36 +543,46 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
         }
         return;
     }
+    // One warp per home cell: the lanes are the cell's atoms and share its candidate rows, so
+    // every candidate is one broadcast read of shared memory and the loops do not diverge.
     const int per_row = shape.cells_per_row;
-    for (int center = shape.home_first + threadIdx.x; center < shape.home_end;
-         center += blockDim.x)
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    for (int c = 1 + warp; c < per_row - 1; c += kMDThreads / kWarp)
     {
-        const int c = home_cell(shape, first, center);
-        const int self = start[4 * per_row + c] + (center - first[4 * per_row + c]);
-        const Pos4<T> me = tile[self];
-        ListWriter list(s.nbr, s.width, center, self);
-        for (int r = 0; r < 9; ++r)
+        const int home = 4 * per_row + c;
+        const int cell_first = first[home];
+        const int tile_first = start[home];
+        const int cell_count = start[home + 1] - tile_first;
+        for (int base = 0; base < cell_count; base += kWarp)
         {
-            const int begin = start[r * per_row + c - 1];
-            const int end = start[r * per_row + c + 2];
-            for (int k = begin; k < end; ++k)
+            const bool active = base + lane < cell_count;
+            const int self = tile_first + (active ? base + lane : 0);
+            const int center = cell_first + base + lane;
+            const Pos4<T> me = tile[self];
+            ListWriter list(s.nbr, s.width, center, s.sentinel);
+            for (int r = 0; r < 9; ++r)
             {
-                if (k == self)
+                const int begin = start[r * per_row + c - 1];
+                const int end = start[r * per_row + c + 2];
+                for (int k = begin; k < end; ++k)
                 {
-                    continue;
-                }
-                const Pos4<T> p = tile[k];
-                if (squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max)
-                {
-                    list.add(k);
+                    const Pos4<T> p = tile[k];
+                    if (active && k != self &&
+                        squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max)
+                    {
+                        list.add(k);
+                    }
                 }
             }
-        }
-        list.finish();
-        s.nbr_count[center] = list.count;
-        if (list.count > s.width)
-        {
-            flag_overflow(s.status, 1, list.count);
+            if (active)
+            {
+                list.finish();
+                s.nbr_count[center] = list.count;
+                if (list.count > s.width)
+                {
+                    flag_overflow(s.status, 1, list.count);
+                }
+            }
         }
     }
 }
@@ -472,31 +590,36 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
 // ---------------------------------------------------------------------------------------
 // Forces, the second half kick and the step's reductions.
 
-enum ForceMode : int
+// The per-atom results of the pair loop, for one center.
+template <typename T>
+struct CenterSums
 {
-    kForceOnly = 0,  // F and E (and W): a first frame or a panel
-    kKick = 1,       // also v += dt/2 F / m, and K in float64
+    T fx, fy, fz;  // single type: in units of 24 eps; several types: kJ/mol/nm
+    T energy;      // single type: sum of p6^2 - p6; several types: kJ/mol
+    T inside;      // single type: pairs inside the cutoff
+    T w[6];        // like the force
 };
 
-template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
-__device__ __forceinline__ void force_center(
+// Loops one center's list: 8 neighbors per 16-B word, every neighbor read from the tile in
+// shared memory, no bounds checks (partial chunks are padded with the far sentinel) and no
+// branch on the cutoff (outside pairs contribute an exact zero). With one atom type the
+// constants 24 eps, 4 eps and u(r_c) are applied once per center, not per pair.
+template <typename T, bool kSmall, bool kMulti, bool kVirial>
+__device__ __forceinline__ CenterSums<T> pair_loop(
     const System<T>& s,
     const Pos4<T>* __restrict__ tile,
     const PairParams<T>* __restrict__ params,
-    int center,
-    int self,
-    double* sums
+    const Pos4<T>& me,
+    int center
 )
 {
-    const Pos4<T> me = tile[self];
+    CenterSums<T> out{};
     const int count = s.nbr_count[center];
-    const int count_used = count < s.width ? count : s.width;
-    T fx = 0, fy = 0, fz = 0, energy = 0;
-    T w[6] = {0, 0, 0, 0, 0, 0};
-    PairParams<T> pp = params[0];
+    const int used = count < s.width ? count : s.width;
+    const int num_chunks = (used + kChunk - 1) / kChunk;
     const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
-    const int num_chunks = (count_used + kChunk - 1) / kChunk;
-    // One 16-B word holds 8 neighbors; the next word is in flight while these are computed.
+    const T cutoff_squared = s.cutoff_squared;
+    const T s2 = params[0].s2;
     uint4 next = num_chunks > 0 ? chunks[0] : make_uint4(0, 0, 0, 0);
     for (int chunk = 0; chunk < num_chunks; ++chunk)
     {
@@ -509,60 +632,91 @@ __device__ __forceinline__ void force_center(
 #pragma unroll
         for (int r = 0; r < kChunk; ++r)
         {
-        if (chunk * kChunk + r >= count_used)
-        {
-            break;
-        }
-        const Pos4<T> p = tile[(packed[r / 2] >> (16 * (r % 2))) & 0xffffu];
-        T dx, dy, dz;
-        if (kSmall)
-        {
-            dx = min_image(me.x, p.x, s.length[0]);
-            dy = min_image(me.y, p.y, s.length[1]);
-            dz = min_image(me.z, p.z, s.length[2]);
-        }
-        else
-        {
-            dx = me.x - p.x;
-            dy = me.y - p.y;
-            dz = me.z - p.z;
-        }
-        const T r2 = squared_norm(dx, dy, dz);
-        if (r2 < s.cutoff_squared)
-        {
+            const Pos4<T> p = tile[(packed[r / 2] >> (16 * (r % 2))) & 0xffffu];
+            T dx, dy, dz;
+            if (kSmall)
+            {
+                dx = min_image(me.x, p.x, s.length[0]);
+                dy = min_image(me.y, p.y, s.length[1]);
+                dz = min_image(me.z, p.z, s.length[2]);
+            }
+            else
+            {
+                dx = me.x - p.x;
+                dy = me.y - p.y;
+                dz = me.z - p.z;
+            }
+            const T r2 = squared_norm(dx, dy, dz);
+            const bool inside = r2 < cutoff_squared;
+            const T inv_r2 = fast_reciprocal(r2);
+            PairParams<T> pp;
             if (kMulti)
             {
                 pp = params[type_pair_row(static_cast<int>(me.w), static_cast<int>(p.w),
                                           s.num_types)];
             }
-            const T inv_r2 = fast_reciprocal(r2);
-            const T q = pp.s2 * inv_r2;
+            const T q = (kMulti ? pp.s2 : s2) * inv_r2;
             const T p6 = q * q * q;
-            const T fs = pp.e24 * inv_r2 * (p6 * (T(2) * p6 - T(1)));
-            energy += pp.e4 * (p6 * (p6 - T(1))) - pp.shift;
-            fx = fma(fs, dx, fx);
-            fy = fma(fs, dy, fy);
-            fz = fma(fs, dz, fz);
+            T fs = inside ? inv_r2 * (p6 * fma(T(2), p6, T(-1))) : T(0);
+            const T u = fma(p6, p6, -p6);
+            if (kMulti)
+            {
+                fs *= pp.e24;
+                out.energy += inside ? fma(pp.e4, u, -pp.shift) : T(0);
+            }
+            else
+            {
+                out.energy += inside ? u : T(0);
+                out.inside += inside ? T(1) : T(0);
+            }
+            out.fx = fma(fs, dx, out.fx);
+            out.fy = fma(fs, dy, out.fy);
+            out.fz = fma(fs, dz, out.fz);
             if (kVirial)
             {
-                w[0] = fma(fs * dx, dx, w[0]);
-                w[1] = fma(fs * dy, dy, w[1]);
-                w[2] = fma(fs * dz, dz, w[2]);
-                w[3] = fma(fs * dx, dy, w[3]);
-                w[4] = fma(fs * dx, dz, w[4]);
-                w[5] = fma(fs * dy, dz, w[5]);
+                out.w[0] = fma(fs * dx, dx, out.w[0]);
+                out.w[1] = fma(fs * dy, dy, out.w[1]);
+                out.w[2] = fma(fs * dz, dz, out.w[2]);
+                out.w[3] = fma(fs * dx, dy, out.w[3]);
+                out.w[4] = fma(fs * dx, dz, out.w[4]);
+                out.w[5] = fma(fs * dy, dz, out.w[5]);
             }
         }
-        }
     }
+    return out;
+}
+
+template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
+__device__ __forceinline__ void force_center(
+    const System<T>& s,
+    const Pos4<T>* __restrict__ tile,
+    const PairParams<T>* __restrict__ params,
+    int center,
+    double* sums
+)
+{
+    const Pos4<T> me = s.pos[center];
+    CenterSums<T> c = pair_loop<T, kSmall, kMulti, kVirial>(s, tile, params, me, center);
+    T scale = T(1);  // kJ/mol/nm per unit of the accumulated force
+    double energy;
+    if (kMulti)
+    {
+        energy = double(c.energy);
+    }
+    else
+    {
+        scale = params[0].e24;
+        energy = double(params[0].e4) * double(c.energy) - double(params[0].shift) * double(c.inside);
+    }
+    const T fx = c.fx * scale, fy = c.fy * scale, fz = c.fz * scale;
     // Each pair is listed from both ends: half of the energy and virial per end.
-    sums[0] += 0.5 * double(energy);
+    sums[0] += 0.5 * energy;
     if (kVirial)
     {
 #pragma unroll
         for (int k = 0; k < 6; ++k)
         {
-            sums[2 + k] += 0.5 * double(w[k]);
+            sums[2 + k] += 0.5 * double(c.w[k] * scale);
         }
     }
     T* f = s.force + 3LL * center;
@@ -571,11 +725,11 @@ __device__ __forceinline__ void force_center(
     f[2] = fz;
     if (kKickStep)
     {
-        const T scale = s.half_dt * s.inv_mass[center];
+        const T kick = s.half_dt * s.inv_mass[center];
         T* v = s.vel + 3LL * center;
-        const T vx = fma(scale, fx, v[0]);
-        const T vy = fma(scale, fy, v[1]);
-        const T vz = fma(scale, fz, v[2]);
+        const T vx = fma(kick, fx, v[0]);
+        const T vy = fma(kick, fy, v[1]);
+        const T vz = fma(kick, fz, v[2]);
         v[0] = vx;
         v[1] = vy;
         v[2] = vz;
@@ -636,15 +790,14 @@ __device__ inline double chain_half_step(double& kinetic, double* q, double* p, 
     return factor;
 }
 
-// Block sums -> the block's slot; the last block reduces the slots in a fixed order, stores
-// the totals and runs the scalar tail.
-template <bool kThermostat, bool kStep>
-__device__ __forceinline__ void reduce_and_tail(double* sums, double* partials, unsigned* ticket,
-                                                double* totals, double* thermo, index_t* rebuild)
-// totals: the kReduced float64 outputs this kernel owns.
+// Each warp reduces its sums in float64 into shared memory and arrives on a block counter; the
+// block's last warp adds the warps' sums in a fixed order into the block's slot of `partials`.
+// No block barrier: a warp leaves as soon as its own centers are done. `arrivals` starts at
+// zero and is made visible by a barrier before any warp arrives.
+__device__ __forceinline__ void block_partial(const double* sums, double* partials,
+                                              unsigned* arrivals,
+                                              double (*warp_sums)[kReduced])
 {
-    __shared__ double warp_sums[kReduced][kMDThreads / kWarp];
-    __shared__ bool last;
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
 #pragma unroll
     for (int k = 0; k < kReduced; ++k)
@@ -652,44 +805,53 @@ __device__ __forceinline__ void reduce_and_tail(double* sums, double* partials, 
         const double v = warp_sum(sums[k]);
         if (lane == 0)
         {
-            warp_sums[k][warp] = v;
+            warp_sums[warp][k] = v;
         }
     }
-    __syncthreads();
-    if (threadIdx.x < kReduced)
+    __threadfence_block();
+    unsigned arrived = 0;
+    if (lane == 0)
     {
-        double v = 0;
-        for (int w = 0; w < kMDThreads / kWarp; ++w)
-        {
-            v += warp_sums[threadIdx.x][w];
-        }
-        partials[static_cast<std::int64_t>(blockIdx.x) * kReduced + threadIdx.x] = v;
+        arrived = atomicAdd(arrivals, 1u);
     }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last)
+    arrived = __shfl_sync(kFullMask, arrived, 0);
+    if (arrived != kWarpsPerBlock - 1)
     {
         return;
     }
-    __threadfence();
-    // Fixed-order sums over the blocks: thread t takes blocks t, t + 128, ...
-    double mine[kReduced];
-#pragma unroll
-    for (int k = 0; k < kReduced; ++k)
+    __threadfence_block();
+    if (lane < kReduced)
     {
-        mine[k] = 0;
+        const volatile double* shared = &warp_sums[0][0];
+        double total = 0;
+        for (int w = 0; w < kWarpsPerBlock; ++w)
+        {
+            total += shared[w * kReduced + lane];
+        }
+        partials[static_cast<std::int64_t>(blockIdx.x) * kReduced + lane] = total;
     }
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+}
+
+constexpr int kFinalizeThreads = 1024;
+
+// One block: the fixed-order sum of the block slots into `totals`, then the scalar tail of a
+// step: the rebuild flag cleared for the next check and, for NVT, the closing half step of the
+// chain against this step's K, whose factor the next drift (or a frame read) applies.
+template <bool kThermostat, bool kStep>
+__global__ void __launch_bounds__(kFinalizeThreads) finalize_kernel(const double* partials,
+                                                                    int blocks, double* totals,
+                                                                    double* thermo,
+                                                                    index_t* rebuild)
+{
+    __shared__ double warp_sums[kFinalizeThreads / kWarp][kReduced];
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    double mine[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < blocks; b += kFinalizeThreads)
     {
 #pragma unroll
         for (int k = 0; k < kReduced; ++k)
         {
-            mine[k] += __ldcg(partials + static_cast<std::int64_t>(b) * kReduced + k);
+            mine[k] += partials[static_cast<std::int64_t>(b) * kReduced + k];
         }
     }
 #pragma unroll
@@ -698,49 +860,51 @@ __device__ __forceinline__ void reduce_and_tail(double* sums, double* partials, 
         const double v = warp_sum(mine[k]);
         if (lane == 0)
         {
-            warp_sums[k][warp] = v;
+            warp_sums[warp][k] = v;
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0)
+    if (warp != 0)
     {
-        double total[kReduced];
-        for (int k = 0; k < kReduced; ++k)
+        return;
+    }
+    double total[kReduced];
+#pragma unroll
+    for (int k = 0; k < kReduced; ++k)
+    {
+        total[k] = warp_sum(warp_sums[lane][k]);
+    }
+    if (lane != 0)
+    {
+        return;
+    }
+    for (int k = 0; k < kReduced; ++k)
+    {
+        totals[k] = total[k];
+    }
+    if (kStep)
+    {
+        rebuild[0] = 0;  // the next step's check starts clean
+    }
+    if (kThermostat)
+    {
+        double kinetic = total[1];
+        double q[3], p[3];
+        for (int k = 0; k < 3; ++k)
         {
-            total[k] = 0;
-            for (int w = 0; w < kMDThreads / kWarp; ++w)
-            {
-                total[k] += warp_sums[k][w];
-            }
-            totals[k] = total[k];
+            q[k] = thermo[kChainB + k];
+            p[k] = thermo[kChainB + 3 + k];
         }
-        *ticket = 0;
-        if (kStep)
+        const double factor = chain_half_step(kinetic, q, p, thermo + kChainMass,
+                                              thermo[kDegrees], thermo[kThermalEnergy],
+                                              thermo[kTimestep]);
+        for (int k = 0; k < 3; ++k)
         {
-            rebuild[0] = 0;  // the next step's check starts clean
+            thermo[kChainA + k] = q[k];
+            thermo[kChainA + 3 + k] = p[k];
         }
-        if (kThermostat)
-        {
-            // The closing half step against this step's K; its factor is applied to the stored
-            // velocities by the next drift (or when the frame is read).
-            double kinetic = total[1];
-            double q[3], p[3];
-            for (int k = 0; k < 3; ++k)
-            {
-                q[k] = thermo[kChainB + k];
-                p[k] = thermo[kChainB + 3 + k];
-            }
-            const double factor = chain_half_step(kinetic, q, p, thermo + kChainMass,
-                                                  thermo[kDegrees], thermo[kThermalEnergy],
-                                                  thermo[kTimestep]);
-            for (int k = 0; k < 3; ++k)
-            {
-                thermo[kChainA + k] = q[k];
-                thermo[kChainA + 3 + k] = p[k];
-            }
-            thermo[kKineticA] = kinetic;
-            thermo[kPendingScale] = factor;
-        }
+        thermo[kKineticA] = kinetic;
+        thermo[kPendingScale] = factor;
     }
 }
 
@@ -752,10 +916,16 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
     __shared__ int start[kTileCells + 1];
     __shared__ int first[kTileCells];
     __shared__ PairParams<T> params[36];
+    __shared__ unsigned arrivals;
+    __shared__ double warp_sums[kWarpsPerBlock][kReduced];
     const int rows = s.num_types * (s.num_types + 1) / 2;
     for (int k = threadIdx.x; k < rows; k += blockDim.x)
     {
         params[k] = pair_params(s.sigma[k], s.epsilon[k], s.cutoff_squared);
+    }
+    if (threadIdx.x == 0)
+    {
+        arrivals = 0;
     }
     double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (kSmall)
@@ -764,12 +934,16 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
         {
             tile[k] = s.pos[k];
         }
+        if (threadIdx.x == 0)
+        {
+            tile[s.sentinel] = far_atom<T>();
+        }
         __syncthreads();
         const int center = blockIdx.x * blockDim.x + threadIdx.x;
         if (center < s.n)
         {
             force_center<T, true, kMulti, kVirial, kKickStep, kThermostat>(s, tile, params, center,
-                                                                          center, sums);
+                                                                          sums);
         }
     }
     else
@@ -777,14 +951,11 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
         const TileShape shape = stage_brick(s, blockIdx.x, s.pos, tile, start, first);
         if (shape.size <= s.tile_cap)
         {
-            const int per_row = shape.cells_per_row;
             for (int center = shape.home_first + threadIdx.x; center < shape.home_end;
                  center += blockDim.x)
             {
-                const int c = home_cell(shape, first, center);
-                const int self = start[4 * per_row + c] + (center - first[4 * per_row + c]);
-                force_center<T, false, kMulti, kVirial, kKickStep, kThermostat>(
-                    s, tile, params, center, self, sums);
+                force_center<T, false, kMulti, kVirial, kKickStep, kThermostat>(s, tile, params,
+                                                                               center, sums);
             }
         }
         else if (threadIdx.x == 0)
@@ -792,8 +963,7 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
             flag_overflow(s.status, 2, shape.size);
         }
     }
-    reduce_and_tail<kThermostat, kKickStep>(sums, s.partials, s.ticket, s.totals, s.thermo,
-                                            s.rebuild);
+    block_partial(sums, s.partials, &arrivals, warp_sums);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1085,6 +1255,13 @@ __global__ void export_kernel(System<T> s, T* __restrict__ positions, T* __restr
 template <typename T>
 __global__ void __launch_bounds__(kMDThreads) kinetic_kernel(System<T> s, int thermostat)
 {
+    __shared__ unsigned arrivals;
+    __shared__ double warp_sums[kWarpsPerBlock][kReduced];
+    if (threadIdx.x == 0)
+    {
+        arrivals = 0;
+    }
+    __syncthreads();
     double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
     const std::int64_t k = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k < s.n)
@@ -1099,8 +1276,7 @@ __global__ void __launch_bounds__(kMDThreads) kinetic_kernel(System<T> s, int th
         }
         sums[1] = 0.5 * double(s.mass[k]) * v2;
     }
-    reduce_and_tail<false, false>(sums, s.partials, s.ticket, s.totals + kReduced, s.thermo,
-                                  s.rebuild);
+    block_partial(sums, s.partials, &arrivals, warp_sums);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1138,7 +1314,6 @@ System<T> view(const nd_md_system* m)
     s.rebuild_count = m->rebuild_count;
     s.status = m->status;
     s.partials = m->partials;
-    s.ticket = m->ticket;
     s.totals = m->totals;
     s.thermo = m->thermostat;
     s.sigma = static_cast<const T*>(m->sigma);
@@ -1156,6 +1331,7 @@ System<T> view(const nd_md_system* m)
                            : m->bricks_x * m->dims[1] * m->dims[2];
     s.width = m->width;
     s.tile_cap = m->tile_capacity;
+    s.sentinel = m->small ? static_cast<index_t>(m->num_atoms) : m->tile_capacity;
     s.num_types = m->num_types;
     s.dt = static_cast<T>(m->timestep);
     s.half_dt = static_cast<T>(0.5 * m->timestep);
@@ -1168,7 +1344,7 @@ System<T> view(const nd_md_system* m)
 template <typename T>
 std::size_t tile_bytes(const System<T>& s)
 {
-    return static_cast<std::size_t>(s.small ? s.n : s.tile_cap) * sizeof(Pos4<T>);
+    return static_cast<std::size_t>(s.sentinel + 1) * sizeof(Pos4<T>);
 }
 
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than any before; the
@@ -1237,6 +1413,9 @@ int launch_force_variant(const System<T>& s, cudaStream_t stream)
         ND_CUDA_TRY(allow_shared(kernel, bytes, granted));                                  \
         kernel<<<s.num_bricks, kMDThreads, bytes, stream>>>(s);                             \
         ND_LAUNCH_CHECK();                                                                  \
+        finalize_kernel<kThermostat, kKickStep><<<1, kFinalizeThreads, 0, stream>>>(        \
+            s.partials, s.num_bricks, s.totals, s.thermo, s.rebuild);                       \
+        ND_LAUNCH_CHECK();                                                                  \
         return ND_OK;                                                                       \
     }
     ND_FORCE_CASE(1, true)
@@ -1303,7 +1482,7 @@ std::int64_t step_launches(const nd_md_system* m)
     {
         rebuild += (scan_tiles(cells + 1) <= 1 ? 1 : 3) + 3;  // scan, place, order, permute
     }
-    return 1 + rebuild + 1;  // drift, rebuild, forces
+    return 1 + rebuild + 2;  // drift, rebuild, forces and their finalize
 }
 
 int check_system(const nd_md_system* m)
@@ -1317,8 +1496,8 @@ int check_system(const nd_md_system* m)
     const std::size_t pos_bytes = m->dtype == ND_FLOAT32 ? 16 : 32;
     if (m->small)
     {
-        ND_REQUIRE(m->num_atoms <= 65535, "a small-box system holds at most 65535 atoms");
-        ND_REQUIRE(static_cast<std::size_t>(m->num_atoms) * pos_bytes <= 200 * 1024,
+        ND_REQUIRE(m->num_atoms <= 65534, "a small-box system holds at most 65534 atoms");
+        ND_REQUIRE(static_cast<std::size_t>(m->num_atoms + 1) * pos_bytes <= 200 * 1024,
                    "a small-box system must fit one shared-memory tile");
     }
     else
@@ -1328,8 +1507,8 @@ int check_system(const nd_md_system* m)
         ND_REQUIRE(m->bricks_x >= 1 && m->bricks_x <= m->dims[0], "bricks_x out of range");
         ND_REQUIRE((m->dims[0] + m->bricks_x - 1) / m->bricks_x <= kMaxBrickCells,
                    "a brick spans too many cells");
-        ND_REQUIRE(m->tile_capacity >= 1 && m->tile_capacity <= 65535 &&
-                       static_cast<std::size_t>(m->tile_capacity) * pos_bytes <= 200 * 1024,
+        ND_REQUIRE(m->tile_capacity >= 1 && m->tile_capacity <= 65534 &&
+                       static_cast<std::size_t>(m->tile_capacity + 1) * pos_bytes <= 200 * 1024,
                    "the tile capacity must fit shared memory and uint16 indices");
     }
     return ND_OK;
@@ -1453,8 +1632,11 @@ int nd_md_kinetic(const nd_md_system* system, int thermostat, nd_stream_t stream
     auto st = static_cast<cudaStream_t>(stream);
     return ND_MD_DISPATCH(system, ([&] {
         using T = std::remove_pointer_t<decltype(s.vel)>;
-        nd::kinetic_kernel<T><<<nd::blocks_for(s.n, nd::kMDThreads), nd::kMDThreads, 0, st>>>(
-            s, thermostat);
+        const unsigned blocks = nd::blocks_for(s.n, nd::kMDThreads);
+        nd::kinetic_kernel<T><<<blocks, nd::kMDThreads, 0, st>>>(s, thermostat);
+        ND_LAUNCH_CHECK();
+        nd::finalize_kernel<false, false><<<1, nd::kFinalizeThreads, 0, st>>>(
+            s.partials, static_cast<int>(blocks), s.totals + nd::kReduced, s.thermo, s.rebuild);
         ND_LAUNCH_CHECK();
         return ND_OK;
     }()));

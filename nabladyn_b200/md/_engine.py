@@ -23,13 +23,14 @@ from .._native import MDSystem, OVERFLOW, call, dtype_code, ptr, stream_handle
 from ..neighbors._neighbor_list import check_cell_lengths, grid
 from ..units import BOLTZMANN
 
-_THREADS = 128           # kMDThreads in md.cu
+_THREADS = 256           # kMDThreads in md.cu
 _MAX_BRICK_CELLS = 14    # kMaxBrickCells in md.cu
 _TILE_BYTES = 200 * 1024  # the dynamic shared memory a tile may take
-_CENTERS_PER_BRICK = 112  # the brick size aimed at: about 4 warps of centers
+_CENTERS_PER_BRICK = 224  # the brick size aimed at: about 7 warps of centers
 # Offsets into the float64 thermostat block (enum Thermo in md.cu).
 CHAIN_A, KINETIC_A, CHAIN_B, KINETIC_B, PENDING_SCALE = 0, 6, 7, 13, 14
 CHAIN_MASS, THERMAL_ENERGY, DEGREES, TIMESTEP = 16, 19, 20, 21
+STAGE_TIMEOUT = 16  # status bit: a tile copy did not complete (kStageTimeout in md.cu)
 
 
 class Engine:
@@ -60,10 +61,10 @@ class Engine:
         dims = grid(lengths, self.radius, dtype)
         small = min(dims) < 3
         position_bytes = 4 * torch.finfo(dtype).bits // 8
-        if small and n * position_bytes > _TILE_BYTES:
+        if small and (n + 1) * position_bytes > _TILE_BYTES:
             raise ValueError(
                 f"a cell with fewer than three list radii ({self.radius} nm) on an axis holds "
-                f"at most {_TILE_BYTES // position_bytes} atoms in this build",
+                f"at most {_TILE_BYTES // position_bytes - 1} atoms in this build",
             )
         bricks_x = 1
         if not small:
@@ -78,7 +79,8 @@ class Engine:
         threshold = allowance * allowance / 4 if allowance > 0 else 0.0
         self.dims, self.small, self.bricks_x = dims, small, bricks_x
         self.capacity_multiplier = float(capacity_multiplier)
-        self.tile_limit = min(65535, _TILE_BYTES // position_bytes)
+        # Tile slots, the sentinel's included, must fit shared memory and uint16 indices.
+        self.tile_limit = min(65534, _TILE_BYTES // position_bytes - 1)
         num_cells = math.prod(dims)
         self.num_cells = num_cells
 
@@ -112,7 +114,6 @@ class Engine:
         t["rebuild"] = torch.zeros(1, **ints)
         t["rebuild_count"] = torch.zeros(1, **ints)
         t["status"] = torch.zeros(4, **ints)
-        t["ticket"] = torch.zeros(1, **ints)
         t["totals"] = torch.zeros(16, **doubles)
         t["thermostat"] = torch.zeros(24, **doubles)
         t["sigma"] = sigma.detach().to(device, dtype).contiguous()
@@ -159,7 +160,7 @@ class Engine:
             "shadow_inverse_masses", "shadow_masses", "shadow_images", "shadow_ids",
             "cell_counts", "cell_offsets", "atom_cell", "slots", "unordered", "order",
             "scan_temp", "neighbors", "neighbor_counts", "rebuild", "rebuild_count", "status",
-            "partials", "ticket", "totals", "thermostat", "sigma", "epsilon",
+            "partials", "totals", "thermostat", "sigma", "epsilon",
         ):
             setattr(s, name, ptr(t[name]))
 
@@ -180,7 +181,7 @@ class Engine:
         masses = masses.detach().to(self.dtype).contiguous()
         images = images.detach().to(torch.int64).contiguous()
         kernel_types = types.detach().to(torch.int32).contiguous() if types is not None else None
-        for name in ("rebuild", "rebuild_count", "status", "ticket", "cell_counts"):
+        for name in ("rebuild", "rebuild_count", "status", "cell_counts"):
             t[name].zero_()
         with torch.cuda.device(self.device):
             stream = self._stream()
@@ -217,7 +218,7 @@ class Engine:
         rebuild, forces. No host sync; a frame that needs more room than the buffers have
         sets the overflow bit, read with ``failure``."""
         s, t = self.system, self.tensors
-        for name in ("rebuild", "status", "ticket", "cell_counts"):
+        for name in ("rebuild", "status", "cell_counts"):
             t[name].zero_()
         with torch.cuda.device(self.device):
             stream = self._stream()
@@ -314,6 +315,8 @@ class Engine:
             causes.append("every cell length must be finite and above twice the cutoff")
         if flags & _native.NON_FINITE:
             causes.append("positions must be finite")
+        if flags & STAGE_TIMEOUT:
+            causes.append("a shared-memory tile copy did not complete")
         if flags & OVERFLOW:
             if neighbors > self.width:
                 causes.append(
