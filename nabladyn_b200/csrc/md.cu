@@ -620,13 +620,16 @@ __device__ __forceinline__ CenterSums<T> pair_loop(
     const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
     const T cutoff_squared = s.cutoff_squared;
     const T s2 = params[0].s2;
+    // Two words in flight ahead of the one being computed: the list streams from HBM.
     uint4 next = num_chunks > 0 ? chunks[0] : make_uint4(0, 0, 0, 0);
+    uint4 after = num_chunks > 1 ? chunks[kWarp] : make_uint4(0, 0, 0, 0);
     for (int chunk = 0; chunk < num_chunks; ++chunk)
     {
         const uint4 word = next;
-        if (chunk + 1 < num_chunks)
+        next = after;
+        if (chunk + 2 < num_chunks)
         {
-            next = chunks[static_cast<std::int64_t>(chunk + 1) * kWarp];
+            after = chunks[static_cast<std::int64_t>(chunk + 2) * kWarp];
         }
         const unsigned packed[4] = {word.x, word.y, word.z, word.w};
 #pragma unroll
