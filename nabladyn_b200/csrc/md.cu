@@ -470,6 +470,55 @@ struct ListWriter
     }
 };
 
+// The same chunks, staged per lane in 16 bytes of shared memory: a hit is one 2-byte store, and
+// every eighth hit stores the chunk to global memory in one 16-byte write. The list build uses
+// it; its hits are sparse and divergent, so the per-hit work is what the warp pays.
+struct StagedListWriter
+{
+    uint4* chunks;
+    std::uint16_t* staged;  // this lane's 8 slots
+    int width;
+    int center;
+    int count;
+
+    __device__ __forceinline__ StagedListWriter(std::uint16_t* list, std::uint16_t* lane_slots,
+                                                int width_, int center_)
+        : chunks(reinterpret_cast<uint4*>(list)), staged(lane_slots), width(width_),
+          center(center_), count(0)
+    {
+    }
+
+    __device__ __forceinline__ void add(unsigned index)
+    {
+        if (count < width)
+        {
+            const int r = count & (kChunk - 1);
+            staged[r] = static_cast<std::uint16_t>(index);
+            if (r == kChunk - 1)
+            {
+                chunks[chunk_index(center, count / kChunk, width)] =
+                    *reinterpret_cast<const uint4*>(staged);
+            }
+        }
+        ++count;
+    }
+
+    // Stores a partial last chunk, its unused slots set to `pad`.
+    __device__ __forceinline__ void finish(unsigned pad)
+    {
+        const int stored = count < width ? count : width;
+        if (stored % kChunk != 0)
+        {
+            for (int r = stored % kChunk; r < kChunk; ++r)
+            {
+                staged[r] = static_cast<std::uint16_t>(pad);
+            }
+            chunks[chunk_index(center, stored / kChunk, width)] =
+                *reinterpret_cast<const uint4*>(staged);
+        }
+    }
+};
+
 __device__ __forceinline__ void flag_overflow(index_t* status, int word, int needed)
 {
     atomicOr(status, kOverflow);
@@ -490,6 +539,7 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
     auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
     __shared__ int start[kTileCells + 1];
     __shared__ int first[kTileCells];
+    __shared__ __align__(16) std::uint16_t lane_slots[kMDThreads][kChunk];
     const T r2max = s.radius_squared;
     if (s.small)
     {
@@ -559,7 +609,7 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             const int self = tile_first + (active ? base + lane : 0);
             const int center = cell_first + base + lane;
             const Pos4<T> me = tile[self];
-            ListWriter list(s.nbr, s.width, center, s.sentinel);
+            StagedListWriter list(s.nbr, lane_slots[threadIdx.x], s.width, center);
             for (int r = 0; r < 9; ++r)
             {
                 const int begin = start[r * per_row + c - 1];
@@ -576,7 +626,7 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             }
             if (active)
             {
-                list.finish();
+                list.finish(s.sentinel);
                 s.nbr_count[center] = list.count;
                 if (list.count > s.width)
                 {
