@@ -194,9 +194,8 @@ typedef struct nd_md_system {
     int64_t* images;         /* [N, 3] */
     int32_t* ids;            /* [N] */
     void* reference_positions; /* [N, 4] T */
-    void* shadow_positions;  /* the permutation's copies of the seven arrays above */
+    void* shadow_positions;  /* the permutation's copies of the arrays above, forces excepted */
     void* shadow_velocities;
-    void* shadow_forces;
     void* shadow_inverse_masses;
     void* shadow_masses;
     int64_t* shadow_images;

@@ -113,7 +113,6 @@ class MDSystem(ctypes.Structure):
         ("reference_positions", ctypes.c_void_p),
         ("shadow_positions", ctypes.c_void_p),
         ("shadow_velocities", ctypes.c_void_p),
-        ("shadow_forces", ctypes.c_void_p),
         ("shadow_inverse_masses", ctypes.c_void_p),
         ("shadow_masses", ctypes.c_void_p),
         ("shadow_images", ctypes.c_void_p),

@@ -8,8 +8,9 @@
 //
 // Layout in HBM. The engine keeps every per-atom array in "cell order": the order of the last
 // rebuild, atoms sorted by cell and by atom id within a cell, so a cell's atoms are one
-// contiguous range. A rebuild re-sorts and permutes the state (positions, velocities, forces,
-// masses, images, ids, types); `ids` maps a slot back to the caller's atom. Positions are
+// contiguous range. A rebuild re-sorts and permutes the state (positions, velocities, masses,
+// images, ids, types); the forces are recomputed in the new order right after it. `ids` maps a
+// slot back to the caller's atom. Positions are
 // [N] x (x, y, z, type) vectors, 16 B in float32, so one load fetches an atom. Between rebuilds
 // positions are NOT wrapped: an atom keeps the image it was binned in, which keeps every
 // precomputed cell image valid; a rebuild wraps them and counts the crossings.
@@ -86,7 +87,6 @@ struct System
     Pos4<T>* ref_pos;
     Pos4<T>* pos_b;
     T* vel_b;
-    T* force_b;
     T* inv_mass_b;
     T* mass_b;
     long long* images_b;
@@ -710,17 +710,18 @@ __device__ __forceinline__ CenterSums<T> pair_loop(
             }
             const T q = (kMulti ? pp.s2 : s2) * inv_r2;
             const T p6 = q * q * q;
-            T fs = inside ? inv_r2 * (p6 * fma(T(2), p6, T(-1))) : T(0);
+            const T mask = inside ? T(1) : T(0);
+            T fs = mask * (inv_r2 * (p6 * fma(T(2), p6, T(-1))));
             const T u = fma(p6, p6, -p6);
             if (kMulti)
             {
                 fs *= pp.e24;
-                out.energy += inside ? fma(pp.e4, u, -pp.shift) : T(0);
+                out.energy = fma(mask, fma(pp.e4, u, -pp.shift), out.energy);
             }
             else
             {
-                out.energy += inside ? u : T(0);
-                out.inside += inside ? T(1) : T(0);
+                out.energy = fma(mask, u, out.energy);
+                out.inside += mask;
             }
             out.fx = fma(fs, dx, out.fx);
             out.fy = fma(fs, dy, out.fy);
@@ -1195,7 +1196,6 @@ __global__ void permute_kernel(System<T> s, int gated)
     for (int a = 0; a < 3; ++a)
     {
         s.vel_b[3 * k + a] = s.vel[3LL * old + a];
-        s.force_b[3 * k + a] = s.force[3LL * old + a];
         s.images_b[3 * k + a] = s.images[3LL * old + a];
     }
     s.inv_mass_b[k] = s.inv_mass[old];
@@ -1225,7 +1225,6 @@ __global__ void commit_kernel(System<T> s, int gated)
     for (int a = 0; a < 3; ++a)
     {
         s.vel[3 * k + a] = s.vel_b[3 * k + a];
-        s.force[3 * k + a] = s.force_b[3 * k + a];
         s.images[3 * k + a] = s.images_b[3 * k + a];
     }
     s.inv_mass[k] = s.inv_mass_b[k];
@@ -1349,7 +1348,6 @@ System<T> view(const nd_md_system* m)
     s.ref_pos = static_cast<Pos4<T>*>(m->reference_positions);
     s.pos_b = static_cast<Pos4<T>*>(m->shadow_positions);
     s.vel_b = static_cast<T*>(m->shadow_velocities);
-    s.force_b = static_cast<T*>(m->shadow_forces);
     s.inv_mass_b = static_cast<T*>(m->shadow_inverse_masses);
     s.mass_b = static_cast<T*>(m->shadow_masses);
     s.images_b = reinterpret_cast<long long*>(m->shadow_images);

@@ -97,8 +97,7 @@ class Engine:
         t["images"] = torch.zeros((n, 3), **longs)
         t["ids"] = torch.zeros(n, **ints)
         t["reference_positions"] = torch.zeros((n, 4), **floats)
-        for name in ("positions", "velocities", "forces", "inverse_masses", "masses", "images",
-                     "ids"):
+        for name in ("positions", "velocities", "inverse_masses", "masses", "images", "ids"):
             t["shadow_" + name] = torch.zeros_like(t[name])
         t["cell_counts"] = torch.zeros(num_cells + 1, **ints)
         t["cell_offsets"] = torch.zeros(num_cells + 1, **ints)
@@ -156,7 +155,7 @@ class Engine:
         s, t = self.system, self.tensors
         for name in (
             "positions", "velocities", "forces", "inverse_masses", "masses", "images", "ids",
-            "reference_positions", "shadow_positions", "shadow_velocities", "shadow_forces",
+            "reference_positions", "shadow_positions", "shadow_velocities",
             "shadow_inverse_masses", "shadow_masses", "shadow_images", "shadow_ids",
             "cell_counts", "cell_offsets", "atom_cell", "slots", "unordered", "order",
             "scan_temp", "neighbors", "neighbor_counts", "rebuild", "rebuild_count", "status",
@@ -200,8 +199,11 @@ class Engine:
                 )
             width = math.ceil(self.capacity_multiplier * needed_neighbors)
             width = max(8, -(-width // 8) * 8)
-            tile = min(self.tile_limit, max(needed_tile, math.ceil(
-                self.capacity_multiplier * needed_tile)))
+            # A tile sums thousands of atoms over tens of cells, so its count fluctuates by
+            # about a percent in a liquid: it gets a quarter of the multiplier's margin plus
+            # 64 slots (the list width, a per-atom count, gets the whole margin).
+            tile_margin = 1.0 + (self.capacity_multiplier - 1.0) / 4
+            tile = min(self.tile_limit, math.ceil(tile_margin * needed_tile) + 64)
             self._size_list(width, tile)
             self._bind()
             t["status"].zero_()
