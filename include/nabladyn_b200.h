@@ -160,6 +160,40 @@ typedef struct nd_lj_pairs_args {
 
 int nd_lj_energy_force_virial(const nd_lj_pairs_args* args, nd_stream_t stream);
 
+/* A batch of F frames of one system (config: the parameter fit of
+ * src/nabladyn/training/_fit.py:245-271). Positions [F, N, 3] wrapped into [0, L), cells [F, 3],
+ * pairs [F, 2, C] (each frame's index padded with self-pairs to the common C). */
+typedef struct nd_lj_batch_args {
+    int dtype;
+    int64_t frames;             /* F */
+    const void* positions;      /* [F, N, 3] */
+    const void* cells;          /* [F, 3] */
+    int64_t num_atoms;          /* N */
+    const int32_t* pairs;       /* [F, 2, C] */
+    int64_t capacity;           /* C */
+    const int32_t* atom_types;  /* [N]; ignored when T == 1 */
+    int32_t num_types;          /* T, 1..8 */
+    const void* sigma;          /* [T(T+1)/2] */
+    const void* epsilon;        /* [T(T+1)/2] */
+    double cutoff;
+    double* energy;             /* forward out: [F] */
+    void* forces;               /* forward out: [F, N, 3] */
+    double* virial;             /* forward out: [F, 3, 3] */
+    const double* energy_grad;  /* backward in: dLoss/dE [F] */
+    const void* forces_grad;    /* backward in: dLoss/dF [F, N, 3] */
+    const double* virial_grad;  /* backward in: dLoss/dW [F, 3, 3] */
+    double* sigma_grad;         /* backward out: dLoss/dsigma [T(T+1)/2], summed over frames */
+    double* epsilon_grad;       /* backward out: dLoss/depsilon [T(T+1)/2] */
+} nd_lj_batch_args;
+
+/* E, F, W of every frame. */
+int nd_lj_batch_forward(const nd_lj_batch_args* args, nd_stream_t stream);
+
+/* The hand-written parameter backward: dLoss/dsigma and dLoss/depsilon from the gradients of
+ * the loss with respect to every frame's E, F and W (the reference takes it by torch.func
+ * double backward). */
+int nd_lj_batch_parameter_backward(const nd_lj_batch_args* args, nd_stream_t stream);
+
 /* ------------------------------------------------------------------------------------------
  * The MD engine: velocity-Verlet (NVE) and Nose-Hoover chain (NVT) steps of a Lennard-Jones
  * system with the neighbor rebuild decided on the GPU.

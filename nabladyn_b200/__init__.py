@@ -7,8 +7,8 @@ on top: ``neighbors.NeighborList``, ``quantity.energy_force_virial``, ``potentia
 and ``md.nve`` / ``md.nvt``.
 """
 
-from . import md, neighbors, observables, potential, quantity, space, units
+from . import md, neighbors, observables, potential, quantity, space, training, units
 
 __version__ = "0.1.0"
 
-__all__ = ("md", "neighbors", "observables", "potential", "quantity", "space", "units")
+__all__ = ("md", "neighbors", "observables", "potential", "quantity", "space", "training", "units")

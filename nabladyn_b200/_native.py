@@ -87,6 +87,31 @@ class LJPairsArgs(ctypes.Structure):
     ]
 
 
+class LJBatchArgs(ctypes.Structure):
+    _fields_ = [
+        ("dtype", ctypes.c_int),
+        ("frames", ctypes.c_int64),
+        ("positions", ctypes.c_void_p),
+        ("cells", ctypes.c_void_p),
+        ("num_atoms", ctypes.c_int64),
+        ("pairs", ctypes.c_void_p),
+        ("capacity", ctypes.c_int64),
+        ("atom_types", ctypes.c_void_p),
+        ("num_types", ctypes.c_int32),
+        ("sigma", ctypes.c_void_p),
+        ("epsilon", ctypes.c_void_p),
+        ("cutoff", ctypes.c_double),
+        ("energy", ctypes.c_void_p),
+        ("forces", ctypes.c_void_p),
+        ("virial", ctypes.c_void_p),
+        ("energy_grad", ctypes.c_void_p),
+        ("forces_grad", ctypes.c_void_p),
+        ("virial_grad", ctypes.c_void_p),
+        ("sigma_grad", ctypes.c_void_p),
+        ("epsilon_grad", ctypes.c_void_p),
+    ]
+
+
 class MDSystem(ctypes.Structure):
     _fields_ = [
         ("dtype", ctypes.c_int),
@@ -160,6 +185,8 @@ _SIGNATURES = {
         ctypes.c_void_p, ctypes.c_void_p,
     ],
     "nd_lj_energy_force_virial": [ctypes.POINTER(LJPairsArgs), ctypes.c_void_p],
+    "nd_lj_batch_forward": [ctypes.POINTER(LJBatchArgs), ctypes.c_void_p],
+    "nd_lj_batch_parameter_backward": [ctypes.POINTER(LJBatchArgs), ctypes.c_void_p],
     "nd_md_import": [
         ctypes.POINTER(MDSystem), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -74,6 +74,14 @@ __global__ void __launch_bounds__(kLJThreads) lj_pairs_kernel(
     double* __restrict__ epsilon_grad
 )
 {
+    // Frame blockIdx.y of a batch of frames with the same atoms and capacity.
+    const std::int64_t frame = blockIdx.y;
+    positions += frame * 3 * num_atoms;
+    cell += frame * 3;
+    pairs += frame * 2 * capacity;
+    energy += frame;
+    forces += frame * 3 * num_atoms;
+    virial += frame * 9;
     const int rows = num_types * (num_types + 1) / 2;
     __shared__ double row_grads[2 * kMaxRows];
     if (kParameterGrads)
@@ -285,7 +293,204 @@ int lj_pairs(const nd_lj_pairs_args* a, cudaStream_t stream)
     return ND_OK;
 }
 
+// The parameter backward of a batch: given the loss's gradients with respect to each frame's
+// energy, forces and virial, accumulates dLoss/dsigma and dLoss/depsilon per type-pair row.
+// For a valid column with d = x_i - x_j and f_s = 24 eps (2 p6^2 - p6) / r^2 (so F_i = f_s d,
+// F_j = -f_s d, W = f_s d (x) d), the pair adds
+//     g_E du/dtheta + (d . (g_F[i] - g_F[j]) + d^T g_W d) df_s/dtheta,
+// with du/deps = 4 (p6^2 - p6) - 4 (pc6^2 - pc6), du/dsigma = 24 eps / sigma (2 p6^2 - p6 -
+// 2 pc6^2 + pc6), df_s/deps = f_s / eps and df_s/dsigma = 144 eps p6 (4 p6 - 1) / (sigma r^2).
+// This is the double backward the reference takes through torch.func
+// (src/nabladyn/training/_fit.py:245-271), written out. Per-row sums are float64.
+template <typename T>
+__global__ void __launch_bounds__(kLJThreads) lj_parameter_backward_kernel(
+    const T* __restrict__ positions,
+    const T* __restrict__ cell,
+    const index_t* __restrict__ pairs,
+    std::int64_t capacity,
+    index_t num_atoms,
+    const index_t* __restrict__ atom_types,
+    int num_types,
+    const T* __restrict__ sigma,
+    const T* __restrict__ epsilon,
+    T cutoff_squared,
+    const double* __restrict__ energy_grad,
+    const T* __restrict__ forces_grad,
+    const double* __restrict__ virial_grad,
+    double* __restrict__ sigma_grad,
+    double* __restrict__ epsilon_grad
+)
+{
+    const std::int64_t frame = blockIdx.y;
+    positions += frame * 3 * num_atoms;
+    cell += frame * 3;
+    pairs += frame * 2 * capacity;
+    forces_grad += frame * 3 * num_atoms;
+    const double ge = energy_grad[frame];
+    double gw[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+    {
+        gw[k] = virial_grad[frame * 9 + k];
+    }
+    const int rows = num_types * (num_types + 1) / 2;
+    __shared__ double row_grads[2 * kMaxRows];
+    for (int k = threadIdx.x; k < 2 * rows; k += blockDim.x)
+    {
+        row_grads[k] = 0.0;
+    }
+    __syncthreads();
+    const T lx = cell[0], ly = cell[1], lz = cell[2];
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t column = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         column < capacity; column += stride)
+    {
+        const index_t i = pairs[column];
+        const index_t j = pairs[capacity + column];
+        if (i == j || static_cast<unsigned>(i) >= static_cast<unsigned>(num_atoms) ||
+            static_cast<unsigned>(j) >= static_cast<unsigned>(num_atoms))
+        {
+            continue;
+        }
+        const T dx = displacement(positions[3LL * i], positions[3LL * j], lx);
+        const T dy = displacement(positions[3LL * i + 1], positions[3LL * j + 1], ly);
+        const T dz = displacement(positions[3LL * i + 2], positions[3LL * j + 2], lz);
+        const T r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < cutoff_squared))
+        {
+            continue;
+        }
+        const int row = atom_types == nullptr ? 0 : pair_row(atom_types[i], atom_types[j], num_types);
+        const double s = sigma[row];
+        const double eps = epsilon[row];
+        const double inv_r2 = 1.0 / double(r2);
+        const double q = s * s * inv_r2;
+        const double p6 = q * q * q;
+        const double qc = s * s / double(cutoff_squared);
+        const double pc6 = qc * qc * qc;
+        const double fs = 24.0 * eps * (2.0 * p6 * p6 - p6) * inv_r2;
+        const double x = dx, y = dy, z = dz;
+        const double dgx = double(forces_grad[3LL * i]) - double(forces_grad[3LL * j]);
+        const double dgy = double(forces_grad[3LL * i + 1]) - double(forces_grad[3LL * j + 1]);
+        const double dgz = double(forces_grad[3LL * i + 2]) - double(forces_grad[3LL * j + 2]);
+        const double g = x * dgx + y * dgy + z * dgz +
+                         x * (gw[0] * x + gw[1] * y + gw[2] * z) +
+                         y * (gw[3] * x + gw[4] * y + gw[5] * z) +
+                         z * (gw[6] * x + gw[7] * y + gw[8] * z);
+        const double du_deps = 4.0 * (p6 * p6 - p6) - 4.0 * (pc6 * pc6 - pc6);
+        const double du_dsigma = 24.0 * eps / s * (2.0 * p6 * p6 - p6 - 2.0 * pc6 * pc6 + pc6);
+        const double dfs_deps = fs / eps;
+        const double dfs_dsigma = 144.0 * eps * p6 * (4.0 * p6 - 1.0) * inv_r2 / s;
+        atomicAdd(row_grads + row, ge * du_dsigma + g * dfs_dsigma);
+        atomicAdd(row_grads + rows + row, ge * du_deps + g * dfs_deps);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < rows; k += blockDim.x)
+    {
+        atomicAdd(sigma_grad + k, row_grads[k]);
+        atomicAdd(epsilon_grad + k, row_grads[rows + k]);
+    }
+}
+
+unsigned pair_blocks(std::int64_t capacity, std::int64_t frames)
+{
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const std::int64_t wanted = (capacity + kLJThreads - 1) / kLJThreads;
+    std::int64_t most = static_cast<std::int64_t>(sms) * 8 / (frames > 0 ? frames : 1);
+    most = most < 1 ? 1 : most;
+    return static_cast<unsigned>(wanted < most ? (wanted > 0 ? wanted : 1) : most);
+}
+
+template <typename T>
+int lj_batch_forward(const nd_lj_batch_args* a, cudaStream_t stream)
+{
+    const std::int64_t n = a->num_atoms, frames = a->frames;
+    ND_CUDA_TRY(cudaMemsetAsync(a->forces, 0, sizeof(T) * 3 * n * frames, stream));
+    ND_CUDA_TRY(cudaMemsetAsync(a->energy, 0, sizeof(double) * frames, stream));
+    ND_CUDA_TRY(cudaMemsetAsync(a->virial, 0, sizeof(double) * 9 * frames, stream));
+    const T rc = static_cast<T>(a->cutoff);
+    const auto* types = a->num_types > 1 ? a->atom_types : nullptr;
+    const dim3 grid(pair_blocks(a->capacity, frames), static_cast<unsigned>(frames));
+    lj_pairs_kernel<T, false, false><<<grid, kLJThreads, 0, stream>>>(
+        static_cast<const T*>(a->positions), static_cast<const T*>(a->cells), a->pairs,
+        a->capacity, static_cast<index_t>(n), types, a->num_types,
+        static_cast<const T*>(a->sigma), static_cast<const T*>(a->epsilon), nullptr, rc * rc,
+        a->energy, static_cast<T*>(a->forces), a->virial, nullptr, nullptr);
+    ND_LAUNCH_CHECK();
+    return ND_OK;
+}
+
+template <typename T>
+int lj_batch_parameter_backward(const nd_lj_batch_args* a, cudaStream_t stream)
+{
+    const int rows = a->num_types * (a->num_types + 1) / 2;
+    ND_CUDA_TRY(cudaMemsetAsync(a->sigma_grad, 0, sizeof(double) * rows, stream));
+    ND_CUDA_TRY(cudaMemsetAsync(a->epsilon_grad, 0, sizeof(double) * rows, stream));
+    const T rc = static_cast<T>(a->cutoff);
+    const auto* types = a->num_types > 1 ? a->atom_types : nullptr;
+    const dim3 grid(pair_blocks(a->capacity, a->frames), static_cast<unsigned>(a->frames));
+    lj_parameter_backward_kernel<T><<<grid, kLJThreads, 0, stream>>>(
+        static_cast<const T*>(a->positions), static_cast<const T*>(a->cells), a->pairs,
+        a->capacity, static_cast<index_t>(a->num_atoms), types, a->num_types,
+        static_cast<const T*>(a->sigma), static_cast<const T*>(a->epsilon), rc * rc,
+        a->energy_grad, static_cast<const T*>(a->forces_grad), a->virial_grad, a->sigma_grad,
+        a->epsilon_grad);
+    ND_LAUNCH_CHECK();
+    return ND_OK;
+}
+
+int check_batch(const nd_lj_batch_args* a, bool backward)
+{
+    ND_REQUIRE(a != nullptr, "the arguments are null");
+    ND_REQUIRE(a->dtype == ND_FLOAT32 || a->dtype == ND_FLOAT64, "positions must be float32 or float64");
+    ND_REQUIRE(a->frames >= 1 && a->frames <= 65535, "1 to 65535 frames per batch");
+    ND_REQUIRE(a->num_atoms >= 1 && a->num_atoms <= INT32_MAX, "N must be in [1, 2**31)");
+    ND_REQUIRE(a->capacity >= 1 && a->capacity <= INT32_MAX, "pairs must be [F, 2, C]");
+    ND_REQUIRE(a->num_types >= 1 && a->num_types <= 8, "1 to 8 atom types are supported");
+    ND_REQUIRE(a->num_types == 1 || a->atom_types != nullptr, "atom_types is null");
+    ND_REQUIRE(a->cutoff > 0, "the cutoff must be positive");
+    ND_REQUIRE(a->positions && a->cells && a->pairs && a->sigma && a->epsilon,
+               "a required pointer is null");
+    if (backward)
+    {
+        ND_REQUIRE(a->energy_grad && a->forces_grad && a->virial_grad && a->sigma_grad &&
+                       a->epsilon_grad,
+                   "a gradient pointer is null");
+    }
+    else
+    {
+        ND_REQUIRE(a->energy && a->forces && a->virial, "an output pointer is null");
+    }
+    return ND_OK;
+}
+
 }  // namespace nd
+
+extern "C" int nd_lj_batch_forward(const nd_lj_batch_args* args, nd_stream_t stream)
+{
+    const int rc = nd::check_batch(args, false);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    auto s = static_cast<cudaStream_t>(stream);
+    return args->dtype == ND_FLOAT32 ? nd::lj_batch_forward<float>(args, s)
+                                     : nd::lj_batch_forward<double>(args, s);
+}
+
+extern "C" int nd_lj_batch_parameter_backward(const nd_lj_batch_args* args, nd_stream_t stream)
+{
+    const int rc = nd::check_batch(args, true);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    auto s = static_cast<cudaStream_t>(stream);
+    return args->dtype == ND_FLOAT32 ? nd::lj_batch_parameter_backward<float>(args, s)
+                                     : nd::lj_batch_parameter_backward<double>(args, s);
+}
 
 extern "C" int nd_lj_energy_force_virial(const nd_lj_pairs_args* args, nd_stream_t stream)
 {

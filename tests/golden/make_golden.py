@@ -17,6 +17,8 @@ Fixtures:
   all-pairs index standing in for the neighbor list.
 * lj_frames_4.npz — four frames of examples/data/lj_frames.npz (216 atoms, two types) with the
   file's labels and the reference's float64 E/F/W for the generating rows.
+* lj_fit_gradient.npz — the reference's loss and its gradient in sigma and epsilon on those
+  frames, from perturbed parameters (its training predict/loss under torch.func).
 """
 
 import os
@@ -177,9 +179,50 @@ def lj_frames() -> None:
     np.savez_compressed(OUT / "lj_frames_4.npz", **out)
 
 
+def lj_fit_gradient() -> None:
+    """The reference's own loss and dLoss/d(sigma, epsilon) on the four lj_frames frames, by
+    its predict/loss under torch.func (src/nabladyn/training/_loss.py, _fit.py:245-271),
+    from parameters perturbed off the generating rows; the all-pairs index as every stack."""
+    from nabladyn.training import _loss
+
+    data = np.load(OUT / "lj_frames_4.npz")
+    n = data["atom_types"].shape[0]
+    sigma0, epsilon0 = data["sigma"], data["epsilon"]
+    sigma = sigma0 * np.array([1.05, 0.97, 1.02])
+    epsilon = epsilon0 * np.array([0.9, 1.1, 0.95])
+    model = potential.lennard_jones(
+        atom_types=torch.tensor(data["atom_types"]),
+        sigma=torch.tensor(sigma), epsilon=torch.tensor(epsilon),
+        cutoff=float(data["cutoff"]), trainable=("sigma", "epsilon"),
+    )
+    frames = data["positions"].shape[0]
+    positions = torch.tensor(data["positions"])
+    cells = torch.tensor(data["cells"])
+    stack = all_pairs(n)[None].expand(frames, 2, -1).contiguous()
+    labels = {"energy": torch.tensor(data["energy"]), "forces": torch.tensor(data["forces"]),
+              "virial": torch.tensor(data["virial"])}
+    channels = ("energy", "forces", "virial")
+    scales = _loss.scales(**labels)
+    weights = {"energy": 1.0, "forces": 1.0, "virial": 1.0}
+
+    def loss(trained):
+        predicted = _loss.predict(model, trained, positions, cells, (stack,), channels)
+        return _loss.loss(predicted, labels, weights, scales)
+
+    params = {"sigma": model.sigma.detach().clone(), "epsilon": model.epsilon.detach().clone()}
+    gradient, (value, terms) = torch.func.grad_and_value(loss, has_aux=True)(params)
+    np.savez_compressed(
+        OUT / "lj_fit_gradient.npz",
+        sigma=sigma, epsilon=epsilon, loss=value.detach().numpy(),
+        sigma_grad=gradient["sigma"].numpy(), epsilon_grad=gradient["epsilon"].numpy(),
+        scales=np.array([scales["energy"], scales["forces"], scales["virial"]]),
+    )
+
+
 if __name__ == "__main__":
     torch.set_num_threads(os.cpu_count() or 1)
     argon()
     md()
     lj_frames()
+    lj_fit_gradient()
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
