@@ -287,6 +287,57 @@ int nd_md_kinetic(const nd_md_system* system, int thermostat, nd_stream_t stream
 /* The float64 slots the partials buffer needs. */
 int nd_md_partial_slots(const nd_md_system* system, int64_t* slots);
 
+/* ------------------------------------------------------------------------------------------
+ * The replica server: many independent float32, one-type Lennard-Jones NVT replicas resident
+ * in one pool, each advanced by one CTA for a budget of steps per launch (the serving workload
+ * of the reference's md.nvt, src/nabladyn/md/_ensembles/_nvt.py:132-179, run for many small
+ * systems at once). A replica's atoms occupy [atom_offset, atom_offset + N) of every per-atom
+ * pool array; its list occupies ceil(N / 32) * 32 * width uint16 from list_offset; its cell
+ * table cells + 1 ints from cell_offset.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct nd_replica {
+    int64_t atom_offset;
+    int64_t list_offset;      /* a multiple of 8 */
+    int64_t cell_offset;
+    int32_t num_atoms;        /* 2 .. 65535 */
+    int32_t width;            /* list slots per atom, a multiple of 8 */
+    int32_t dims[3];          /* cells per axis, each >= 1, product <= 4096 */
+    int32_t steps_left;       /* decremented by every step run */
+    int32_t status;           /* ND_STATUS_* bits */
+    int32_t rebuild_count;
+    float cell[3];
+    float widths[3];
+    float cutoff;
+    float radius;             /* cutoff + skin */
+    float threshold_squared;  /* the reuse threshold, as the engine's */
+    float timestep;
+    float sigma;
+    float epsilon;
+    double energy;            /* E after the last step run (or at admission) */
+    double thermostat[24];    /* the engine's float64 chain block */
+} nd_replica;
+
+typedef struct nd_replica_pool {
+    nd_replica* replicas;      /* [slots] */
+    void* positions;           /* [atoms, 4] float32 */
+    void* velocities;          /* [atoms, 3] float32 */
+    void* forces;              /* [atoms, 3] float32 */
+    void* masses;              /* [atoms] float32 */
+    void* inverse_masses;      /* [atoms] float32 */
+    int64_t* images;           /* [atoms, 3] */
+    void* reference_positions; /* [atoms, 4] float32 */
+    uint16_t* neighbors;       /* the lists */
+    int32_t* neighbor_counts;  /* [atoms] */
+    int32_t* sorted;           /* [atoms] */
+    int32_t* scratch;          /* [atoms] */
+    int32_t* cell_starts;      /* the cell tables */
+} nd_replica_pool;
+
+/* mode 0: admit the listed slots (wrap, build, first forces). mode 1: run each listed slot for
+ * min(budgets[k], steps_left) steps. One CTA per listed slot; slots never interact. */
+int nd_serve_run(const nd_replica_pool* pool, const int32_t* slots, const int32_t* budgets,
+                 int32_t count, int32_t mode, nd_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -162,6 +162,48 @@ class MDSystem(ctypes.Structure):
     ]
 
 
+class Replica(ctypes.Structure):
+    _fields_ = [
+        ("atom_offset", ctypes.c_int64),
+        ("list_offset", ctypes.c_int64),
+        ("cell_offset", ctypes.c_int64),
+        ("num_atoms", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("dims", ctypes.c_int32 * 3),
+        ("steps_left", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("rebuild_count", ctypes.c_int32),
+        ("cell", ctypes.c_float * 3),
+        ("widths", ctypes.c_float * 3),
+        ("cutoff", ctypes.c_float),
+        ("radius", ctypes.c_float),
+        ("threshold_squared", ctypes.c_float),
+        ("timestep", ctypes.c_float),
+        ("sigma", ctypes.c_float),
+        ("epsilon", ctypes.c_float),
+        ("energy", ctypes.c_double),
+        ("thermostat", ctypes.c_double * 24),
+    ]
+
+
+class ReplicaPool(ctypes.Structure):
+    _fields_ = [
+        ("replicas", ctypes.c_void_p),
+        ("positions", ctypes.c_void_p),
+        ("velocities", ctypes.c_void_p),
+        ("forces", ctypes.c_void_p),
+        ("masses", ctypes.c_void_p),
+        ("inverse_masses", ctypes.c_void_p),
+        ("images", ctypes.c_void_p),
+        ("reference_positions", ctypes.c_void_p),
+        ("neighbors", ctypes.c_void_p),
+        ("neighbor_counts", ctypes.c_void_p),
+        ("sorted", ctypes.c_void_p),
+        ("scratch", ctypes.c_void_p),
+        ("cell_starts", ctypes.c_void_p),
+    ]
+
+
 # name -> (argument types); every entry point returns int.
 _SIGNATURES = {
     "nd_abi_version": [],
@@ -204,6 +246,10 @@ _SIGNATURES = {
     ],
     "nd_md_kinetic": [ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_void_p],
     "nd_md_partial_slots": [ctypes.POINTER(MDSystem), c_int64_p],
+    "nd_serve_run": [
+        ctypes.POINTER(ReplicaPool), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+        ctypes.c_int32, ctypes.c_void_p,
+    ],
 }
 
 # Every symbol include/nabladyn_b200.h declares.

@@ -1,0 +1,553 @@
+// The replica server: many independent Lennard-Jones NVT replicas (tens to thousands of atoms
+// each) resident in one pool, advanced by a persistent kernel in which each CTA owns one
+// replica and runs a whole budget of steps: the chain half steps, the drift, the on-GPU reuse
+// check, the rebuild, the forces and the second half kick, separated by block barriers only.
+// No per-step launch, no grid-wide synchronisation: replicas never wait on each other, so a
+// replica's arithmetic (and its result, bit for bit) does not depend on its batch-mates.
+//
+// It serves the same step as the MD engine (src/nabladyn/md/_ensembles/_nvt.py:88-129,
+// _nve.py:39-58, _chain.py:36-83, the reuse rule of src/nabladyn/neighbors/csrc/update/
+// update.cuh:21-116) for systems too small to fill a GPU one at a time. Positions stay unwrapped
+// between rebuilds and every pair takes its minimum image. The neighbor list is the engine's
+// chunked full list of uint16 replica-local indices; a rebuild sorts the replica into cells
+// (deterministically, by atom index within a cell) in the CTA, or tests all pairs when an axis
+// has fewer than three cells.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+#include "geometry.cuh"
+#include "md_common.cuh"
+
+namespace nd {
+
+constexpr int kServeThreads = 512;
+constexpr int kServeWarps = kServeThreads / kWarp;
+constexpr int kServeMaxCells = 4096;
+
+struct ServePool
+{
+    nd_replica* replicas;
+    Pos4<float>* pos;
+    float* vel;
+    float* force;
+    float* mass;
+    float* inv_mass;
+    long long* images;
+    Pos4<float>* ref_pos;
+    std::uint16_t* nbr;
+    index_t* nbr_count;
+    index_t* sorted;
+    index_t* scratch;
+    index_t* cell_start;
+};
+
+// The scalar fields of one replica, in shared memory for the CTA.
+struct ReplicaScalars
+{
+    int n;
+    int width;
+    int dims[3];
+    int cells;
+    float cell[3];
+    float widths[3];
+    float cutoff_squared;
+    float radius_squared;
+    float threshold_squared;
+    float dt;
+    float half_dt;
+    PairParams<float> lj;
+    int status;
+    int rebuild_count;
+    int steps_left;
+};
+
+// Block sum of one double per thread, in a fixed order; every thread gets the total.
+__device__ double block_sum(double value, double* warp_sums)
+{
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    value = warp_sum(value);
+    if (lane == 0)
+    {
+        warp_sums[warp] = value;
+    }
+    __syncthreads();
+    double total = 0;
+    for (int w = 0; w < kServeWarps; ++w)
+    {
+        total += warp_sums[w];
+    }
+    __syncthreads();
+    return total;
+}
+
+// Exclusive scan of counts[0, cells) in place (counts[cells] gets the total), kServeMaxCells at
+// most: each thread owns 8 consecutive counts, the 512 thread sums are scanned by warps.
+__device__ void block_scan_cells(int* counts, int cells, int* warp_totals)
+{
+    constexpr int kPer = kServeMaxCells / kServeThreads;
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    const int base = threadIdx.x * kPer;
+    int local[kPer];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+    {
+        local[k] = base + k < cells ? counts[base + k] : 0;
+        sum += local[k];
+    }
+    int inclusive = sum;
+#pragma unroll
+    for (int offset = 1; offset < kWarp; offset *= 2)
+    {
+        const int up = __shfl_up_sync(kFullMask, inclusive, offset);
+        inclusive += lane >= offset ? up : 0;
+    }
+    if (lane == kWarp - 1)
+    {
+        warp_totals[warp] = inclusive;
+    }
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < warp; ++w)
+    {
+        before += warp_totals[w];
+    }
+    int running = before + inclusive - sum;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+    {
+        if (base + k < cells)
+        {
+            counts[base + k] = running;
+        }
+        running += local[k];
+    }
+    if (threadIdx.x == kServeThreads - 1)
+    {
+        counts[cells] = running;
+    }
+    __syncthreads();
+}
+
+// Wraps the positions (counting crossings into the images), stores the reference frame and
+// rebuilds the list. Called by the whole CTA.
+__device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<float>* ref,
+                                long long* images, std::uint16_t* nbr, index_t* nbr_count,
+                                index_t* sorted, index_t* scratch, index_t* cell_start,
+                                int* counts, int* warp_totals, int* status_flags)
+{
+    const int n = r.n;
+    for (int i = threadIdx.x; i < n; i += kServeThreads)
+    {
+        Pos4<float> p = pos[i];
+        long long c[3];
+        p.x = wrap_axis(p.x, r.cell[0], c[0]);
+        p.y = wrap_axis(p.y, r.cell[1], c[1]);
+        p.z = wrap_axis(p.z, r.cell[2], c[2]);
+        if (c[0] | c[1] | c[2])
+        {
+            images[3LL * i] += c[0];
+            images[3LL * i + 1] += c[1];
+            images[3LL * i + 2] += c[2];
+        }
+        pos[i] = p;
+        ref[i] = p;
+    }
+    const bool grid = r.dims[0] >= 3 && r.dims[1] >= 3 && r.dims[2] >= 3;
+    if (grid)
+    {
+        // Counting sort by cell (the slot parked in nbr_count, rewritten by the list below),
+        // then each cell's range ordered by atom index, so the order is deterministic.
+        for (int c = threadIdx.x; c <= r.cells; c += kServeThreads)
+        {
+            counts[c] = 0;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kServeThreads)
+        {
+            const Pos4<float> p = pos[i];
+            const int c = axis_bin(p.x, r.widths[0], r.dims[0]) +
+                          r.dims[0] * (axis_bin(p.y, r.widths[1], r.dims[1]) +
+                                       r.dims[1] * axis_bin(p.z, r.widths[2], r.dims[2]));
+            scratch[i] = c;
+            nbr_count[i] = atomicAdd(counts + c, 1);
+        }
+        __syncthreads();
+        block_scan_cells(counts, r.cells, warp_totals);
+        for (int c = threadIdx.x; c <= r.cells; c += kServeThreads)
+        {
+            cell_start[c] = counts[c];
+        }
+        for (int i = threadIdx.x; i < n; i += kServeThreads)
+        {
+            sorted[counts[scratch[i]] + nbr_count[i]] = i;
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < r.cells; c += kServeThreads)
+        {
+            const int begin = counts[c], end = counts[c + 1];
+            for (int k = begin + 1; k < end; ++k)
+            {
+                const int atom = sorted[k];
+                int m = k - 1;
+                while (m >= begin && sorted[m] > atom)
+                {
+                    sorted[m + 1] = sorted[m];
+                    --m;
+                }
+                sorted[m + 1] = atom;
+            }
+        }
+        __syncthreads();
+    }
+    else
+    {
+        __syncthreads();
+    }
+    // The list: every neighbor j != i closer than the list radius, minimum image.
+    for (int i = threadIdx.x; i < n; i += kServeThreads)
+    {
+        const Pos4<float> me = pos[i];
+        ListWriter list(nbr, r.width, i, 0xffffu);
+        if (grid)
+        {
+            const int hx = axis_bin(me.x, r.widths[0], r.dims[0]);
+            const int hy = axis_bin(me.y, r.widths[1], r.dims[1]);
+            const int hz = axis_bin(me.z, r.widths[2], r.dims[2]);
+            for (int dz = -1; dz <= 1; ++dz)
+            {
+                const int cz = (hz + dz + r.dims[2]) % r.dims[2];
+                for (int dy = -1; dy <= 1; ++dy)
+                {
+                    const int cy = (hy + dy + r.dims[1]) % r.dims[1];
+                    for (int dx = -1; dx <= 1; ++dx)
+                    {
+                        const int cx = (hx + dx + r.dims[0]) % r.dims[0];
+                        const int c = cx + r.dims[0] * (cy + r.dims[1] * cz);
+                        for (int k = cell_start[c]; k < cell_start[c + 1]; ++k)
+                        {
+                            const int j = sorted[k];
+                            const Pos4<float> p = pos[j];
+                            const float d2 = squared_norm(min_image(me.x, p.x, r.cell[0]),
+                                                          min_image(me.y, p.y, r.cell[1]),
+                                                          min_image(me.z, p.z, r.cell[2]));
+                            if (j != i && d2 < r.radius_squared)
+                            {
+                                list.add(j);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        else
+        {
+            for (int j = 0; j < n; ++j)
+            {
+                const Pos4<float> p = pos[j];
+                const float d2 = squared_norm(min_image(me.x, p.x, r.cell[0]),
+                                              min_image(me.y, p.y, r.cell[1]),
+                                              min_image(me.z, p.z, r.cell[2]));
+                if (j != i && d2 < r.radius_squared)
+                {
+                    list.add(j);
+                }
+            }
+        }
+        list.finish();
+        nbr_count[i] = list.count;
+        if (list.count > r.width)
+        {
+            atomicOr(status_flags, kOverflow);
+        }
+    }
+    __syncthreads();
+}
+
+// Forces at the current positions; with `kick`, also the second half kick, returning the
+// thread's part of K (float64); always the thread's part of E.
+template <bool kKick>
+__device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, float* vel,
+                               float* force, const float* mass, const float* inv_mass,
+                               const std::uint16_t* nbr, const index_t* nbr_count,
+                               double& kinetic, double& energy)
+{
+    for (int i = threadIdx.x; i < r.n; i += kServeThreads)
+    {
+        const Pos4<float> me = pos[i];
+        const int count = nbr_count[i] < r.width ? nbr_count[i] : r.width;
+        const uint4* chunks = reinterpret_cast<const uint4*>(nbr) + chunk_index(i, 0, r.width);
+        float fx = 0, fy = 0, fz = 0, esum = 0, inside_count = 0;
+        for (int chunk = 0; chunk * kChunk < count; ++chunk)
+        {
+            const uint4 word = chunks[static_cast<std::int64_t>(chunk) * kWarp];
+            const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+            for (int k = 0; k < kChunk; ++k)
+            {
+                if (chunk * kChunk + k >= count)
+                {
+                    break;
+                }
+                const Pos4<float> p = pos[(packed[k / 2] >> (16 * (k % 2))) & 0xffffu];
+                const float dx = min_image(me.x, p.x, r.cell[0]);
+                const float dy = min_image(me.y, p.y, r.cell[1]);
+                const float dz = min_image(me.z, p.z, r.cell[2]);
+                const float r2 = squared_norm(dx, dy, dz);
+                const float mask = r2 < r.cutoff_squared ? 1.0f : 0.0f;
+                const float inv_r2 = fast_reciprocal(r2);
+                const float q = r.lj.s2 * inv_r2;
+                const float p6 = q * q * q;
+                const float fs = mask * (inv_r2 * (p6 * fmaf(2.0f, p6, -1.0f)));
+                esum = fmaf(mask, fmaf(p6, p6, -p6), esum);
+                inside_count += mask;
+                fx = fmaf(fs, dx, fx);
+                fy = fmaf(fs, dy, fy);
+                fz = fmaf(fs, dz, fz);
+            }
+        }
+        fx *= r.lj.e24;
+        fy *= r.lj.e24;
+        fz *= r.lj.e24;
+        energy += 0.5 * (double(r.lj.e4) * esum - double(r.lj.shift) * inside_count);
+        float* f = force + 3LL * i;
+        f[0] = fx;
+        f[1] = fy;
+        f[2] = fz;
+        if (kKick)
+        {
+            const float kick = r.half_dt * inv_mass[i];
+            float* v = vel + 3LL * i;
+            const float vx = fmaf(kick, fx, v[0]);
+            const float vy = fmaf(kick, fy, v[1]);
+            const float vz = fmaf(kick, fz, v[2]);
+            v[0] = vx;
+            v[1] = vy;
+            v[2] = vz;
+            kinetic += 0.5 * double(mass[i]) * (double(vx) * vx + double(vy) * vy + double(vz) * vz);
+        }
+    }
+}
+
+// mode 0: wrap, rebuild and the first forces of newly admitted replicas. mode 1: run each
+// listed replica for min(budget, steps left) NVT steps.
+__global__ void __launch_bounds__(kServeThreads) serve_kernel(ServePool p, const int* slots,
+                                                              const int* budgets, int mode)
+{
+    __shared__ ReplicaScalars r;
+    __shared__ double thermo[kThermoSize];
+    __shared__ int counts[kServeMaxCells + 1];
+    __shared__ double warp_sums[kServeWarps];
+    __shared__ float scales[2];
+    __shared__ int flags;
+    __shared__ int warp_totals[kServeWarps];
+    nd_replica* replica = p.replicas + slots[blockIdx.x];
+    if (threadIdx.x == 0)
+    {
+        r.n = replica->num_atoms;
+        r.width = replica->width;
+        r.cells = 1;
+        for (int a = 0; a < 3; ++a)
+        {
+            r.dims[a] = replica->dims[a];
+            r.cells *= replica->dims[a];
+            r.cell[a] = replica->cell[a];
+            r.widths[a] = replica->widths[a];
+        }
+        r.cutoff_squared = replica->cutoff * replica->cutoff;
+        r.radius_squared = replica->radius * replica->radius;
+        r.threshold_squared = replica->threshold_squared;
+        r.dt = replica->timestep;
+        r.half_dt = 0.5f * replica->timestep;
+        r.lj = pair_params(replica->sigma, replica->epsilon, r.cutoff_squared);
+        r.status = replica->status;
+        r.rebuild_count = replica->rebuild_count;
+        r.steps_left = replica->steps_left;
+        flags = 0;
+    }
+    for (int k = threadIdx.x; k < kThermoSize; k += kServeThreads)
+    {
+        thermo[k] = replica->thermostat[k];
+    }
+    __syncthreads();
+    const std::int64_t a0 = replica->atom_offset;
+    Pos4<float>* pos = p.pos + a0;
+    Pos4<float>* ref = p.ref_pos + a0;
+    float* vel = p.vel + 3 * a0;
+    float* force = p.force + 3 * a0;
+    const float* mass = p.mass + a0;
+    const float* inv_mass = p.inv_mass + a0;
+    long long* images = p.images + 3 * a0;
+    std::uint16_t* nbr = p.nbr + replica->list_offset;
+    index_t* nbr_count = p.nbr_count + a0;
+    index_t* sorted = p.sorted + a0;
+    index_t* scratch = p.scratch + a0;
+    index_t* cell_start = p.cell_start + replica->cell_offset;
+
+    if (mode == 0)
+    {
+        rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start, counts,
+                        warp_totals, &flags);
+        double kinetic = 0, energy = 0;
+        replica_forces<false>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, kinetic, energy);
+        energy = block_sum(energy, warp_sums);
+        if (threadIdx.x == 0)
+        {
+            replica->status = r.status | flags;
+            replica->rebuild_count = r.rebuild_count + 1;
+            replica->energy = energy;
+        }
+        return;
+    }
+    const int budget = budgets[blockIdx.x] < r.steps_left ? budgets[blockIdx.x] : r.steps_left;
+    int done = 0;
+    double last_energy = replica->energy;  // thread 0's copy
+    for (; done < budget; ++done)
+    {
+        if (r.status != 0)
+        {
+            break;
+        }
+        if (threadIdx.x == 0)
+        {
+            // The opening chain half step; the previous closing factor is still pending.
+            double kinetic = thermo[kKineticA];
+            double q[3], pc[3];
+            for (int k = 0; k < 3; ++k)
+            {
+                q[k] = thermo[kChainA + k];
+                pc[k] = thermo[kChainA + 3 + k];
+            }
+            const double factor = chain_half_step(kinetic, q, pc, thermo + kChainMass,
+                                                  thermo[kDegrees], thermo[kThermalEnergy],
+                                                  thermo[kTimestep]);
+            scales[0] = static_cast<float>(thermo[kPendingScale]);
+            scales[1] = static_cast<float>(factor);
+            for (int k = 0; k < 3; ++k)
+            {
+                thermo[kChainB + k] = q[k];
+                thermo[kChainB + 3 + k] = pc[k];
+            }
+        }
+        __syncthreads();
+        int moved = 0, bad = 0;
+        for (int i = threadIdx.x; i < r.n; i += kServeThreads)
+        {
+            float* v = vel + 3LL * i;
+            const float* f = force + 3LL * i;
+            const float kick = r.half_dt * inv_mass[i];
+            const float vx = fmaf(kick, f[0], (v[0] * scales[0]) * scales[1]);
+            const float vy = fmaf(kick, f[1], (v[1] * scales[0]) * scales[1]);
+            const float vz = fmaf(kick, f[2], (v[2] * scales[0]) * scales[1]);
+            v[0] = vx;
+            v[1] = vy;
+            v[2] = vz;
+            Pos4<float> x = pos[i];
+            x.x = fmaf(r.dt, vx, x.x);
+            x.y = fmaf(r.dt, vy, x.y);
+            x.z = fmaf(r.dt, vz, x.z);
+            pos[i] = x;
+            bad |= !(isfinite(x.x) && isfinite(x.y) && isfinite(x.z));
+            const Pos4<float> x0 = ref[i];
+            moved |= squared_norm(x.x - x0.x, x.y - x0.y, x.z - x0.z) >= r.threshold_squared;
+        }
+        if (__syncthreads_or(bad))
+        {
+            if (threadIdx.x == 0)
+            {
+                r.status |= kNonFinite;
+            }
+            __syncthreads();
+            break;
+        }
+        if (__syncthreads_or(moved))
+        {
+            rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start,
+                            counts, warp_totals, &flags);
+            if (threadIdx.x == 0)
+            {
+                ++r.rebuild_count;
+                r.status |= flags;
+            }
+        }
+        double kinetic = 0, energy = 0;
+        replica_forces<true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, kinetic, energy);
+        kinetic = block_sum(kinetic, warp_sums);
+        energy = block_sum(energy, warp_sums);
+        if (threadIdx.x == 0)
+        {
+            last_energy = energy;
+            // The closing chain half step against this step's K.
+            double q[3], pc[3];
+            for (int k = 0; k < 3; ++k)
+            {
+                q[k] = thermo[kChainB + k];
+                pc[k] = thermo[kChainB + 3 + k];
+            }
+            const double factor = chain_half_step(kinetic, q, pc, thermo + kChainMass,
+                                                  thermo[kDegrees], thermo[kThermalEnergy],
+                                                  thermo[kTimestep]);
+            for (int k = 0; k < 3; ++k)
+            {
+                thermo[kChainA + k] = q[k];
+                thermo[kChainA + 3 + k] = pc[k];
+            }
+            thermo[kKineticA] = kinetic;
+            thermo[kPendingScale] = factor;
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < kThermoSize; k += kServeThreads)
+    {
+        replica->thermostat[k] = thermo[k];
+    }
+    if (threadIdx.x == 0)
+    {
+        replica->steps_left = r.steps_left - done;
+        replica->status = r.status;
+        replica->rebuild_count = r.rebuild_count;
+        replica->energy = last_energy;
+    }
+}
+
+}  // namespace nd
+
+extern "C" int nd_serve_run(const nd_replica_pool* pool, const int32_t* slots,
+                            const int32_t* budgets, int32_t count, int32_t mode,
+                            nd_stream_t stream)
+{
+    ND_REQUIRE(pool != nullptr && slots != nullptr, "the pool or the slot list is null");
+    ND_REQUIRE(mode == 0 || (mode == 1 && budgets != nullptr), "mode is 0 (admit) or 1 (run)");
+    ND_REQUIRE(count >= 0 && count <= 1 << 20, "count out of range");
+    ND_REQUIRE(pool->replicas && pool->positions && pool->velocities && pool->forces &&
+                   pool->masses && pool->inverse_masses && pool->images &&
+                   pool->reference_positions && pool->neighbors && pool->neighbor_counts &&
+                   pool->sorted && pool->scratch && pool->cell_starts,
+               "a pool buffer is null");
+    if (count == 0)
+    {
+        return ND_OK;
+    }
+    nd::ServePool p;
+    p.replicas = pool->replicas;
+    p.pos = static_cast<nd::Pos4<float>*>(pool->positions);
+    p.vel = static_cast<float*>(pool->velocities);
+    p.force = static_cast<float*>(pool->forces);
+    p.mass = static_cast<float*>(pool->masses);
+    p.inv_mass = static_cast<float*>(pool->inverse_masses);
+    p.images = reinterpret_cast<long long*>(pool->images);
+    p.ref_pos = static_cast<nd::Pos4<float>*>(pool->reference_positions);
+    p.nbr = pool->neighbors;
+    p.nbr_count = pool->neighbor_counts;
+    p.sorted = pool->sorted;
+    p.scratch = pool->scratch;
+    p.cell_start = pool->cell_starts;
+    nd::serve_kernel<<<count, nd::kServeThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        p, slots, budgets, mode);
+    ND_LAUNCH_CHECK();
+    return ND_OK;
+}

@@ -1,0 +1,348 @@
+"""The replica server: a device pool of resident replicas and the continuous-batching loop.
+
+Each request is an independent one-type Lennard-Jones NVT simulation (the reference's
+``md.nvt``, src/nabladyn/md/_ensembles/_nvt.py:132-179, in float32). The server
+
+* admits a request when a slot and room in the HBM budget are free (first fit over the pool's
+  atom ranges), uploads its frame and has the replica kernel build its list and first forces;
+* every round launches the replica kernel once over all active slots, each slot with a budget
+  of steps inversely proportional to its size, so a round costs about the same on every SM and
+  small replicas are not held back by large ones;
+* harvests replicas whose steps are done, hands back their frame and frees their room, so
+  requests that arrived meanwhile are admitted in the next round.
+
+Replicas never interact on the device: each is advanced by its own CTA, so a replica's result
+does not depend on which others share its rounds.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .._native import Replica, ReplicaPool, call, stream_handle
+from ..neighbors._neighbor_list import check_cell_lengths, grid
+from ..units import BOLTZMANN
+
+_ALIGN = 32          # atoms per allocation unit (one warp of list chunks)
+_MAX_CELLS = 4096    # kServeMaxCells in serve.cu
+_WIDTH = 192         # list slots per atom: room for ~1.5x the mean count at 22 atoms/nm^3
+_BYTES_PER_ATOM = 16 + 12 + 12 + 4 + 4 + 24 + 16 + 2 * _WIDTH + 4 + 4 + 4
+_CHAIN_A, _KINETIC_A, _PENDING, _CHAIN_MASS, _KT, _DEGREES, _TIMESTEP = 0, 6, 14, 16, 19, 20, 21
+
+
+@dataclass
+class ReplicaRequest:
+    """One MD job: a frame, its thermostat settings and the number of NVT steps.
+
+    positions and velocities [N, 3] in nm and nm/ps, masses [N] in Da, cell [3] in nm (host
+    arrays); ``arrival`` in seconds after serving starts.
+    """
+
+    positions: np.ndarray
+    velocities: np.ndarray
+    masses: np.ndarray
+    cell: np.ndarray
+    temperature: float
+    steps: int
+    timestep: float = 0.004
+    thermostat_timescale: float = 0.1
+    sigma: float = 0.34
+    epsilon: float = 0.996
+    cutoff: float = 1.0
+    skin: float = 0.1
+    arrival: float = 0.0
+    name: object = None
+
+
+@dataclass
+class ReplicaResult:
+    """A finished replica: its final frame (positions wrapped into the cell), its potential
+    energy, and its times in seconds after serving started."""
+
+    name: object
+    positions: np.ndarray
+    velocities: np.ndarray
+    images: np.ndarray
+    energy: float
+    status: int
+    rebuilds: int
+    arrival: float
+    admitted: float
+    finished: float
+    num_atoms: int
+    steps: int
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+@dataclass
+class _Active:
+    request: ReplicaRequest
+    slot: int
+    offset: int
+    units: int
+    admitted: float
+    steps_left: int = field(default=0)
+
+
+class ReplicaServer:
+    """Resident replicas in one device pool, advanced in rounds by the replica kernel.
+
+    ``budget_bytes`` bounds the pool (about 0.5 kB per atom); ``max_slots`` bounds the replicas
+    resident at once; ``round_atom_steps`` is the work a slot gets per round, in atom-steps.
+    """
+
+    def __init__(self, *, device: torch.device | str = "cuda", budget_bytes: int = 4 << 30,
+                 max_slots: int = 2048, round_atom_steps: int = 200_000):
+        self.device = torch.device(device)
+        self.max_slots = int(max_slots)
+        self.round_atom_steps = int(round_atom_steps)
+        self.capacity = max(_ALIGN, (int(budget_bytes) // _BYTES_PER_ATOM) // _ALIGN * _ALIGN)
+        n, dev = self.capacity, self.device
+        f32 = {"dtype": torch.float32, "device": dev}
+        i32 = {"dtype": torch.int32, "device": dev}
+        self.buffers = {
+            "positions": torch.zeros((n, 4), **f32),
+            "velocities": torch.zeros((n, 3), **f32),
+            "forces": torch.zeros((n, 3), **f32),
+            "masses": torch.ones(n, **f32),
+            "inverse_masses": torch.ones(n, **f32),
+            "images": torch.zeros((n, 3), dtype=torch.int64, device=dev),
+            "reference_positions": torch.zeros((n, 4), **f32),
+            "neighbors": torch.zeros(n * _WIDTH, dtype=torch.uint16, device=dev),
+            "neighbor_counts": torch.zeros(n, **i32),
+            "sorted": torch.zeros(n, **i32),
+            "scratch": torch.zeros(n, **i32),
+            "cell_starts": torch.zeros(self.max_slots * (_MAX_CELLS + 1), **i32),
+        }
+        self.table = torch.zeros(self.max_slots * ctypes.sizeof(Replica), dtype=torch.uint8,
+                                 device=dev)
+        pool = ReplicaPool(replicas=self.table.data_ptr())
+        for name, tensor in self.buffers.items():
+            setattr(pool, name, tensor.data_ptr())
+        self.pool = pool
+        self._free_units = [(0, n // _ALIGN)]  # (first unit, units), sorted, merged
+        self._free_slots = list(range(self.max_slots - 1, -1, -1))
+
+    # -- room ----------------------------------------------------------------------------
+
+    def _take(self, units: int) -> int | None:
+        for k, (first, length) in enumerate(self._free_units):
+            if length >= units:
+                if length == units:
+                    self._free_units.pop(k)
+                else:
+                    self._free_units[k] = (first + units, length - units)
+                return first
+        return None
+
+    def _give(self, first: int, units: int) -> None:
+        spans = sorted(self._free_units + [(first, units)])
+        merged = []
+        for start, length in spans:
+            if merged and merged[-1][0] + merged[-1][1] == start:
+                merged[-1] = (merged[-1][0], merged[-1][1] + length)
+            else:
+                merged.append((start, length))
+        self._free_units = merged
+
+    def fits(self, num_atoms: int) -> bool:
+        units = -(-num_atoms // _ALIGN)
+        return bool(self._free_slots) and any(length >= units for _, length in self._free_units)
+
+    # -- admission -----------------------------------------------------------------------
+
+    def _describe(self, request: ReplicaRequest, slot: int,
+                  offset: int) -> tuple[Replica, np.ndarray]:
+        """The slot record of a request and its float32 velocities, center of mass removed."""
+        n = int(request.positions.shape[0])
+        if not 2 <= n <= 65535:
+            raise ValueError("a replica holds 2 to 65535 atoms")
+        lengths = [float(x) for x in request.cell]
+        check_cell_lengths(lengths, request.cutoff)
+        radius = float(request.cutoff) + float(request.skin)
+        dims = grid(lengths, radius, torch.float32)
+        if min(dims) < 3:
+            dims = [1, 1, 1]  # every pair is tested
+        while math.prod(dims) > _MAX_CELLS:
+            axis = int(np.argmax(dims))
+            dims[axis] -= 1
+        eps = float(np.finfo(np.float32).eps)
+        allowance = radius - float(request.cutoff) - 32 * eps * max(lengths)
+        record = Replica()
+        record.atom_offset = offset
+        record.list_offset = offset * _WIDTH
+        record.cell_offset = slot * (_MAX_CELLS + 1)
+        record.num_atoms = n
+        record.width = _WIDTH
+        for a in range(3):
+            record.dims[a] = dims[a]
+            record.cell[a] = lengths[a]
+            record.widths[a] = float(np.float32(lengths[a] / dims[a]))
+        record.cutoff = request.cutoff
+        record.radius = radius
+        record.threshold_squared = allowance * allowance / 4 if allowance > 0 else 0.0
+        record.timestep = request.timestep
+        record.sigma = request.sigma
+        record.epsilon = request.epsilon
+        record.steps_left = int(request.steps)
+        masses = np.asarray(request.masses, dtype=np.float64)
+        velocities = np.asarray(request.velocities, dtype=np.float64)
+        velocities = velocities - (masses[:, None] * velocities).sum(axis=0) / masses.sum()
+        velocities32 = velocities.astype(np.float32)
+        kinetic = 0.5 * float((masses[:, None] * velocities32.astype(np.float64) ** 2).sum())
+        kT = BOLTZMANN * float(request.temperature)
+        degrees = 3 * n - 3
+        base = kT * float(request.thermostat_timescale) ** 2
+        record.thermostat[_KINETIC_A] = kinetic
+        record.thermostat[_PENDING] = 1.0
+        record.thermostat[_CHAIN_MASS] = degrees * base
+        record.thermostat[_CHAIN_MASS + 1] = base
+        record.thermostat[_CHAIN_MASS + 2] = base
+        record.thermostat[_KT] = kT
+        record.thermostat[_DEGREES] = degrees
+        record.thermostat[_TIMESTEP] = request.timestep
+        return record, velocities32
+
+    def _write_record(self, slot: int, record: Replica) -> None:
+        size = ctypes.sizeof(Replica)
+        raw = torch.frombuffer(bytearray(ctypes.string_at(ctypes.addressof(record), size)),
+                               dtype=torch.uint8)
+        self.table[slot * size:(slot + 1) * size].copy_(raw)
+
+    def _upload(self, request: ReplicaRequest, slot: int, offset: int) -> None:
+        record, velocities32 = self._describe(request, slot, offset)
+        n = record.num_atoms
+        b = self.buffers
+        positions = torch.zeros((n, 4), dtype=torch.float32)
+        positions[:, :3] = torch.from_numpy(np.asarray(request.positions, dtype=np.float32))
+        masses = torch.from_numpy(np.asarray(request.masses, dtype=np.float32))
+        b["positions"][offset:offset + n].copy_(positions)
+        b["velocities"][offset:offset + n].copy_(torch.from_numpy(velocities32))
+        b["forces"][offset:offset + n].zero_()
+        b["masses"][offset:offset + n].copy_(masses)
+        b["inverse_masses"][offset:offset + n].copy_(1.0 / masses)
+        b["images"][offset:offset + n].zero_()
+        self._write_record(slot, record)
+
+    def _launch(self, slots: list[int], budgets: list[int] | None, mode: int) -> None:
+        if not slots:
+            return
+        slot_tensor = torch.tensor(slots, dtype=torch.int32, device=self.device)
+        budget_tensor = (torch.tensor(budgets, dtype=torch.int32, device=self.device)
+                         if budgets is not None else None)
+        with torch.cuda.device(self.device):
+            call("nd_serve_run", self.pool, slot_tensor.data_ptr(),
+                 budget_tensor.data_ptr() if budget_tensor is not None else None,
+                 len(slots), mode, stream_handle(self.device))
+
+    def _records(self) -> np.ndarray:
+        """The slot table on the host, as raw bytes per slot."""
+        return self.table.view(self.max_slots, ctypes.sizeof(Replica)).cpu().numpy()
+
+    @staticmethod
+    def _int_field(raw: np.ndarray, name: str) -> np.ndarray:
+        """One int32 field of every slot, read straight from the table's bytes."""
+        offset = getattr(Replica, name).offset
+        return np.ascontiguousarray(raw[:, offset:offset + 4]).view(np.int32)[:, 0]
+
+    def _harvest(self, active: _Active, raw: np.ndarray, now: float) -> ReplicaResult:
+        record = Replica.from_buffer_copy(raw.tobytes())
+        n, offset = record.num_atoms, active.offset
+        cell = torch.tensor(list(record.cell), dtype=torch.float32, device=self.device)
+        unwrapped = self.buffers["positions"][offset:offset + n, :3]
+        crossings = torch.floor(unwrapped / cell)
+        wrapped = unwrapped - crossings * cell
+        below = wrapped < 0
+        wrapped = torch.where(below, wrapped + cell, wrapped)
+        crossings = torch.where(below, crossings - 1, crossings)
+        above = wrapped >= cell
+        wrapped = torch.where(above, wrapped - cell, wrapped)
+        crossings = torch.where(above, crossings + 1, crossings)
+        scale = np.float32(record.thermostat[_PENDING])
+        velocities = self.buffers["velocities"][offset:offset + n] * float(scale)
+        images = self.buffers["images"][offset:offset + n] + crossings.to(torch.int64)
+        result = ReplicaResult(
+            name=active.request.name,
+            positions=wrapped.cpu().numpy(),
+            velocities=velocities.cpu().numpy(),
+            images=images.cpu().numpy(),
+            energy=float(record.energy),
+            status=int(record.status),
+            rebuilds=int(record.rebuild_count),
+            arrival=float(active.request.arrival),
+            admitted=active.admitted,
+            finished=now,
+            num_atoms=n,
+            steps=int(active.request.steps) - int(record.steps_left),
+        )
+        self._give(active.offset // _ALIGN, active.units)
+        self._free_slots.append(active.slot)
+        return result
+
+    # -- the loop ------------------------------------------------------------------------
+
+    def serve(self, requests: list[ReplicaRequest], *, realtime: bool = True) -> list[ReplicaResult]:
+        """Serve requests by their arrival times; returns the results in completion order.
+
+        With ``realtime`` the arrivals follow the wall clock from the call (a request is
+        admitted only once its arrival time has passed); without, all are present at once.
+        Syncs with the host once per round.
+        """
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        for request in pending:
+            n = request.positions.shape[0]
+            if -(-n // _ALIGN) > self.capacity // _ALIGN:
+                raise ValueError(f"a replica of {n} atoms exceeds the server's budget")
+        active: dict[int, _Active] = {}
+        results: list[ReplicaResult] = []
+        start = time.perf_counter()
+        while pending or active:
+            now = time.perf_counter() - start
+            admitted = []
+            while pending and (not realtime or pending[0].arrival <= now):
+                request = pending[0]
+                units = -(-request.positions.shape[0] // _ALIGN)
+                if not self._free_slots:
+                    break
+                first = self._take(units)
+                if first is None:
+                    break
+                pending.popleft()
+                slot = self._free_slots.pop()
+                offset = first * _ALIGN
+                self._upload(request, slot, offset)
+                active[slot] = _Active(request, slot, offset, units, now, int(request.steps))
+                admitted.append(slot)
+            self._launch(admitted, None, 0)
+            if not active:
+                if pending and realtime:
+                    time.sleep(max(0.0, min(pending[0].arrival - now, 0.001)))
+                continue
+            slots = list(active)
+            budgets = [max(1, min(active[s].steps_left,
+                                  -(-self.round_atom_steps // active[s].request.positions.shape[0])))
+                       for s in slots]
+            self._launch(slots, budgets, 1)
+            raw = self._records()
+            now = time.perf_counter() - start
+            steps_left_all = self._int_field(raw, "steps_left")
+            status_all = self._int_field(raw, "status")
+            for slot in slots:
+                steps_left, status = int(steps_left_all[slot]), int(status_all[slot])
+                active[slot].steps_left = steps_left
+                if steps_left == 0 or status != 0:
+                    results.append(self._harvest(active.pop(slot), raw[slot], now))
+        return results
+
+
+__all__ = ("ReplicaRequest", "ReplicaResult", "ReplicaServer")

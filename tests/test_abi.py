@@ -87,3 +87,21 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_native, "CORE_PATH", tmp_path / "libnabladyn_b200.so")
     with pytest.raises(RuntimeError, match="not built"):
         _native.lib()
+
+
+def test_replica_record_layout_and_pool_allocator():
+    """The ctypes record matches the header's layout; the server's first-fit allocator merges
+    freed ranges (no device needed)."""
+    from nabladyn_b200.serving import ReplicaServer
+
+    assert ctypes.sizeof(_native.Replica) == 304
+    assert _native.Replica.energy.offset == 104
+    server = ReplicaServer(device="cpu", budget_bytes=1 << 22, max_slots=4)
+    total = server.capacity // 32
+    a, b = server._take(3), server._take(5)
+    assert (a, b) == (0, 3)
+    server._give(a, 3)
+    assert server._free_units == [(0, 3), (8, total - 8)]
+    server._give(b, 5)
+    assert server._free_units == [(0, total)]
+    assert server._take(total + 1) is None

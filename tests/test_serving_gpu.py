@@ -1,0 +1,83 @@
+"""The replica server on the GPU: each served replica against the reference's own NVT
+trajectory, the same result alone and in a mix (bit for bit: replicas never interact), and
+admission within the HBM budget.
+
+Tolerances: float32 replicas against the reference's float32 20-step trajectory to 2e-4 nm and
+2e-3 nm/ps (two float32 summation orders); alone against mixed exactly.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from nabladyn_b200 import lattice
+from nabladyn_b200.serving import ReplicaRequest, ReplicaServer, serving_requests
+from oracle import lj
+from oracle import neighbors as on
+
+pytestmark = pytest.mark.gpu
+
+
+def argon_request(argon, steps, name="argon"):
+    return ReplicaRequest(positions=argon["positions"], velocities=argon["velocities"],
+                          masses=np.full(512, 39.948), cell=argon["cell"], temperature=120.0,
+                          steps=steps, name=name)
+
+
+def test_served_replica_matches_reference_trajectory(argon, argon_md, cuda):
+    server = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=64)
+    others = serving_requests(12, seed=3, steps=20, largest=3000)
+    results = {r.name: r for r in server.serve([argon_request(argon, 20)] + others,
+                                                realtime=False)}
+    mine = results["argon"]
+    assert mine.status == 0 and mine.steps == 20
+    np.testing.assert_allclose(mine.positions, argon_md["NVT_f32_20_positions"], atol=2e-4)
+    np.testing.assert_allclose(mine.velocities, argon_md["NVT_f32_20_velocities"], atol=2e-3)
+    np.testing.assert_array_equal(mine.images, argon_md["NVT_f32_20_images"])
+    assert mine.energy == pytest.approx(float(argon_md["NVT_f32_20_energy"]), rel=1e-4)
+
+
+def test_alone_equals_mixed(cuda):
+    requests = serving_requests(24, seed=5, steps=60, largest=6000, rate=400.0)
+    chosen = [requests[3], requests[10]]
+    alone = {}
+    for request in chosen:
+        server = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=8)
+        alone[request.name] = server.serve([request], realtime=False)[0]
+    server = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=32,
+                           round_atom_steps=50_000)
+    mixed = {r.name: r for r in server.serve(requests, realtime=True)}
+    for request in chosen:
+        a, b = alone[request.name], mixed[request.name]
+        assert a.status == b.status == 0
+        np.testing.assert_array_equal(a.positions, b.positions)
+        np.testing.assert_array_equal(a.velocities, b.velocities)
+        assert a.energy == b.energy
+
+
+def test_grid_replica_energy_against_oracle(cuda):
+    positions, cell = lattice.fcc(10, 10 * 0.5745, 0.03, seed=9)  # 4,000 atoms, >= 3 cells/axis
+    request = ReplicaRequest(positions=positions, velocities=np.zeros_like(positions),
+                             masses=np.full(len(positions), 39.948), cell=cell,
+                             temperature=120.0, steps=0, name="grid")
+    server = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=4)
+    result = server.serve([request], realtime=False)[0]
+    wrapped = on.wrap(positions, cell)
+    first, second, _ = on.pairs(wrapped, cell, 1.0)
+    energy, _, _ = lj.energy_force_virial(wrapped, cell, first, second, [0.34], [0.996], 1.0)
+    assert result.energy == pytest.approx(energy, rel=1e-5)
+
+
+def test_admission_stays_within_budget(cuda):
+    requests = serving_requests(16, seed=11, steps=40, smallest=300, largest=2500)
+    server = ReplicaServer(device=cuda, budget_bytes=3 << 20, max_slots=16)
+    capacity = server.capacity
+    results = server.serve(requests, realtime=False)
+    assert len(results) == 16 and all(r.status == 0 and r.steps == 40 for r in results)
+    # At any admission time, the atoms resident (rounded to 32) fit the pool.
+    events = sorted(set(r.admitted for r in results))
+    for t in events:
+        resident = sum(-(-r.num_atoms // 32) * 32 for r in results
+                       if r.admitted <= t < r.finished)
+        assert resident <= capacity
+    assert len({r.admitted for r in results}) > 1  # the budget made some wait
