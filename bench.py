@@ -195,6 +195,71 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_serving(device, requests: int, plain_sample: int, rate: float | None) -> dict:
+    """The serving workload: ``requests`` independent argon NVT replicas (64-16,384 atoms,
+    500 steps) through the replica server with Poisson arrivals at ``rate`` per second (None:
+    all at once, over-subscribed), against the plain path: a sample of the same requests one
+    at a time through md.nvt (construction, capture and run)."""
+    import torch
+
+    from nabladyn_b200 import md, potential
+    from nabladyn_b200.serving import ReplicaServer, serving_requests
+
+    work = serving_requests(requests, seed=7, rate=rate)
+    server = ReplicaServer(device=device, budget_bytes=16 << 30, max_slots=2048)
+    server.serve(serving_requests(8, seed=99, steps=20), realtime=False)  # warm-up
+    torch.cuda.synchronize(device)
+    start = time.perf_counter()
+    results = server.serve(work, realtime=rate is not None)
+    wall = time.perf_counter() - start
+    latencies = np.array([r.latency for r in results])
+    replica_steps = sum(r.steps for r in results)
+    atom_steps = sum(r.steps * r.num_atoms for r in results)
+    failed = sum(1 for r in results if r.status != 0)
+    # Plain: the same requests one at a time through md.nvt, on a seeded sample.
+    sample = [work[k] for k in np.random.default_rng(1).choice(len(work), plain_sample, replace=False)]
+    plain_total = plain_run = 0.0
+    plain_steps = 0
+    for request in sample:
+        t0 = time.perf_counter()
+        n = request.positions.shape[0]
+        model = potential.lennard_jones(
+            atom_types=torch.zeros(n, dtype=torch.int64, device=device),
+            sigma=torch.tensor([request.sigma], device=device),
+            epsilon=torch.tensor([request.epsilon], device=device), cutoff=request.cutoff)
+        simulation = md.nvt(
+            model, torch.tensor(request.positions, dtype=torch.float32, device=device),
+            torch.tensor(request.velocities, dtype=torch.float32, device=device),
+            torch.tensor(request.masses, dtype=torch.float32, device=device),
+            torch.tensor(request.cell, dtype=torch.float32, device=device),
+            timestep=request.timestep, temperature=request.temperature,
+            thermostat_timescale=request.thermostat_timescale, skin=request.skin)
+        t1 = time.perf_counter()
+        simulation.run(request.steps)
+        simulation.state()
+        torch.cuda.synchronize(device)
+        t2 = time.perf_counter()
+        plain_total += t2 - t0
+        plain_run += t2 - t1
+        plain_steps += request.steps
+    served_rate = replica_steps / wall
+    plain_rate = plain_steps / plain_total
+    return {
+        "workload": f"{requests} LJ argon NVT replicas, N log-uniform 64-16384, 500 steps, "
+                    f"fp32, arrivals {'Poisson ' + str(rate) + '/s' if rate else 'all at t=0'}",
+        "replica_steps_per_s": served_rate,
+        "atom_steps_per_s": atom_steps / wall,
+        "wall_s": wall,
+        "latency_p50_s": float(np.percentile(latencies, 50)),
+        "latency_p99_s": float(np.percentile(latencies, 99)),
+        "failed": failed,
+        "plain_replica_steps_per_s": plain_rate,
+        "plain_run_only_replica_steps_per_s": plain_steps / plain_run,
+        "plain_sample": plain_sample,
+        "vs_plain": served_rate / plain_rate,
+    }
+
+
 def run_reference_cuda(args) -> None:
     """The reference's own GPU path on this B200: its md.nve (Inductor programs around its
     CUDA neighbor operator, one CUDA Graph per step), installed in baseline/_ref. Not a driver
@@ -341,6 +406,9 @@ def run_ours(args) -> None:
     d2h = (3 * n * 3 * 4 + n * 3 * 8) / chunk
 
     cpu = cpu_port_rate() if (rank == 0 and world == 1) else None
+    serving = None
+    if args.serving and rank == 0:
+        serving = run_serving(device, args.serving, plain_sample=16, rate=None)
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -390,6 +458,7 @@ def run_ours(args) -> None:
             "gpu_launches": engine.step_launches * args.steps,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -402,9 +471,21 @@ def main() -> None:
     parser.add_argument("--steps", type=int, default=1000)
     parser.add_argument("--warmup", type=int, default=10)
     parser.add_argument("--impl", choices=("ours", "reference", "reference-cuda"), default="ours")
+    parser.add_argument("--serving", type=int, default=4096,
+                        help="requests of the serving workload (0 skips it)")
+    parser.add_argument("--serving-rate", type=float, default=None,
+                        help="with --workload serving: Poisson arrivals per second")
+    parser.add_argument("--workload", choices=("large", "serving"), default="large")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "serving":
+        import torch
+
+        device = torch.device("cuda", 0)
+        print(json.dumps(run_serving(device, args.serving, plain_sample=16,
+                                     rate=args.serving_rate)), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference-cuda":
