@@ -260,6 +260,45 @@ def run_serving(device, requests: int, plain_sample: int, rate: float | None) ->
     }
 
 
+def small_system(module, device, dtype):
+    """The plain small workload: 512 argon atoms on an 8^3 simple-cubic lattice in L = 2.90 nm
+    with 0.02 nm seeded jitter, 120 K Maxwell-Boltzmann velocities; built with ``module``
+    (this package or the reference), returns its NVT simulation."""
+    import torch
+
+    from nabladyn_b200 import lattice
+
+    positions, cell = lattice.simple_cubic(8, 2.90, 0.02, seed=512)
+    n = positions.shape[0]
+    model = module.potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64, device=device),
+        sigma=torch.tensor([SIGMA], dtype=dtype, device=device),
+        epsilon=torch.tensor([EPSILON], dtype=dtype, device=device), cutoff=CUTOFF)
+    masses = torch.full((n,), MASS, dtype=dtype, device=device)
+    velocities = module.md.maxwell_boltzmann(masses, TEMPERATURE, seed=512)
+    return module.md.nvt(model, torch.tensor(positions, dtype=dtype, device=device), velocities,
+                         masses, torch.tensor(cell, dtype=dtype, device=device),
+                         timestep=TIMESTEP, temperature=TEMPERATURE, thermostat_timescale=0.1)
+
+
+def run_small(module, device, steps: int, label: str) -> dict:
+    """2,500 NVT steps (fp32) of the 512-atom system, timed by CUDA events after warm-up."""
+    import torch
+
+    simulation = small_system(module, device, torch.float32)
+    simulation.run(100)
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    simulation.run(steps)
+    end.record()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end)
+    return {"impl": label, "workload": "512-atom argon NVT, fp32, dt 4 fs, NHC(3) at 120 K",
+            "steps": steps, "us_per_step": 1e3 * ms / steps, "steps_per_s": steps / (ms / 1e3),
+            "ns_per_day": steps / (ms / 1e3) * 0.004 * 86400 / 1000}
+
+
 def run_reference_cuda(args) -> None:
     """The reference's own GPU path on this B200: its md.nve (Inductor programs around its
     CUDA neighbor operator, one CUDA Graph per step), installed in baseline/_ref. Not a driver
@@ -272,6 +311,11 @@ def run_reference_cuda(args) -> None:
     from nabladyn_b200 import lattice
 
     device = torch.device("cuda", 0)
+    if args.workload == "small":
+        import nabladyn
+
+        print(json.dumps(run_small(nabladyn, device, args.steps, "reference-cuda")), flush=True)
+        return
     positions, cell = lattice.fcc(ATOMS_PER_SIDE_CELLS, LENGTH, 0.02, 2024)
     n = positions.shape[0]
     dtype = torch.float32
@@ -475,10 +519,18 @@ def main() -> None:
                         help="requests of the serving workload (0 skips it)")
     parser.add_argument("--serving-rate", type=float, default=None,
                         help="with --workload serving: Poisson arrivals per second")
-    parser.add_argument("--workload", choices=("large", "serving"), default="large")
+    parser.add_argument("--workload", choices=("large", "serving", "small"), default="large")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "small" and args.impl == "ours":
+        import torch
+
+        import nabladyn_b200
+
+        print(json.dumps(run_small(nabladyn_b200, torch.device("cuda", 0), args.steps, "ours")),
+              flush=True)
+        return
     if args.workload == "serving":
         import torch
 
