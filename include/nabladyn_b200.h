@@ -338,6 +338,39 @@ typedef struct nd_replica_pool {
 int nd_serve_run(const nd_replica_pool* pool, const int32_t* slots, const int32_t* budgets,
                  int32_t count, int32_t mode, nd_stream_t stream);
 
+/* ---- SchNet (src/nabladyn/potential/_schnet/_potential.py:45-208) ---------------------------
+ * E, F and W of a SchNet model with 64 features and 2..64 Gaussians over a [2, C] pair list,
+ * float32 positions, BF16 tcgen05 tensor cores with FP32 accumulation for every 64 x 64 product,
+ * the reverse pass by hand, E and W in float64. Replaces the reference's autograd evaluation
+ * of SchNet._energy_wrapped under quantity.energy_force_virial (src/nabladyn/quantity.py:93-117);
+ * the reference has no native counterpart. */
+typedef struct nd_schnet_args {
+    int64_t num_atoms;          /* N */
+    int64_t num_columns;        /* C: columns of pairs */
+    int32_t interactions;       /* blocks */
+    int32_t num_types;          /* T */
+    int32_t gaussians;          /* K, 2..64 */
+    int32_t reserved;
+    double cutoff;              /* nm */
+    const float* positions;     /* [N, 3], wrapped into [0, L) */
+    const float* cell;          /* [3] */
+    const int32_t* pairs;       /* [2, C]: first atoms, then second atoms; equal = padding */
+    const int64_t* atom_types;  /* [N] in [0, T) */
+    const void* weights;        /* nd_schnet_weight_bytes bytes, 256-byte aligned (packed by
+                                   the host: per block ten 64 x 64 BF16 operand images, then
+                                   float32 biases, readout and the embedding tables) */
+    void* workspace;            /* nd_schnet_workspace_bytes bytes, 256-byte aligned */
+    double* energy;             /* [1] */
+    float* forces;              /* [N, 3] or NULL */
+    double* virial;             /* [9] or NULL */
+    int32_t* status;            /* [2]: pairs within the cutoff, status bits (1: a pair index
+                                   out of range; 16: a tensor-core product did not complete) */
+} nd_schnet_args;
+
+int64_t nd_schnet_weight_bytes(int32_t interactions, int32_t num_types);
+int64_t nd_schnet_workspace_bytes(int64_t num_atoms, int64_t num_columns, int32_t interactions);
+int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

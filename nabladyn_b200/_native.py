@@ -204,6 +204,28 @@ class ReplicaPool(ctypes.Structure):
     ]
 
 
+class SchNetArgs(ctypes.Structure):
+    _fields_ = [
+        ("num_atoms", ctypes.c_int64),
+        ("num_columns", ctypes.c_int64),
+        ("interactions", ctypes.c_int32),
+        ("num_types", ctypes.c_int32),
+        ("gaussians", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("cutoff", ctypes.c_double),
+        ("positions", ctypes.c_void_p),
+        ("cell", ctypes.c_void_p),
+        ("pairs", ctypes.c_void_p),
+        ("atom_types", ctypes.c_void_p),
+        ("weights", ctypes.c_void_p),
+        ("workspace", ctypes.c_void_p),
+        ("energy", ctypes.c_void_p),
+        ("forces", ctypes.c_void_p),
+        ("virial", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+    ]
+
+
 # name -> (argument types); every entry point returns int.
 _SIGNATURES = {
     "nd_abi_version": [],
@@ -250,10 +272,17 @@ _SIGNATURES = {
         ctypes.POINTER(ReplicaPool), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
         ctypes.c_int32, ctypes.c_void_p,
     ],
+    "nd_schnet_energy_force_virial": [ctypes.POINTER(SchNetArgs), ctypes.c_void_p],
+}
+
+# name -> (argument types) of the entry points that return a byte count (int64, -1 on error).
+_SIZES = {
+    "nd_schnet_weight_bytes": [ctypes.c_int32, ctypes.c_int32],
+    "nd_schnet_workspace_bytes": [ctypes.c_int64, ctypes.c_int64, ctypes.c_int32],
 }
 
 # Every symbol include/nabladyn_b200.h declares.
-EXPORTED = ("nd_last_error", *_SIGNATURES)
+EXPORTED = ("nd_last_error", *_SIGNATURES, *_SIZES)
 
 
 def _missing(path: Path) -> RuntimeError:
@@ -277,6 +306,10 @@ def lib() -> ctypes.CDLL:
                 for name, argtypes in _SIGNATURES.items():
                     function = getattr(loaded, name)
                     function.restype = ctypes.c_int
+                    function.argtypes = argtypes
+                for name, argtypes in _SIZES.items():
+                    function = getattr(loaded, name)
+                    function.restype = ctypes.c_int64
                     function.argtypes = argtypes
                 _lib = loaded
     return _lib

@@ -1,0 +1,1246 @@
+// SchNet energy, forces and virial with the dense layers on BF16 tcgen05 tensor cores.
+//
+// The model is src/nabladyn/potential/_schnet/_potential.py:45-208 (64 features, K <= 64
+// Gaussians, any number of blocks). The reference differentiates it with autograd
+// (src/nabladyn/quantity.py:93-117); here the reverse pass is written out:
+//
+//   forward, per block b:  v = x A^T;  per pair p = (a, b) within the cutoff
+//       z1 = g(r) B1^T + b1,  f_raw = ssp(z1) B2^T + b2,  f = f_raw C(r),
+//       m_a += f * v_b,  m_b += f * v_a;
+//     h = m D1^T + d1,  x += ssp(h) D2^T + d2;  E = sum_i ssp(x R1^T + e1) R2^T + e2
+//   reverse:  G = dE/dx = (sigmoid(y) * R2) R1;  per block, last first:
+//     Gh = (G D2) * sigmoid(h),  Gm = Gh D1;  per pair  Gf = Gm_a * v_b + Gm_b * v_a,
+//       Gv_b += f * Gm_a,  Gv_a += f * Gm_b,
+//       dE/dr += C'(r) (Gf . f_raw) + [((Gf C) B2 * sigmoid(z1)) B1] . g'(r);
+//     G += Gv A
+//   F_a -= dE/dr d / r,  F_b += dE/dr d / r,  W -= dE/dr d d^T / r.
+//
+// Every 64 x 64 product runs as a 128-row tile on the tensor cores: a [128 x 64] BF16 row
+// tile (one pair or one atom per thread of a 128-thread CTA) times a BF16 weight image,
+// FP32 accumulation in tensor memory (umma.cuh). The per-pair products (filter network
+// forward, and its reverse) run in persistent CTAs that keep their weight images in shared
+// memory; the atom-wise products in one CTA per 128 atoms. Everything else is FP32, the
+// energy and virial sums FP64 in a fixed order. Messages, their reverse and forces are
+// scattered with FP32 vector atomics.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "common.cuh"
+#include "umma.cuh"
+
+namespace nd {
+namespace {
+
+constexpr int kFeatures = 64;
+constexpr int kHidden = 32;      // the readout's hidden layer, features / 2
+constexpr int kTile = 128;       // rows per tensor-core tile = threads per CTA
+constexpr int kImagesPerBlock = 10;
+constexpr float kLn2 = 0.693147180559945309f;
+
+// Status bits of the SchNet status word.
+constexpr int kBadPair = 1;       // a pair index outside [0, N)
+constexpr int kProductLost = 16;  // a tensor-core product did not complete in time
+
+// Weight images of one block, in this order.
+enum Image : int
+{
+    kB1 = 0,   // filter1.weight [64 out][K in, zero-padded to 64]
+    kB2 = 1,   // filter2.weight [out][in]
+    kB2T = 2,  // its transpose
+    kB1T = 3,  // filter1.weight^T [K, zero-padded to 64][64]
+    kA = 4,    // atoms.weight
+    kAT = 5,
+    kD1 = 6,   // update1.weight
+    kD1T = 7,
+    kD2 = 8,   // update2.weight
+    kD2T = 9,
+};
+
+// Byte layout of the packed parameter block (nd_schnet_weight_bytes).
+struct WeightLayout
+{
+    std::int64_t vectors;  // per block: b1, b2, d1, d2 (64 floats each)
+    std::int64_t readout;  // R1 [32][64], e1 [32], R2 [32], e2 (padded to 32)
+    std::int64_t tables;   // embedding [T][64], v0 = embedding A0^T [T][64]
+    std::int64_t total;
+
+    __host__ __device__ WeightLayout(int blocks, int types)
+    {
+        vectors = static_cast<std::int64_t>(blocks) * kImagesPerBlock * umma::kImageBytes;
+        readout = vectors + static_cast<std::int64_t>(blocks) * 4 * kFeatures * 4;
+        tables = readout + (kHidden * kFeatures + 3 * kHidden) * 4;
+        total = tables + 2 * static_cast<std::int64_t>(types) * kFeatures * 4;
+    }
+};
+
+__host__ __device__ inline std::int64_t align256(std::int64_t bytes)
+{
+    return (bytes + 255) / 256 * 256;
+}
+
+constexpr int kVirialSlots = 1024;  // per-CTA virial partials of the last reverse pass
+
+// Byte layout of the workspace (nd_schnet_workspace_bytes).
+struct Workspace
+{
+    std::int64_t counters, pairs, geometry, x, v, h, m, grad, grad_m, grad_v, dedr, energy,
+        virial, total;
+
+    Workspace(std::int64_t atoms, std::int64_t columns, int blocks)
+    {
+        const std::int64_t row = atoms * kFeatures * 4;
+        const std::int64_t tiles = (atoms + kTile - 1) / kTile;
+        counters = 0;
+        pairs = 256;
+        geometry = pairs + align256(columns * 8);
+        x = geometry + align256(columns * 16);
+        v = x + align256(row);
+        h = v + blocks * align256(row);
+        m = h + blocks * align256(row);
+        grad = m + align256(row);
+        grad_m = grad + align256(row);
+        grad_v = grad_m + align256(row);
+        dedr = grad_v + align256(row);
+        energy = dedr + align256(columns * 4);
+        virial = energy + align256(tiles * 8);
+        total = virial + align256(kVirialSlots * 9 * 8);
+    }
+};
+
+__device__ __forceinline__ float approx_reciprocal(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// ln(1 + e^x) - ln 2 and its derivative, in FP32 with the hardware exp and log; the results
+// feed BF16 operands.
+__device__ __forceinline__ float softplus_shifted(float x)
+{
+    return fmaxf(x, 0.0f) + __logf(1.0f + __expf(-fabsf(x))) - kLn2;
+}
+
+__device__ __forceinline__ float sigmoid(float x)
+{
+    return approx_reciprocal(1.0f + __expf(-x));
+}
+
+// Shared-memory staging of weight images and bias vectors, by all 128 threads.
+__device__ __forceinline__ void copy_bytes(unsigned char* to, const unsigned char* from, int bytes)
+{
+    for (int i = threadIdx.x * 16; i < bytes; i += kTile * 16)
+    {
+        *reinterpret_cast<uint4*>(to + i) = __ldg(reinterpret_cast<const uint4*>(from + i));
+    }
+}
+
+// The per-CTA tensor-core context: tensor memory, the completion barrier and its phase.
+struct Cores
+{
+    std::uint64_t* barrier;
+    std::uint32_t* slot;
+    std::uint32_t tmem;  // this warp's lanes, column 0
+    unsigned phase;
+
+    __device__ void open(std::uint64_t* barrier_, std::uint32_t* slot_, std::uint32_t columns)
+    {
+        barrier = barrier_;
+        slot = slot_;
+        phase = 0;
+        if (threadIdx.x == 0)
+        {
+            umma::barrier_init(barrier);
+        }
+        if (threadIdx.x < 32)
+        {
+            umma::allocate(slot, columns);
+        }
+        umma::fence_before_sync();
+        __syncthreads();
+        umma::fence_after_sync();
+        tmem = *slot + ((32u * (threadIdx.x / 32)) << 16);
+    }
+
+    // D[column offset] = tile * image^T, after every thread wrote its row of the tile; waits
+    // for the product. False (on every thread) when it did not complete in time.
+    __device__ bool run(std::uint32_t column, const unsigned char* tile, const unsigned char* image)
+    {
+        umma::fence_operands();
+        umma::fence_before_sync();
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            umma::fence_after_sync();
+            umma::product(*slot + column, umma::smem_address(tile), umma::smem_address(image));
+            umma::commit(barrier);
+        }
+        const bool done = umma::barrier_wait(barrier, phase);
+        phase ^= 1u;
+        const bool lost = __syncthreads_or(!done);
+        umma::fence_after_sync();
+        return !lost;
+    }
+
+    __device__ void close(std::uint32_t columns)
+    {
+        umma::fence_before_sync();
+        __syncthreads();
+        if (threadIdx.x < 32)
+        {
+            umma::fence_after_sync();
+            umma::deallocate(*slot, columns);
+        }
+    }
+};
+
+// Gaussians g_k(r) = exp(-(r / D - k)^2 / 2), k < K, zero above, into this thread's row.
+__device__ __forceinline__ void store_basis(unsigned char* tile, float r_over_width, int gaussians,
+                                            bool live)
+{
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+    {
+        float values[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+        {
+            const int k = 8 * c + e;
+            const float u = r_over_width - static_cast<float>(k);
+            values[e] = (live && k < gaussians) ? __expf(-0.5f * u * u) : 0.0f;
+        }
+        umma::store8(tile, threadIdx.x, c, values);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pairs within the cutoff, compacted: (a, b) and (d, r), d = r_a - r_b of the minimum image
+// as src/nabladyn/space.py:11-19 rounds it.
+
+__global__ void compact_kernel(const float* __restrict__ positions, const float* __restrict__ cell,
+                               const std::int32_t* __restrict__ pairs, std::int64_t columns,
+                               std::int64_t atoms, float cutoff_squared, int2* __restrict__ kept,
+                               float4* __restrict__ geometry, int* __restrict__ counters)
+{
+    const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool keep = false;
+    int2 ab = make_int2(0, 0);
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c < columns)
+    {
+        ab = make_int2(pairs[c], pairs[columns + c]);
+        if (ab.x != ab.y)
+        {
+            if (ab.x < 0 || ab.y < 0 || ab.x >= atoms || ab.y >= atoms)
+            {
+                atomicOr(counters + 1, kBadPair);
+            }
+            else
+            {
+                float d[3];
+#pragma unroll
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const float length = cell[axis];
+                    const float left = positions[3 * ab.x + axis];
+                    const float right = positions[3 * ab.y + axis];
+                    const float raw = left - right;
+                    const float half = 0.5f * length;
+                    d[axis] = (left - (raw > half ? length : 0.0f)) -
+                              (right - (raw < -half ? length : 0.0f));
+                }
+                const float squared = __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])),
+                                                __fmul_rn(d[2], d[2]));
+                keep = squared < cutoff_squared;
+                g = make_float4(d[0], d[1], d[2], sqrtf(squared));
+            }
+        }
+    }
+    const unsigned ballot = __ballot_sync(kFullMask, keep);
+    if (ballot == 0)
+    {
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(ballot) - 1;
+    int base = 0;
+    if (lane == leader)
+    {
+        base = atomicAdd(counters, __popc(ballot));
+    }
+    base = __shfl_sync(kFullMask, base, leader);
+    if (keep)
+    {
+        const int slot = base + __popc(ballot & ((1u << lane) - 1u));
+        kept[slot] = ab;
+        geometry[slot] = g;
+    }
+}
+
+// x = embedding[type], v0 = (embedding A0^T)[type].
+__global__ void embed_kernel(const std::int64_t* __restrict__ types, std::int64_t atoms,
+                             const float* __restrict__ table, const float* __restrict__ table_v,
+                             float* __restrict__ x, float* __restrict__ v)
+{
+    const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= atoms * 16)
+    {
+        return;
+    }
+    const std::int64_t atom = i / 16;
+    const int q = static_cast<int>(i % 16);
+    const std::int64_t type = types[atom];
+    reinterpret_cast<float4*>(x)[i] = reinterpret_cast<const float4*>(table)[type * 16 + q];
+    reinterpret_cast<float4*>(v)[i] = reinterpret_cast<const float4*>(table_v)[type * 16 + q];
+}
+
+struct PairPass
+{
+    const int2* pairs;
+    const float4* geometry;
+    int* counters;
+    const unsigned char* images;  // this block's ten images
+    const float* b1;
+    const float* b2;
+    const float* v;           // [N][64] this block's x A^T
+    float* m;                 // forward: messages
+    const float* grad_m;      // reverse: Gm
+    float* grad_v;            // reverse: Gv (null for the first block)
+    float* dedr;              // reverse: per-pair dE/dr over the blocks so far
+    float* forces;            // reverse, last pass: F (null when not wanted)
+    double* virial;           // reverse, last pass: per-CTA partials [gridDim.x][9]
+    float width;              // Gaussian spacing D
+    float phase;              // pi / r_c
+    int gaussians;
+    int first;                // reverse: the first pass (last block) starts dE/dr
+    int last;                 // reverse: the last pass (block 0) applies forces and virial
+};
+
+// Shared memory of the pair passes: weight images, the basis tile, one work tile, biases.
+constexpr int kPairForwardShared = 2 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
+constexpr int kPairReverseShared = 4 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
+
+__global__ void __launch_bounds__(kTile) pair_forward_kernel(PairPass a)
+{
+    extern __shared__ __align__(1024) unsigned char shared[];
+    unsigned char* image_b1 = shared;
+    unsigned char* image_b2 = image_b1 + umma::kImageBytes;
+    unsigned char* basis = image_b2 + umma::kImageBytes;
+    unsigned char* work = basis + umma::kTileBytes;
+    float* bias1 = reinterpret_cast<float*>(work + umma::kTileBytes);
+    float* bias2 = bias1 + kFeatures;
+    auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
+    auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
+
+    copy_bytes(image_b1, a.images + kB1 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b2, a.images + kB2 * umma::kImageBytes, umma::kImageBytes);
+    if (threadIdx.x < kFeatures)
+    {
+        bias1[threadIdx.x] = a.b1[threadIdx.x];
+        bias2[threadIdx.x] = a.b2[threadIdx.x];
+    }
+    Cores cores;
+    cores.open(barrier, slot, 64);
+    const int count = *reinterpret_cast<volatile int*>(a.counters);
+    const float4* v4 = reinterpret_cast<const float4*>(a.v);
+    float4* m4 = reinterpret_cast<float4*>(a.m);
+
+    for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
+    {
+        const int p = tile * kTile + threadIdx.x;
+        const bool live = p < count;
+        int2 ab = make_int2(0, 0);
+        float4 g = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (live)
+        {
+            ab = a.pairs[p];
+            g = a.geometry[p];
+        }
+        const float envelope = live ? 0.5f * (__cosf(g.w * a.phase) + 1.0f) : 0.0f;
+        store_basis(basis, g.w / a.width, a.gaussians, live);
+        if (!cores.run(0, basis, image_b1))
+        {
+            if (threadIdx.x == 0)
+            {
+                atomicOr(a.counters + 1, kProductLost);
+            }
+            break;
+        }
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float z[32];
+            umma::load32(cores.tmem + 32 * half, z);
+            umma::wait_loads();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float s[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                {
+                    s[e] = softplus_shifted(z[8 * c + e] + bias1[32 * half + 8 * c + e]);
+                }
+                umma::store8(work, threadIdx.x, 4 * half + c, s);
+            }
+        }
+        if (!cores.run(0, work, image_b2))
+        {
+            if (threadIdx.x == 0)
+            {
+                atomicOr(a.counters + 1, kProductLost);
+            }
+            break;
+        }
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float f[32];
+            umma::load32(cores.tmem + 32 * half, f);
+            umma::wait_loads();
+            if (live)
+            {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                {
+                    const int k = 32 * half + 4 * q;
+                    const float4 filter = make_float4((f[4 * q] + bias2[k]) * envelope,
+                                                      (f[4 * q + 1] + bias2[k + 1]) * envelope,
+                                                      (f[4 * q + 2] + bias2[k + 2]) * envelope,
+                                                      (f[4 * q + 3] + bias2[k + 3]) * envelope);
+                    const float4 va = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.x) + k / 4);
+                    const float4 vb = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4);
+                    atomicAdd(m4 + 16 * static_cast<std::int64_t>(ab.x) + k / 4,
+                              make_float4(filter.x * vb.x, filter.y * vb.y, filter.z * vb.z,
+                                          filter.w * vb.w));
+                    atomicAdd(m4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4,
+                              make_float4(filter.x * va.x, filter.y * va.y, filter.z * va.z,
+                                          filter.w * va.w));
+                }
+            }
+        }
+    }
+    cores.close(64);
+}
+
+// Eight BF16 values of this thread's row of a tile, as floats.
+__device__ __forceinline__ void unpack8(const unsigned char* tile, int c, float* out)
+{
+    const uint4 word = *reinterpret_cast<const uint4*>(tile + umma::image_offset(threadIdx.x, 8 * c));
+    const std::uint32_t parts[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        out[2 * i] = __uint_as_float(parts[i] << 16);
+        out[2 * i + 1] = __uint_as_float(parts[i] & 0xFFFF0000u);
+    }
+}
+
+__global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
+{
+    extern __shared__ __align__(1024) unsigned char shared[];
+    unsigned char* image_b1 = shared;
+    unsigned char* image_b2 = image_b1 + umma::kImageBytes;
+    unsigned char* image_b2t = image_b2 + umma::kImageBytes;
+    unsigned char* image_b1t = image_b2t + umma::kImageBytes;
+    unsigned char* basis = image_b1t + umma::kImageBytes;
+    unsigned char* work = basis + umma::kTileBytes;
+    float* bias1 = reinterpret_cast<float*>(work + umma::kTileBytes);
+    float* bias2 = bias1 + kFeatures;
+    auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
+    auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
+
+    copy_bytes(image_b1, a.images + kB1 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b2, a.images + kB2 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b2t, a.images + kB2T * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b1t, a.images + kB1T * umma::kImageBytes, umma::kImageBytes);
+    if (threadIdx.x < kFeatures)
+    {
+        bias1[threadIdx.x] = a.b1[threadIdx.x];
+        bias2[threadIdx.x] = a.b2[threadIdx.x];
+    }
+    // Columns 0-63 keep z1 - b1 for the whole tile; 64-127 take the other products in turn.
+    Cores cores;
+    cores.open(barrier, slot, 128);
+    const int count = *reinterpret_cast<volatile int*>(a.counters);
+    const float4* v4 = reinterpret_cast<const float4*>(a.v);
+    const float4* gm4 = reinterpret_cast<const float4*>(a.grad_m);
+    float4* gv4 = reinterpret_cast<float4*>(a.grad_v);
+    double w[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
+    bool lost = false;
+
+    for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
+    {
+        const int p = tile * kTile + threadIdx.x;
+        const bool live = p < count;
+        int2 ab = make_int2(0, 0);
+        float4 g = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (live)
+        {
+            ab = a.pairs[p];
+            g = a.geometry[p];
+        }
+        float sine, cosine;
+        __sincosf(g.w * a.phase, &sine, &cosine);
+        const float envelope = live ? 0.5f * (cosine + 1.0f) : 0.0f;
+        const float slope = live ? -0.5f * a.phase * sine : 0.0f;
+        const float t = g.w / a.width;
+        store_basis(basis, t, a.gaussians, live);
+        if (!cores.run(0, basis, image_b1))
+        {
+            lost = true;
+            break;
+        }
+        // ssp(z1) into the work tile; z1 - b1 stays in columns 0-63.
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float z[32];
+            umma::load32(cores.tmem + 32 * half, z);
+            umma::wait_loads();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float s[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                {
+                    s[e] = softplus_shifted(z[8 * c + e] + bias1[32 * half + 8 * c + e]);
+                }
+                umma::store8(work, threadIdx.x, 4 * half + c, s);
+            }
+        }
+        if (!cores.run(64, work, image_b2))
+        {
+            lost = true;
+            break;
+        }
+        // f_raw, Gf = Gm_a v_b + Gm_b v_a, C' Gf . f_raw, Gv, and Gf C into the work tile.
+        float along = 0.0f;
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float f[32];
+            umma::load32(cores.tmem + 64 + 32 * half, f);
+            umma::wait_loads();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float scaled[8];
+#pragma unroll
+                for (int e2 = 0; e2 < 2; ++e2)
+                {
+                    const int q = 2 * c + e2;
+                    const int k = 32 * half + 4 * q;
+                    float4 gf = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (live)
+                    {
+                        const std::int64_t ra = 16 * static_cast<std::int64_t>(ab.x) + k / 4;
+                        const std::int64_t rb = 16 * static_cast<std::int64_t>(ab.y) + k / 4;
+                        const float4 va = __ldg(v4 + ra);
+                        const float4 vb = __ldg(v4 + rb);
+                        const float4 ga = __ldg(gm4 + ra);
+                        const float4 gb = __ldg(gm4 + rb);
+                        gf = make_float4(ga.x * vb.x + gb.x * va.x, ga.y * vb.y + gb.y * va.y,
+                                         ga.z * vb.z + gb.z * va.z, ga.w * vb.w + gb.w * va.w);
+                        const float f0 = f[4 * q] + bias2[k];
+                        const float f1 = f[4 * q + 1] + bias2[k + 1];
+                        const float f2 = f[4 * q + 2] + bias2[k + 2];
+                        const float f3 = f[4 * q + 3] + bias2[k + 3];
+                        along += gf.x * f0 + gf.y * f1 + gf.z * f2 + gf.w * f3;
+                        if (gv4 != nullptr)
+                        {
+                            atomicAdd(gv4 + rb, make_float4(f0 * envelope * ga.x, f1 * envelope * ga.y,
+                                                            f2 * envelope * ga.z, f3 * envelope * ga.w));
+                            atomicAdd(gv4 + ra, make_float4(f0 * envelope * gb.x, f1 * envelope * gb.y,
+                                                            f2 * envelope * gb.z, f3 * envelope * gb.w));
+                        }
+                    }
+                    scaled[4 * e2] = gf.x * envelope;
+                    scaled[4 * e2 + 1] = gf.y * envelope;
+                    scaled[4 * e2 + 2] = gf.z * envelope;
+                    scaled[4 * e2 + 3] = gf.w * envelope;
+                }
+                umma::store8(work, threadIdx.x, 4 * half + c, scaled);
+            }
+        }
+        if (!cores.run(64, work, image_b2t))
+        {
+            lost = true;
+            break;
+        }
+        // ((Gf C) B2) * sigmoid(z1) into the work tile.
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float q[32];
+            float z[32];
+            umma::load32(cores.tmem + 64 + 32 * half, q);
+            umma::load32(cores.tmem + 32 * half, z);
+            umma::wait_loads();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float s[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                {
+                    s[e] = q[8 * c + e] * sigmoid(z[8 * c + e] + bias1[32 * half + 8 * c + e]);
+                }
+                umma::store8(work, threadIdx.x, 4 * half + c, s);
+            }
+        }
+        if (!cores.run(64, work, image_b1t))
+        {
+            lost = true;
+            break;
+        }
+        // dE/dr = C' Gf . f_raw + sum_k [..]_k g_k', g_k' = -g_k (r / D - k) / D.
+        float through = 0.0f;
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float u[32];
+            umma::load32(cores.tmem + 64 + 32 * half, u);
+            umma::wait_loads();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float basis_values[8];
+                unpack8(basis, 4 * half + c, basis_values);
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                {
+                    const int k = 32 * half + 8 * c + e;
+                    through -= u[8 * c + e] * basis_values[e] * (t - static_cast<float>(k));
+                }
+            }
+        }
+        if (live)
+        {
+            float total = slope * along + through / a.width;
+            if (!a.first)
+            {
+                total += a.dedr[p];
+            }
+            if (!a.last)
+            {
+                a.dedr[p] = total;
+            }
+            else
+            {
+                const float scale = total / g.w;
+                const float ux = scale * g.x, uy = scale * g.y, uz = scale * g.z;
+                if (a.forces != nullptr)
+                {
+                    atomicAdd(a.forces + 3 * static_cast<std::int64_t>(ab.x), -ux);
+                    atomicAdd(a.forces + 3 * static_cast<std::int64_t>(ab.x) + 1, -uy);
+                    atomicAdd(a.forces + 3 * static_cast<std::int64_t>(ab.x) + 2, -uz);
+                    atomicAdd(a.forces + 3 * static_cast<std::int64_t>(ab.y), ux);
+                    atomicAdd(a.forces + 3 * static_cast<std::int64_t>(ab.y) + 1, uy);
+                    atomicAdd(a.forces + 3 * static_cast<std::int64_t>(ab.y) + 2, uz);
+                }
+                w[0] -= static_cast<double>(ux) * g.x;
+                w[1] -= static_cast<double>(uy) * g.y;
+                w[2] -= static_cast<double>(uz) * g.z;
+                w[3] -= static_cast<double>(ux) * g.y;
+                w[4] -= static_cast<double>(ux) * g.z;
+                w[5] -= static_cast<double>(uy) * g.z;
+            }
+        }
+    }
+    if (lost && threadIdx.x == 0)
+    {
+        atomicOr(a.counters + 1, kProductLost);
+    }
+    if (a.last && a.virial != nullptr)
+    {
+        __shared__ double sums[4][6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+        {
+            const double s = warp_sum(w[k]);
+            if ((threadIdx.x & 31) == 0)
+            {
+                sums[threadIdx.x / 32][k] = s;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double t6[6];
+            for (int k = 0; k < 6; ++k)
+            {
+                t6[k] = ((sums[0][k] + sums[1][k]) + sums[2][k]) + sums[3][k];
+            }
+            double* out = a.virial + 9 * static_cast<std::int64_t>(blockIdx.x);
+            out[0] = t6[0];
+            out[4] = t6[1];
+            out[8] = t6[2];
+            out[1] = out[3] = t6[3];
+            out[2] = out[6] = t6[4];
+            out[5] = out[7] = t6[5];
+        }
+    }
+    cores.close(128);
+}
+
+struct AtomPass
+{
+    std::int64_t atoms;
+    const unsigned char* images;       // this block's images
+    const unsigned char* next_images;  // forward: the next block's (for v); reverse: its (for Gv A)
+    const float* d1;
+    const float* d2;
+    const float* m;        // forward
+    float* h;              // forward: writes; reverse: reads
+    float* x;              // forward: updated in place
+    float* v_next;         // forward: the next block's v (null for the last block)
+    const float* readout;  // forward, last block: R1, e1, R2, e2
+    float* grad;           // forward, last block: writes dE/dx; reverse: reads, updates
+    const float* grad_v;   // reverse: Gv of the next block (null for the last block)
+    float* grad_m;         // reverse: writes Gm
+    double* energy;        // forward, last block: per-CTA partials
+    int* counters;
+};
+
+constexpr int kAtomShared = 3 * umma::kImageBytes + umma::kTileBytes +
+                            (kHidden * kFeatures + 3 * kHidden) * 4 + 2 * 256 + 64;
+
+__device__ __forceinline__ void load_row(const float* source, std::int64_t row, bool live, float* out)
+{
+    const float4* s4 = reinterpret_cast<const float4*>(source) + 16 * row;
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+    {
+        const float4 value = live ? s4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+        out[4 * q] = value.x;
+        out[4 * q + 1] = value.y;
+        out[4 * q + 2] = value.z;
+        out[4 * q + 3] = value.w;
+    }
+}
+
+__device__ __forceinline__ void store_tile_row(unsigned char* tile, const float* values)
+{
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+    {
+        umma::store8(tile, threadIdx.x, c, values + 8 * c);
+    }
+}
+
+// The 64 accumulator columns of this thread's row.
+__device__ __forceinline__ void load_row_tmem(std::uint32_t tmem, float* out)
+{
+    float part[32];
+    umma::load32(tmem, part);
+    umma::wait_loads();
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+    {
+        out[i] = part[i];
+    }
+    umma::load32(tmem + 32, part);
+    umma::wait_loads();
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+    {
+        out[32 + i] = part[i];
+    }
+}
+
+__device__ __forceinline__ void store_row(float* target, std::int64_t row, const float* values)
+{
+    float4* t4 = reinterpret_cast<float4*>(target) + 16 * row;
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+    {
+        t4[q] = make_float4(values[4 * q], values[4 * q + 1], values[4 * q + 2], values[4 * q + 3]);
+    }
+}
+
+// h = m D1^T + d1, x += ssp(h) D2^T + d2, then v' = x A'^T, or on the last block the readout:
+// e = ssp(x R1^T + e1) R2^T + e2 and dE/dx.
+template <bool kLast>
+__global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
+{
+    extern __shared__ __align__(1024) unsigned char shared[];
+    unsigned char* image_d1 = shared;
+    unsigned char* image_d2 = image_d1 + umma::kImageBytes;
+    unsigned char* image_a = image_d2 + umma::kImageBytes;
+    unsigned char* tile = image_a + umma::kImageBytes;
+    float* readout = reinterpret_cast<float*>(tile + umma::kTileBytes);
+    float* bias1 = readout + kHidden * kFeatures + 3 * kHidden;
+    float* bias2 = bias1 + kFeatures;
+    auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
+    auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
+
+    copy_bytes(image_d1, a.images + kD1 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_d2, a.images + kD2 * umma::kImageBytes, umma::kImageBytes);
+    if (!kLast)
+    {
+        copy_bytes(image_a, a.next_images + kA * umma::kImageBytes, umma::kImageBytes);
+    }
+    else
+    {
+        for (int i = threadIdx.x; i < kHidden * kFeatures + 3 * kHidden; i += kTile)
+        {
+            readout[i] = a.readout[i];
+        }
+    }
+    if (threadIdx.x < kFeatures)
+    {
+        bias1[threadIdx.x] = a.d1[threadIdx.x];
+        bias2[threadIdx.x] = a.d2[threadIdx.x];
+    }
+    Cores cores;
+    cores.open(barrier, slot, 64);
+    const std::int64_t row = static_cast<std::int64_t>(blockIdx.x) * kTile + threadIdx.x;
+    const bool live = row < a.atoms;
+    double energy = 0.0;
+    bool ok = true;
+    {
+        float values[kFeatures];
+        load_row(a.m, row, live, values);
+        store_tile_row(tile, values);
+        ok = cores.run(0, tile, image_d1);
+        if (ok)
+        {
+            load_row_tmem(cores.tmem, values);
+#pragma unroll
+            for (int k = 0; k < kFeatures; ++k)
+            {
+                values[k] += bias1[k];
+            }
+            if (live)
+            {
+                store_row(a.h, row, values);
+            }
+#pragma unroll
+            for (int k = 0; k < kFeatures; ++k)
+            {
+                values[k] = softplus_shifted(values[k]);
+            }
+            store_tile_row(tile, values);
+            ok = cores.run(0, tile, image_d2);
+        }
+        if (ok)
+        {
+            float x[kFeatures];
+            load_row(a.x, row, live, x);
+            load_row_tmem(cores.tmem, values);
+#pragma unroll
+            for (int k = 0; k < kFeatures; ++k)
+            {
+                x[k] += values[k] + bias2[k];
+            }
+            if (!kLast)
+            {
+                if (live)
+                {
+                    store_row(a.x, row, x);
+                }
+                store_tile_row(tile, x);
+                ok = cores.run(0, tile, image_a);
+                if (ok)
+                {
+                    load_row_tmem(cores.tmem, values);
+                    if (live)
+                    {
+                        store_row(a.v_next, row, values);
+                    }
+                }
+            }
+            else
+            {
+                const float* r1 = readout;
+                const float* e1 = readout + kHidden * kFeatures;
+                const float* r2 = e1 + kHidden;
+                const float e2 = r2[kHidden];
+                float grad[kFeatures];
+#pragma unroll
+                for (int k = 0; k < kFeatures; ++k)
+                {
+                    grad[k] = 0.0f;
+                }
+                float e = e2;
+                for (int j = 0; j < kHidden; ++j)
+                {
+                    float y = e1[j];
+#pragma unroll
+                    for (int k = 0; k < kFeatures; ++k)
+                    {
+                        y = fmaf(x[k], r1[j * kFeatures + k], y);
+                    }
+                    e += softplus_shifted(y) * r2[j];
+                    const float s = sigmoid(y) * r2[j];
+#pragma unroll
+                    for (int k = 0; k < kFeatures; ++k)
+                    {
+                        grad[k] = fmaf(s, r1[j * kFeatures + k], grad[k]);
+                    }
+                }
+                if (live)
+                {
+                    store_row(a.grad, row, grad);
+                    energy = e;
+                }
+            }
+        }
+    }
+    if (!ok && threadIdx.x == 0)
+    {
+        atomicOr(a.counters + 1, kProductLost);
+    }
+    if (kLast)
+    {
+        __shared__ double sums[4];
+        const double s = warp_sum(energy);
+        if ((threadIdx.x & 31) == 0)
+        {
+            sums[threadIdx.x / 32] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            a.energy[blockIdx.x] = ((sums[0] + sums[1]) + sums[2]) + sums[3];
+        }
+    }
+    cores.close(64);
+}
+
+// Reverse of one block's atom-wise layers: G += Gv' A' (the next block's messages), then
+// Gh = (G D2) * sigmoid(h) and Gm = Gh D1.
+__global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
+{
+    extern __shared__ __align__(1024) unsigned char shared[];
+    unsigned char* image_d2t = shared;
+    unsigned char* image_d1t = image_d2t + umma::kImageBytes;
+    unsigned char* image_at = image_d1t + umma::kImageBytes;
+    unsigned char* tile = image_at + umma::kImageBytes;
+    auto* barrier = reinterpret_cast<std::uint64_t*>(tile + umma::kTileBytes);
+    auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
+
+    copy_bytes(image_d2t, a.images + kD2T * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_d1t, a.images + kD1T * umma::kImageBytes, umma::kImageBytes);
+    const bool chained = a.grad_v != nullptr;
+    if (chained)
+    {
+        copy_bytes(image_at, a.next_images + kAT * umma::kImageBytes, umma::kImageBytes);
+    }
+    Cores cores;
+    cores.open(barrier, slot, 64);
+    const std::int64_t row = static_cast<std::int64_t>(blockIdx.x) * kTile + threadIdx.x;
+    const bool live = row < a.atoms;
+    bool ok = true;
+    float grad[kFeatures];
+    float values[kFeatures];
+    load_row(a.grad, row, live, grad);
+    if (chained)
+    {
+        load_row(a.grad_v, row, live, values);
+        store_tile_row(tile, values);
+        ok = cores.run(0, tile, image_at);
+        if (ok)
+        {
+            load_row_tmem(cores.tmem, values);
+#pragma unroll
+            for (int k = 0; k < kFeatures; ++k)
+            {
+                grad[k] += values[k];
+            }
+            if (live)
+            {
+                store_row(a.grad, row, grad);
+            }
+        }
+    }
+    if (ok)
+    {
+        store_tile_row(tile, grad);
+        ok = cores.run(0, tile, image_d2t);
+    }
+    if (ok)
+    {
+        float h[kFeatures];
+        load_row(a.h, row, live, h);
+        load_row_tmem(cores.tmem, values);
+#pragma unroll
+        for (int k = 0; k < kFeatures; ++k)
+        {
+            values[k] *= sigmoid(h[k]);
+        }
+        store_tile_row(tile, values);
+        ok = cores.run(0, tile, image_d1t);
+    }
+    if (ok)
+    {
+        load_row_tmem(cores.tmem, values);
+        if (live)
+        {
+            store_row(a.grad_m, row, values);
+        }
+    }
+    if (!ok && threadIdx.x == 0)
+    {
+        atomicOr(a.counters + 1, kProductLost);
+    }
+    cores.close(64);
+}
+
+// E and W from the per-CTA partials in a fixed order; the status word out.
+__global__ void finalize_kernel(const double* __restrict__ energy_partials, int energy_count,
+                                const double* __restrict__ virial_partials, int virial_count,
+                                double* energy, double* virial)
+{
+    __shared__ double sums[10][8];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x / 32;
+    double e = 0.0;
+    for (int i = threadIdx.x; i < energy_count; i += blockDim.x)
+    {
+        e += energy_partials[i];
+    }
+    e = warp_sum(e);
+    if (lane == 0)
+    {
+        sums[0][warp] = e;
+    }
+    for (int c = 0; c < 9; ++c)
+    {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < virial_count; i += blockDim.x)
+        {
+            s += virial_partials[9 * i + c];
+        }
+        s = warp_sum(s);
+        if (lane == 0)
+        {
+            sums[1 + c][warp] = s;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 10)
+    {
+        double total = 0.0;
+        for (int w = 0; w < 8; ++w)
+        {
+            total += sums[threadIdx.x][w];
+        }
+        if (threadIdx.x == 0)
+        {
+            if (energy != nullptr)
+            {
+                energy[0] = total;
+            }
+        }
+        else if (virial != nullptr)
+        {
+            virial[threadIdx.x - 1] = total;
+        }
+    }
+}
+
+int pair_grid(const void* kernel, int shared_bytes)
+{
+    static int sms = 0;
+    if (sms == 0)
+    {
+        int device = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTile, shared_bytes);
+    return std::max(1, per_sm) * std::max(1, sms);
+}
+
+}  // namespace
+}  // namespace nd
+
+extern "C" {
+
+int64_t nd_schnet_weight_bytes(int32_t interactions, int32_t num_types)
+{
+    if (interactions < 1 || num_types < 1)
+    {
+        return -1;
+    }
+    return nd::WeightLayout(interactions, num_types).total;
+}
+
+int64_t nd_schnet_workspace_bytes(int64_t num_atoms, int64_t num_columns, int32_t interactions)
+{
+    if (num_atoms < 1 || num_columns < 0 || interactions < 1)
+    {
+        return -1;
+    }
+    return nd::Workspace(num_atoms, num_columns, interactions).total;
+}
+
+int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream_handle)
+{
+    using namespace nd;
+    ND_REQUIRE(args != nullptr, "args is null");
+    const nd_schnet_args& s = *args;
+    ND_REQUIRE(s.num_atoms >= 1 && s.num_atoms <= (int64_t{1} << 30), "num_atoms out of range");
+    ND_REQUIRE(s.num_columns >= 0 && s.num_columns < (int64_t{1} << 31), "num_columns out of range");
+    ND_REQUIRE(s.interactions >= 1 && s.interactions <= 64, "interactions out of range");
+    ND_REQUIRE(s.num_types >= 1, "num_types must be positive");
+    ND_REQUIRE(s.gaussians >= 2 && s.gaussians <= 64, "gaussians must lie in [2, 64]");
+    ND_REQUIRE(s.cutoff > 0.0, "cutoff must be positive");
+    ND_REQUIRE(s.positions && s.cell && s.atom_types && s.weights && s.workspace && s.status,
+               "a required buffer is null");
+    ND_REQUIRE(s.num_columns == 0 || s.pairs != nullptr, "pairs is null");
+    ND_REQUIRE(reinterpret_cast<std::uintptr_t>(s.workspace) % 256 == 0 &&
+                   reinterpret_cast<std::uintptr_t>(s.weights) % 256 == 0,
+               "weights and workspace must be 256-byte aligned");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
+    const WeightLayout wl(s.interactions, s.num_types);
+    const Workspace ws(s.num_atoms, s.num_columns, s.interactions);
+    auto* weights = static_cast<const unsigned char*>(s.weights);
+    auto* base = static_cast<unsigned char*>(s.workspace);
+    auto at = [&](std::int64_t offset) { return base + offset; };
+    const std::int64_t row_bytes = align256(s.num_atoms * kFeatures * 4);
+    auto block_images = [&](int b) { return weights + static_cast<std::int64_t>(b) * kImagesPerBlock * umma::kImageBytes; };
+    auto block_vector = [&](int b, int j) {
+        return reinterpret_cast<const float*>(weights + wl.vectors + (static_cast<std::int64_t>(b) * 4 + j) * kFeatures * 4);
+    };
+    int* counters = reinterpret_cast<int*>(at(ws.counters));
+    auto* pairs = reinterpret_cast<int2*>(at(ws.pairs));
+    auto* geometry = reinterpret_cast<float4*>(at(ws.geometry));
+    auto* x = reinterpret_cast<float*>(at(ws.x));
+    auto v = [&](int b) { return reinterpret_cast<float*>(at(ws.v + b * row_bytes)); };
+    auto h = [&](int b) { return reinterpret_cast<float*>(at(ws.h + b * row_bytes)); };
+    auto* m = reinterpret_cast<float*>(at(ws.m));
+    auto* grad = reinterpret_cast<float*>(at(ws.grad));
+    auto* grad_m = reinterpret_cast<float*>(at(ws.grad_m));
+    auto* grad_v = reinterpret_cast<float*>(at(ws.grad_v));
+    auto* dedr = reinterpret_cast<float*>(at(ws.dedr));
+    auto* energy_partials = reinterpret_cast<double*>(at(ws.energy));
+    auto* virial_partials = reinterpret_cast<double*>(at(ws.virial));
+    const int atom_tiles = static_cast<int>((s.num_atoms + kTile - 1) / kTile);
+    const bool reverse = s.forces != nullptr || s.virial != nullptr;
+
+    static bool configured = false;
+    if (!configured)
+    {
+        ND_CUDA_TRY(cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairForwardShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairReverseShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(atom_forward_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(atom_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(atom_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        configured = true;
+    }
+    const int forward_grid = pair_grid(reinterpret_cast<const void*>(pair_forward_kernel), kPairForwardShared);
+    const int reverse_grid = std::min(kVirialSlots, pair_grid(reinterpret_cast<const void*>(pair_reverse_kernel), kPairReverseShared));
+
+    ND_CUDA_TRY(cudaMemsetAsync(counters, 0, 256, stream));
+    if (s.forces != nullptr)
+    {
+        ND_CUDA_TRY(cudaMemsetAsync(s.forces, 0, s.num_atoms * 3 * sizeof(float), stream));
+    }
+    if (s.num_columns > 0)
+    {
+        compact_kernel<<<blocks_for(s.num_columns), kThreads, 0, stream>>>(
+            s.positions, s.cell, s.pairs, s.num_columns, s.num_atoms,
+            static_cast<float>(s.cutoff * s.cutoff), pairs, geometry, counters);
+        ND_LAUNCH_CHECK();
+    }
+    embed_kernel<<<blocks_for(s.num_atoms * 16), kThreads, 0, stream>>>(
+        s.atom_types, s.num_atoms, reinterpret_cast<const float*>(weights + wl.tables),
+        reinterpret_cast<const float*>(weights + wl.tables + s.num_types * kFeatures * 4), x, v(0));
+    ND_LAUNCH_CHECK();
+
+    PairPass pass{};
+    pass.pairs = pairs;
+    pass.geometry = geometry;
+    pass.counters = counters;
+    pass.width = static_cast<float>(s.cutoff / (s.gaussians - 1));
+    pass.phase = static_cast<float>(3.14159265358979323846 / s.cutoff);
+    pass.gaussians = s.gaussians;
+    const float* readout = reinterpret_cast<const float*>(weights + wl.readout);
+    for (int b = 0; b < s.interactions; ++b)
+    {
+        const bool last = b == s.interactions - 1;
+        ND_CUDA_TRY(cudaMemsetAsync(m, 0, s.num_atoms * kFeatures * 4, stream));
+        pass.images = block_images(b);
+        pass.b1 = block_vector(b, 0);
+        pass.b2 = block_vector(b, 1);
+        pass.v = v(b);
+        pass.m = m;
+        pair_forward_kernel<<<forward_grid, kTile, kPairForwardShared, stream>>>(pass);
+        ND_LAUNCH_CHECK();
+        AtomPass atoms{};
+        atoms.atoms = s.num_atoms;
+        atoms.images = block_images(b);
+        atoms.next_images = last ? nullptr : block_images(b + 1);
+        atoms.d1 = block_vector(b, 2);
+        atoms.d2 = block_vector(b, 3);
+        atoms.m = m;
+        atoms.h = h(b);
+        atoms.x = x;
+        atoms.v_next = last ? nullptr : v(b + 1);
+        atoms.readout = readout;
+        atoms.grad = grad;
+        atoms.energy = energy_partials;
+        atoms.counters = counters;
+        if (last)
+        {
+            atom_forward_kernel<true><<<atom_tiles, kTile, kAtomShared, stream>>>(atoms);
+        }
+        else
+        {
+            atom_forward_kernel<false><<<atom_tiles, kTile, kAtomShared, stream>>>(atoms);
+        }
+        ND_LAUNCH_CHECK();
+    }
+    if (reverse)
+    {
+        ND_CUDA_TRY(cudaMemsetAsync(virial_partials, 0, kVirialSlots * 9 * sizeof(double), stream));
+        for (int b = s.interactions - 1; b >= 0; --b)
+        {
+            const bool last = b == s.interactions - 1;
+            AtomPass atoms{};
+            atoms.atoms = s.num_atoms;
+            atoms.images = block_images(b);
+            atoms.next_images = last ? nullptr : block_images(b + 1);
+            atoms.h = h(b);
+            atoms.grad = grad;
+            atoms.grad_v = last ? nullptr : grad_v;
+            atoms.grad_m = grad_m;
+            atoms.counters = counters;
+            atom_reverse_kernel<<<atom_tiles, kTile, kAtomShared, stream>>>(atoms);
+            ND_LAUNCH_CHECK();
+            if (b > 0)
+            {
+                ND_CUDA_TRY(cudaMemsetAsync(grad_v, 0, s.num_atoms * kFeatures * 4, stream));
+            }
+            pass.images = block_images(b);
+            pass.b1 = block_vector(b, 0);
+            pass.b2 = block_vector(b, 1);
+            pass.v = v(b);
+            pass.grad_m = grad_m;
+            pass.grad_v = b > 0 ? grad_v : nullptr;
+            pass.dedr = dedr;
+            pass.first = last ? 1 : 0;
+            pass.last = b == 0 ? 1 : 0;
+            pass.forces = s.forces;
+            pass.virial = virial_partials;
+            pair_reverse_kernel<<<reverse_grid, kTile, kPairReverseShared, stream>>>(pass);
+            ND_LAUNCH_CHECK();
+        }
+    }
+    finalize_kernel<<<1, 256, 0, stream>>>(energy_partials, atom_tiles, virial_partials,
+                                           reverse ? reverse_grid : 0, s.energy,
+                                           reverse ? s.virial : nullptr);
+    ND_LAUNCH_CHECK();
+    ND_CUDA_TRY(cudaMemcpyAsync(s.status, counters, 2 * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    return ND_OK;
+}
+
+}  // extern "C"

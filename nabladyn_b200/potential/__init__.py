@@ -2,5 +2,6 @@
 
 from ._base import Potential
 from ._lennard_jones import LennardJones, lennard_jones, pair_index
+from ._schnet import SchNet, schnet
 
-__all__ = ("Potential", "LennardJones", "lennard_jones", "pair_index")
+__all__ = ("Potential", "LennardJones", "lennard_jones", "pair_index", "SchNet", "schnet")

@@ -216,6 +216,9 @@ class _LJEnergy(torch.autograd.Function):
 class LennardJones(Potential):
     """12-6 Lennard-Jones shifted to zero at the cutoff; built by ``lennard_jones``."""
 
+    # E, F and W always come from the fused pair kernel (float32 and float64).
+    _fused_kernel = True
+
     def __init__(self, *, atom_types: Tensor, sigma: Tensor, epsilon: Tensor, cutoff: Real,
                  trainable=()):
         super().__init__()

@@ -5,9 +5,10 @@ The API of src/nabladyn/quantity.py:88-184: each function binds an energy, any c
 ``(positions, cell, pairs)``. E is in kJ/mol, F = -dE/dpositions [N, 3] in kJ/mol/nm and
 W = -dE/dstrain at zero strain [3, 3] in kJ/mol.
 
-For the Lennard-Jones model (the model itself, or its ``_energy_wrapped``) every binding runs
-the fused CUDA pair kernel once: E, F and W come out of the same pass, with E and W reduced in
-float64. Any other energy is differentiated by ``torch.func`` exactly as the reference does.
+For the Lennard-Jones model and float32 SchNet models of 64 features (the model itself, or its
+``_energy_wrapped``) every binding runs the fused CUDA kernels once: E, F and W come out of the
+same pass, with E and W reduced in float64. Any other energy is differentiated by
+``torch.func`` exactly as the reference does.
 """
 
 from collections.abc import Callable
@@ -16,24 +17,26 @@ import torch
 from torch import Tensor
 
 from .neighbors import NeighborPairs
-from .potential._base import _check_pairs, _check_tensor
-from .potential._lennard_jones import LennardJones
+from .potential._base import Potential, _check_pairs, _check_tensor
 from . import space
 
 
 def _fused(energy_fn):
-    """(model, wraps) when ``energy_fn`` is a Lennard-Jones model or its wrapped energy."""
-    if isinstance(energy_fn, LennardJones):
+    """(model, wraps) when ``energy_fn`` is a model with fused kernels (Lennard-Jones, or a
+    SchNet the kernels cover) or its wrapped energy."""
+    if isinstance(energy_fn, Potential) and getattr(energy_fn, "_fused_kernel", False):
         return energy_fn, True
     owner = getattr(energy_fn, "__self__", None)
-    if isinstance(owner, LennardJones) and getattr(energy_fn, "__func__", None) is (
-        LennardJones._energy_wrapped
+    if (
+        isinstance(owner, Potential)
+        and getattr(owner, "_fused_kernel", False)
+        and getattr(energy_fn, "__func__", None) is type(owner)._energy_wrapped
     ):
         return owner, False
     return None, False
 
 
-def _fused_evaluate(model: LennardJones, wraps: bool):
+def _fused_evaluate(model: Potential, wraps: bool):
     def evaluate(positions: Tensor, cell: Tensor, pairs: NeighborPairs):
         if wraps:
             # The model's own call checks its inputs and wraps the positions.

@@ -19,6 +19,11 @@ Fixtures:
   file's labels and the reference's float64 E/F/W for the generating rows.
 * lj_fit_gradient.npz — the reference's loss and its gradient in sigma and epsilon on those
   frames, from perturbed parameters (its training predict/loss under torch.func).
+* schnet_343.npz — 343 coarse-grained beads (7^3 simple-cubic sites at 10 per nm^3, 0.02 nm
+  seeded jitter, two seeded types), the reference's SchNet (64 features, 3 blocks, 50
+  Gaussians, cutoff 1.2 nm, seed 0) built in float64 and float32, its E/F/W over every pair
+  by quantity.energy_force_virial, and its seeded weights (also for one type, the bead
+  workload's topology) under its state-dict names.
 """
 
 import os
@@ -219,10 +224,43 @@ def lj_fit_gradient() -> None:
     )
 
 
+def schnet() -> None:
+    n_side, density, cutoff = 7, 10.0, 1.2
+    n = n_side**3
+    length = (n / density) ** (1.0 / 3.0)
+    rng = np.random.default_rng(343)
+    grid = np.stack(np.meshgrid(*(np.arange(n_side),) * 3, indexing="ij"), axis=-1).reshape(-1, 3)
+    positions = ((grid + 0.5) * (length / n_side) + rng.normal(0.0, 0.02, (n, 3))) % length
+    types = rng.permutation(np.arange(n) % 2)
+    cell = np.full(3, length)
+    # int64 columns: torch 2.11's CPU scatter_add takes no int32 index (the reference pins
+    # torch 2.13); the pair set is the same.
+    pairs = NeighborPairs(all_pairs(n).long(), n, cutoff)
+    out = {"positions": positions, "cell": cell, "atom_types": types, "cutoff": cutoff}
+    for dtype, tag in ((torch.float64, "64"), (torch.float32, "32")):
+        model = potential.schnet(atom_types=torch.tensor(types), num_types=2, cutoff=cutoff,
+                                 dtype=dtype)
+        e, f, w = quantity.energy_force_virial(model)(
+            torch.tensor(positions, dtype=dtype), torch.tensor(cell, dtype=dtype), pairs,
+        )
+        out[f"energy{tag}"] = e.detach().numpy()
+        out[f"forces{tag}"] = f.detach().numpy()
+        out[f"virial{tag}"] = w.detach().numpy()
+        if dtype == torch.float64:
+            for name, value in model.state_dict().items():
+                out[f"weight:{name}"] = value.numpy()
+    one_type = potential.schnet(atom_types=torch.zeros(4, dtype=torch.int64), num_types=1,
+                                cutoff=cutoff, dtype=torch.float64)
+    for name in ("embedding", "blocks.0.atoms.weight", "readout2.weight"):
+        out[f"weight1:{name}"] = one_type.state_dict()[name].numpy()
+    np.savez_compressed(OUT / "schnet_343.npz", **out)
+
+
 if __name__ == "__main__":
     torch.set_num_threads(os.cpu_count() or 1)
     argon()
     md()
     lj_frames()
     lj_fit_gradient()
+    schnet()
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))

@@ -1,0 +1,84 @@
+"""SchNet on the CPU: the float64 oracle against the reference's own numbers, the model's
+seeded weights against the reference's, and the parameter block's layout.
+
+The fixture tests/golden/schnet_343.npz holds the reference's SchNet (seed 0, 64 features,
+3 blocks, 50 Gaussians, cutoff 1.2 nm) evaluated by its quantity.energy_force_virial on 343
+beads, and its weights under its state-dict names.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from nabladyn_b200 import potential, quantity
+from nabladyn_b200.neighbors import NeighborPairs
+from nabladyn_b200.potential import _schnet_kernels
+from oracle import schnet as oracle
+
+GOLDEN = "tests/golden/schnet_343.npz"
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return dict(np.load(GOLDEN))
+
+
+def weights_of(golden, prefix="weight:"):
+    return {k[len(prefix):]: v for k, v in golden.items() if k.startswith(prefix)}
+
+
+def test_oracle_matches_reference(golden):
+    n = golden["positions"].shape[0]
+    first, second = np.triu_indices(n, 1)
+    e, f, w = oracle.energy_force_virial(golden["positions"], golden["cell"], first, second,
+                                         golden["atom_types"], weights_of(golden), 1.2, 50, 3)
+    assert e == pytest.approx(float(golden["energy64"]), rel=1e-12)
+    np.testing.assert_allclose(f, golden["forces64"], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(w, golden["virial64"], rtol=1e-10, atol=1e-9)
+
+
+def test_seeded_weights_match_reference(golden):
+    types = torch.tensor(golden["atom_types"])
+    model = potential.schnet(atom_types=types, num_types=2, cutoff=1.2, dtype=torch.float64)
+    ours = model.state_dict()
+    reference = weights_of(golden)
+    assert sorted(ours) == sorted(reference)
+    for name, value in reference.items():
+        np.testing.assert_array_equal(ours[name].numpy(), value, err_msg=name)
+    one = potential.schnet(atom_types=torch.zeros(4, dtype=torch.int64), num_types=1,
+                           cutoff=1.2, dtype=torch.float64).state_dict()
+    for name, value in weights_of(golden, "weight1:").items():
+        np.testing.assert_array_equal(one[name].numpy(), value, err_msg=name)
+
+
+def test_torch_definition_matches_reference(golden):
+    """The model's own definition (the torch.func path float64 models take)."""
+    n = golden["positions"].shape[0]
+    model = potential.schnet(atom_types=torch.tensor(golden["atom_types"]), num_types=2,
+                             cutoff=1.2, dtype=torch.float64)
+    first, second = np.triu_indices(n, 1)
+    pairs = NeighborPairs(torch.tensor(np.stack([first, second]), dtype=torch.int32), n, 1.2)
+    e, f, w = quantity.energy_force_virial(model)(
+        torch.tensor(golden["positions"]), torch.tensor(golden["cell"]), pairs)
+    assert float(e) == pytest.approx(float(golden["energy64"]), rel=1e-12)
+    np.testing.assert_allclose(f.numpy(), golden["forces64"], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(w.numpy(), golden["virial64"], rtol=1e-10, atol=1e-9)
+
+
+def test_parameter_block_layout(golden):
+    model = potential.schnet(atom_types=torch.tensor(golden["atom_types"]), num_types=2,
+                             cutoff=1.2)
+    blob = _schnet_kernels.pack(model)
+    assert blob.numel() == _schnet_kernels.weight_bytes(3, 2)
+    images = blob[: 3 * 10 * 8192].view(torch.bfloat16).reshape(3, 10, 4096).float()
+    w = model.blocks[1].filter2.weight.detach().to(torch.bfloat16).float()
+    for row, k in ((0, 0), (5, 9), (17, 63), (63, 40)):
+        offset = (row // 8) * 512 + (k // 8) * 64 + (row % 8) * 8 + k % 8
+        assert images[1, 1, offset] == w[row, k]          # filter2
+        assert images[1, 2, offset] == w[k, row]          # filter2^T
+    b1 = model.blocks[0].filter1.weight.detach().to(torch.bfloat16).float()
+    for row, k in ((3, 49), (3, 50), (63, 63)):
+        offset = (row // 8) * 512 + (k // 8) * 64 + (row % 8) * 8 + k % 8
+        assert images[0, 0, offset] == (b1[row, k] if k < 50 else 0.0)    # filter1
+        assert images[0, 3, offset] == (b1[k, row] if row < 50 else 0.0)   # filter1^T
+    assert _schnet_kernels.workspace_bytes(343, 58653, 3) > 0
