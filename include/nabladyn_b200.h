@@ -363,8 +363,10 @@ typedef struct nd_schnet_args {
     double* energy;             /* [1] */
     float* forces;              /* [N, 3] or NULL */
     double* virial;             /* [9] or NULL */
-    int32_t* status;            /* [2]: pairs within the cutoff, status bits (1: a pair index
-                                   out of range; 16: a tensor-core product did not complete) */
+    int32_t* status;            /* [4]: pairs within the cutoff, status bits (1: a pair index
+                                   out of range; 16: a tensor-core product did not complete
+                                   within its bounded wait), and for that case the first
+                                   kernel stage (16 * kernel + product) and tile that gave up */
 } nd_schnet_args;
 
 int64_t nd_schnet_weight_bytes(int32_t interactions, int32_t num_types);

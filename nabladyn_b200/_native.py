@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import ctypes
 from pathlib import Path
-from threading import Lock
+from threading import RLock
 
 import torch
 
@@ -21,7 +21,8 @@ ND_OK, ND_EINVAL, ND_ECUDA = 0, 1, 2
 ND_FLOAT32, ND_FLOAT64 = 0, 1
 INVALID_CELL, NON_FINITE, OVERFLOW = 1, 2, 8
 
-_LOCK = Lock()
+# Reentrant: neighbor_ops() loads the core library under the same lock.
+_LOCK = RLock()
 _lib: ctypes.CDLL | None = None
 _ops_loaded = False
 

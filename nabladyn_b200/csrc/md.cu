@@ -154,14 +154,23 @@ __device__ __forceinline__ bool barrier_try_wait(std::uint64_t* barrier, unsigne
     return done != 0;
 }
 
-// Waits for phase 0 of the barrier, at most kWaitLimit polls; false when it gave up.
+// Waits for phase 0 of the barrier, at most kWaitLimit polls and 0.5 s (a poll may suspend
+// the thread for a while); false when it gave up.
 __device__ __forceinline__ bool barrier_wait_bounded(std::uint64_t* barrier)
 {
+    std::uint64_t start;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(start));
     for (int poll = 0; poll < kWaitLimit; ++poll)
     {
         if (barrier_try_wait(barrier, 0))
         {
             return true;
+        }
+        std::uint64_t now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (now - start > 500000000ull)
+        {
+            return false;
         }
     }
     return false;

@@ -146,11 +146,15 @@ struct Cores
     std::uint32_t tmem;  // this warp's lanes, column 0
     unsigned phase;
 
-    __device__ void open(std::uint64_t* barrier_, std::uint32_t* slot_, std::uint32_t columns)
+    __device__ void open(std::uint64_t* barrier_, std::uint32_t* slot_, std::uint32_t columns,
+                         int* counters_, int stage_)
     {
         barrier = barrier_;
         slot = slot_;
         phase = 0;
+        counters = counters_;
+        stage = stage_;
+        tile_index = -1;
         if (threadIdx.x == 0)
         {
             umma::barrier_init(barrier);
@@ -165,9 +169,15 @@ struct Cores
         tmem = *slot + ((32u * (threadIdx.x / 32)) << 16);
     }
 
+    int* counters;  // [4]: pairs, status bits, first stage that gave up, its tile
+    int stage;      // the kernel's stage code, for the diagnostics
+    int tile_index; // the tile in work, for the diagnostics
+
     // D[column offset] = tile * image^T, after every thread wrote its row of the tile; waits
-    // for the product. False (on every thread) when it did not complete in time.
-    __device__ bool run(std::uint32_t column, const unsigned char* tile, const unsigned char* image)
+    // for the product. False (on every thread) when it did not complete in time; then the
+    // status bit is set and the first stage and tile that gave up are recorded.
+    __device__ bool run(std::uint32_t column, const unsigned char* tile, const unsigned char* image,
+                        int step)
     {
         umma::fence_operands();
         umma::fence_before_sync();
@@ -182,6 +192,14 @@ struct Cores
         phase ^= 1u;
         const bool lost = __syncthreads_or(!done);
         umma::fence_after_sync();
+        if (lost && threadIdx.x == 0)
+        {
+            atomicOr(counters + 1, kProductLost);
+            if (atomicCAS(counters + 2, 0, 16 * stage + step) == 0)
+            {
+                counters[3] = tile_index;
+            }
+        }
         return !lost;
     }
 
@@ -343,7 +361,7 @@ __global__ void __launch_bounds__(kTile) pair_forward_kernel(PairPass a)
         bias2[threadIdx.x] = a.b2[threadIdx.x];
     }
     Cores cores;
-    cores.open(barrier, slot, 64);
+    cores.open(barrier, slot, 64, a.counters, 1);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
     const float4* v4 = reinterpret_cast<const float4*>(a.v);
     float4* m4 = reinterpret_cast<float4*>(a.m);
@@ -360,13 +378,10 @@ __global__ void __launch_bounds__(kTile) pair_forward_kernel(PairPass a)
             g = a.geometry[p];
         }
         const float envelope = live ? 0.5f * (__cosf(g.w * a.phase) + 1.0f) : 0.0f;
+        cores.tile_index = tile;
         store_basis(basis, g.w / a.width, a.gaussians, live);
-        if (!cores.run(0, basis, image_b1))
+        if (!cores.run(0, basis, image_b1, 1))
         {
-            if (threadIdx.x == 0)
-            {
-                atomicOr(a.counters + 1, kProductLost);
-            }
             break;
         }
 #pragma unroll
@@ -387,12 +402,8 @@ __global__ void __launch_bounds__(kTile) pair_forward_kernel(PairPass a)
                 umma::store8(work, threadIdx.x, 4 * half + c, s);
             }
         }
-        if (!cores.run(0, work, image_b2))
+        if (!cores.run(0, work, image_b2, 2))
         {
-            if (threadIdx.x == 0)
-            {
-                atomicOr(a.counters + 1, kProductLost);
-            }
             break;
         }
 #pragma unroll
@@ -464,13 +475,12 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
     }
     // Columns 0-63 keep z1 - b1 for the whole tile; 64-127 take the other products in turn.
     Cores cores;
-    cores.open(barrier, slot, 128);
+    cores.open(barrier, slot, 128, a.counters, 2);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
     const float4* v4 = reinterpret_cast<const float4*>(a.v);
     const float4* gm4 = reinterpret_cast<const float4*>(a.grad_m);
     float4* gv4 = reinterpret_cast<float4*>(a.grad_v);
     double w[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
-    bool lost = false;
 
     for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
     {
@@ -488,10 +498,10 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
         const float envelope = live ? 0.5f * (cosine + 1.0f) : 0.0f;
         const float slope = live ? -0.5f * a.phase * sine : 0.0f;
         const float t = g.w / a.width;
+        cores.tile_index = tile;
         store_basis(basis, t, a.gaussians, live);
-        if (!cores.run(0, basis, image_b1))
+        if (!cores.run(0, basis, image_b1, 1))
         {
-            lost = true;
             break;
         }
         // ssp(z1) into the work tile; z1 - b1 stays in columns 0-63.
@@ -513,9 +523,8 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
                 umma::store8(work, threadIdx.x, 4 * half + c, s);
             }
         }
-        if (!cores.run(64, work, image_b2))
+        if (!cores.run(64, work, image_b2, 2))
         {
-            lost = true;
             break;
         }
         // f_raw, Gf = Gm_a v_b + Gm_b v_a, C' Gf . f_raw, Gv, and Gf C into the work tile.
@@ -567,9 +576,8 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
                 umma::store8(work, threadIdx.x, 4 * half + c, scaled);
             }
         }
-        if (!cores.run(64, work, image_b2t))
+        if (!cores.run(64, work, image_b2t, 3))
         {
-            lost = true;
             break;
         }
         // ((Gf C) B2) * sigmoid(z1) into the work tile.
@@ -593,9 +601,8 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
                 umma::store8(work, threadIdx.x, 4 * half + c, s);
             }
         }
-        if (!cores.run(64, work, image_b1t))
+        if (!cores.run(64, work, image_b1t, 4))
         {
-            lost = true;
             break;
         }
         // dE/dr = C' Gf . f_raw + sum_k [..]_k g_k', g_k' = -g_k (r / D - k) / D.
@@ -651,10 +658,6 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
                 w[5] -= static_cast<double>(uy) * g.z;
             }
         }
-    }
-    if (lost && threadIdx.x == 0)
-    {
-        atomicOr(a.counters + 1, kProductLost);
     }
     if (a.last && a.virial != nullptr)
     {
@@ -798,7 +801,8 @@ __global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
         bias2[threadIdx.x] = a.d2[threadIdx.x];
     }
     Cores cores;
-    cores.open(barrier, slot, 64);
+    cores.open(barrier, slot, 64, a.counters, 3);
+    cores.tile_index = blockIdx.x;
     const std::int64_t row = static_cast<std::int64_t>(blockIdx.x) * kTile + threadIdx.x;
     const bool live = row < a.atoms;
     double energy = 0.0;
@@ -807,7 +811,7 @@ __global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
         float values[kFeatures];
         load_row(a.m, row, live, values);
         store_tile_row(tile, values);
-        ok = cores.run(0, tile, image_d1);
+        ok = cores.run(0, tile, image_d1, 1);
         if (ok)
         {
             load_row_tmem(cores.tmem, values);
@@ -826,7 +830,7 @@ __global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
                 values[k] = softplus_shifted(values[k]);
             }
             store_tile_row(tile, values);
-            ok = cores.run(0, tile, image_d2);
+            ok = cores.run(0, tile, image_d2, 2);
         }
         if (ok)
         {
@@ -845,7 +849,7 @@ __global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
                     store_row(a.x, row, x);
                 }
                 store_tile_row(tile, x);
-                ok = cores.run(0, tile, image_a);
+                ok = cores.run(0, tile, image_a, 3);
                 if (ok)
                 {
                     load_row_tmem(cores.tmem, values);
@@ -892,10 +896,6 @@ __global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
             }
         }
     }
-    if (!ok && threadIdx.x == 0)
-    {
-        atomicOr(a.counters + 1, kProductLost);
-    }
     if (kLast)
     {
         __shared__ double sums[4];
@@ -933,7 +933,8 @@ __global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
         copy_bytes(image_at, a.next_images + kAT * umma::kImageBytes, umma::kImageBytes);
     }
     Cores cores;
-    cores.open(barrier, slot, 64);
+    cores.open(barrier, slot, 64, a.counters, 4);
+    cores.tile_index = blockIdx.x;
     const std::int64_t row = static_cast<std::int64_t>(blockIdx.x) * kTile + threadIdx.x;
     const bool live = row < a.atoms;
     bool ok = true;
@@ -944,7 +945,7 @@ __global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
     {
         load_row(a.grad_v, row, live, values);
         store_tile_row(tile, values);
-        ok = cores.run(0, tile, image_at);
+        ok = cores.run(0, tile, image_at, 1);
         if (ok)
         {
             load_row_tmem(cores.tmem, values);
@@ -962,7 +963,7 @@ __global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
     if (ok)
     {
         store_tile_row(tile, grad);
-        ok = cores.run(0, tile, image_d2t);
+        ok = cores.run(0, tile, image_d2t, 2);
     }
     if (ok)
     {
@@ -975,7 +976,7 @@ __global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
             values[k] *= sigmoid(h[k]);
         }
         store_tile_row(tile, values);
-        ok = cores.run(0, tile, image_d1t);
+        ok = cores.run(0, tile, image_d1t, 3);
     }
     if (ok)
     {
@@ -984,10 +985,6 @@ __global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
         {
             store_row(a.grad_m, row, values);
         }
-    }
-    if (!ok && threadIdx.x == 0)
-    {
-        atomicOr(a.counters + 1, kProductLost);
     }
     cores.close(64);
 }
@@ -1239,7 +1236,7 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
                                            reverse ? reverse_grid : 0, s.energy,
                                            reverse ? s.virial : nullptr);
     ND_LAUNCH_CHECK();
-    ND_CUDA_TRY(cudaMemcpyAsync(s.status, counters, 2 * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    ND_CUDA_TRY(cudaMemcpyAsync(s.status, counters, 4 * sizeof(int), cudaMemcpyDeviceToDevice, stream));
     return ND_OK;
 }
 

@@ -27,6 +27,7 @@ constexpr int kCols = 64;           // N and K of every product
 constexpr int kImageBytes = 64 * 64 * 2;   // one 64 x 64 BF16 weight image
 constexpr int kTileBytes = 128 * 64 * 2;   // one 128 x 64 BF16 row tile
 constexpr int kWaitLimit = 1 << 22;        // mbarrier polls before a product counts as lost
+constexpr std::uint64_t kWaitNanoseconds = 500000000;  // and at most 0.5 s of waiting
 
 // Byte offset of element (row, k) in an operand image.
 __host__ __device__ constexpr std::uint32_t image_offset(int row, int k)
@@ -103,9 +104,11 @@ __device__ __forceinline__ void fence_operands()
 }
 
 // Tensor-memory allocation of `columns` (a power of two, at least 32), by one whole warp;
-// the base address lands in `*slot`.
+// the base address lands in `*slot`. Like every .sync.aligned instruction here it needs the
+// warp converged, which __syncwarp() guarantees after data-dependent branches.
 __device__ __forceinline__ void allocate(std::uint32_t* slot, std::uint32_t columns)
 {
+    __syncwarp();
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_address(slot)),
                  "r"(columns)
@@ -115,6 +118,7 @@ __device__ __forceinline__ void allocate(std::uint32_t* slot, std::uint32_t colu
 
 __device__ __forceinline__ void deallocate(std::uint32_t tmem, std::uint32_t columns)
 {
+    __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(columns)
                  : "memory");
@@ -125,6 +129,7 @@ __device__ __forceinline__ void deallocate(std::uint32_t tmem, std::uint32_t col
 __device__ __forceinline__ void load32(std::uint32_t tmem, float (&out)[32])
 {
     std::uint32_t r[32];
+    __syncwarp();
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
         "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
@@ -145,6 +150,7 @@ __device__ __forceinline__ void load32(std::uint32_t tmem, float (&out)[32])
 
 __device__ __forceinline__ void wait_loads()
 {
+    __syncwarp();
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
@@ -167,14 +173,27 @@ __device__ __forceinline__ bool barrier_test(std::uint64_t* barrier, unsigned ph
     return done != 0;
 }
 
-// Waits for `phase` of the barrier, at most kWaitLimit polls; false when it gave up.
+__device__ __forceinline__ std::uint64_t nanoseconds()
+{
+    std::uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for `phase` of the barrier, at most kWaitLimit polls and kWaitNanoseconds (a poll
+// may suspend the thread for a while); false when it gave up.
 __device__ __forceinline__ bool barrier_wait(std::uint64_t* barrier, unsigned phase)
 {
+    const std::uint64_t start = nanoseconds();
     for (int poll = 0; poll < kWaitLimit; ++poll)
     {
         if (barrier_test(barrier, phase))
         {
             return true;
+        }
+        if (nanoseconds() - start > kWaitNanoseconds)
+        {
+            return false;
         }
     }
     return false;

@@ -50,8 +50,16 @@ def shifted_softplus(x: Tensor) -> Tensor:
 
 
 def _dense(inputs: int, outputs: int, bias: bool = True) -> nn.Linear:
-    """A float64 layer whose values the model's seed sets afterwards."""
-    return nn.utils.skip_init(nn.Linear, inputs, outputs, bias=bias, dtype=torch.float64)
+    """An uninitialised float64 ``nn.Linear`` (weight, then bias); the model's seed sets it."""
+    layer = nn.Linear.__new__(nn.Linear)
+    nn.Module.__init__(layer)
+    layer.in_features, layer.out_features = inputs, outputs
+    layer.weight = nn.Parameter(torch.empty((outputs, inputs), dtype=torch.float64))
+    if bias:
+        layer.bias = nn.Parameter(torch.empty(outputs, dtype=torch.float64))
+    else:
+        layer.register_parameter("bias", None)
+    return layer
 
 
 class _Interaction(nn.Module):

@@ -87,7 +87,8 @@ def energy_force_virial(model, positions: Tensor, cell: Tensor, pairs: NeighborP
                         forces: bool = True, virial: bool = True):
     """(E, F [N, 3], W [3, 3]) in the model's dtype from the fused kernels; positions wrapped.
 
-    The count of pairs within the cutoff and the status bits land in ``model._status`` [2]
+    The count of pairs within the cutoff, the status bits and the diagnostics of a tensor-core
+    product that did not complete land in ``model._status`` [4]
     (int32, on the device; read without a sync only when wanted).
     """
     device = positions.device
@@ -103,7 +104,7 @@ def energy_force_virial(model, positions: Tensor, cell: Tensor, pairs: NeighborP
     energy = torch.empty(1, dtype=torch.float64, device=device)
     out_forces = torch.empty((n, 3), dtype=torch.float32, device=device) if forces else None
     out_virial = torch.empty(9, dtype=torch.float64, device=device) if virial else None
-    status = torch.empty(2, dtype=torch.int32, device=device)
+    status = torch.empty(4, dtype=torch.int32, device=device)
     positions = positions.contiguous()
     cell = cell.contiguous()
     args = SchNetArgs(

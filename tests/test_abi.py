@@ -105,3 +105,17 @@ def test_replica_record_layout_and_pool_allocator():
     server._give(b, 5)
     assert server._free_units == [(0, total)]
     assert server._take(total + 1) is None
+
+
+def test_torch_ops_load_first_in_a_fresh_process():
+    """Loading the torch.library layer before any other native call (a NeighborList as the
+    first use) loads the core library under the same lock and returns."""
+    import subprocess
+    import sys
+
+    code = ("from nabladyn_b200 import _native; ops = _native.neighbor_ops(); "
+            "print(ops.scan_temp_bytes is not None)")
+    done = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                          timeout=120)
+    assert done.returncode == 0, done.stderr
+    assert done.stdout.strip() == "True"
