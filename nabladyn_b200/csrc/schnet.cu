@@ -1042,7 +1042,10 @@ __global__ void finalize_kernel(const double* __restrict__ energy_partials, int 
     }
 }
 
-int pair_grid(const void* kernel, int shared_bytes)
+// Resident CTAs per SM times the SM count, for a persistent grid: the least of the register
+// file, shared memory (227 KB a CTA can use, 1 KB reserved per CTA) and tensor memory (512
+// columns) over one CTA's needs.
+int pair_grid(const void* kernel, int shared_bytes, int tmem_columns)
 {
     static int sms = 0;
     if (sms == 0)
@@ -1051,9 +1054,18 @@ int pair_grid(const void* kernel, int shared_bytes)
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTile, shared_bytes);
-    return std::max(1, per_sm) * std::max(1, sms);
+    int per_sm = 1;
+    cudaFuncAttributes attributes{};
+    if (cudaFuncGetAttributes(&attributes, kernel) == cudaSuccess)
+    {
+        const int registers = ((attributes.numRegs * 32 + 255) / 256) * 256 * (kTile / 32);
+        const int by_registers = 65536 / std::max(1, registers);
+        const int by_shared =
+            (228 * 1024) / (shared_bytes + static_cast<int>(attributes.sharedSizeBytes) + 1024);
+        per_sm = std::max(1, std::min({by_registers, by_shared, 512 / tmem_columns}));
+    }
+    cudaGetLastError();
+    return per_sm * std::max(1, sms);
 }
 
 }  // namespace
@@ -1131,10 +1143,12 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
         ND_CUDA_TRY(cudaFuncSetAttribute(atom_forward_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
         ND_CUDA_TRY(cudaFuncSetAttribute(atom_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
         ND_CUDA_TRY(cudaFuncSetAttribute(atom_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
         configured = true;
     }
-    const int forward_grid = pair_grid(reinterpret_cast<const void*>(pair_forward_kernel), kPairForwardShared);
-    const int reverse_grid = std::min(kVirialSlots, pair_grid(reinterpret_cast<const void*>(pair_reverse_kernel), kPairReverseShared));
+    const int forward_grid = pair_grid(reinterpret_cast<const void*>(pair_forward_kernel), kPairForwardShared, 64);
+    const int reverse_grid = std::min(kVirialSlots, pair_grid(reinterpret_cast<const void*>(pair_reverse_kernel), kPairReverseShared, 128));
 
     ND_CUDA_TRY(cudaMemsetAsync(counters, 0, 256, stream));
     if (s.forces != nullptr)
