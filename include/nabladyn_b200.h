@@ -373,6 +373,33 @@ int64_t nd_schnet_weight_bytes(int32_t interactions, int32_t num_types);
 int64_t nd_schnet_workspace_bytes(int64_t num_atoms, int64_t num_columns, int32_t interactions);
 int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream);
 
+/* ---- Integrator of frames in the caller's order ------------------------------------------
+ * Velocity Verlet with the Nose-Hoover chain of three (src/nabladyn/md/_ensembles/_nve.py:39-58,
+ * _nvt.py:88-129, _chain.py:23-105) for any potential: the caller runs its neighbor update and
+ * forces between nd_integrate_open and nd_integrate_close. The thermostat block has the MD
+ * engine's layout (nd_md_system.thermostat); totals[1] gets the step's K, totals[9] the K of
+ * nd_integrate_kinetic. Replaces the ensemble halves the reference compiles with Inductor. */
+typedef struct nd_integrator {
+    int dtype;               /* ND_FLOAT32 or ND_FLOAT64 */
+    int64_t num_atoms;
+    void* positions;         /* [N, 3], wrapped into [0, L) */
+    void* velocities;        /* [N, 3] (the pending chain factor not yet applied) */
+    const void* forces;      /* [N, 3] */
+    const void* masses;      /* [N] */
+    int64_t* images;         /* [N, 3] */
+    const void* cell;        /* [3] */
+    double* thermostat;      /* [24] */
+    double* partials;        /* [nd_integrate_partial_slots] */
+    double* totals;          /* [16] */
+    int32_t* status;         /* [1]: bit 2 a non-finite coordinate */
+    double timestep;         /* ps */
+} nd_integrator;
+
+int nd_integrate_partial_slots(int64_t num_atoms, int64_t* slots);
+int nd_integrate_open(const nd_integrator* s, int thermostat, nd_stream_t stream);
+int nd_integrate_close(const nd_integrator* s, int thermostat, nd_stream_t stream);
+int nd_integrate_kinetic(const nd_integrator* s, int thermostat, nd_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

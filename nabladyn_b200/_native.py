@@ -227,6 +227,24 @@ class SchNetArgs(ctypes.Structure):
     ]
 
 
+class Integrator(ctypes.Structure):
+    _fields_ = [
+        ("dtype", ctypes.c_int),
+        ("num_atoms", ctypes.c_int64),
+        ("positions", ctypes.c_void_p),
+        ("velocities", ctypes.c_void_p),
+        ("forces", ctypes.c_void_p),
+        ("masses", ctypes.c_void_p),
+        ("images", ctypes.c_void_p),
+        ("cell", ctypes.c_void_p),
+        ("thermostat", ctypes.c_void_p),
+        ("partials", ctypes.c_void_p),
+        ("totals", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("timestep", ctypes.c_double),
+    ]
+
+
 # name -> (argument types); every entry point returns int.
 _SIGNATURES = {
     "nd_abi_version": [],
@@ -274,6 +292,10 @@ _SIGNATURES = {
         ctypes.c_int32, ctypes.c_void_p,
     ],
     "nd_schnet_energy_force_virial": [ctypes.POINTER(SchNetArgs), ctypes.c_void_p],
+    "nd_integrate_partial_slots": [ctypes.c_int64, c_int64_p],
+    "nd_integrate_open": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],
+    "nd_integrate_close": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],
+    "nd_integrate_kinetic": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],
 }
 
 # name -> (argument types) of the entry points that return a byte count (int64, -1 on error).

@@ -23,7 +23,7 @@ INCLUDE = ROOT / "include"
 LIB = PACKAGE / "_lib"
 OBJ = LIB / "obj"
 
-CUDA_SOURCES = ("neighbors.cu", "lj.cu", "md.cu", "serve.cu", "schnet.cu")
+CUDA_SOURCES = ("neighbors.cu", "lj.cu", "md.cu", "serve.cu", "schnet.cu", "integrate.cu")
 CXX_SOURCES = ("abi.cpp",)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # IEEE arithmetic as in the reference build: no fast math, no flush-to-zero.

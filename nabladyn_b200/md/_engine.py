@@ -241,7 +241,7 @@ class Engine:
         th[CHAIN_A + 3:CHAIN_A + 6] = momenta.detach().cpu().double()
         th[KINETIC_A] = kinetic
         th[PENDING_SCALE] = 1.0
-        th[CHAIN_MASS:CHAIN_MASS + 3] = torch.tensor([degrees * base, base, base])
+        th[CHAIN_MASS:CHAIN_MASS + 3] = torch.tensor([degrees * base, base, base], dtype=torch.float64)
         th[THERMAL_ENERGY] = kT
         th[DEGREES] = degrees
         th[TIMESTEP] = self.system.timestep

@@ -2,9 +2,11 @@
 
 Mirrors src/nabladyn/md/_simulation.py (Simulation :126-421, nve/nvt in _ensembles): the same
 constructors, ``run`` / ``sample`` / ``state`` contract, panel fields, status polling every
-1,000 steps and failure latching. The step itself is the engine's (md.cu): a drift kernel with
-the reuse check, the rebuild behind a device flag, and a force kernel with the second half
-kick and the float64 tail; ``run`` replays graphs of one step and of ``_CHUNK`` steps.
+1,000 steps and failure latching. For Lennard-Jones the step is the engine's (md.cu): a drift
+kernel with the reuse check, the rebuild behind a device flag, and a force kernel with the
+second half kick and the float64 tail. Any other model runs in the pair engine
+(``PairEngine``: the integrator kernels, the neighbor operator and the model's forces, fused
+tensor-core kernels for SchNet). ``run`` replays graphs of one step and of ``_CHUNK`` steps.
 """
 
 from __future__ import annotations
@@ -22,9 +24,18 @@ from ..potential import Potential
 from ..potential._lennard_jones import LennardJones
 from ..units import BOLTZMANN
 from ._engine import CHAIN_A, CHAIN_MASS, DEGREES, PENDING_SCALE, THERMAL_ENERGY, Engine
+from ._pair_engine import PairEngine
 from ._state import ChainState, State
 
 _STATUS_INTERVAL = 1000  # steps between reads of the status
+
+
+def _kernel_types(model):
+    """The int32 types the Lennard-Jones engine takes for a multi-type model, else None."""
+    if isinstance(model, LennardJones) and model.num_types > 1:
+        return model._kernel_types
+    return None
+
 _CHUNK = 64  # steps per replay of the long graph
 FIELDS = ("potential_energy", "kinetic_energy", "total_energy", "temperature", "pressure")
 
@@ -97,8 +108,6 @@ class Simulation:
     ):
         if not isinstance(model, Potential):
             raise TypeError("model must be a Potential")
-        if not isinstance(model, LennardJones):
-            raise TypeError("the B200 MD engine runs Lennard-Jones models")
         num_atoms, device = model.num_atoms, model.device
         _check_frame(model, positions, velocities, masses, cell)
         if images is None:
@@ -130,25 +139,37 @@ class Simulation:
         if self._thermostat and num_atoms < 2:
             raise ValueError("NVT needs at least 2 atoms, for 3N - 3 degrees of freedom")
         cell = cell.detach().clone()
-        self._engine = Engine(
-            num_types=model.num_types,
-            sigma=model.sigma,
-            epsilon=model.epsilon,
-            cutoff=model.cutoff,
-            cell=cell,
-            num_atoms=num_atoms,
-            timestep=timestep,
-            skin=float(skin),
-            capacity_multiplier=float(capacity_multiplier),
-            dtype=model.dtype,
-            device=device,
-        )
+        if isinstance(model, LennardJones):
+            self._engine = Engine(
+                num_types=model.num_types,
+                sigma=model.sigma,
+                epsilon=model.epsilon,
+                cutoff=model.cutoff,
+                cell=cell,
+                num_atoms=num_atoms,
+                timestep=timestep,
+                skin=float(skin),
+                capacity_multiplier=float(capacity_multiplier),
+                dtype=model.dtype,
+                device=device,
+            )
+        else:
+            self._engine = PairEngine(
+                model=model,
+                cell=cell,
+                num_atoms=num_atoms,
+                timestep=timestep,
+                skin=float(skin),
+                capacity_multiplier=float(capacity_multiplier),
+                dtype=model.dtype,
+                device=device,
+            )
         wrapped, crossings = space.wrap(positions.detach(), cell)
         # The center-of-mass velocity is a constant of motion; at zero it leaves 3N - 3 degrees
         # of freedom for the temperature and the thermostat.
         column = masses[:, None]
         velocities = velocities - (column * velocities).sum(dim=0) / masses.sum()
-        types = model._kernel_types if model.num_types > 1 else None
+        types = _kernel_types(model)
         self._engine.load(wrapped, velocities, masses, images + crossings, types)
         self._model, self._masses, self._timestep, self._cell = model, masses, timestep, cell
         self._degrees_of_freedom = 3 * num_atoms - 3
@@ -302,7 +323,7 @@ class Simulation:
         if images is None:
             images = torch.zeros((model.num_atoms, 3), dtype=torch.int64, device=model.device)
         wrapped, crossings = space.wrap(positions.detach(), self._cell)
-        types = model._kernel_types if model.num_types > 1 else None
+        types = _kernel_types(model)
         self._engine.reload(wrapped, velocities.detach(), self._masses, images + crossings, types)
         if self._thermostat:
             self._engine.thermostat[PENDING_SCALE] = 1.0

@@ -83,13 +83,29 @@ def packed(model) -> Tensor:
     return model._packed[1]
 
 
+def launch(model, positions: Tensor, cell: Tensor, index: Tensor, *, energy: Tensor,
+           forces: Tensor | None, virial: Tensor | None, status: Tensor,
+           workspace: Tensor) -> None:
+    """Launch the kernels into given buffers: energy [1] float64, forces [N, 3] float32 or
+    None, virial [9] float64 or None, status [4] int32, and a workspace of at least
+    ``workspace_bytes`` for the index's columns. No allocation, no host sync: capturable."""
+    args = SchNetArgs(
+        num_atoms=model.num_atoms, num_columns=index.shape[1], interactions=len(model.blocks),
+        num_types=model.num_types, gaussians=model.gaussians, reserved=0,
+        cutoff=model.cutoff, positions=ptr(positions), cell=ptr(cell), pairs=ptr(index),
+        atom_types=ptr(model.atom_types), weights=ptr(packed(model)), workspace=ptr(workspace),
+        energy=ptr(energy), forces=ptr(forces), virial=ptr(virial), status=ptr(status),
+    )
+    call("nd_schnet_energy_force_virial", ctypes.byref(args), stream_handle(positions.device))
+
+
 def energy_force_virial(model, positions: Tensor, cell: Tensor, pairs: NeighborPairs,
                         forces: bool = True, virial: bool = True):
     """(E, F [N, 3], W [3, 3]) in the model's dtype from the fused kernels; positions wrapped.
 
     The count of pairs within the cutoff, the status bits and the diagnostics of a tensor-core
-    product that did not complete land in ``model._status`` [4]
-    (int32, on the device; read without a sync only when wanted).
+    product that did not complete land in ``model._status`` [4] (int32, on the device; read
+    without a sync only when wanted).
     """
     device = positions.device
     n = model.num_atoms
@@ -97,28 +113,18 @@ def energy_force_virial(model, positions: Tensor, cell: Tensor, pairs: NeighborP
     if index.dtype != torch.int32:
         index = index.to(torch.int32)
     index = index.contiguous()
-    columns = index.shape[1]
-    weights = packed(model)
-    workspace = torch.empty(workspace_bytes(n, columns, len(model.blocks)), dtype=torch.uint8,
-                            device=device)
+    workspace = torch.empty(workspace_bytes(n, index.shape[1], len(model.blocks)),
+                            dtype=torch.uint8, device=device)
     energy = torch.empty(1, dtype=torch.float64, device=device)
     out_forces = torch.empty((n, 3), dtype=torch.float32, device=device) if forces else None
     out_virial = torch.empty(9, dtype=torch.float64, device=device) if virial else None
     status = torch.empty(4, dtype=torch.int32, device=device)
-    positions = positions.contiguous()
-    cell = cell.contiguous()
-    args = SchNetArgs(
-        num_atoms=n, num_columns=columns, interactions=len(model.blocks),
-        num_types=model.num_types, gaussians=model.gaussians, reserved=0,
-        cutoff=model.cutoff, positions=ptr(positions), cell=ptr(cell), pairs=ptr(index),
-        atom_types=ptr(model.atom_types), weights=ptr(weights), workspace=ptr(workspace),
-        energy=ptr(energy), forces=ptr(out_forces), virial=ptr(out_virial), status=ptr(status),
-    )
-    call("nd_schnet_energy_force_virial", ctypes.byref(args), stream_handle(device))
+    launch(model, positions.contiguous(), cell.contiguous(), index, energy=energy,
+           forces=out_forces, virial=out_virial, status=status, workspace=workspace)
     model._status = status
     e = energy[0].to(model.dtype)
     w = out_virial.view(3, 3).to(model.dtype) if virial else None
     return e, out_forces, w
 
 
-__all__ = ("pack", "packed", "energy_force_virial", "weight_bytes", "workspace_bytes")
+__all__ = ("pack", "packed", "launch", "energy_force_virial", "weight_bytes", "workspace_bytes")

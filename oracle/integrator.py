@@ -45,15 +45,24 @@ def chain_half_step(kinetic, q, p, mass, degrees, kT, dt):
 
 
 def run(positions, velocities, masses, cell, sigma, epsilon, cutoff, dt, steps,
-        temperature=None, timescale=None):
-    """float64 NVE (or NVT when ``temperature`` is given) from a frame; returns the final frame."""
+        temperature=None, timescale=None, evaluate=None):
+    """float64 NVE (or NVT when ``temperature`` is given) from a frame; returns the final frame.
+
+    Forces are Lennard-Jones over all pairs, or ``evaluate(x) -> (energy, forces)`` of wrapped
+    positions when given (any other potential's oracle).
+    """
     x = wrap(np.asarray(positions, dtype=np.float64), np.asarray(cell, dtype=np.float64))
     v = np.asarray(velocities, dtype=np.float64).copy()
     m = np.asarray(masses, dtype=np.float64)
     v = v - (m[:, None] * v).sum(axis=0) / m.sum()
     n = x.shape[0]
     first, second = lj.all_pairs(n)
-    _, f, _ = lj.energy_force_virial(x, cell, first, second, sigma, epsilon, cutoff)
+    if evaluate is None:
+        def evaluate(frame):
+            e, forces, _ = lj.energy_force_virial(frame, cell, first, second, sigma, epsilon,
+                                                  cutoff)
+            return e, forces
+    _, f = evaluate(x)
     thermostat = temperature is not None
     if thermostat:
         kT = BOLTZMANN * temperature
@@ -70,7 +79,7 @@ def run(positions, velocities, masses, cell, sigma, epsilon, cutoff, dt, steps,
             kinetic *= factor * factor
         v = v + 0.5 * dt * f / m[:, None]
         x = wrap(x + dt * v, np.asarray(cell, dtype=np.float64))
-        energy, f, _ = lj.energy_force_virial(x, cell, first, second, sigma, epsilon, cutoff)
+        energy, f = evaluate(x)
         v = v + 0.5 * dt * f / m[:, None]
         if thermostat:
             kinetic = 0.5 * float((m[:, None] * v * v).sum())
