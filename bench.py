@@ -51,11 +51,17 @@ STEP_FLOPS_PER_ATOM = 44.2 * 26
 
 
 def load_peaks() -> dict:
+    """HBM copy GB/s and dense BF16 TFLOP/s (burst and sustained) measured on this pool's
+    B200s, else the earlier pool measurement (6.65 TB/s, 1.59 and 1.4 PFLOP/s)."""
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
         peaks = json.loads(path.read_text())
-        return {"hbm_gbs": float(peaks["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        bf16 = float(peaks.get("bf16_tflops", 1590.0))
+        return {"hbm_gbs": float(peaks["hbm_gbs"]), "bf16_tflops": bf16,
+                "bf16_tflops_sustained": float(peaks.get("bf16_tflops_sustained", bf16)),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "source": "fallback"}
 
 
 class ClockSampler:
@@ -301,6 +307,87 @@ def run_small(module, device, steps: int, label: str) -> dict:
             "ns_per_day": steps / (ms / 1e3) * 0.004 * 86400 / 1000}
 
 
+BEAD_MASS = 32.04  # the bead workload's mass: methanol, Da
+
+
+def schnet_system(module, device, dtype):
+    """The SchNet bead workload: 32,768 coarse-grained beads on a 32^3 simple-cubic lattice at
+    10 per nm^3 (L = 14.86 nm) with 0.02 nm seeded jitter; SchNet of 64 features, 3 blocks,
+    50 Gaussians, cutoff 1.2 nm, seed 0, one bead type; 300 K Maxwell-Boltzmann velocities.
+    Built with ``module`` (this package or the reference); returns its NVT simulation
+    (dt 0.01 ps, tau 0.1 ps, skin 0.1 nm) and the model."""
+    import torch
+
+    from nabladyn_b200 import lattice
+
+    n_side = 32
+    n = n_side**3
+    length = (n / 10.0) ** (1.0 / 3.0)
+    positions, cell = lattice.simple_cubic(n_side, length, 0.02, seed=n)
+    model = module.potential.schnet(atom_types=torch.zeros(n, dtype=torch.int64, device=device),
+                                    num_types=1, cutoff=1.2, dtype=dtype)
+    masses = torch.full((n,), BEAD_MASS, dtype=dtype, device=device)
+    velocities = module.md.maxwell_boltzmann(masses, 300.0, seed=n)
+    simulation = module.md.nvt(model, torch.tensor(positions % cell, dtype=dtype, device=device),
+                               velocities, masses, torch.tensor(cell, dtype=dtype, device=device),
+                               timestep=0.01, temperature=300.0, thermostat_timescale=0.1,
+                               skin=SKIN)
+    return simulation, model
+
+
+SCHNET_WORKLOAD = ("SchNet beads NVT, 32,768 beads (32^3 lattice, 10/nm^3), F=64, 3 blocks, "
+                   "K=50, r_c 1.2 nm, dt 0.01 ps, 300 K, fp32 (BF16 tensor-core filters)")
+# Algorithmic tensor-core work per pair within the cutoff and step: per block the filter
+# network forward (50x64 + 64x64) and its reverse for the forces (64x64 + 64x50), 2 flop per
+# multiply-add: 3 * 2 * 2 * (50 * 64 + 64 * 64) = 87,552 flop.
+SCHNET_FLOP_PER_PAIR = 3 * 2 * 2 * (50 * 64 + 64 * 64)
+
+
+def run_schnet(module, device, steps: int, warmup: int, label: str) -> dict:
+    """``steps`` NVT steps of the bead workload after ``warmup``, timed by CUDA events; then
+    the force error of the last frame against a float64 evaluation of the same network."""
+    import torch
+
+    simulation, model = schnet_system(module, device, torch.float32)
+    simulation.run(max(3, warmup))
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    simulation.run(steps)
+    end.record()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end)
+    n = model.num_atoms
+    out = {"impl": label, "workload": SCHNET_WORKLOAD, "steps": steps,
+           "ms_per_step": ms / steps, "steps_per_s": steps / (ms / 1e3),
+           "atom_steps_per_s": n * steps / (ms / 1e3)}
+    state = simulation.state()
+    exact = module.potential.schnet(atom_types=model.atom_types, num_types=1, cutoff=1.2,
+                                    dtype=torch.float64)
+    listing = module.neighbors.NeighborList(1.2, skin=SKIN)
+    x64, cell64 = state.positions.double(), state.cell.double()
+    listing.allocate(x64, cell64)
+    pairs = listing.tensors()
+    if pairs.index.dtype != torch.int64 and module.__name__ == "nabladyn":
+        pairs = pairs._replace(index=pairs.index.long())
+    _, f64, _ = module.quantity.energy_force_virial(exact)(x64, cell64, pairs)
+    ours = state.forces.double()
+    out["force_error_vs_fp64"] = float((ours - f64).norm() / f64.norm())
+    out["temperature_K"] = float(simulation.sample()["temperature"])
+    if label == "ours":
+        engine = simulation._engine
+        pairs_in_cutoff = int(engine.tensors["model_status"][0])
+        flop = SCHNET_FLOP_PER_PAIR * pairs_in_cutoff
+        peaks = load_peaks()
+        achieved = flop / (ms / steps / 1e3) / 1e12
+        out["pairs_within_cutoff"] = pairs_in_cutoff
+        out["roofline"] = {"bound": "tensor", "achieved": achieved,
+                           "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
+                           "frac": achieved / peaks["bf16_tflops_sustained"],
+                           "flop_per_step": flop, "peak_source": peaks["source"]}
+    return out
+
+
 def run_reference_cuda(args) -> None:
     """The reference's own GPU path on this B200: its md.nve (Inductor programs around its
     CUDA neighbor operator, one CUDA Graph per step), installed in baseline/_ref. Not a driver
@@ -317,6 +404,16 @@ def run_reference_cuda(args) -> None:
         import nabladyn
 
         print(json.dumps(run_small(nabladyn, device, args.steps, "reference-cuda")), flush=True)
+        return
+    if args.workload == "schnet":
+        import nabladyn
+
+        try:
+            result = run_schnet(nabladyn, device, args.steps, args.warmup, "reference-cuda")
+        except Exception as error:  # the reference's own failure, reported as its line
+            result = {"impl": "reference-cuda", "workload": SCHNET_WORKLOAD,
+                      "unavailable": f"{type(error).__name__}: {str(error).splitlines()[0]}"}
+        print(json.dumps(result), flush=True)
         return
     positions, cell = lattice.fcc(ATOMS_PER_SIDE_CELLS, LENGTH, 0.02, 2024)
     n = positions.shape[0]
@@ -520,10 +617,19 @@ def main() -> None:
                         help="requests of the serving workload (0 skips it)")
     parser.add_argument("--serving-rate", type=float, default=None,
                         help="with --workload serving: Poisson arrivals per second")
-    parser.add_argument("--workload", choices=("large", "serving", "small"), default="large")
+    parser.add_argument("--workload", choices=("large", "serving", "small", "schnet"),
+                        default="large")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "schnet" and args.impl == "ours":
+        import torch
+
+        import nabladyn_b200
+
+        print(json.dumps(run_schnet(nabladyn_b200, torch.device("cuda", 0), args.steps,
+                                    args.warmup, "ours")), flush=True)
+        return
     if args.workload == "small" and args.impl == "ours":
         import torch
 
