@@ -124,9 +124,12 @@ __device__ __forceinline__ float softplus_shifted(float x)
     return fmaxf(x, 0.0f) + __logf(1.0f + __expf(-fabsf(x))) - kLn2;
 }
 
+// 1 / (1 + e^-x) = (1 + tanh(x / 2)) / 2, with the hardware tanh (one special-function op).
 __device__ __forceinline__ float sigmoid(float x)
 {
-    return approx_reciprocal(1.0f + __expf(-x));
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * x));
+    return fmaf(0.5f, t, 0.5f);
 }
 
 // Shared-memory staging of weight images and bias vectors, by all 128 threads.
@@ -338,16 +341,18 @@ struct PairPass
 };
 
 // Shared memory of the pair passes: weight images, the basis tile, one work tile, biases.
-constexpr int kPairForwardShared = 2 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
-constexpr int kPairReverseShared = 4 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
+// Shared memory of the pair passes: weight images, one row tile (each product's operand
+// replaces the last once that product completed), biases, barrier and tensor-memory slot.
+constexpr int kPairForwardShared = 2 * umma::kImageBytes + umma::kTileBytes + 2 * 256 + 64;
+constexpr int kPairReverseShared = 4 * umma::kImageBytes + umma::kTileBytes + 2 * 256 + 64;
 
-__global__ void __launch_bounds__(kTile) pair_forward_kernel(PairPass a)
+__global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
 {
     extern __shared__ __align__(1024) unsigned char shared[];
     unsigned char* image_b1 = shared;
     unsigned char* image_b2 = image_b1 + umma::kImageBytes;
     unsigned char* basis = image_b2 + umma::kImageBytes;
-    unsigned char* work = basis + umma::kTileBytes;
+    unsigned char* work = basis;  // the basis is dead once the first product completed
     float* bias1 = reinterpret_cast<float*>(work + umma::kTileBytes);
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
@@ -437,20 +442,7 @@ __global__ void __launch_bounds__(kTile) pair_forward_kernel(PairPass a)
     cores.close(64);
 }
 
-// Eight BF16 values of this thread's row of a tile, as floats.
-__device__ __forceinline__ void unpack8(const unsigned char* tile, int c, float* out)
-{
-    const uint4 word = *reinterpret_cast<const uint4*>(tile + umma::image_offset(threadIdx.x, 8 * c));
-    const std::uint32_t parts[4] = {word.x, word.y, word.z, word.w};
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-    {
-        out[2 * i] = __uint_as_float(parts[i] << 16);
-        out[2 * i + 1] = __uint_as_float(parts[i] & 0xFFFF0000u);
-    }
-}
-
-__global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
+__global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
 {
     extern __shared__ __align__(1024) unsigned char shared[];
     unsigned char* image_b1 = shared;
@@ -458,7 +450,7 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
     unsigned char* image_b2t = image_b2 + umma::kImageBytes;
     unsigned char* image_b1t = image_b2t + umma::kImageBytes;
     unsigned char* basis = image_b1t + umma::kImageBytes;
-    unsigned char* work = basis + umma::kTileBytes;
+    unsigned char* work = basis;  // each operand replaces the last once its product completed
     float* bias1 = reinterpret_cast<float*>(work + umma::kTileBytes);
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
@@ -605,7 +597,8 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
         {
             break;
         }
-        // dE/dr = C' Gf . f_raw + sum_k [..]_k g_k', g_k' = -g_k (r / D - k) / D.
+        // dE/dr = C' Gf . f_raw + sum_k [..]_k g_k', g_k' = -g_k (r / D - k) / D, with the
+        // Gaussians evaluated again in FP32 (columns k >= K hold zeros).
         float through = 0.0f;
 #pragma unroll
         for (int half = 0; half < 2; ++half)
@@ -614,16 +607,12 @@ __global__ void __launch_bounds__(kTile) pair_reverse_kernel(PairPass a)
             umma::load32(cores.tmem + 64 + 32 * half, u);
             umma::wait_loads();
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int e = 0; e < 32; ++e)
             {
-                float basis_values[8];
-                unpack8(basis, 4 * half + c, basis_values);
-#pragma unroll
-                for (int e = 0; e < 8; ++e)
-                {
-                    const int k = 32 * half + 8 * c + e;
-                    through -= u[8 * c + e] * basis_values[e] * (t - static_cast<float>(k));
-                }
+                const int k = 32 * half + e;
+                const float offset = t - static_cast<float>(k);
+                const float g = k < a.gaussians ? __expf(-0.5f * offset * offset) : 0.0f;
+                through -= u[e] * g * offset;
             }
         }
         if (live)
