@@ -388,6 +388,119 @@ def run_schnet(module, device, steps: int, warmup: int, label: str) -> dict:
     return out
 
 
+GRADIENT_WORKLOAD = ("LJ parameter gradient: 2-type mixture, 4,096 atoms (16^3 lattice, "
+                     "21/nm^3), 64 frames, loss over E/F/W in fp32, dLoss/d(sigma, epsilon)")
+
+
+def gradient_data(device):
+    """The differentiation workload: 64 jittered frames of a 16^3 simple-cubic lattice at 21 per
+    nm^3 (L = 5.80 nm), types 50/50 seeded, labels from sigma rows (0.34, 0.32, 0.30) and
+    epsilon rows (0.996, 0.8, 0.6) in float64, start parameters off by a seeded +-10%."""
+    import numpy as np
+    import torch
+
+    from nabladyn_b200 import lattice, potential, training
+
+    n_side, frames = 16, 64
+    n = n_side**3
+    length = (n / 21.0) ** (1.0 / 3.0)
+    rng = np.random.default_rng(n)
+    types = torch.tensor(rng.permutation(np.arange(n) % 2), device=device)
+    positions = np.stack([lattice.simple_cubic(n_side, length, 0.02, seed=100 + f)[0] % length
+                          for f in range(frames)])
+    x = torch.tensor(positions, device=device)
+    cells = torch.full((frames, 3), length, dtype=torch.float64, device=device)
+    stack = training.pair_stack(x, cells, CUTOFF)
+    sigma = torch.tensor([0.34, 0.32, 0.30], dtype=torch.float64, device=device)
+    epsilon = torch.tensor([0.996, 0.8, 0.6], dtype=torch.float64, device=device)
+    target = potential.lennard_jones(atom_types=types, sigma=sigma, epsilon=epsilon,
+                                     cutoff=CUTOFF)
+    with torch.no_grad():
+        labels = training.predict(target, {}, x, cells, (stack,), ("energy", "forces", "virial"))
+    start = torch.tensor(rng.uniform(0.9, 1.1, 6), device=device)
+    return {"types": types, "positions": x.float(), "cells": cells.float(), "stack": stack,
+            "labels": {k: v.float() for k, v in labels.items()},
+            "sigma": (sigma * start[:3]).float(), "epsilon": (epsilon * start[3:]).float()}
+
+
+def run_gradient(module, device, steps: int, warmup: int, label: str) -> dict:
+    """``steps`` evaluations of the loss and dLoss/d(sigma, epsilon) over all 64 frames, after
+    ``warmup``, timed by CUDA events: this package's hand-written backward, or the
+    reference's compiled gradient_program (torch.func double backward under Inductor)."""
+    import torch
+
+    data = gradient_data(device)
+    channels = ("energy", "forces", "virial")
+    model = module.potential.lennard_jones(
+        atom_types=data["types"], sigma=data["sigma"], epsilon=data["epsilon"], cutoff=CUTOFF,
+        trainable=("sigma", "epsilon"))
+    from nabladyn_b200 import training
+
+    scales = training.scales(**data["labels"])
+    weights = {"energy": 1.0, "forces": 1.0, "virial": 1.0}
+    if label == "ours":
+        def evaluate():
+            params = {"sigma": model.sigma.detach().clone().requires_grad_(True),
+                      "epsilon": model.epsilon.detach().clone().requires_grad_(True)}
+            predicted = module.training.predict(model, params, data["positions"], data["cells"],
+                                                (data["stack"],), channels)
+            value, _ = module.training.loss(predicted, data["labels"], weights, scales)
+            value.backward()
+            return value, params["sigma"].grad
+    else:
+        from nabladyn.training import _fit
+
+        program = _fit.gradient_program(model, channels)
+        tensor = lambda v: torch.tensor(v, dtype=torch.float32, device=device)  # noqa: E731
+        t_weights = {k: tensor(v) for k, v in weights.items()}
+        t_scales = {k: tensor(v) for k, v in scales.items()}
+
+        def evaluate():
+            params = {"sigma": model.sigma.detach(), "epsilon": model.epsilon.detach()}
+            gradient, (value, _) = program(params, data["positions"], data["cells"],
+                                           (data["stack"],), data["labels"], None, t_weights,
+                                           t_scales)
+            return value, gradient["sigma"]
+
+    for _ in range(max(3, warmup)):
+        value, grad = evaluate()
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        value, grad = evaluate()
+    end.record()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end) / steps
+    # The float64 gradient of the same loss, by this package's backward (which matches the
+    # reference's float64 gradient to 1e-9), as the accuracy yardstick of both arms.
+    exact = training_gradient64(data, channels, weights, scales)
+    error = float((grad.double() - exact).norm() / exact.norm())
+    return {"impl": label, "workload": GRADIENT_WORKLOAD, "evaluations": steps,
+            "ms_per_gradient": ms, "frames_per_s": 64 / (ms / 1e3),
+            "loss": float(value), "dloss_dsigma": grad.tolist(),
+            "dloss_dsigma_error_vs_fp64": error,
+            "pairs_columns": int(data["stack"].shape[2])}
+
+
+def training_gradient64(data, channels, weights, scales):
+    """dLoss/dsigma of the differentiation workload in float64."""
+    import nabladyn_b200
+
+    model = nabladyn_b200.potential.lennard_jones(
+        atom_types=data["types"], sigma=data["sigma"].double(),
+        epsilon=data["epsilon"].double(), cutoff=CUTOFF, trainable=("sigma", "epsilon"))
+    params = {"sigma": model.sigma.detach().clone().requires_grad_(True),
+              "epsilon": model.epsilon.detach().clone().requires_grad_(True)}
+    predicted = nabladyn_b200.training.predict(model, params, data["positions"].double(),
+                                               data["cells"].double(), (data["stack"],),
+                                               channels)
+    labels = {k: v.double() for k, v in data["labels"].items()}
+    value, _ = nabladyn_b200.training.loss(predicted, labels, weights, scales)
+    value.backward()
+    return params["sigma"].grad
+
+
 def run_reference_cuda(args) -> None:
     """The reference's own GPU path on this B200: its md.nve (Inductor programs around its
     CUDA neighbor operator, one CUDA Graph per step), installed in baseline/_ref. Not a driver
@@ -404,6 +517,16 @@ def run_reference_cuda(args) -> None:
         import nabladyn
 
         print(json.dumps(run_small(nabladyn, device, args.steps, "reference-cuda")), flush=True)
+        return
+    if args.workload == "gradient":
+        import nabladyn
+
+        try:
+            result = run_gradient(nabladyn, device, args.steps, args.warmup, "reference-cuda")
+        except Exception as error:  # the reference's own failure, reported as its line
+            result = {"impl": "reference-cuda", "workload": GRADIENT_WORKLOAD,
+                      "unavailable": f"{type(error).__name__}: {str(error).splitlines()[0]}"}
+        print(json.dumps(result), flush=True)
         return
     if args.workload == "schnet":
         import nabladyn
@@ -617,11 +740,20 @@ def main() -> None:
                         help="requests of the serving workload (0 skips it)")
     parser.add_argument("--serving-rate", type=float, default=None,
                         help="with --workload serving: Poisson arrivals per second")
-    parser.add_argument("--workload", choices=("large", "serving", "small", "schnet"),
+    parser.add_argument("--workload",
+                        choices=("large", "serving", "small", "schnet", "gradient"),
                         default="large")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "gradient" and args.impl == "ours":
+        import torch
+
+        import nabladyn_b200
+
+        print(json.dumps(run_gradient(nabladyn_b200, torch.device("cuda", 0), args.steps,
+                                      args.warmup, "ours")), flush=True)
+        return
     if args.workload == "schnet" and args.impl == "ours":
         import torch
 
