@@ -501,6 +501,87 @@ def training_gradient64(data, channels, weights, scales):
     return params["sigma"].grad
 
 
+TRAIN_WORKLOAD = ("SchNet training step: 32 frames of the 32,768-bead system, loss over E/F/W "
+                  "(labels from the seed-1 network), gradient in every parameter, fp32, "
+                  "chunks of 2 frames")
+
+
+def run_schnet_training(module, device, steps: int, warmup: int, label: str) -> dict:
+    """``steps`` training steps (loss and gradient over 32 frames) after ``warmup``. Both arms
+    run the reference's algorithm (torch.func double backward through the model, vmapped over
+    a chunk of frames): eagerly here, under the reference's Inductor compile there."""
+    import numpy as np
+    import torch
+
+    import nabladyn_b200
+    from nabladyn_b200 import lattice, training
+
+    n_side, frames, chunk = 32, 32, 2
+    n = n_side**3
+    length = (n / 10.0) ** (1.0 / 3.0)
+    positions = torch.tensor(np.stack([
+        lattice.simple_cubic(n_side, length, 0.03, seed=500 + f)[0] % length
+        for f in range(frames)]), dtype=torch.float32, device=device)
+    cells = torch.full((frames, 3), length, dtype=torch.float32, device=device)
+    stack = training.pair_stack(positions, cells, 1.2)
+    types = torch.zeros(n, dtype=torch.int64, device=device)
+    teacher = nabladyn_b200.potential.schnet(atom_types=types, num_types=1, cutoff=1.2, seed=1)
+    labels = {"energy": [], "forces": [], "virial": []}
+    for f in range(frames):
+        pairs = nabladyn_b200.neighbors.NeighborPairs(stack[f], n, 1.2)
+        e, force, w = nabladyn_b200.quantity.energy_force_virial(teacher)(positions[f], cells[f],
+                                                                         pairs)
+        labels["energy"].append(e)
+        labels["forces"].append(force)
+        labels["virial"].append(w)
+    labels = {k: torch.stack(v) for k, v in labels.items()}
+    scales = training.scales(**labels)
+    weights = {"energy": 1.0, "forces": 1.0, "virial": 1.0}
+    model = module.potential.schnet(atom_types=types, num_types=1, cutoff=1.2, trainable=True)
+    params = {k: v.detach().clone() for k, v in model.named_parameters()}
+    if label == "ours":
+        def evaluate():
+            return training.loss_and_gradient(model, params, positions, cells, (stack,), labels,
+                                              weights, scales, chunk=chunk)
+    else:
+        from nabladyn.training import _fit
+
+        program = _fit.gradient_program(model, ("energy", "forces", "virial"))
+        as_tensor = lambda v: torch.tensor(v, dtype=torch.float32, device=device)  # noqa: E731
+        t_weights = {k: as_tensor(v) for k, v in weights.items()}
+        t_scales = {k: as_tensor(v) for k, v in scales.items()}
+        long_stack = stack.long()
+
+        def evaluate():
+            total, gradient = 0.0, None
+            for begin in range(0, frames, chunk):
+                end = begin + chunk
+                part = {k: v[begin:end] for k, v in labels.items()}
+                coefficients = torch.full((end - begin,), 1.0 / frames, device=device)
+                grads, (value, _) = program(params, positions[begin:end], cells[begin:end],
+                                            (long_stack[begin:end],), part, coefficients,
+                                            t_weights, t_scales)
+                total = total + value
+                gradient = grads if gradient is None else {
+                    k: gradient[k] + grads[k] for k in grads}
+            return total, gradient
+
+    for _ in range(max(1, warmup)):
+        value, gradient = evaluate()
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        value, gradient = evaluate()
+    end.record()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end) / steps
+    norm = float(torch.sqrt(sum(g.double().square().sum() for g in gradient.values())))
+    return {"impl": label, "workload": TRAIN_WORKLOAD, "steps": steps,
+            "ms_per_training_step": ms, "loss": float(value), "gradient_norm": norm,
+            "peak_memory_gb": torch.cuda.max_memory_allocated(device) / 1e9}
+
+
 def run_reference_cuda(args) -> None:
     """The reference's own GPU path on this B200: its md.nve (Inductor programs around its
     CUDA neighbor operator, one CUDA Graph per step), installed in baseline/_ref. Not a driver
@@ -517,6 +598,17 @@ def run_reference_cuda(args) -> None:
         import nabladyn
 
         print(json.dumps(run_small(nabladyn, device, args.steps, "reference-cuda")), flush=True)
+        return
+    if args.workload == "schnet-train":
+        import nabladyn
+
+        try:
+            result = run_schnet_training(nabladyn, device, args.steps, args.warmup,
+                                         "reference-cuda")
+        except Exception as error:  # the reference's own failure, reported as its line
+            result = {"impl": "reference-cuda", "workload": TRAIN_WORKLOAD,
+                      "unavailable": f"{type(error).__name__}: {str(error).splitlines()[0]}"}
+        print(json.dumps(result), flush=True)
         return
     if args.workload == "gradient":
         import nabladyn
@@ -741,11 +833,20 @@ def main() -> None:
     parser.add_argument("--serving-rate", type=float, default=None,
                         help="with --workload serving: Poisson arrivals per second")
     parser.add_argument("--workload",
-                        choices=("large", "serving", "small", "schnet", "gradient"),
+                        choices=("large", "serving", "small", "schnet", "gradient",
+                                 "schnet-train"),
                         default="large")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "schnet-train" and args.impl == "ours":
+        import torch
+
+        import nabladyn_b200
+
+        print(json.dumps(run_schnet_training(nabladyn_b200, torch.device("cuda", 0), args.steps,
+                                             args.warmup, "ours")), flush=True)
+        return
     if args.workload == "gradient" and args.impl == "ours":
         import torch
 

@@ -87,13 +87,18 @@ def predict(model: LennardJones, parameters: Mapping[str, Tensor], positions: Te
             cells: Tensor, stacks: tuple[Tensor, ...], channels: tuple[str, ...]) -> dict[str, Tensor]:
     """The channels of F frames by name, differentiable in ``parameters``.
 
+    Lennard-Jones runs the batched kernels and the hand-written backward; any other model the
+    reference's torch.func algorithm (``_generic.predict``).
+
     positions [F, N, 3] (anywhere), cells [F, 3], ``stacks`` one [F, 2, C] pair stack per
     cutoff of the model (one for Lennard-Jones); ``parameters`` replaces the model's "sigma"
     and/or "epsilon". Gives energy [F], forces [F, N, 3], virial [F, 3, 3]. Gradients flow to
     the parameters only.
     """
     if not isinstance(model, LennardJones):
-        raise TypeError("the batched kernels predict Lennard-Jones models")
+        from ._generic import predict as generic_predict
+
+        return generic_predict(model, parameters, positions, cells, stacks, channels)
     unknown = set(channels) - set(CHANNELS)
     if not channels or unknown:
         raise ValueError(f"channels must be a nonempty subsequence of {CHANNELS}")

@@ -24,6 +24,9 @@ Fixtures:
   Gaussians, cutoff 1.2 nm, seed 0) built in float64 and float32, its E/F/W over every pair
   by quantity.energy_force_virial, and its seeded weights (also for one type, the bead
   workload's topology) under its state-dict names.
+* schnet_fit_gradient.npz — the reference's SchNet training loss over E/F/W on three frames of
+  that system (labels from the seed-1 network) and its gradient in four of the seed-0
+  network's parameters, by its training predict/loss under torch.func.
 """
 
 import os
@@ -256,6 +259,44 @@ def schnet() -> None:
     np.savez_compressed(OUT / "schnet_343.npz", **out)
 
 
+def schnet_fit_gradient() -> None:
+    from nabladyn.training import _loss
+
+    g = np.load(OUT / "schnet_343.npz")
+    n, cutoff = g["positions"].shape[0], 1.2
+    rng = np.random.default_rng(3)
+    frames = np.stack([(g["positions"] + rng.normal(0.0, 0.01, g["positions"].shape))
+                       % g["cell"] for _ in range(3)])
+    types = torch.tensor(g["atom_types"])
+    positions = torch.tensor(frames)
+    cells = torch.tensor(np.stack([g["cell"]] * 3))
+    stack = all_pairs(n).long()[None].expand(3, 2, -1).contiguous()
+    channels = ("energy", "forces", "virial")
+    target = potential.schnet(atom_types=types, num_types=2, cutoff=cutoff, seed=1,
+                              dtype=torch.float64)
+    labels = _loss.predict(target, {}, positions, cells, (stack,), channels)
+    labels = {k: v.detach() for k, v in labels.items()}
+    model = potential.schnet(atom_types=types, num_types=2, cutoff=cutoff, trainable=True,
+                             dtype=torch.float64)
+    scales = _loss.scales(**labels)
+    weights = {"energy": 1.0, "forces": 1.0, "virial": 1.0}
+    names = ("embedding", "blocks.0.filter1.weight", "blocks.2.update2.bias", "readout1.weight")
+    params = {k: v.detach().clone() for k, v in model.named_parameters()}
+
+    def loss(trained):
+        predicted = _loss.predict(model, trained, positions, cells, (stack,), channels)
+        return _loss.loss(predicted, labels, weights, scales)
+
+    gradient, (value, _) = torch.func.grad_and_value(loss, has_aux=True)(params)
+    out = {"positions": frames, "cells": cells.numpy(), "loss": value.detach().numpy(),
+           "scales": np.array([scales["energy"], scales["forces"], scales["virial"]])}
+    for name in names:
+        out[f"grad:{name}"] = gradient[name].numpy()
+    for name in channels:
+        out[f"label:{name}"] = labels[name].numpy()
+    np.savez_compressed(OUT / "schnet_fit_gradient.npz", **out)
+
+
 if __name__ == "__main__":
     torch.set_num_threads(os.cpu_count() or 1)
     argon()
@@ -263,4 +304,5 @@ if __name__ == "__main__":
     lj_frames()
     lj_fit_gradient()
     schnet()
+    schnet_fit_gradient()
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))

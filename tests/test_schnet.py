@@ -82,3 +82,29 @@ def test_parameter_block_layout(golden):
         assert images[0, 0, offset] == (b1[row, k] if k < 50 else 0.0)    # filter1
         assert images[0, 3, offset] == (b1[k, row] if row < 50 else 0.0)   # filter1^T
     assert _schnet_kernels.workspace_bytes(343, 58653, 3) > 0
+
+
+def test_training_gradient_matches_reference(golden):
+    """The SchNet training step (the reference's torch.func algorithm, run here in chunks of
+    two frames) against the reference's own loss and gradient on three frames."""
+    from nabladyn_b200 import training
+
+    fit = dict(np.load("tests/golden/schnet_fit_gradient.npz"))
+    n = golden["positions"].shape[0]
+    model = potential.schnet(atom_types=torch.tensor(golden["atom_types"]), num_types=2,
+                             cutoff=1.2, trainable=True, dtype=torch.float64)
+    first, second = np.triu_indices(n, 1)
+    stack = torch.tensor(np.stack([first, second]), dtype=torch.int32)[None].expand(3, 2, -1)
+    labels = {name: torch.tensor(fit[f"label:{name}"]) for name in ("energy", "forces", "virial")}
+    scales = dict(zip(("energy", "forces", "virial"), fit["scales"].tolist()))
+    params = {k: v.detach().clone() for k, v in model.named_parameters()}
+    value, gradient = training.loss_and_gradient(
+        model, params, torch.tensor(fit["positions"]), torch.tensor(fit["cells"]),
+        (stack.contiguous(),), labels, {"energy": 1.0, "forces": 1.0, "virial": 1.0}, scales,
+        chunk=2)
+    assert float(value) == pytest.approx(float(fit["loss"]), rel=1e-10)
+    for key in fit:
+        if key.startswith("grad:"):
+            name = key[len("grad:"):]
+            np.testing.assert_allclose(gradient[name].numpy(), fit[key], rtol=1e-8,
+                                       atol=1e-8 * np.abs(fit[key]).max(), err_msg=name)
