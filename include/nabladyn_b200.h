@@ -375,10 +375,12 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
 
 /* ---- Integrator of frames in the caller's order ------------------------------------------
  * Velocity Verlet with the Nose-Hoover chain of three (src/nabladyn/md/_ensembles/_nve.py:39-58,
- * _nvt.py:88-129, _chain.py:23-105) for any potential: the caller runs its neighbor update and
- * forces between nd_integrate_open and nd_integrate_close. The thermostat block has the MD
- * engine's layout (nd_md_system.thermostat); totals[1] gets the step's K, totals[9] the K of
- * nd_integrate_kinetic. Replaces the ensemble halves the reference compiles with Inductor. */
+ * _nvt.py:88-129, _chain.py:23-105) and isotropic MTK NPT with chains on the particles and the
+ * barostat (_npt.py:66-251) for any potential: the caller runs its neighbor update and forces
+ * (with the virial for NPT) between nd_integrate_open and nd_integrate_close. `mode` is 0 NVE,
+ * 1 NVT, 2 NPT. The thermostat block has the MD engine's layout (nd_md_system.thermostat);
+ * totals[1] gets the step's K, totals[9] the K of nd_integrate_kinetic. Replaces the ensemble
+ * halves the reference compiles with Inductor. */
 typedef struct nd_integrator {
     int dtype;               /* ND_FLOAT32 or ND_FLOAT64 */
     int64_t num_atoms;
@@ -387,18 +389,22 @@ typedef struct nd_integrator {
     const void* forces;      /* [N, 3] */
     const void* masses;      /* [N] */
     int64_t* images;         /* [N, 3] */
-    const void* cell;        /* [3] */
+    void* cell;              /* [3]; NPT rescales it */
     double* thermostat;      /* [24] */
     double* partials;        /* [nd_integrate_partial_slots] */
     double* totals;          /* [16] */
     int32_t* status;         /* [1]: bit 2 a non-finite coordinate */
     double timestep;         /* ps */
+    double* barostat;        /* [32] for NPT (else NULL): p_eps, its chain q[3] p[3] and masses
+                                [3], box mass, pressure, alpha = 1 + 1/N, the float64 cell [3],
+                                this step's drag and growth */
+    const double* virial;    /* [9] W of the last forces, for NPT (else NULL) */
 } nd_integrator;
 
 int nd_integrate_partial_slots(int64_t num_atoms, int64_t* slots);
-int nd_integrate_open(const nd_integrator* s, int thermostat, nd_stream_t stream);
-int nd_integrate_close(const nd_integrator* s, int thermostat, nd_stream_t stream);
-int nd_integrate_kinetic(const nd_integrator* s, int thermostat, nd_stream_t stream);
+int nd_integrate_open(const nd_integrator* s, int mode, nd_stream_t stream);
+int nd_integrate_close(const nd_integrator* s, int mode, nd_stream_t stream);
+int nd_integrate_kinetic(const nd_integrator* s, int mode, nd_stream_t stream);
 
 #ifdef __cplusplus
 }

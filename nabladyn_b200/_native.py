@@ -242,6 +242,8 @@ class Integrator(ctypes.Structure):
         ("totals", ctypes.c_void_p),
         ("status", ctypes.c_void_p),
         ("timestep", ctypes.c_double),
+        ("barostat", ctypes.c_void_p),
+        ("virial", ctypes.c_void_p),
     ]
 
 

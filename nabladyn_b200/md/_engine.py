@@ -284,6 +284,10 @@ class Engine:
                  ptr(out["forces"]), ptr(out["images"]), int(thermostat), self._stream())
         return out
 
+    def volume(self) -> float:
+        """The cell volume in nm^3 (the LJ engine's cell is fixed)."""
+        return math.prod(self.lengths)
+
     @property
     def status(self) -> Tensor:
         return self.tensors["status"]

@@ -44,7 +44,6 @@ class PairEngine:
         self.num_atoms = n = int(num_atoms)
         self.lengths = lengths
         self.radius = float(model.cutoff) + float(skin)
-        self.cell = cell.detach().to(device, dtype).contiguous()
         self.neighbors = NeighborList(model.cutoff, skin=skin,
                                       capacity_multiplier=capacity_multiplier)
         self._fused = isinstance(model, SchNet) and model._fused_kernel
@@ -65,7 +64,11 @@ class PairEngine:
             "model_status": torch.zeros(4, dtype=torch.int32, device=device),
             "energy": torch.zeros(1, dtype=torch.float64, device=device),
             "virial": torch.zeros(9, dtype=torch.float64, device=device),
+            "cell": cell.detach().to(device, dtype).contiguous().clone(),
+            "barostat": torch.zeros(32, dtype=torch.float64, device=device),
         }
+        self.cell = self.tensors["cell"]  # NPT rescales it in place
+        self._npt = False
         self.workspace = None
         t = self.tensors
         self.system = Integrator(
@@ -73,7 +76,7 @@ class PairEngine:
             velocities=ptr(t["velocities"]), forces=ptr(t["forces"]), masses=ptr(t["masses"]),
             images=ptr(t["images"]), cell=ptr(self.cell), thermostat=ptr(t["thermostat"]),
             partials=ptr(t["partials"]), totals=ptr(t["totals"]), status=ptr(t["status"]),
-            timestep=float(timestep),
+            timestep=float(timestep), barostat=ptr(t["barostat"]), virial=ptr(t["virial"]),
         )
         self._evaluate = None if self._fused else quantity.energy_force_virial(
             model._energy_wrapped)
@@ -132,6 +135,24 @@ class PairEngine:
         th[TIMESTEP] = self.system.timestep
         self.tensors["thermostat"].copy_(th)
 
+    def set_barostat(self, *, temperature: float, pressure: float, timescale: float,
+                     momentum: Tensor, positions: Tensor, momenta: Tensor) -> None:
+        """The isotropic MTK barostat: box momentum, its chain of three (masses kT tau_b^2),
+        box mass 3 (N + 1) kT tau_b^2, pressure, alpha = 1 + 1/N and the float64 cell."""
+        box = torch.zeros(32, dtype=torch.float64)
+        kT = BOLTZMANN * temperature
+        base = kT * timescale * timescale
+        box[0] = float(momentum)
+        box[1:4] = positions.detach().cpu().double()
+        box[4:7] = momenta.detach().cpu().double()
+        box[7:10] = torch.tensor([base, base, base], dtype=torch.float64)
+        box[10] = 3 * (self.num_atoms + 1) * base
+        box[11] = pressure
+        box[12] = 1.0 + 1.0 / self.num_atoms
+        box[13:16] = self.cell.detach().cpu().double()
+        self.tensors["barostat"].copy_(box)
+        self._npt = True
+
     # -- calls -----------------------------------------------------------------------------
 
     def _model_forces(self, virial: bool) -> None:
@@ -150,14 +171,15 @@ class PairEngine:
             t["forces"].copy_(forces.detach())
             t["virial"].copy_(w.detach().reshape(9))
 
-    def step(self, thermostat: bool) -> None:
+    def step(self, mode: int) -> None:
+        """One step: mode 0 NVE, 1 NVT, 2 NPT."""
         t = self.tensors
         with torch.cuda.device(self.device):
             stream = self._stream()
-            call("nd_integrate_open", self.system, int(thermostat), stream)
+            call("nd_integrate_open", self.system, int(mode), stream)
             self.neighbors._update_wrapped(t["positions"], self.cell)
-            self._model_forces(virial=False)
-            call("nd_integrate_close", self.system, int(thermostat), stream)
+            self._model_forces(virial=int(mode) == 2)
+            call("nd_integrate_close", self.system, int(mode), stream)
             t["totals"][0:1].copy_(t["energy"])
 
     def forces(self, virial: bool) -> None:
@@ -182,7 +204,18 @@ class PairEngine:
         if thermostat:
             velocities *= t["thermostat"][PENDING_SCALE].to(self.dtype)
         return {"positions": t["positions"].clone(), "velocities": velocities,
-                "forces": t["forces"].clone(), "images": t["images"].clone()}
+                "forces": t["forces"].clone(), "images": t["images"].clone(),
+                "cell": t["cell"].clone()}
+
+    def volume(self) -> float:
+        """The cell volume in nm^3 (the float64 master cell under NPT). Syncs."""
+        if self._npt:
+            return float(self.tensors["barostat"][13:16].prod())
+        return float(self.tensors["cell"].double().prod())
+
+    @property
+    def barostat(self) -> Tensor:
+        return self.tensors["barostat"]
 
     @property
     def status(self) -> Tensor:

@@ -25,7 +25,7 @@ from ..potential._lennard_jones import LennardJones
 from ..units import BOLTZMANN
 from ._engine import CHAIN_A, CHAIN_MASS, DEGREES, PENDING_SCALE, THERMAL_ENERGY, Engine
 from ._pair_engine import PairEngine
-from ._state import ChainState, State
+from ._state import BarostatState, ChainState, State
 
 _STATUS_INTERVAL = 1000  # steps between reads of the status
 
@@ -135,11 +135,13 @@ class Simulation:
             raise TypeError("positions must be a CUDA float32 or float64 tensor")
         if not bool(torch.isfinite(positions).all()):
             raise ValueError("positions must be finite")
-        self._thermostat = ensemble["name"] == "NVT"
+        name = ensemble["name"]
+        self._thermostat = name in ("NVT", "NPT")
+        self._mode = {"NVE": 0, "NVT": 1, "NPT": 2}[name]
         if self._thermostat and num_atoms < 2:
-            raise ValueError("NVT needs at least 2 atoms, for 3N - 3 degrees of freedom")
+            raise ValueError(f"{name} needs at least 2 atoms, for 3N - 3 degrees of freedom")
         cell = cell.detach().clone()
-        if isinstance(model, LennardJones):
+        if isinstance(model, LennardJones) and name != "NPT":
             self._engine = Engine(
                 num_types=model.num_types,
                 sigma=model.sigma,
@@ -173,10 +175,12 @@ class Simulation:
         self._engine.load(wrapped, velocities, masses, images + crossings, types)
         self._model, self._masses, self._timestep, self._cell = model, masses, timestep, cell
         self._degrees_of_freedom = 3 * num_atoms - 3
-        self._settings = {key: value for key, value in ensemble.items() if key != "chain"}
+        self._settings = {key: value for key, value in ensemble.items()
+                          if key not in ("chain", "barostat")}
         self._settings["ensemble"] = ensemble["name"]
         self._settings.pop("name")
-        self._fields = FIELDS + (("conserved_energy",) if self._thermostat else ())
+        self._fields = FIELDS + {0: (), 1: ("conserved_energy",),
+                                 2: ("volume", "conserved_energy")}[self._mode]
         if self._thermostat:
             chain = ensemble.get("chain")
             if chain is None:
@@ -192,6 +196,25 @@ class Simulation:
                 positions=chain_q,
                 momenta=chain_p,
                 kinetic=kinetic,
+            )
+        if self._mode == 2:
+            barostat = ensemble.get("barostat")
+            momentum = torch.zeros((), dtype=torch.float64)
+            box_q = torch.zeros(3, dtype=torch.float64)
+            box_p = torch.zeros(3, dtype=torch.float64)
+            if barostat is not None:
+                if (not isinstance(barostat.momentum, Tensor) or barostat.momentum.shape != ()
+                        or barostat.momentum.dtype != torch.float64
+                        or barostat.momentum.device != device):
+                    raise ValueError(f"barostat.momentum must be a [] float64 tensor on {device}")
+                momentum = barostat.momentum
+                if barostat.chain is not None:
+                    _check_chain(barostat.chain, device, "barostat.chain")
+                    box_q, box_p = barostat.chain[0], barostat.chain[1]
+            self._engine.set_barostat(
+                temperature=ensemble["temperature"], pressure=ensemble["pressure"],
+                timescale=ensemble["barostat_timescale"], momentum=momentum,
+                positions=box_q, momenta=box_p,
             )
         self._failure: str | None = None
         self._graphs = self._capture()
@@ -298,14 +321,22 @@ class Simulation:
             thermostat = ChainState(
                 th[CHAIN_A:CHAIN_A + 3].clone(), th[CHAIN_A + 3:CHAIN_A + 6].clone(),
             )
+        barostat = None
+        cell = self._cell.clone()
+        if self._mode == 2:
+            box = self._engine.barostat
+            barostat = BarostatState(box[0].clone(), ChainState(box[1:4].clone(),
+                                                                box[4:7].clone()))
+            cell = frame["cell"]
         return State(
             frame["positions"],
             frame["velocities"],
             frame["forces"],
-            self._cell.clone(),
+            cell,
             frame["images"],
             self._step,
             thermostat,
+            barostat,
         )
 
     def set_frame(self, positions: Tensor, velocities: Tensor, *, images: Tensor | None = None,
@@ -341,7 +372,7 @@ class Simulation:
         side.wait_stream(current)
         with torch.cuda.stream(side):
             for _ in range(3):
-                engine.step(self._thermostat)
+                engine.step(self._mode)
         current.wait_stream(side)
         self._check(self._step + 3)  # a first frame that fails in the warm-up
         graphs = {}
@@ -349,7 +380,7 @@ class Simulation:
             graph = torch.cuda.CUDAGraph()
             with torch.cuda.graph(graph):
                 for _ in range(length):
-                    engine.step(self._thermostat)
+                    engine.step(self._mode)
             graphs[length] = graph
         engine.restore(saved)
         torch.cuda.synchronize(engine.device)
@@ -370,7 +401,7 @@ class Simulation:
         totals = engine.totals.tolist()
         energy, kinetic = totals[0], totals[9]
         w_trace = totals[2] + totals[3] + totals[4]
-        volume = math.prod(engine.lengths)
+        volume = engine.volume()
         values = [
             energy,
             kinetic,
@@ -385,6 +416,15 @@ class Simulation:
             kT, degrees = th[THERMAL_ENERGY], th[DEGREES]
             bath = sum(pk * pk / (2.0 * mk) for pk, mk in zip(p, mass))
             bath += degrees * kT * q[0] + kT * (q[1] + q[2])
+            if self._mode == 2:
+                # The barostat's chain (one degree of freedom), P V and the box's kinetic energy
+                # (src/nabladyn/md/_ensembles/_npt.py:196-221).
+                box = engine.barostat.tolist()
+                box_q, box_p, box_mass = box[1:4], box[4:7], box[7:10]
+                bath += sum(pk * pk / (2.0 * mk) for pk, mk in zip(box_p, box_mass))
+                bath += kT * (box_q[0] + box_q[1] + box_q[2])
+                bath += box[11] * volume + box[0] * box[0] / (2.0 * box[10])
+                values.append(volume)
             values.append(energy + kinetic + bath)
         # Values in the model's dtype, as the reference's panel row.
         return torch.tensor(values, dtype=torch.float64).to(self._model.dtype).tolist()
@@ -447,4 +487,40 @@ def nvt(model, positions, velocities, masses, cell, *, timestep, temperature,
     )
 
 
-__all__ = ("FIELDS", "Simulation", "nve", "nvt")
+def npt(model, positions, velocities, masses, cell, *, timestep, temperature, pressure,
+        thermostat_timescale, barostat_timescale, skin=0.1, capacity_multiplier=1.25,
+        images=None, step=0, thermostat: ChainState | None = None,
+        barostat: BarostatState | None = None) -> Simulation:
+    """Build a simulation at constant pressure and temperature, by isotropic MTK.
+
+    Takes ``nvt``'s arguments plus ``pressure`` in kJ/mol/nm^3 (``units.BAR`` converts),
+    ``barostat_timescale`` tau_b in ps and, to continue a run, the ``barostat`` state (box
+    momentum [] float64 and its chain). Chains of three act on the particles and on the
+    barostat; the box mass is 3 (N + 1) kT tau_b^2; the cell keeps its aspect ratio and scales
+    about the origin (src/nabladyn/md/_ensembles/_npt.py:66-311). The panel adds ``volume`` and
+    ``conserved_energy`` (U + K + PV + the box's kinetic energy + both chains' energies). Runs
+    in the pair engine for every model (the cell changes every step).
+    """
+    _check_thermostat_settings(temperature, thermostat_timescale)
+    if (isinstance(barostat_timescale, bool) or not isinstance(barostat_timescale, Real)
+            or not math.isfinite(barostat_timescale) or barostat_timescale <= 0):
+        raise ValueError("barostat_timescale must be a finite positive number")
+    if isinstance(pressure, bool) or not isinstance(pressure, Real) or not math.isfinite(pressure):
+        raise ValueError("pressure must be a finite number")
+    return Simulation(
+        model, positions, velocities, masses, cell,
+        ensemble={
+            "name": "NPT",
+            "temperature": float(temperature),
+            "pressure": float(pressure),
+            "thermostat_timescale": float(thermostat_timescale),
+            "barostat_timescale": float(barostat_timescale),
+            "chain": thermostat,
+            "barostat": barostat,
+        },
+        timestep=timestep, skin=skin, capacity_multiplier=capacity_multiplier, images=images,
+        step=step,
+    )
+
+
+__all__ = ("FIELDS", "Simulation", "nve", "nvt", "npt")

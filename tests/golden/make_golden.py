@@ -11,8 +11,8 @@ Fixtures:
   cutoff, so no neighbor list is involved) and the documented known answers
   (examples/README.md:55-56): 29,014 pairs within 1.1 nm, 21,398 within 1.0 nm, capacity
   36,268, E = -2,526.17 kJ/mol, max |F| = 386.06 kJ/mol/nm.
-* argon_512_md.npz — 20 NVE and 20 NVT steps of that frame, float64 and float32, made by the
-  reference's own ensemble halves (src/nabladyn/md/_ensembles/_nve.py, _nvt.py, _chain.py) in
+* argon_512_md.npz — 20 NVE, 20 NVT and 20 NPT (50 bar, barostat timescale 0.5 ps) steps of
+  that frame, float64 and float32, made by the reference's own ensemble halves (src/nabladyn/md/_ensembles/_nve.py, _nvt.py, _chain.py) in
   the order Simulation._capture runs them (src/nabladyn/md/_simulation.py:331-348), with the
   all-pairs index standing in for the neighbor list.
 * lj_frames_4.npz — four frames of examples/data/lj_frames.npz (216 atoms, two types) with the
@@ -42,12 +42,14 @@ sys.path.insert(0, str(REFERENCE / "src"))
 
 from nabladyn import potential, quantity, space  # noqa: E402
 from nabladyn.md._ensembles._nve import NVE  # noqa: E402
+from nabladyn.md._ensembles._npt import NPT  # noqa: E402
 from nabladyn.md._ensembles._nvt import NVT  # noqa: E402
 from nabladyn.md._state import _Frame  # noqa: E402
 from nabladyn.neighbors import NeighborPairs  # noqa: E402
 from nabladyn.observables import kinetic_energy  # noqa: E402
 
 SIGMA, EPSILON, MASS, CUTOFF = 0.34, 0.996, 39.948, 1.0
+NPT_PRESSURE = 50 * 0.0602214076  # 50 bar in kJ/mol/nm^3
 
 
 def all_pairs(n: int) -> torch.Tensor:
@@ -109,16 +111,21 @@ def trajectory(dtype, ensemble_name: str, steps: int, record=(1, 5, 20)):
              "energy": energy.detach().numpy().copy()}
     if ensemble_name == "NVE":
         ensemble = NVE(0.004, masses, frame)
-    else:
+    elif ensemble_name == "NVT":
         ensemble = NVT(0.004, masses, frame, temperature=120.0, timescale=0.1, chain=None)
-    step_eval = quantity.energy_and_force(model._energy_wrapped)
+    else:
+        ensemble = NPT(0.004, masses, frame, temperature=120.0, pressure=NPT_PRESSURE,
+                       thermostat_timescale=0.1, barostat_timescale=0.5, thermostat=None,
+                       barostat=None)
+    step_eval = quantity.energy_force_virial(model._energy_wrapped)
     records = {}
     with torch.no_grad():
         for step in range(1, steps + 1):
             ensemble.first_half(frame)
-            energy, forces = step_eval(frame.positions, frame.cell, pairs)
+            energy, forces, virial = step_eval(frame.positions, frame.cell, pairs)
             frame.energy.copy_(energy)
             frame.forces.copy_(forces)
+            frame.virial.copy_(virial)
             ensemble.second_half(frame)
             if ensemble.closing is not None:
                 ensemble.closing(frame)
@@ -131,9 +138,14 @@ def trajectory(dtype, ensemble_name: str, steps: int, record=(1, 5, 20)):
                     "energy": frame.energy.numpy().copy(),
                     "kinetic": kinetic_energy(frame.velocities, masses).double().numpy().copy(),
                 }
-                if ensemble_name == "NVT":
+                if ensemble_name in ("NVT", "NPT"):
                     entry["chain_positions"] = ensemble._positions.numpy().copy()
                     entry["chain_momenta"] = ensemble._momenta.numpy().copy()
+                if ensemble_name == "NPT":
+                    entry["cell"] = frame.cell.numpy().copy()
+                    entry["box_momentum"] = ensemble._box_momentum.numpy().copy()
+                    entry["box_chain_positions"] = ensemble._box_positions.numpy().copy()
+                    entry["box_chain_momenta"] = ensemble._box_momenta.numpy().copy()
                 records[step] = entry
     return start, records
 
@@ -141,7 +153,7 @@ def trajectory(dtype, ensemble_name: str, steps: int, record=(1, 5, 20)):
 def md() -> None:
     out = {}
     for dtype, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
-        for name in ("NVE", "NVT"):
+        for name in ("NVE", "NVT", "NPT"):
             start, records = trajectory(dtype, name, 20)
             out[f"{name}_{tag}_start_positions"] = start["positions"]
             out[f"{name}_{tag}_start_velocities"] = start["velocities"]
