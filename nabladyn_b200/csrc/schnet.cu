@@ -86,15 +86,18 @@ constexpr int kVirialSlots = 1024;  // per-CTA virial partials of the last rever
 // Byte layout of the workspace (nd_schnet_workspace_bytes).
 struct Workspace
 {
-    std::int64_t counters, pairs, geometry, x, v, h, m, grad, grad_m, grad_v, dedr, energy,
-        virial, total;
+    std::int64_t counters, block_counts, block_offsets, pairs, geometry, x, v, h, m, grad,
+        grad_m, grad_v, dedr, energy, virial, total;
 
     Workspace(std::int64_t atoms, std::int64_t columns, int blocks)
     {
         const std::int64_t row = atoms * kFeatures * 4;
         const std::int64_t tiles = (atoms + kTile - 1) / kTile;
+        const std::int64_t column_blocks = (columns + kThreads - 1) / kThreads;
         counters = 0;
-        pairs = 256;
+        block_counts = 256;
+        block_offsets = block_counts + align256(column_blocks * 4);
+        pairs = block_offsets + align256(column_blocks * 4);
         geometry = pairs + align256(columns * 8);
         x = geometry + align256(columns * 16);
         v = x + align256(row);
@@ -241,61 +244,157 @@ __device__ __forceinline__ void store_basis(unsigned char* tile, float r_over_wi
 // Pairs within the cutoff, compacted: (a, b) and (d, r), d = r_a - r_b of the minimum image
 // as src/nabladyn/space.py:11-19 rounds it.
 
-__global__ void compact_kernel(const float* __restrict__ positions, const float* __restrict__ cell,
-                               const std::int32_t* __restrict__ pairs, std::int64_t columns,
-                               std::int64_t atoms, float cutoff_squared, int2* __restrict__ kept,
-                               float4* __restrict__ geometry, int* __restrict__ counters)
+// Whether column c is a pair within the cutoff, with its atoms and geometry.
+__device__ __forceinline__ bool column_pair(const float* __restrict__ positions,
+                                            const float* __restrict__ cell,
+                                            const std::int32_t* __restrict__ pairs,
+                                            std::int64_t columns, std::int64_t c,
+                                            std::int64_t atoms, float cutoff_squared, int2& ab,
+                                            float4& g, int* counters)
 {
+    if (c >= columns)
+    {
+        return false;
+    }
+    ab = make_int2(pairs[c], pairs[columns + c]);
+    if (ab.x == ab.y)
+    {
+        return false;
+    }
+    if (ab.x < 0 || ab.y < 0 || ab.x >= atoms || ab.y >= atoms)
+    {
+        atomicOr(counters + 1, kBadPair);
+        return false;
+    }
+    float d[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis)
+    {
+        const float length = cell[axis];
+        const float left = positions[3 * ab.x + axis];
+        const float right = positions[3 * ab.y + axis];
+        const float raw = left - right;
+        const float half = 0.5f * length;
+        d[axis] = (left - (raw > half ? length : 0.0f)) - (right - (raw < -half ? length : 0.0f));
+    }
+    const float squared = __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])),
+                                    __fmul_rn(d[2], d[2]));
+    g = make_float4(d[0], d[1], d[2], sqrtf(squared));
+    return squared < cutoff_squared;
+}
+
+// The compaction keeps the list's column order (count per block, scan, write), so the pairs
+// of one first atom stay contiguous, as the list stores them.
+__global__ void __launch_bounds__(kThreads) compact_count_kernel(
+    const float* __restrict__ positions, const float* __restrict__ cell,
+    const std::int32_t* __restrict__ pairs, std::int64_t columns, std::int64_t atoms,
+    float cutoff_squared, int* __restrict__ block_counts, int* __restrict__ counters)
+{
+    int2 ab;
+    float4 g;
     const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool keep = false;
+    const bool keep = column_pair(positions, cell, pairs, columns, c, atoms, cutoff_squared, ab,
+                                  g, counters);
+    const int count = __syncthreads_count(keep);
+    if (threadIdx.x == 0)
+    {
+        block_counts[blockIdx.x] = count;
+    }
+}
+
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads) compact_scan_kernel(
+    const int* __restrict__ block_counts, int blocks, int* __restrict__ block_offsets,
+    int* __restrict__ counters)
+{
+    __shared__ int warp_totals[kScanThreads / kWarp];
+    __shared__ int carry;
+    if (threadIdx.x == 0)
+    {
+        carry = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x / 32;
+    for (int base = 0; base < blocks; base += kScanThreads)
+    {
+        const int i = base + threadIdx.x;
+        const int value = i < blocks ? block_counts[i] : 0;
+        int inclusive = value;
+#pragma unroll
+        for (int offset = 1; offset < 32; offset *= 2)
+        {
+            const int other = __shfl_up_sync(kFullMask, inclusive, offset);
+            inclusive += lane >= offset ? other : 0;
+        }
+        if (lane == 31)
+        {
+            warp_totals[warp] = inclusive;
+        }
+        __syncthreads();
+        if (warp == 0)
+        {
+            int total = warp_totals[lane];
+#pragma unroll
+            for (int offset = 1; offset < 32; offset *= 2)
+            {
+                const int other = __shfl_up_sync(kFullMask, total, offset);
+                total += lane >= offset ? other : 0;
+            }
+            warp_totals[lane] = total;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = (warp > 0 ? warp_totals[warp - 1] : 0) + inclusive - value;
+        if (i < blocks)
+        {
+            block_offsets[i] = carry + before;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            carry += warp_totals[kScanThreads / kWarp - 1];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        counters[0] = carry;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) compact_write_kernel(
+    const float* __restrict__ positions, const float* __restrict__ cell,
+    const std::int32_t* __restrict__ pairs, std::int64_t columns, std::int64_t atoms,
+    float cutoff_squared, const int* __restrict__ block_offsets, int2* __restrict__ kept,
+    float4* __restrict__ geometry, int* __restrict__ counters)
+{
+    __shared__ int warp_base[kThreads / kWarp];
     int2 ab = make_int2(0, 0);
     float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (c < columns)
+    const std::int64_t c = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool keep = column_pair(positions, cell, pairs, columns, c, atoms, cutoff_squared, ab,
+                                  g, counters);
+    const unsigned ballot = __ballot_sync(kFullMask, keep);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x / 32;
+    if (lane == 0)
     {
-        ab = make_int2(pairs[c], pairs[columns + c]);
-        if (ab.x != ab.y)
+        warp_base[warp] = __popc(ballot);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int running = block_offsets[blockIdx.x];
+        for (int w = 0; w < kThreads / kWarp; ++w)
         {
-            if (ab.x < 0 || ab.y < 0 || ab.x >= atoms || ab.y >= atoms)
-            {
-                atomicOr(counters + 1, kBadPair);
-            }
-            else
-            {
-                float d[3];
-#pragma unroll
-                for (int axis = 0; axis < 3; ++axis)
-                {
-                    const float length = cell[axis];
-                    const float left = positions[3 * ab.x + axis];
-                    const float right = positions[3 * ab.y + axis];
-                    const float raw = left - right;
-                    const float half = 0.5f * length;
-                    d[axis] = (left - (raw > half ? length : 0.0f)) -
-                              (right - (raw < -half ? length : 0.0f));
-                }
-                const float squared = __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])),
-                                                __fmul_rn(d[2], d[2]));
-                keep = squared < cutoff_squared;
-                g = make_float4(d[0], d[1], d[2], sqrtf(squared));
-            }
+            const int count = warp_base[w];
+            warp_base[w] = running;
+            running += count;
         }
     }
-    const unsigned ballot = __ballot_sync(kFullMask, keep);
-    if (ballot == 0)
-    {
-        return;
-    }
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(ballot) - 1;
-    int base = 0;
-    if (lane == leader)
-    {
-        base = atomicAdd(counters, __popc(ballot));
-    }
-    base = __shfl_sync(kFullMask, base, leader);
+    __syncthreads();
     if (keep)
     {
-        const int slot = base + __popc(ballot & ((1u << lane) - 1u));
+        const int slot = warp_base[warp] + __popc(ballot & ((1u << lane) - 1u));
         kept[slot] = ab;
         geometry[slot] = g;
     }
@@ -344,7 +443,43 @@ struct PairPass
 // Shared memory of the pair passes: weight images, one row tile (each product's operand
 // replaces the last once that product completed), biases, barrier and tensor-memory slot.
 constexpr int kPairForwardShared = 2 * umma::kImageBytes + umma::kTileBytes + 2 * 256 + 64;
-constexpr int kPairReverseShared = 4 * umma::kImageBytes + umma::kTileBytes + 2 * 256 + 64;
+constexpr int kPairReverseShared = 4 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
+
+// Adds columns [32 half, 32 half + 32) of every pair's first-atom vector `part` to row
+// first[p] of `target` [N][64]. The tile's pairs keep the list's order, so a first atom's
+// pairs are runs of rows: the rows are staged in shared memory (16 KB, float4 chunks swizzled
+// by row against bank conflicts), each warp sums 32 rows column by column, and one atomic per
+// run and column replaces one per pair. Dead rows carry first = -1.
+__device__ __forceinline__ void add_runs(float* stage, const int* first, float* target, int half,
+                                         const float (&part)[32])
+{
+    float4* row = reinterpret_cast<float4*>(stage) + threadIdx.x * 8;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+    {
+        row[q ^ (threadIdx.x & 7)] =
+            make_float4(part[4 * q], part[4 * q + 1], part[4 * q + 2], part[4 * q + 3]);
+    }
+    __syncthreads();
+    const int column = threadIdx.x & 31;
+    const int begin = (threadIdx.x >> 5) * 32;
+    float sum = 0.0f;
+    for (int r = begin; r < begin + 32; ++r)
+    {
+        sum += stage[(r * 8 + ((column >> 2) ^ (r & 7))) * 4 + (column & 3)];
+        const int atom = first[r];
+        if (r == begin + 31 || first[r + 1] != atom)
+        {
+            if (atom >= 0)
+            {
+                atomicAdd(target + static_cast<std::int64_t>(atom) * kFeatures + 32 * half + column,
+                          sum);
+            }
+            sum = 0.0f;
+        }
+    }
+    __syncthreads();
+}
 
 __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
 {
@@ -370,6 +505,7 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
     const int count = *reinterpret_cast<volatile int*>(a.counters);
     const float4* v4 = reinterpret_cast<const float4*>(a.v);
     float4* m4 = reinterpret_cast<float4*>(a.m);
+    __shared__ int tile_first[kTile];
 
     for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
     {
@@ -383,6 +519,7 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
             g = a.geometry[p];
         }
         const float envelope = live ? 0.5f * (__cosf(g.w * a.phase) + 1.0f) : 0.0f;
+        tile_first[threadIdx.x] = live ? ab.x : -1;
         cores.tile_index = tile;
         store_basis(basis, g.w / a.width, a.gaussians, live);
         if (!cores.run(0, basis, image_b1, 1))
@@ -417,26 +554,30 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
             float f[32];
             umma::load32(cores.tmem + 32 * half, f);
             umma::wait_loads();
-            if (live)
-            {
+            float part[32];
 #pragma unroll
-                for (int q = 0; q < 8; ++q)
+            for (int q = 0; q < 8; ++q)
+            {
+                const int k = 32 * half + 4 * q;
+                const float4 filter = make_float4((f[4 * q] + bias2[k]) * envelope,
+                                                  (f[4 * q + 1] + bias2[k + 1]) * envelope,
+                                                  (f[4 * q + 2] + bias2[k + 2]) * envelope,
+                                                  (f[4 * q + 3] + bias2[k + 3]) * envelope);
+                float4 vb = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (live)
                 {
-                    const int k = 32 * half + 4 * q;
-                    const float4 filter = make_float4((f[4 * q] + bias2[k]) * envelope,
-                                                      (f[4 * q + 1] + bias2[k + 1]) * envelope,
-                                                      (f[4 * q + 2] + bias2[k + 2]) * envelope,
-                                                      (f[4 * q + 3] + bias2[k + 3]) * envelope);
                     const float4 va = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.x) + k / 4);
-                    const float4 vb = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4);
-                    atomicAdd(m4 + 16 * static_cast<std::int64_t>(ab.x) + k / 4,
-                              make_float4(filter.x * vb.x, filter.y * vb.y, filter.z * vb.z,
-                                          filter.w * vb.w));
+                    vb = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4);
                     atomicAdd(m4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4,
                               make_float4(filter.x * va.x, filter.y * va.y, filter.z * va.z,
                                           filter.w * va.w));
                 }
+                part[4 * q] = filter.x * vb.x;
+                part[4 * q + 1] = filter.y * vb.y;
+                part[4 * q + 2] = filter.z * vb.z;
+                part[4 * q + 3] = filter.w * vb.w;
             }
+            add_runs(reinterpret_cast<float*>(work), tile_first, a.m, half, part);
         }
     }
     cores.close(64);
@@ -451,7 +592,8 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
     unsigned char* image_b1t = image_b2t + umma::kImageBytes;
     unsigned char* basis = image_b1t + umma::kImageBytes;
     unsigned char* work = basis;  // each operand replaces the last once its product completed
-    float* bias1 = reinterpret_cast<float*>(work + umma::kTileBytes);
+    float* stage = reinterpret_cast<float*>(work + umma::kTileBytes);  // Gv runs, 16 KB
+    float* bias1 = stage + kTile * 32;
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
     auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
@@ -472,6 +614,7 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
     const float4* v4 = reinterpret_cast<const float4*>(a.v);
     const float4* gm4 = reinterpret_cast<const float4*>(a.grad_m);
     float4* gv4 = reinterpret_cast<float4*>(a.grad_v);
+    __shared__ int tile_first[kTile];
     double w[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
 
     for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
@@ -490,6 +633,7 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
         const float envelope = live ? 0.5f * (cosine + 1.0f) : 0.0f;
         const float slope = live ? -0.5f * a.phase * sine : 0.0f;
         const float t = g.w / a.width;
+        tile_first[threadIdx.x] = live ? ab.x : -1;
         cores.tile_index = tile;
         store_basis(basis, t, a.gaussians, live);
         if (!cores.run(0, basis, image_b1, 1))
@@ -527,6 +671,7 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
             float f[32];
             umma::load32(cores.tmem + 64 + 32 * half, f);
             umma::wait_loads();
+            float part[32];
 #pragma unroll
             for (int c = 0; c < 4; ++c)
             {
@@ -537,6 +682,7 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
                     const int q = 2 * c + e2;
                     const int k = 32 * half + 4 * q;
                     float4 gf = make_float4(0.f, 0.f, 0.f, 0.f);
+                    float4 to_first = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (live)
                     {
                         const std::int64_t ra = 16 * static_cast<std::int64_t>(ab.x) + k / 4;
@@ -556,16 +702,24 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
                         {
                             atomicAdd(gv4 + rb, make_float4(f0 * envelope * ga.x, f1 * envelope * ga.y,
                                                             f2 * envelope * ga.z, f3 * envelope * ga.w));
-                            atomicAdd(gv4 + ra, make_float4(f0 * envelope * gb.x, f1 * envelope * gb.y,
-                                                            f2 * envelope * gb.z, f3 * envelope * gb.w));
+                            to_first = make_float4(f0 * envelope * gb.x, f1 * envelope * gb.y,
+                                                   f2 * envelope * gb.z, f3 * envelope * gb.w);
                         }
                     }
+                    part[4 * q] = to_first.x;
+                    part[4 * q + 1] = to_first.y;
+                    part[4 * q + 2] = to_first.z;
+                    part[4 * q + 3] = to_first.w;
                     scaled[4 * e2] = gf.x * envelope;
                     scaled[4 * e2 + 1] = gf.y * envelope;
                     scaled[4 * e2 + 2] = gf.z * envelope;
                     scaled[4 * e2 + 3] = gf.w * envelope;
                 }
                 umma::store8(work, threadIdx.x, 4 * half + c, scaled);
+            }
+            if (gv4 != nullptr)
+            {
+                add_runs(stage, tile_first, a.grad_v, half, part);
             }
         }
         if (!cores.run(64, work, image_b2t, 3))
@@ -1146,9 +1300,20 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
     }
     if (s.num_columns > 0)
     {
-        compact_kernel<<<blocks_for(s.num_columns), kThreads, 0, stream>>>(
-            s.positions, s.cell, s.pairs, s.num_columns, s.num_atoms,
-            static_cast<float>(s.cutoff * s.cutoff), pairs, geometry, counters);
+        const unsigned column_blocks = blocks_for(s.num_columns);
+        auto* block_counts = reinterpret_cast<int*>(at(ws.block_counts));
+        auto* block_offsets = reinterpret_cast<int*>(at(ws.block_offsets));
+        const float cutoff_squared = static_cast<float>(s.cutoff * s.cutoff);
+        compact_count_kernel<<<column_blocks, kThreads, 0, stream>>>(
+            s.positions, s.cell, s.pairs, s.num_columns, s.num_atoms, cutoff_squared,
+            block_counts, counters);
+        ND_LAUNCH_CHECK();
+        compact_scan_kernel<<<1, kScanThreads, 0, stream>>>(
+            block_counts, static_cast<int>(column_blocks), block_offsets, counters);
+        ND_LAUNCH_CHECK();
+        compact_write_kernel<<<column_blocks, kThreads, 0, stream>>>(
+            s.positions, s.cell, s.pairs, s.num_columns, s.num_atoms, cutoff_squared,
+            block_offsets, pairs, geometry, counters);
         ND_LAUNCH_CHECK();
     }
     embed_kernel<<<blocks_for(s.num_atoms * 16), kThreads, 0, stream>>>(
