@@ -812,7 +812,10 @@ def run_ours(args) -> None:
             },
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps_per_call": chunk},
-            "gpu_launches": engine.step_launches * args.steps,
+            # Per step the drift, the rebuild condition, the forces and their finalize; the
+            # rebuild's kernels only in steps whose conditional node takes the rebuild.
+            "gpu_launches": (4 * args.steps + rebuilds * (engine.step_launches - 3)
+                             if not engine.small else engine.step_launches * args.steps),
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "serving": serving,

@@ -333,6 +333,15 @@ typedef struct nd_replica_pool {
     int32_t* cell_starts;      /* the cell tables */
 } nd_replica_pool;
 
+/* A CUDA graph of `steps` steps of the system (no virial) whose rebuild kernels run in the body
+ * of a conditional IF node, set on the device from the reuse check's flag: a step that reuses
+ * the list launches four kernels. The graph bakes in the system's buffers. Replaces the
+ * reference's capture of its whole step into one CUDA Graph (src/nabladyn/md/_simulation.py:
+ * 366-402), whose rebuild is gated inside the operator's kernels. */
+int nd_md_graph_create(const nd_md_system* system, int thermostat, int steps, void** graph_out);
+int nd_md_graph_launch(void* graph, nd_stream_t stream);
+int nd_md_graph_destroy(void* graph);
+
 /* mode 0: admit the listed slots (wrap, build, first forces). mode 1: run each listed slot for
  * min(budgets[k], steps_left) steps. One CTA per listed slot; slots never interact. */
 int nd_serve_run(const nd_replica_pool* pool, const int32_t* slots, const int32_t* budgets,

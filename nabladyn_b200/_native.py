@@ -289,6 +289,10 @@ _SIGNATURES = {
     ],
     "nd_md_kinetic": [ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_void_p],
     "nd_md_partial_slots": [ctypes.POINTER(MDSystem), c_int64_p],
+    "nd_md_graph_create": [ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_int,
+                           ctypes.POINTER(ctypes.c_void_p)],
+    "nd_md_graph_launch": [ctypes.c_void_p, ctypes.c_void_p],
+    "nd_md_graph_destroy": [ctypes.c_void_p],
     "nd_serve_run": [
         ctypes.POINTER(ReplicaPool), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
         ctypes.c_int32, ctypes.c_void_p,

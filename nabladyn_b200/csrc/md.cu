@@ -1289,6 +1289,112 @@ std::int64_t step_launches(const nd_md_system* m)
     return 1 + rebuild + 2;  // drift, rebuild, forces and their finalize
 }
 
+// Sets the rebuild branch of a step graph from the device flag the drift kernel wrote.
+__global__ void rebuild_condition_kernel(cudaGraphConditionalHandle handle,
+                                         const index_t* rebuild, const index_t* status)
+{
+    cudaGraphSetConditional(handle, rebuilding(rebuild, status) ? 1u : 0u);
+}
+
+// A graph of `steps` steps in which each step's rebuild kernels sit in the body of a
+// conditional IF node: a one-thread kernel after the drift sets the condition from the device
+// flag, so steps that reuse the list launch only the drift, that kernel, the forces and their
+// finalize. Built by capture into a graph we own (the body by capture into the node's graph).
+template <typename T>
+int build_step_graph(const System<T>& s, std::int64_t num_cells, int thermostat, int steps,
+                     cudaGraph_t graph)
+{
+    cudaStream_t main = nullptr, body_stream = nullptr;
+    ND_CUDA_TRY(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
+    const cudaError_t created = cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking);
+    if (created != cudaSuccess)
+    {
+        cudaStreamDestroy(main);
+        ND_CUDA_TRY(created);
+    }
+    auto fail = [&](int rc) {
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(body_stream, &partial);
+        cudaStreamEndCapture(main, &partial);
+        cudaGetLastError();
+        cudaStreamDestroy(body_stream);
+        cudaStreamDestroy(main);
+        return rc;
+    };
+    if (cudaStreamBeginCaptureToGraph(main, graph, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    {
+        set_error("a step graph could not begin its capture");
+        return fail(ND_ECUDA);
+    }
+    for (int step = 0; step < steps; ++step)
+    {
+        int rc = launch_step(s, num_cells, thermostat, 0, 0, main);
+        if (rc != ND_OK)
+        {
+            return fail(rc);
+        }
+        cudaGraphConditionalHandle handle;
+        if (cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault) !=
+            cudaSuccess)
+        {
+            set_error("a step graph could not create its conditional handle");
+            return fail(ND_ECUDA);
+        }
+        rebuild_condition_kernel<<<1, 1, 0, main>>>(handle, s.rebuild, s.status);
+        cudaStreamCaptureStatus capture_status;
+        const cudaGraphNode_t* dependencies = nullptr;
+        std::size_t count = 0;
+        if (cudaStreamGetCaptureInfo(main, &capture_status, nullptr, nullptr, &dependencies,
+                                     &count) != cudaSuccess)
+        {
+            set_error("a step graph could not read its capture");
+            return fail(ND_ECUDA);
+        }
+        cudaGraphNodeParams params = {};
+        params.type = cudaGraphNodeTypeConditional;
+        params.conditional.handle = handle;
+        params.conditional.type = cudaGraphCondTypeIf;
+        params.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, graph, dependencies, count, &params) != cudaSuccess ||
+            cudaStreamUpdateCaptureDependencies(main, &node, 1,
+                                                cudaStreamSetCaptureDependencies) != cudaSuccess)
+        {
+            set_error("a step graph could not add its conditional rebuild");
+            return fail(ND_ECUDA);
+        }
+        cudaGraph_t body = params.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        {
+            set_error("a step graph could not capture its rebuild");
+            return fail(ND_ECUDA);
+        }
+        rc = launch_rebuild(s, num_cells, 1, body_stream);
+        if (rc != ND_OK)
+        {
+            return fail(rc);
+        }
+        if (cudaStreamEndCapture(body_stream, &body) != cudaSuccess)
+        {
+            set_error("a step graph could not end its rebuild capture");
+            return fail(ND_ECUDA);
+        }
+        rc = launch_step(s, num_cells, thermostat, 0, 2, main);
+        if (rc != ND_OK)
+        {
+            return fail(rc);
+        }
+    }
+    cudaGraph_t captured = graph;
+    const cudaError_t ended = cudaStreamEndCapture(main, &captured);
+    cudaStreamDestroy(body_stream);
+    cudaStreamDestroy(main);
+    ND_CUDA_TRY(ended);
+    return ND_OK;
+}
+
 int check_system(const nd_md_system* m)
 {
     ND_REQUIRE(m != nullptr, "the system is null");
@@ -1404,6 +1510,51 @@ int nd_md_step_launches(const nd_md_system* system, int64_t* launches)
     }
     ND_REQUIRE(launches != nullptr, "launches is null");
     *launches = nd::step_launches(system);
+    return ND_OK;
+}
+
+int nd_md_graph_create(const nd_md_system* system, int thermostat, int steps, void** graph_out)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    ND_REQUIRE(steps >= 1 && steps <= 4096, "steps must lie in [1, 4096]");
+    ND_REQUIRE(graph_out != nullptr, "graph_out is null");
+    const std::int64_t cells =
+        static_cast<std::int64_t>(system->dims[0]) * system->dims[1] * system->dims[2];
+    cudaGraph_t graph = nullptr;
+    ND_CUDA_TRY(cudaGraphCreate(&graph, 0));
+    const int built = ND_MD_DISPATCH(system,
+                                     nd::build_step_graph(s, cells, thermostat, steps, graph));
+    if (built != ND_OK)
+    {
+        cudaGraphDestroy(graph);
+        return built;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t instantiated = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ND_CUDA_TRY(instantiated);
+    *graph_out = exec;
+    return ND_OK;
+}
+
+int nd_md_graph_launch(void* graph, nd_stream_t stream)
+{
+    ND_REQUIRE(graph != nullptr, "the graph is null");
+    ND_CUDA_TRY(cudaGraphLaunch(static_cast<cudaGraphExec_t>(graph),
+                                static_cast<cudaStream_t>(stream)));
+    return ND_OK;
+}
+
+int nd_md_graph_destroy(void* graph)
+{
+    if (graph != nullptr)
+    {
+        ND_CUDA_TRY(cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph)));
+    }
     return ND_OK;
 }
 

@@ -33,6 +33,25 @@ CHAIN_MASS, THERMAL_ENERGY, DEGREES, TIMESTEP = 16, 19, 20, 21
 STAGE_TIMEOUT = 16  # status bit: a tile copy did not complete (kStageTimeout in md.cu)
 
 
+class StepGraph:
+    """An instantiated step graph of the engine (``nd_md_graph_create``); ``replay`` launches
+    it on torch's current stream."""
+
+    def __init__(self, handle: int, device: torch.device):
+        self.handle, self.device = handle, device
+
+    def replay(self) -> None:
+        call("nd_md_graph_launch", self.handle, stream_handle(self.device))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            try:
+                _native.lib().nd_md_graph_destroy(self.handle)
+            except Exception:
+                pass
+            self.handle = None
+
+
 class Engine:
     """One Lennard-Jones system in the MD engine: its buffers, its frame and its calls."""
 
@@ -246,6 +265,14 @@ class Engine:
         th[DEGREES] = degrees
         th[TIMESTEP] = self.system.timestep
         self.tensors["thermostat"].copy_(th)
+
+    def make_graph(self, thermostat: bool, steps: int) -> "StepGraph":
+        """A CUDA graph of ``steps`` steps whose rebuild runs behind a conditional node."""
+        handle = _native.ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            call("nd_md_graph_create", self.system, int(thermostat), int(steps),
+                 _native.ctypes.byref(handle))
+        return StepGraph(handle.value, self.device)
 
     def step(self, thermostat: bool) -> None:
         with torch.cuda.device(self.device):

@@ -376,6 +376,16 @@ class Simulation:
         current.wait_stream(side)
         self._check(self._step + 3)  # a first frame that fails in the warm-up
         graphs = {}
+        if isinstance(engine, Engine) and not engine.small:
+            # On the grid path the LJ engine builds its own graphs, each step's nine rebuild
+            # kernels behind a conditional node set from the device flag (on the small-box
+            # path the three gated launches cost less than the node); the build only reads
+            # the state.
+            engine.restore(saved)
+            torch.cuda.synchronize(engine.device)
+            for length in (1, _CHUNK):
+                graphs[length] = engine.make_graph(self._thermostat, length)
+            return graphs
         for length in (1, _CHUNK):
             graph = torch.cuda.CUDAGraph()
             with torch.cuda.graph(graph):
