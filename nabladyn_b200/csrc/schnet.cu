@@ -20,8 +20,8 @@
 // FP32 accumulation in tensor memory (umma.cuh). The per-pair products (filter network
 // forward, and its reverse) run in persistent CTAs that keep their weight images in shared
 // memory; the atom-wise products in one CTA per 128 atoms. Everything else is FP32, the
-// energy and virial sums FP64 in a fixed order. Messages, their reverse and forces are
-// scattered with FP32 vector atomics.
+// energy and virial sums FP64 in a fixed order. The feature rows the pair kernels gather
+// (v and Gm) are stored in BF16; messages, their reverse and forces are summed in FP32.
 
 #include <cuda_runtime.h>
 
@@ -133,6 +133,21 @@ __device__ __forceinline__ float sigmoid(float x)
     float t;
     asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * x));
     return fmaf(0.5f, t, 0.5f);
+}
+
+// Feature rows that the pair kernels gather (v = x A^T and Gm) are kept in BF16: 128 B per
+// row. Four consecutive features as one 8-byte word, widened to floats.
+__device__ __forceinline__ float4 load4(const uint2* __restrict__ rows, std::int64_t group)
+{
+    const uint2 word = __ldg(rows + group);
+    return make_float4(__uint_as_float(word.x << 16), __uint_as_float(word.x & 0xFFFF0000u),
+                       __uint_as_float(word.y << 16), __uint_as_float(word.y & 0xFFFF0000u));
+}
+
+__device__ __forceinline__ std::uint32_t pack2(float lo, float hi)
+{
+    __nv_bfloat162 pair = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<std::uint32_t*>(&pair);
 }
 
 // Shared-memory staging of weight images and bias vectors, by all 128 threads.
@@ -414,7 +429,8 @@ __global__ void embed_kernel(const std::int64_t* __restrict__ types, std::int64_
     const int q = static_cast<int>(i % 16);
     const std::int64_t type = types[atom];
     reinterpret_cast<float4*>(x)[i] = reinterpret_cast<const float4*>(table)[type * 16 + q];
-    reinterpret_cast<float4*>(v)[i] = reinterpret_cast<const float4*>(table_v)[type * 16 + q];
+    const float4 value = reinterpret_cast<const float4*>(table_v)[type * 16 + q];
+    reinterpret_cast<uint2*>(v)[i] = make_uint2(pack2(value.x, value.y), pack2(value.z, value.w));
 }
 
 struct PairPass
@@ -425,9 +441,9 @@ struct PairPass
     const unsigned char* images;  // this block's ten images
     const float* b1;
     const float* b2;
-    const float* v;           // [N][64] this block's x A^T
+    const float* v;           // [N][64] BF16: this block's x A^T
     float* m;                 // forward: messages
-    const float* grad_m;      // reverse: Gm
+    const float* grad_m;      // reverse: Gm, [N][64] BF16
     float* grad_v;            // reverse: Gv (null for the first block)
     float* dedr;              // reverse: per-pair dE/dr over the blocks so far
     float* forces;            // reverse, last pass: F (null when not wanted)
@@ -503,7 +519,7 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
     Cores cores;
     cores.open(barrier, slot, 64, a.counters, 1);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
-    const float4* v4 = reinterpret_cast<const float4*>(a.v);
+    const uint2* v2 = reinterpret_cast<const uint2*>(a.v);
     float4* m4 = reinterpret_cast<float4*>(a.m);
     __shared__ int tile_first[kTile];
 
@@ -566,8 +582,8 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
                 float4 vb = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (live)
                 {
-                    const float4 va = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.x) + k / 4);
-                    vb = __ldg(v4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4);
+                    const float4 va = load4(v2, 16 * static_cast<std::int64_t>(ab.x) + k / 4);
+                    vb = load4(v2, 16 * static_cast<std::int64_t>(ab.y) + k / 4);
                     atomicAdd(m4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4,
                               make_float4(filter.x * va.x, filter.y * va.y, filter.z * va.z,
                                           filter.w * va.w));
@@ -611,8 +627,8 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
     Cores cores;
     cores.open(barrier, slot, 128, a.counters, 2);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
-    const float4* v4 = reinterpret_cast<const float4*>(a.v);
-    const float4* gm4 = reinterpret_cast<const float4*>(a.grad_m);
+    const uint2* v2 = reinterpret_cast<const uint2*>(a.v);
+    const uint2* gm2 = reinterpret_cast<const uint2*>(a.grad_m);
     float4* gv4 = reinterpret_cast<float4*>(a.grad_v);
     __shared__ int tile_first[kTile];
     double w[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
@@ -687,10 +703,10 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
                     {
                         const std::int64_t ra = 16 * static_cast<std::int64_t>(ab.x) + k / 4;
                         const std::int64_t rb = 16 * static_cast<std::int64_t>(ab.y) + k / 4;
-                        const float4 va = __ldg(v4 + ra);
-                        const float4 vb = __ldg(v4 + rb);
-                        const float4 ga = __ldg(gm4 + ra);
-                        const float4 gb = __ldg(gm4 + rb);
+                        const float4 va = load4(v2, ra);
+                        const float4 vb = load4(v2, rb);
+                        const float4 ga = load4(gm2, ra);
+                        const float4 gb = load4(gm2, rb);
                         gf = make_float4(ga.x * vb.x + gb.x * va.x, ga.y * vb.y + gb.y * va.y,
                                          ga.z * vb.z + gb.z * va.z, ga.w * vb.w + gb.w * va.w);
                         const float f0 = f[4 * q] + bias2[k];
@@ -844,11 +860,11 @@ struct AtomPass
     const float* m;        // forward
     float* h;              // forward: writes; reverse: reads
     float* x;              // forward: updated in place
-    float* v_next;         // forward: the next block's v (null for the last block)
+    float* v_next;         // forward: the next block's v in BF16 (null for the last block)
     const float* readout;  // forward, last block: R1, e1, R2, e2
     float* grad;           // forward, last block: writes dE/dx; reverse: reads, updates
     const float* grad_v;   // reverse: Gv of the next block (null for the last block)
-    float* grad_m;         // reverse: writes Gm
+    float* grad_m;         // reverse: writes Gm in BF16
     double* energy;        // forward, last block: per-CTA partials
     int* counters;
 };
@@ -906,6 +922,19 @@ __device__ __forceinline__ void store_row(float* target, std::int64_t row, const
     for (int q = 0; q < 16; ++q)
     {
         t4[q] = make_float4(values[4 * q], values[4 * q + 1], values[4 * q + 2], values[4 * q + 3]);
+    }
+}
+
+__device__ __forceinline__ void store_row_bf16(float* target, std::int64_t row, const float* values)
+{
+    uint4* t4 = reinterpret_cast<uint4*>(target) + 8 * row;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+    {
+        t4[q] = make_uint4(pack2(values[8 * q], values[8 * q + 1]),
+                           pack2(values[8 * q + 2], values[8 * q + 3]),
+                           pack2(values[8 * q + 4], values[8 * q + 5]),
+                           pack2(values[8 * q + 6], values[8 * q + 7]));
     }
 }
 
@@ -998,7 +1027,7 @@ __global__ void __launch_bounds__(kTile) atom_forward_kernel(AtomPass a)
                     load_row_tmem(cores.tmem, values);
                     if (live)
                     {
-                        store_row(a.v_next, row, values);
+                        store_row_bf16(a.v_next, row, values);
                     }
                 }
             }
@@ -1126,7 +1155,7 @@ __global__ void __launch_bounds__(kTile) atom_reverse_kernel(AtomPass a)
         load_row_tmem(cores.tmem, values);
         if (live)
         {
-            store_row(a.grad_m, row, values);
+            store_row_bf16(a.grad_m, row, values);
         }
     }
     cores.close(64);
