@@ -51,6 +51,7 @@ constexpr int kMaxBrickCells = 14;                  // home cells per brick, at 
 constexpr int kMaxRowCells = kMaxBrickCells + 2;    // tile cells per row
 constexpr int kTileCells = 9 * kMaxRowCells;        // tile cells, at most
 constexpr int kReduced = 8;                         // E, K, W xx yy zz xy xz yz
+constexpr int kSmallLanes = 8;  // small-box forces: lanes sharing one atom's list
 
 // The device view of one system, built from nd_md_system.
 template <typename T>
@@ -93,6 +94,7 @@ struct System
     T widths[3];
     index_t bricks_x;
     index_t num_bricks;
+    index_t force_blocks;  // the force kernel's grid: bricks, or kSmallLanes lanes per atom
     index_t width;
     index_t tile_cap;
     index_t sentinel;  // the tile slot of the far-away atom that pads partial list chunks
@@ -715,6 +717,141 @@ __global__ void __launch_bounds__(kFinalizeThreads) finalize_kernel(const double
     }
 }
 
+// The small box's pair loop split over kSmallLanes lanes: lane `part` takes chunks part,
+// part + kSmallLanes, ...; the lanes' sums meet in a fixed shuffle tree, so a box of a few
+// hundred atoms fills many SMs instead of two.
+template <typename T, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
+__device__ __forceinline__ void force_center_split(const System<T>& s,
+                                                   const Pos4<T>* __restrict__ tile,
+                                                   const PairParams<T>* __restrict__ params,
+                                                   int center, int part, double* sums)
+{
+    CenterSums<T> c{};
+    const bool real = center < s.n;
+    const Pos4<T> me = real ? tile[center] : far_atom<T>();
+    if (real)
+    {
+        const int count = s.nbr_count[center];
+        const int used = count < s.width ? count : s.width;
+        const int num_chunks = (used + kChunk - 1) / kChunk;
+        const uint4* chunks =
+            reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
+        const T cutoff_squared = s.cutoff_squared;
+        const T s2 = params[0].s2;
+        for (int chunk = part; chunk < num_chunks; chunk += kSmallLanes)
+        {
+            const uint4 word = chunks[static_cast<std::int64_t>(chunk) * kWarp];
+            const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+            for (int r = 0; r < kChunk; ++r)
+            {
+                const Pos4<T> p = tile[(packed[r / 2] >> (16 * (r % 2))) & 0xffffu];
+                const T dx = min_image(me.x, p.x, s.length[0]);
+                const T dy = min_image(me.y, p.y, s.length[1]);
+                const T dz = min_image(me.z, p.z, s.length[2]);
+                const T r2 = squared_norm(dx, dy, dz);
+                const bool inside = r2 < cutoff_squared;
+                const T inv_r2 = fast_reciprocal(r2);
+                PairParams<T> pp;
+                if (kMulti)
+                {
+                    pp = params[type_pair_row(static_cast<int>(me.w), static_cast<int>(p.w),
+                                              s.num_types)];
+                }
+                const T q = (kMulti ? pp.s2 : s2) * inv_r2;
+                const T p6 = q * q * q;
+                const T mask = inside ? T(1) : T(0);
+                T fs = mask * (inv_r2 * (p6 * fma(T(2), p6, T(-1))));
+                const T u = fma(p6, p6, -p6);
+                if (kMulti)
+                {
+                    fs *= pp.e24;
+                    c.energy = fma(mask, fma(pp.e4, u, -pp.shift), c.energy);
+                }
+                else
+                {
+                    c.energy = fma(mask, u, c.energy);
+                    c.inside += mask;
+                }
+                c.fx = fma(fs, dx, c.fx);
+                c.fy = fma(fs, dy, c.fy);
+                c.fz = fma(fs, dz, c.fz);
+                if (kVirial)
+                {
+                    c.w[0] = fma(fs * dx, dx, c.w[0]);
+                    c.w[1] = fma(fs * dy, dy, c.w[1]);
+                    c.w[2] = fma(fs * dz, dz, c.w[2]);
+                    c.w[3] = fma(fs * dx, dy, c.w[3]);
+                    c.w[4] = fma(fs * dx, dz, c.w[4]);
+                    c.w[5] = fma(fs * dy, dz, c.w[5]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int offset = kSmallLanes / 2; offset > 0; offset /= 2)
+    {
+        c.fx += __shfl_xor_sync(kFullMask, c.fx, offset);
+        c.fy += __shfl_xor_sync(kFullMask, c.fy, offset);
+        c.fz += __shfl_xor_sync(kFullMask, c.fz, offset);
+        c.energy += __shfl_xor_sync(kFullMask, c.energy, offset);
+        c.inside += __shfl_xor_sync(kFullMask, c.inside, offset);
+        if (kVirial)
+        {
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+            {
+                c.w[k] += __shfl_xor_sync(kFullMask, c.w[k], offset);
+            }
+        }
+    }
+    if (!real || part != 0)
+    {
+        return;
+    }
+    T scale = T(1);
+    double energy;
+    if (kMulti)
+    {
+        energy = double(c.energy);
+    }
+    else
+    {
+        scale = params[0].e24;
+        energy = double(params[0].e4) * double(c.energy) - double(params[0].shift) * double(c.inside);
+    }
+    const T fx = c.fx * scale, fy = c.fy * scale, fz = c.fz * scale;
+    sums[0] += 0.5 * energy;
+    if (kVirial)
+    {
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+        {
+            sums[2 + k] += 0.5 * double(c.w[k] * scale);
+        }
+    }
+    T* f = s.force + 3LL * center;
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = fz;
+    if (kKickStep)
+    {
+        const T kick = s.half_dt * s.inv_mass[center];
+        T* v = s.vel + 3LL * center;
+        const T vx = fma(kick, fx, v[0]);
+        const T vy = fma(kick, fy, v[1]);
+        const T vz = fma(kick, fz, v[2]);
+        v[0] = vx;
+        v[1] = vy;
+        v[2] = vz;
+        if (kThermostat)
+        {
+            sums[1] += 0.5 * double(s.mass[center]) *
+                       (double(vx) * vx + double(vy) * vy + double(vz) * vz);
+        }
+    }
+}
+
 template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
 __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
 {
@@ -746,12 +883,9 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
             tile[s.sentinel] = far_atom<T>();
         }
         __syncthreads();
-        const int center = blockIdx.x * blockDim.x + threadIdx.x;
-        if (center < s.n)
-        {
-            force_center<T, true, kMulti, kVirial, kKickStep, kThermostat>(s, tile, params, center,
-                                                                          sums);
-        }
+        const int global = blockIdx.x * blockDim.x + threadIdx.x;
+        force_center_split<T, kMulti, kVirial, kKickStep, kThermostat>(
+            s, tile, params, global / kSmallLanes, global % kSmallLanes, sums);
     }
     else
     {
@@ -1133,6 +1267,9 @@ System<T> view(const nd_md_system* m)
     s.small = m->small;
     s.num_bricks = s.small ? static_cast<index_t>((m->num_atoms + kMDThreads - 1) / kMDThreads)
                            : m->bricks_x * m->dims[1] * m->dims[2];
+    s.force_blocks =
+        s.small ? static_cast<index_t>((m->num_atoms * kSmallLanes + kMDThreads - 1) / kMDThreads)
+                : s.num_bricks;
     s.width = m->width;
     s.tile_cap = m->tile_capacity;
     s.sentinel = m->small ? static_cast<index_t>(m->num_atoms) : m->tile_capacity;
@@ -1215,10 +1352,10 @@ int launch_force_variant(const System<T>& s, cudaStream_t stream)
         auto kernel = force_kernel<T, SMALL, MULTI, kVirial, kKickStep, kThermostat>;       \
         static std::size_t granted = 0;                                                     \
         ND_CUDA_TRY(allow_shared(kernel, bytes, granted));                                  \
-        kernel<<<s.num_bricks, kMDThreads, bytes, stream>>>(s);                             \
+        kernel<<<s.force_blocks, kMDThreads, bytes, stream>>>(s);                           \
         ND_LAUNCH_CHECK();                                                                  \
         finalize_kernel<kThermostat, kKickStep><<<1, kFinalizeThreads, 0, stream>>>(        \
-            s.partials, s.num_bricks, s.totals, s.thermo, s.rebuild);                       \
+            s.partials, s.force_blocks, s.totals, s.thermo, s.rebuild);                     \
         ND_LAUNCH_CHECK();                                                                  \
         return ND_OK;                                                                       \
     }
@@ -1606,9 +1743,9 @@ int nd_md_partial_slots(const nd_md_system* system, int64_t* slots)
     }
     ND_REQUIRE(slots != nullptr, "slots is null");
     const std::int64_t bricks =
-        system->small ? (system->num_atoms + nd::kMDThreads - 1) / nd::kMDThreads
-                      : static_cast<std::int64_t>(system->bricks_x) * system->dims[1] *
-                            system->dims[2];
+        system->small
+            ? (system->num_atoms * nd::kSmallLanes + nd::kMDThreads - 1) / nd::kMDThreads
+            : static_cast<std::int64_t>(system->bricks_x) * system->dims[1] * system->dims[2];
     const std::int64_t atoms = (system->num_atoms + nd::kMDThreads - 1) / nd::kMDThreads;
     *slots = (bricks > atoms ? bricks : atoms) * nd::kReduced;
     return ND_OK;
