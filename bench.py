@@ -688,28 +688,15 @@ def run_reference_cuda(args) -> None:
 
 def run_ours(args) -> None:
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from nabladyn_b200.replicas import Ranks
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    if world > 1:
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(value: float) -> float:
-        if world == 1:
-            return value
-        tensor = torch.tensor([value], dtype=torch.float64, device=device)
-        dist.all_reduce(tensor, op=dist.ReduceOp.MAX)
-        return float(tensor)
+    ranks = Ranks("nccl", device, timeout_s=300)
+    world, rank = ranks.world, ranks.rank
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     simulation, host, n = build_system(torch, device, seed=2024 + rank)
     engine = simulation._engine
@@ -838,8 +825,7 @@ def run_ours(args) -> None:
             "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main() -> None:
