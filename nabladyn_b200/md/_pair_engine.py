@@ -44,8 +44,10 @@ class PairEngine:
         self.num_atoms = n = int(num_atoms)
         self.lengths = lengths
         self.radius = float(model.cutoff) + float(skin)
+        # A list per cutoff of the model's parts (a sum gives each part its own list).
         self.neighbors = NeighborList(model.cutoff, skin=skin,
-                                      capacity_multiplier=capacity_multiplier)
+                                      capacity_multiplier=capacity_multiplier,
+                                      inner_cutoffs=tuple(model._list_cutoffs[:-1]))
         self._fused = isinstance(model, SchNet) and model._fused_kernel
         slots = torch.empty(1, dtype=torch.int64)
         call("nd_integrate_partial_slots", n,

@@ -3,5 +3,7 @@
 from ._base import Potential
 from ._lennard_jones import LennardJones, lennard_jones, pair_index
 from ._schnet import SchNet, schnet
+from ._sum import Sum, sum
 
-__all__ = ("Potential", "LennardJones", "lennard_jones", "pair_index", "SchNet", "schnet")
+__all__ = ("Potential", "LennardJones", "lennard_jones", "pair_index", "SchNet", "schnet",
+           "Sum", "sum")

@@ -24,6 +24,8 @@ Fixtures:
   Gaussians, cutoff 1.2 nm, seed 0) built in float64 and float32, its E/F/W over every pair
   by quantity.energy_force_virial, and its seeded weights (also for one type, the bead
   workload's topology) under its state-dict names.
+* sum_343.npz — the reference's potential.sum of a two-type Lennard-Jones (cutoff 1.0 nm) and
+  its SchNet (cutoff 1.2 nm, seed 0) on the schnet_343 frame, float64 E/F/W over every pair.
 * schnet_fit_gradient.npz — the reference's SchNet training loss over E/F/W on three frames of
   that system (labels from the seed-1 network) and its gradient in four of the seed-0
   network's parameters, by its training predict/loss under torch.func.
@@ -271,6 +273,27 @@ def schnet() -> None:
     np.savez_compressed(OUT / "schnet_343.npz", **out)
 
 
+SUM_SIGMA, SUM_EPSILON = [0.30, 0.32, 0.34], [0.5, 0.6, 0.7]
+
+
+def sum_of_models() -> None:
+    g = np.load(OUT / "schnet_343.npz")
+    n = g["positions"].shape[0]
+    types = torch.tensor(g["atom_types"])
+    lj = potential.lennard_jones(atom_types=types,
+                                 sigma=torch.tensor(SUM_SIGMA, dtype=torch.float64),
+                                 epsilon=torch.tensor(SUM_EPSILON, dtype=torch.float64),
+                                 cutoff=1.0)
+    net = potential.schnet(atom_types=types, num_types=2, cutoff=1.2, dtype=torch.float64)
+    model = potential.sum(lj, net)
+    pairs = NeighborPairs(all_pairs(n).long(), n, 1.2)
+    e, f, w = quantity.energy_force_virial(model)(torch.tensor(g["positions"]),
+                                                  torch.tensor(g["cell"]), pairs)
+    np.savez_compressed(OUT / "sum_343.npz", energy=e.detach().numpy(),
+                        forces=f.detach().numpy(), virial=w.detach().numpy(),
+                        sigma=np.array(SUM_SIGMA), epsilon=np.array(SUM_EPSILON))
+
+
 def schnet_fit_gradient() -> None:
     from nabladyn.training import _loss
 
@@ -317,4 +340,5 @@ if __name__ == "__main__":
     lj_fit_gradient()
     schnet()
     schnet_fit_gradient()
+    sum_of_models()
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
