@@ -108,3 +108,36 @@ def test_training_gradient_matches_reference(golden):
             name = key[len("grad:"):]
             np.testing.assert_allclose(gradient[name].numpy(), fit[key], rtol=1e-8,
                                        atol=1e-8 * np.abs(fit[key]).max(), err_msg=name)
+
+
+def test_oracle_parameter_gradient_matches_reference(golden):
+    """The oracle's hand-written second-order parameter gradient (forward-over-reverse along
+    the loss's force and virial adjoints), summed over three frames, against the reference's
+    own torch.func loss and gradient."""
+    fit = dict(np.load("tests/golden/schnet_fit_gradient.npz"))
+    n = golden["positions"].shape[0]
+    first, second = np.triu_indices(n, 1)
+    weights = weights_of(golden)
+    scales = dict(zip(("energy", "forces", "virial"), fit["scales"].tolist()))
+    channel_weights = {"energy": 1.0, "forces": 1.0, "virial": 1.0}
+    frames = fit["positions"].shape[0]
+    total, gradient = 0.0, None
+    for f in range(frames):
+        cell = fit["cells"][f]
+        x = fit["positions"][f] % cell
+        e, forces, virial = oracle.energy_force_virial(x, cell, first, second,
+                                                       golden["atom_types"], weights, 1.2, 50, 3)
+        labels = {name: fit[f"label:{name}"][f] for name in ("energy", "forces", "virial")}
+        value, e_bar, f_bar, w_bar = oracle.loss_adjoints(
+            {"energy": e, "forces": forces, "virial": virial}, labels, channel_weights, scales,
+            1.0 / frames)
+        total += value
+        part = oracle.loss_parameter_gradient(x, cell, first, second, golden["atom_types"],
+                                              weights, 1.2, 50, 3, e_bar, f_bar, w_bar)
+        gradient = part if gradient is None else {k: gradient[k] + part[k] for k in part}
+    assert total == pytest.approx(float(fit["loss"]), rel=1e-10)
+    for key in fit:
+        if key.startswith("grad:"):
+            name = key[len("grad:"):]
+            np.testing.assert_allclose(gradient[name], fit[key], rtol=1e-8,
+                                       atol=1e-8 * np.abs(fit[key]).max(), err_msg=name)
