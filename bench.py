@@ -519,14 +519,14 @@ def training_gradient64(data, channels, weights, scales):
 
 
 TRAIN_WORKLOAD = ("SchNet training step: 32 frames of the 32,768-bead system, loss over E/F/W "
-                  "(labels from the seed-1 network), gradient in every parameter, fp32, "
-                  "chunks of 2 frames")
+                  "(labels from the seed-1 network), gradient in every parameter, fp32")
 
 
 def run_schnet_training(module, device, steps: int, warmup: int, label: str) -> dict:
-    """``steps`` training steps (loss and gradient over 32 frames) after ``warmup``. Both arms
-    run the reference's algorithm (torch.func double backward through the model, vmapped over
-    a chunk of frames): eagerly here, under the reference's Inductor compile there."""
+    """``steps`` training steps (loss and gradient over 32 frames) after ``warmup``. Here the
+    fused kernels with the written-out second-order pass (tcgen05 tangent kernels for the pair
+    terms), frame by frame; there the reference's algorithm (torch.func double backward through
+    the model, vmapped over chunks of 2 frames) under its Inductor compile."""
     import numpy as np
     import torch
 

@@ -382,6 +382,44 @@ int64_t nd_schnet_weight_bytes(int32_t interactions, int32_t num_types);
 int64_t nd_schnet_workspace_bytes(int64_t num_atoms, int64_t num_columns, int32_t interactions);
 int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream);
 
+/* The per-pair passes of SchNet's parameter gradient of a training loss over E, F and W, by
+ * forward-over-reverse along the loss's adjoints: one block's filter network with its
+ * derivative along each pair's rate rdot = (d . (dL/dF_a - dL/dF_b) + d^T dL/dW d) / r.
+ * direction 0 (forward) adds the block's messages m and m_dot; direction 1 (reverse) adds
+ * v_bar and v_dot_bar and writes every pair's BF16 rows (g, g_dot, s, s_dot, z_bar, z_dot_bar,
+ * u_bar, u_dot_bar), from which the filter weights' gradients are sums over pairs. Reads the
+ * compacted pairs in `workspace` of the nd_schnet_energy_force_virial call just made with the
+ * same weights, positions, pairs and sizes. Replaces the double backward of the reference's
+ * torch.func gradient program (src/nabladyn/training/_fit.py:245-271) for the pair terms; the
+ * reference has no native counterpart. */
+typedef struct nd_schnet_tangent_args {
+    int64_t num_atoms;              /* N, as in the E/F/W call */
+    int64_t num_columns;            /* C, as in the E/F/W call */
+    int32_t interactions;
+    int32_t num_types;
+    int32_t gaussians;
+    int32_t block;                  /* the interaction block, 0 .. interactions - 1 */
+    double cutoff;
+    const void* weights;            /* the packed parameter block of the E/F/W call */
+    void* workspace;                /* the workspace that call filled */
+    const float* force_adjoint;     /* [N, 3] dL/dF */
+    const double* virial_adjoint;   /* [9] dL/dW, row-major */
+    const void* v;                  /* [N, 64] BF16: this block's x A^T */
+    const void* v_dot;              /* [N, 64] BF16: its derivative along the direction */
+    float* m;                       /* forward: [N, 64], added to */
+    float* m_dot;                   /* forward: [N, 64], added to */
+    const void* m_bar;              /* reverse: [N, 64] BF16 */
+    const void* m_dot_bar;          /* reverse: [N, 64] BF16 */
+    float* v_bar;                   /* reverse: [N, 64], added to */
+    float* v_dot_bar;               /* reverse: [N, 64], added to */
+    void* pair_rows;                /* reverse: [8, capacity, 64] BF16, rows of pairs in the
+                                       compacted order; rows past the pair count untouched */
+    int64_t capacity;               /* at least num_columns */
+    int32_t* status;                /* [4], as for nd_schnet_energy_force_virial */
+} nd_schnet_tangent_args;
+
+int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction, nd_stream_t stream);
+
 /* ---- Integrator of frames in the caller's order ------------------------------------------
  * Velocity Verlet with the Nose-Hoover chain of three (src/nabladyn/md/_ensembles/_nve.py:39-58,
  * _nvt.py:88-129, _chain.py:23-105) and isotropic MTK NPT with chains on the particles and the

@@ -227,6 +227,33 @@ class SchNetArgs(ctypes.Structure):
     ]
 
 
+class SchNetTangentArgs(ctypes.Structure):
+    _fields_ = [
+        ("num_atoms", ctypes.c_int64),
+        ("num_columns", ctypes.c_int64),
+        ("interactions", ctypes.c_int32),
+        ("num_types", ctypes.c_int32),
+        ("gaussians", ctypes.c_int32),
+        ("block", ctypes.c_int32),
+        ("cutoff", ctypes.c_double),
+        ("weights", ctypes.c_void_p),
+        ("workspace", ctypes.c_void_p),
+        ("force_adjoint", ctypes.c_void_p),
+        ("virial_adjoint", ctypes.c_void_p),
+        ("v", ctypes.c_void_p),
+        ("v_dot", ctypes.c_void_p),
+        ("m", ctypes.c_void_p),
+        ("m_dot", ctypes.c_void_p),
+        ("m_bar", ctypes.c_void_p),
+        ("m_dot_bar", ctypes.c_void_p),
+        ("v_bar", ctypes.c_void_p),
+        ("v_dot_bar", ctypes.c_void_p),
+        ("pair_rows", ctypes.c_void_p),
+        ("capacity", ctypes.c_int64),
+        ("status", ctypes.c_void_p),
+    ]
+
+
 class Integrator(ctypes.Structure):
     _fields_ = [
         ("dtype", ctypes.c_int),
@@ -298,6 +325,7 @@ _SIGNATURES = {
         ctypes.c_int32, ctypes.c_void_p,
     ],
     "nd_schnet_energy_force_virial": [ctypes.POINTER(SchNetArgs), ctypes.c_void_p],
+    "nd_schnet_tangent": [ctypes.POINTER(SchNetTangentArgs), ctypes.c_int32, ctypes.c_void_p],
     "nd_integrate_partial_slots": [ctypes.c_int64, c_int64_p],
     "nd_integrate_open": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],
     "nd_integrate_close": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],

@@ -23,7 +23,8 @@ INCLUDE = ROOT / "include"
 LIB = PACKAGE / "_lib"
 OBJ = LIB / "obj"
 
-CUDA_SOURCES = ("neighbors.cu", "lj.cu", "md.cu", "serve.cu", "schnet.cu", "integrate.cu")
+CUDA_SOURCES = ("neighbors.cu", "lj.cu", "md.cu", "serve.cu", "schnet.cu", "schnet_tangent.cu",
+                "integrate.cu")
 CXX_SOURCES = ("abi.cpp",)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # IEEE arithmetic as in the reference build: no fast math, no flush-to-zero.

@@ -182,6 +182,15 @@ struct Cores
     __device__ bool run(std::uint32_t column, const unsigned char* tile, const unsigned char* image,
                         int step)
     {
+        return run2(column, tile, image, 0, nullptr, nullptr, step);
+    }
+
+    // As run, with a second product D[column2] = tile2 * image2^T (when tile2 is not null)
+    // issued behind the first and completing on the same commit.
+    __device__ bool run2(std::uint32_t column, const unsigned char* tile, const unsigned char* image,
+                         std::uint32_t column2, const unsigned char* tile2,
+                         const unsigned char* image2, int step)
+    {
         umma::fence_operands();
         umma::fence_before_sync();
         __syncthreads();
@@ -189,6 +198,11 @@ struct Cores
         {
             umma::fence_after_sync();
             umma::product(*slot + column, umma::smem_address(tile), umma::smem_address(image));
+            if (tile2 != nullptr)
+            {
+                umma::product(*slot + column2, umma::smem_address(tile2),
+                              umma::smem_address(image2));
+            }
             umma::commit(barrier);
         }
         const bool done = umma::barrier_wait(barrier, phase);

@@ -1,0 +1,593 @@
+// The per-pair passes of the SchNet parameter gradient of a training loss over E, F and W.
+//
+// The reference differentiates its loss with torch.func through a double backward
+// (src/nabladyn/training/_fit.py:245-271, _loss.py:49-102). Written out: with the loss's
+// adjoints e_bar = dL/dE, f_bar = dL/dF [N, 3] and w_bar = dL/dW [3, 3], F = -dE/dr and
+// W = -dE/d(strain) make f_bar . F + w_bar : W the derivative of -E along a direction in which
+// each pair's distance moves at
+//     rdot = (d . (f_bar_a - f_bar_b) + d^T w_bar d) / r,
+// so dL/dtheta = d/dtheta (e_bar E - Edot): a forward pass carrying beside each value its
+// derivative along rdot, then one reverse pass over both streams. Per block, the pair work:
+//
+//   forward:  g, g_dot = g * (-(r / D - k) / D) rdot;  z, z_dot = (g, g_dot) B1^T (+ b1 on z);
+//             s = ssp(z), s_dot = sigmoid(z) z_dot;  u, u_dot = (s, s_dot) B2^T (+ b2 on u);
+//             f = u C, f_dot = u_dot C + u C' rdot;
+//             m_a += f v_b, m_b += f v_a, m_dot_a += f_dot v_b + f v_dot_b, m_dot_b likewise;
+//   reverse, given m_bar and m_dot_bar from the atom-wise layers:
+//             fb = m_bar_a v_b + m_bar_b v_a + m_dot_bar_a v_dot_b + m_dot_bar_b v_dot_a,
+//             fdb = m_dot_bar_a v_b + m_dot_bar_b v_a;
+//             v_bar_b += f m_bar_a + f_dot m_dot_bar_a, v_dot_bar_b += f m_dot_bar_a, and for a;
+//             u_bar = fb C + fdb C' rdot, u_dot_bar = fdb C;
+//             (s_bar, s_dot_bar) = (u_bar, u_dot_bar) B2;
+//             z_bar = s_bar sigmoid(z) + s_dot_bar z_dot sigmoid'(z), z_dot_bar = s_dot_bar sigmoid(z).
+//
+// The reverse pass writes every pair's BF16 rows g, g_dot, s, s_dot, z_bar, z_dot_bar, u_bar,
+// u_dot_bar, so the filter weights' gradients, sums over pairs (B1: z_bar^T g + z_dot_bar^T
+// g_dot, B2: u_bar^T s + u_dot_bar^T s_dot, the biases the column sums of z_bar and u_bar), are
+// plain GEMMs for the caller, as are the atom-wise 64 x 64 layers. Each products' pair (value,
+// tangent) runs as two 128 x 64 x 64 BF16 tcgen05 products on one commit; the tiles' rows are
+// pairs in the compacted order of the preceding nd_schnet_energy_force_virial call, whose
+// workspace this pass reads.
+
+#include "schnet.cuh"
+
+namespace nd {
+namespace {
+
+// Per-pair rows of the reverse pass, in this order, [8][capacity][64] BF16.
+enum Row : int
+{
+    kRowG = 0,
+    kRowGDot = 1,
+    kRowS = 2,
+    kRowSDot = 3,
+    kRowZBar = 4,
+    kRowZDotBar = 5,
+    kRowUBar = 6,
+    kRowUDotBar = 7,
+};
+
+struct TangentPass
+{
+    const int2* pairs;
+    const float4* geometry;
+    int* counters;
+    const unsigned char* images;  // this block's ten images
+    const float* b1;
+    const float* b2;
+    const float* force_adjoint;    // [N][3]
+    const double* virial_adjoint;  // [9]
+    const uint2* v;                // [N][64] BF16
+    const uint2* v_dot;
+    float* m;                      // forward: [N][64], added to
+    float* m_dot;
+    const uint2* m_bar;            // reverse: [N][64] BF16
+    const uint2* m_dot_bar;
+    float* v_bar;                  // reverse: [N][64], added to
+    float* v_dot_bar;
+    uint4* rows;                   // reverse: [8][capacity][64] BF16 as 16-byte words
+    std::int64_t capacity;
+    float width;  // Gaussian spacing D
+    float phase;  // pi / r_c
+    int gaussians;
+};
+
+// The pair's geometry and the rate rdot at which the loss's direction moves its distance.
+struct PairTerms
+{
+    int2 ab;
+    float4 g;        // d, r
+    bool live;
+    float envelope;  // C(r)
+    float moving;    // C'(r) rdot
+    float rate;      // rdot
+};
+
+__device__ __forceinline__ PairTerms pair_terms(const TangentPass& a, const float* wbar, int p,
+                                                int count)
+{
+    PairTerms t;
+    t.live = p < count;
+    t.ab = make_int2(0, 0);
+    t.g = make_float4(0.f, 0.f, 0.f, 1.f);
+    t.rate = 0.0f;
+    if (t.live)
+    {
+        t.ab = a.pairs[p];
+        t.g = a.geometry[p];
+        const float* fa = a.force_adjoint + 3 * static_cast<std::int64_t>(t.ab.x);
+        const float* fb = a.force_adjoint + 3 * static_cast<std::int64_t>(t.ab.y);
+        const float d[3] = {t.g.x, t.g.y, t.g.z};
+        float along = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+        {
+            along += d[i] * (__ldg(fa + i) - __ldg(fb + i));
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+            {
+                along += d[i] * wbar[3 * i + j] * d[j];
+            }
+        }
+        t.rate = along / t.g.w;
+    }
+    float sine, cosine;
+    __sincosf(t.g.w * a.phase, &sine, &cosine);
+    t.envelope = t.live ? 0.5f * (cosine + 1.0f) : 0.0f;
+    t.moving = t.live ? -0.5f * a.phase * sine * t.rate : 0.0f;
+    return t;
+}
+
+// Row p of per-pair array `kind`, or null for a dead row.
+__device__ __forceinline__ uint4* pair_row(const TangentPass& a, int kind, int p, bool live)
+{
+    return live ? a.rows + (static_cast<std::int64_t>(kind) * a.capacity + p) * 8 : nullptr;
+}
+
+// g_k = exp(-(t - k)^2 / 2) (zero for k >= K) and g_dot_k = g_k (t - k) scale, scale = -rdot / D,
+// into this thread's row of two tiles, and into HBM rows when given.
+__device__ __forceinline__ void store_basis_tangent(unsigned char* tile, unsigned char* tile_dot,
+                                                    float t, float scale, int gaussians, bool live,
+                                                    uint4* row, uint4* row_dot)
+{
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+    {
+        float g[8];
+        float gd[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+        {
+            const int k = 8 * c + e;
+            const float u = t - static_cast<float>(k);
+            g[e] = (live && k < gaussians) ? __expf(-0.5f * u * u) : 0.0f;
+            gd[e] = g[e] * u * scale;
+        }
+        const uint4 word = umma::pack8(g);
+        const uint4 word_dot = umma::pack8(gd);
+        *reinterpret_cast<uint4*>(tile + umma::image_offset(threadIdx.x, 8 * c)) = word;
+        *reinterpret_cast<uint4*>(tile_dot + umma::image_offset(threadIdx.x, 8 * c)) = word_dot;
+        if (row != nullptr)
+        {
+            row[c] = word;
+            row_dot[c] = word_dot;
+        }
+    }
+}
+
+// s = ssp(z + b1) and s_dot = sigmoid(z + b1) z_dot from tensor-memory columns 0-63 (z - b1) and
+// 64-127 (z_dot) into this thread's row of two tiles, and into HBM rows when given.
+__device__ __forceinline__ void store_activations(std::uint32_t tmem, const float* bias1,
+                                                  unsigned char* tile, unsigned char* tile_dot,
+                                                  uint4* row, uint4* row_dot)
+{
+#pragma unroll
+    for (int half = 0; half < 2; ++half)
+    {
+        float z[32];
+        float zd[32];
+        umma::load32(tmem + 32 * half, z);
+        umma::load32(tmem + 64 + 32 * half, zd);
+        umma::wait_loads();
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            float s[8];
+            float sd[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+            {
+                const float x = z[8 * c + e] + bias1[32 * half + 8 * c + e];
+                s[e] = softplus_shifted(x);
+                sd[e] = sigmoid(x) * zd[8 * c + e];
+            }
+            const int column = 4 * half + c;
+            const uint4 word = umma::pack8(s);
+            const uint4 word_dot = umma::pack8(sd);
+            *reinterpret_cast<uint4*>(tile + umma::image_offset(threadIdx.x, 8 * column)) = word;
+            *reinterpret_cast<uint4*>(tile_dot + umma::image_offset(threadIdx.x, 8 * column)) =
+                word_dot;
+            if (row != nullptr)
+            {
+                row[column] = word;
+                row_dot[column] = word_dot;
+            }
+        }
+    }
+}
+
+// Shared memory: weight images, two row tiles, (reverse) a 16 KB run stage, biases, barrier
+// and tensor-memory slot.
+constexpr int kTangentForwardShared = 2 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
+constexpr int kTangentReverseShared = 3 * umma::kImageBytes + 3 * umma::kTileBytes + 2 * 256 + 64;
+
+__global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a)
+{
+    extern __shared__ __align__(1024) unsigned char shared[];
+    unsigned char* image_b1 = shared;
+    unsigned char* image_b2 = image_b1 + umma::kImageBytes;
+    unsigned char* tile = image_b2 + umma::kImageBytes;
+    unsigned char* tile_dot = tile + umma::kTileBytes;
+    float* stage = reinterpret_cast<float*>(tile);  // first-atom runs, once the products are done
+    float* bias1 = reinterpret_cast<float*>(tile_dot + umma::kTileBytes);
+    float* bias2 = bias1 + kFeatures;
+    auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
+    auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
+    __shared__ int tile_first[kTile];
+    __shared__ float wbar[9];
+
+    copy_bytes(image_b1, a.images + kB1 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b2, a.images + kB2 * umma::kImageBytes, umma::kImageBytes);
+    if (threadIdx.x < kFeatures)
+    {
+        bias1[threadIdx.x] = a.b1[threadIdx.x];
+        bias2[threadIdx.x] = a.b2[threadIdx.x];
+    }
+    if (threadIdx.x < 9)
+    {
+        wbar[threadIdx.x] = static_cast<float>(a.virial_adjoint[threadIdx.x]);
+    }
+    // Columns 0-63: z, then u; 64-127: z_dot, then u_dot.
+    Cores cores;
+    cores.open(barrier, slot, 128, a.counters, 5);
+    const int count = *reinterpret_cast<volatile int*>(a.counters);
+    float4* m4 = reinterpret_cast<float4*>(a.m);
+    float4* md4 = reinterpret_cast<float4*>(a.m_dot);
+
+    for (int index = blockIdx.x; index * kTile < count; index += gridDim.x)
+    {
+        const int p = index * kTile + threadIdx.x;
+        const PairTerms t = pair_terms(a, wbar, p, count);
+        tile_first[threadIdx.x] = t.live ? t.ab.x : -1;
+        cores.tile_index = index;
+        store_basis_tangent(tile, tile_dot, t.g.w / a.width, -t.rate / a.width, a.gaussians,
+                            t.live, nullptr, nullptr);
+        if (!cores.run2(0, tile, image_b1, 64, tile_dot, image_b1, 1))
+        {
+            break;
+        }
+        store_activations(cores.tmem, bias1, tile, tile_dot, nullptr, nullptr);
+        if (!cores.run2(0, tile, image_b2, 64, tile_dot, image_b2, 2))
+        {
+            break;
+        }
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float u[32];
+            float ud[32];
+            umma::load32(cores.tmem + 32 * half, u);
+            umma::load32(cores.tmem + 64 + 32 * half, ud);
+            umma::wait_loads();
+            float first[32];
+            float first_dot[32];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                const int k = 32 * half + 4 * q;
+                float f[4];
+                float fd[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const float raw = u[4 * q + j] + bias2[k + j];
+                    f[j] = raw * t.envelope;
+                    fd[j] = ud[4 * q + j] * t.envelope + raw * t.moving;
+                }
+                float4 vb = make_float4(0.f, 0.f, 0.f, 0.f);
+                float4 vdb = vb;
+                if (t.live)
+                {
+                    const std::int64_t ra = 16 * static_cast<std::int64_t>(t.ab.x) + k / 4;
+                    const std::int64_t rb = 16 * static_cast<std::int64_t>(t.ab.y) + k / 4;
+                    const float4 va = load4(a.v, ra);
+                    const float4 vda = load4(a.v_dot, ra);
+                    vb = load4(a.v, rb);
+                    vdb = load4(a.v_dot, rb);
+                    atomicAdd(m4 + rb, make_float4(f[0] * va.x, f[1] * va.y, f[2] * va.z,
+                                                   f[3] * va.w));
+                    atomicAdd(md4 + rb, make_float4(fd[0] * va.x + f[0] * vda.x,
+                                                    fd[1] * va.y + f[1] * vda.y,
+                                                    fd[2] * va.z + f[2] * vda.z,
+                                                    fd[3] * va.w + f[3] * vda.w));
+                }
+                first[4 * q] = f[0] * vb.x;
+                first[4 * q + 1] = f[1] * vb.y;
+                first[4 * q + 2] = f[2] * vb.z;
+                first[4 * q + 3] = f[3] * vb.w;
+                first_dot[4 * q] = fd[0] * vb.x + f[0] * vdb.x;
+                first_dot[4 * q + 1] = fd[1] * vb.y + f[1] * vdb.y;
+                first_dot[4 * q + 2] = fd[2] * vb.z + f[2] * vdb.z;
+                first_dot[4 * q + 3] = fd[3] * vb.w + f[3] * vdb.w;
+            }
+            add_runs(stage, tile_first, a.m, half, first);
+            add_runs(stage, tile_first, a.m_dot, half, first_dot);
+        }
+    }
+    cores.close(128);
+}
+
+__global__ void __launch_bounds__(kTile, 2) tangent_reverse_kernel(TangentPass a)
+{
+    extern __shared__ __align__(1024) unsigned char shared[];
+    unsigned char* image_b1 = shared;
+    unsigned char* image_b2 = image_b1 + umma::kImageBytes;
+    unsigned char* image_b2t = image_b2 + umma::kImageBytes;
+    unsigned char* tile = image_b2t + umma::kImageBytes;
+    unsigned char* tile_dot = tile + umma::kTileBytes;
+    float* stage = reinterpret_cast<float*>(tile_dot + umma::kTileBytes);  // 16 KB
+    float* bias1 = stage + kTile * 32;
+    float* bias2 = bias1 + kFeatures;
+    auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
+    auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
+    __shared__ int tile_first[kTile];
+    __shared__ float wbar[9];
+
+    copy_bytes(image_b1, a.images + kB1 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b2, a.images + kB2 * umma::kImageBytes, umma::kImageBytes);
+    copy_bytes(image_b2t, a.images + kB2T * umma::kImageBytes, umma::kImageBytes);
+    if (threadIdx.x < kFeatures)
+    {
+        bias1[threadIdx.x] = a.b1[threadIdx.x];
+        bias2[threadIdx.x] = a.b2[threadIdx.x];
+    }
+    if (threadIdx.x < 9)
+    {
+        wbar[threadIdx.x] = static_cast<float>(a.virial_adjoint[threadIdx.x]);
+    }
+    // Columns 0-63 keep z - b1 and 64-127 z_dot for the whole tile; 128-191 take u, then s_bar;
+    // 192-255 u_dot, then s_dot_bar.
+    Cores cores;
+    cores.open(barrier, slot, 256, a.counters, 6);
+    const int count = *reinterpret_cast<volatile int*>(a.counters);
+    float4* vbar4 = reinterpret_cast<float4*>(a.v_bar);
+    float4* vdbar4 = reinterpret_cast<float4*>(a.v_dot_bar);
+
+    for (int index = blockIdx.x; index * kTile < count; index += gridDim.x)
+    {
+        const int p = index * kTile + threadIdx.x;
+        const PairTerms t = pair_terms(a, wbar, p, count);
+        tile_first[threadIdx.x] = t.live ? t.ab.x : -1;
+        cores.tile_index = index;
+        store_basis_tangent(tile, tile_dot, t.g.w / a.width, -t.rate / a.width, a.gaussians,
+                            t.live, pair_row(a, kRowG, p, t.live), pair_row(a, kRowGDot, p, t.live));
+        if (!cores.run2(0, tile, image_b1, 64, tile_dot, image_b1, 1))
+        {
+            break;
+        }
+        store_activations(cores.tmem, bias1, tile, tile_dot, pair_row(a, kRowS, p, t.live),
+                          pair_row(a, kRowSDot, p, t.live));
+        if (!cores.run2(128, tile, image_b2, 192, tile_dot, image_b2, 2))
+        {
+            break;
+        }
+        uint4* row_ub = pair_row(a, kRowUBar, p, t.live);
+        uint4* row_udb = pair_row(a, kRowUDotBar, p, t.live);
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float u[32];
+            float ud[32];
+            umma::load32(cores.tmem + 128 + 32 * half, u);
+            umma::load32(cores.tmem + 192 + 32 * half, ud);
+            umma::wait_loads();
+            float first[32];
+            float first_dot[32];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float ub[8];
+                float udb[8];
+#pragma unroll
+                for (int e2 = 0; e2 < 2; ++e2)
+                {
+                    const int q = 2 * c + e2;
+                    const int k = 32 * half + 4 * q;
+                    float f[4];
+                    float fd[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                    {
+                        const float raw = u[4 * q + j] + bias2[k + j];
+                        f[j] = raw * t.envelope;
+                        fd[j] = ud[4 * q + j] * t.envelope + raw * t.moving;
+                    }
+                    float fb[4] = {0.f, 0.f, 0.f, 0.f};
+                    float fdb[4] = {0.f, 0.f, 0.f, 0.f};
+                    float to_first[4] = {0.f, 0.f, 0.f, 0.f};
+                    float to_first_dot[4] = {0.f, 0.f, 0.f, 0.f};
+                    if (t.live)
+                    {
+                        const std::int64_t ra = 16 * static_cast<std::int64_t>(t.ab.x) + k / 4;
+                        const std::int64_t rb = 16 * static_cast<std::int64_t>(t.ab.y) + k / 4;
+                        const float4 va4 = load4(a.v, ra);
+                        const float4 vb4 = load4(a.v, rb);
+                        const float4 vda4 = load4(a.v_dot, ra);
+                        const float4 vdb4 = load4(a.v_dot, rb);
+                        const float4 ma4 = load4(a.m_bar, ra);
+                        const float4 mb4 = load4(a.m_bar, rb);
+                        const float4 mda4 = load4(a.m_dot_bar, ra);
+                        const float4 mdb4 = load4(a.m_dot_bar, rb);
+                        const float va[4] = {va4.x, va4.y, va4.z, va4.w};
+                        const float vb[4] = {vb4.x, vb4.y, vb4.z, vb4.w};
+                        const float vda[4] = {vda4.x, vda4.y, vda4.z, vda4.w};
+                        const float vdb[4] = {vdb4.x, vdb4.y, vdb4.z, vdb4.w};
+                        const float ma[4] = {ma4.x, ma4.y, ma4.z, ma4.w};
+                        const float mb[4] = {mb4.x, mb4.y, mb4.z, mb4.w};
+                        const float mda[4] = {mda4.x, mda4.y, mda4.z, mda4.w};
+                        const float mdb[4] = {mdb4.x, mdb4.y, mdb4.z, mdb4.w};
+                        float to_second[4];
+                        float to_second_dot[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                        {
+                            fb[j] = ma[j] * vb[j] + mb[j] * va[j] + mda[j] * vdb[j] +
+                                    mdb[j] * vda[j];
+                            fdb[j] = mda[j] * vb[j] + mdb[j] * va[j];
+                            to_second[j] = f[j] * ma[j] + fd[j] * mda[j];
+                            to_second_dot[j] = f[j] * mda[j];
+                            to_first[j] = f[j] * mb[j] + fd[j] * mdb[j];
+                            to_first_dot[j] = f[j] * mdb[j];
+                        }
+                        atomicAdd(vbar4 + rb, make_float4(to_second[0], to_second[1],
+                                                          to_second[2], to_second[3]));
+                        atomicAdd(vdbar4 + rb, make_float4(to_second_dot[0], to_second_dot[1],
+                                                           to_second_dot[2], to_second_dot[3]));
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                    {
+                        first[4 * q + j] = to_first[j];
+                        first_dot[4 * q + j] = to_first_dot[j];
+                        ub[4 * e2 + j] = fb[j] * t.envelope + fdb[j] * t.moving;
+                        udb[4 * e2 + j] = fdb[j] * t.envelope;
+                    }
+                }
+                const int column = 4 * half + c;
+                const uint4 word = umma::pack8(ub);
+                const uint4 word_dot = umma::pack8(udb);
+                *reinterpret_cast<uint4*>(tile + umma::image_offset(threadIdx.x, 8 * column)) = word;
+                *reinterpret_cast<uint4*>(tile_dot + umma::image_offset(threadIdx.x, 8 * column)) =
+                    word_dot;
+                if (row_ub != nullptr)
+                {
+                    row_ub[column] = word;
+                    row_udb[column] = word_dot;
+                }
+            }
+            add_runs(stage, tile_first, a.v_bar, half, first);
+            add_runs(stage, tile_first, a.v_dot_bar, half, first_dot);
+        }
+        if (!cores.run2(128, tile, image_b2t, 192, tile_dot, image_b2t, 3))
+        {
+            break;
+        }
+        uint4* row_zb = pair_row(a, kRowZBar, p, t.live);
+        uint4* row_zdb = pair_row(a, kRowZDotBar, p, t.live);
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            float sb[32];
+            float sdb[32];
+            float z[32];
+            float zd[32];
+            umma::load32(cores.tmem + 128 + 32 * half, sb);
+            umma::load32(cores.tmem + 192 + 32 * half, sdb);
+            umma::load32(cores.tmem + 32 * half, z);
+            umma::load32(cores.tmem + 64 + 32 * half, zd);
+            umma::wait_loads();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                float zb[8];
+                float zdb[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                {
+                    const int i = 8 * c + e;
+                    const float sg = sigmoid(z[i] + bias1[32 * half + i]);
+                    zb[e] = sb[i] * sg + sdb[i] * zd[i] * sg * (1.0f - sg);
+                    zdb[e] = sdb[i] * sg;
+                }
+                if (row_zb != nullptr)
+                {
+                    row_zb[4 * half + c] = umma::pack8(zb);
+                    row_zdb[4 * half + c] = umma::pack8(zdb);
+                }
+            }
+        }
+    }
+    cores.close(256);
+}
+
+}  // namespace
+}  // namespace nd
+
+extern "C" {
+
+int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction,
+                      nd_stream_t stream_handle)
+{
+    using namespace nd;
+    ND_REQUIRE(args != nullptr, "args is null");
+    ND_REQUIRE(direction == 0 || direction == 1, "direction must be 0 (forward) or 1 (reverse)");
+    const nd_schnet_tangent_args& s = *args;
+    ND_REQUIRE(s.num_atoms >= 1 && s.num_atoms <= (int64_t{1} << 30), "num_atoms out of range");
+    ND_REQUIRE(s.num_columns >= 0 && s.num_columns < (int64_t{1} << 31), "num_columns out of range");
+    ND_REQUIRE(s.interactions >= 1 && s.interactions <= 64, "interactions out of range");
+    ND_REQUIRE(s.block >= 0 && s.block < s.interactions, "block out of range");
+    ND_REQUIRE(s.num_types >= 1, "num_types must be positive");
+    ND_REQUIRE(s.gaussians >= 2 && s.gaussians <= 64, "gaussians must lie in [2, 64]");
+    ND_REQUIRE(s.cutoff > 0.0, "cutoff must be positive");
+    ND_REQUIRE(s.weights && s.workspace && s.force_adjoint && s.virial_adjoint && s.v && s.v_dot &&
+                   s.status,
+               "a required buffer is null");
+    ND_REQUIRE(reinterpret_cast<std::uintptr_t>(s.workspace) % 256 == 0 &&
+                   reinterpret_cast<std::uintptr_t>(s.weights) % 256 == 0,
+               "weights and workspace must be 256-byte aligned");
+    if (direction == 0)
+    {
+        ND_REQUIRE(s.m && s.m_dot, "the forward pass needs m and m_dot");
+    }
+    else
+    {
+        ND_REQUIRE(s.m_bar && s.m_dot_bar && s.v_bar && s.v_dot_bar && s.pair_rows,
+                   "the reverse pass needs m_bar, m_dot_bar, v_bar, v_dot_bar and pair_rows");
+        ND_REQUIRE(s.capacity >= s.num_columns, "capacity must be at least num_columns");
+        ND_REQUIRE(reinterpret_cast<std::uintptr_t>(s.pair_rows) % 16 == 0,
+                   "pair_rows must be 16-byte aligned");
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
+    const WeightLayout wl(s.interactions, s.num_types);
+    const Workspace ws(s.num_atoms, s.num_columns, s.interactions);
+    auto* weights = static_cast<const unsigned char*>(s.weights);
+    auto* base = static_cast<unsigned char*>(s.workspace);
+
+    TangentPass pass{};
+    pass.pairs = reinterpret_cast<const int2*>(base + ws.pairs);
+    pass.geometry = reinterpret_cast<const float4*>(base + ws.geometry);
+    pass.counters = reinterpret_cast<int*>(base + ws.counters);
+    pass.images = weights + static_cast<std::int64_t>(s.block) * kImagesPerBlock * umma::kImageBytes;
+    pass.b1 = reinterpret_cast<const float*>(weights + wl.vectors + (static_cast<std::int64_t>(s.block) * 4) * kFeatures * 4);
+    pass.b2 = reinterpret_cast<const float*>(weights + wl.vectors + (static_cast<std::int64_t>(s.block) * 4 + 1) * kFeatures * 4);
+    pass.force_adjoint = s.force_adjoint;
+    pass.virial_adjoint = s.virial_adjoint;
+    pass.v = static_cast<const uint2*>(s.v);
+    pass.v_dot = static_cast<const uint2*>(s.v_dot);
+    pass.m = s.m;
+    pass.m_dot = s.m_dot;
+    pass.m_bar = static_cast<const uint2*>(s.m_bar);
+    pass.m_dot_bar = static_cast<const uint2*>(s.m_dot_bar);
+    pass.v_bar = s.v_bar;
+    pass.v_dot_bar = s.v_dot_bar;
+    pass.rows = static_cast<uint4*>(s.pair_rows);
+    pass.capacity = s.capacity;
+    pass.width = static_cast<float>(s.cutoff / (s.gaussians - 1));
+    pass.phase = static_cast<float>(3.14159265358979323846 / s.cutoff);
+    pass.gaussians = s.gaussians;
+
+    static bool configured = false;
+    if (!configured)
+    {
+        ND_CUDA_TRY(cudaFuncSetAttribute(tangent_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTangentForwardShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(tangent_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTangentReverseShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(tangent_forward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+        ND_CUDA_TRY(cudaFuncSetAttribute(tangent_reverse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+        configured = true;
+    }
+    if (direction == 0)
+    {
+        const int grid = pair_grid(reinterpret_cast<const void*>(tangent_forward_kernel), kTangentForwardShared, 128);
+        tangent_forward_kernel<<<grid, kTile, kTangentForwardShared, stream>>>(pass);
+    }
+    else
+    {
+        const int grid = pair_grid(reinterpret_cast<const void*>(tangent_reverse_kernel), kTangentReverseShared, 256);
+        tangent_reverse_kernel<<<grid, kTile, kTangentReverseShared, stream>>>(pass);
+    }
+    ND_LAUNCH_CHECK();
+    ND_CUDA_TRY(cudaMemcpyAsync(s.status, pass.counters, 4 * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    return ND_OK;
+}
+
+}  // extern "C"

@@ -42,31 +42,38 @@ def workspace_bytes(num_atoms: int, num_columns: int, interactions: int) -> int:
 
 
 @torch.no_grad()
-def pack(model) -> Tensor:
-    """The model's parameter block, uint8 on the model's device."""
+def pack(model, values=None) -> Tensor:
+    """The model's parameter block, uint8 on the model's device; ``values`` (name -> tensor)
+    stand in for the model's own parameters of those names."""
+    given = dict(model.named_parameters())
+    if values is not None:
+        given.update(values)
+
+    def get(name: str) -> Tensor:
+        return given[name].detach().float()
+
     images, vectors = [], []
-    for block in model.blocks:
-        b1 = block.filter1.weight.detach().float()
-        b2 = block.filter2.weight.detach().float()
-        a = block.atoms.weight.detach().float()
-        d1 = block.update1.weight.detach().float()
-        d2 = block.update2.weight.detach().float()
+    for b in range(len(model.blocks)):
+        b1 = get(f"blocks.{b}.filter1.weight")
+        b2 = get(f"blocks.{b}.filter2.weight")
+        a = get(f"blocks.{b}.atoms.weight")
+        d1 = get(f"blocks.{b}.update1.weight")
+        d2 = get(f"blocks.{b}.update2.weight")
         for matrix in (_padded(b1, 64, 64), b2, b2.T, _padded(b1.T, 64, 64), a, a.T, d1, d1.T,
                        d2, d2.T):
             images.append(_image(matrix.contiguous()))
-        vectors += [block.filter1.bias, block.filter2.bias, block.update1.bias,
-                    block.update2.bias]
+        vectors += [get(f"blocks.{b}.{name}.bias")
+                    for name in ("filter1", "filter2", "update1", "update2")]
     e2 = torch.zeros(32, dtype=torch.float32, device=model.device)
-    e2[0] = model.readout2.bias.detach().float()[0]
+    e2[0] = get("readout2.bias")[0]
     floats = torch.cat([
-        *(v.detach().float() for v in vectors),
-        model.readout1.weight.detach().float().reshape(-1),
-        model.readout1.bias.detach().float(),
-        model.readout2.weight.detach().float().reshape(-1),
+        *vectors,
+        get("readout1.weight").reshape(-1),
+        get("readout1.bias"),
+        get("readout2.weight").reshape(-1),
         e2,
-        model.embedding.detach().float().reshape(-1),
-        (model.embedding.detach().float() @ model.blocks[0].atoms.weight.detach().float().T)
-        .reshape(-1),
+        get("embedding").reshape(-1),
+        (get("embedding") @ get("blocks.0.atoms.weight").T).reshape(-1),
     ])
     blob = torch.cat([torch.cat(images).view(torch.uint8), floats.view(torch.uint8)])
     expected = weight_bytes(len(model.blocks), model.num_types)
@@ -85,15 +92,17 @@ def packed(model) -> Tensor:
 
 def launch(model, positions: Tensor, cell: Tensor, index: Tensor, *, energy: Tensor,
            forces: Tensor | None, virial: Tensor | None, status: Tensor,
-           workspace: Tensor) -> None:
+           workspace: Tensor, weights: Tensor | None = None) -> None:
     """Launch the kernels into given buffers: energy [1] float64, forces [N, 3] float32 or
     None, virial [9] float64 or None, status [4] int32, and a workspace of at least
-    ``workspace_bytes`` for the index's columns. No allocation, no host sync: capturable."""
+    ``workspace_bytes`` for the index's columns; ``weights`` a parameter block from ``pack``
+    in place of the model's own. No allocation, no host sync: capturable."""
     args = SchNetArgs(
         num_atoms=model.num_atoms, num_columns=index.shape[1], interactions=len(model.blocks),
         num_types=model.num_types, gaussians=model.gaussians, reserved=0,
         cutoff=model.cutoff, positions=ptr(positions), cell=ptr(cell), pairs=ptr(index),
-        atom_types=ptr(model.atom_types), weights=ptr(packed(model)), workspace=ptr(workspace),
+        atom_types=ptr(model.atom_types),
+        weights=ptr(packed(model) if weights is None else weights), workspace=ptr(workspace),
         energy=ptr(energy), forces=ptr(forces), virial=ptr(virial), status=ptr(status),
     )
     call("nd_schnet_energy_force_virial", ctypes.byref(args), stream_handle(positions.device))

@@ -1,7 +1,9 @@
-"""Predictions and parameter gradients for models without a hand-written parameter backward.
+"""Predictions and parameter gradients of any Potential by the reference's algorithm.
 
-For any Potential other than Lennard-Jones (SchNet in particular) the channels of a batch of
-frames and their gradient in the trained parameters come from the reference's own algorithm
+A float32 SchNet on a GPU takes its loss gradient from the fused kernels and their written-out
+second-order pass (``_schnet_gradient``). For other models (and float64 SchNet) the channels of
+a batch of frames and their gradient in the trained parameters come from the reference's own
+algorithm
 (src/nabladyn/training/_loss.py:49-102, _fit.py:245-271): the model's definition under
 ``torch.func.functional_call``, E/F/W by ``torch.func`` (so a force or virial loss
 differentiates twice), vmapped over frames. ``loss_and_gradient`` runs the frames in chunks,
@@ -18,6 +20,7 @@ from torch import Tensor
 
 from .. import quantity
 from ..neighbors import NeighborPairs
+from . import _schnet_gradient
 from ._loss import loss as batch_loss
 
 _QUANTITIES = {
@@ -57,7 +60,20 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
                       weights: Mapping[str, float], scales: Mapping[str, float],
                       chunk: int = 4) -> tuple[Tensor, dict[str, Tensor]]:
     """The batch loss (frames weighted 1/B) and its gradient in ``parameters``, ``chunk``
-    frames at a time."""
+    frames at a time (a fused SchNet runs frame by frame on its kernels instead)."""
+    if _schnet_gradient.supported(model):
+        return _schnet_gradient.loss_and_gradient(model, parameters, positions, cells, stacks,
+                                                  labels, weights, scales)
+    return torch_func_loss_and_gradient(model, parameters, positions, cells, stacks, labels,
+                                        weights, scales, chunk)
+
+
+def torch_func_loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor,
+                                 cells: Tensor, stacks: tuple[Tensor, ...],
+                                 labels: Mapping[str, Tensor], weights: Mapping[str, float],
+                                 scales: Mapping[str, float],
+                                 chunk: int = 4) -> tuple[Tensor, dict[str, Tensor]]:
+    """``loss_and_gradient`` by the reference's torch.func algorithm, for any model."""
     frames = positions.shape[0]
     channels = tuple(name for name in ("energy", "forces", "virial") if name in labels)
     trained = {name: value.detach() for name, value in parameters.items()}
@@ -81,4 +97,4 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
     return total, gradient
 
 
-__all__ = ("predict", "loss_and_gradient")
+__all__ = ("predict", "loss_and_gradient", "torch_func_loss_and_gradient")
