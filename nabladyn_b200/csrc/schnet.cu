@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
     Cores cores;
     cores.open(barrier, slot, 64, a.counters, 1);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
-    const uint2* v2 = reinterpret_cast<const uint2*>(a.v);
+    const uint4* v8 = reinterpret_cast<const uint4*>(a.v);
     float4* m4 = reinterpret_cast<float4*>(a.m);
     __shared__ int tile_first[kTile];
 
@@ -309,26 +309,32 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
             umma::wait_loads();
             float part[32];
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
+            for (int c = 0; c < 4; ++c)
             {
-                const int k = 32 * half + 4 * q;
-                const float4 filter = make_float4((f[4 * q] + bias2[k]) * envelope,
-                                                  (f[4 * q + 1] + bias2[k + 1]) * envelope,
-                                                  (f[4 * q + 2] + bias2[k + 2]) * envelope,
-                                                  (f[4 * q + 3] + bias2[k + 3]) * envelope);
-                float4 vb = make_float4(0.f, 0.f, 0.f, 0.f);
+                const int k = 32 * half + 8 * c;
+                float filter[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    filter[j] = (f[8 * c + j] + bias2[k + j]) * envelope;
+                }
+                float vb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 if (live)
                 {
-                    const float4 va = load4(v2, 16 * static_cast<std::int64_t>(ab.x) + k / 4);
-                    vb = load4(v2, 16 * static_cast<std::int64_t>(ab.y) + k / 4);
-                    atomicAdd(m4 + 16 * static_cast<std::int64_t>(ab.y) + k / 4,
-                              make_float4(filter.x * va.x, filter.y * va.y, filter.z * va.z,
-                                          filter.w * va.w));
+                    const std::int64_t gb = 8 * static_cast<std::int64_t>(ab.y) + k / 8;
+                    float va[8];
+                    load8(v8, 8 * static_cast<std::int64_t>(ab.x) + k / 8, va);
+                    load8(v8, gb, vb);
+                    atomicAdd(m4 + 2 * gb, make_float4(filter[0] * va[0], filter[1] * va[1],
+                                                       filter[2] * va[2], filter[3] * va[3]));
+                    atomicAdd(m4 + 2 * gb + 1, make_float4(filter[4] * va[4], filter[5] * va[5],
+                                                           filter[6] * va[6], filter[7] * va[7]));
                 }
-                part[4 * q] = filter.x * vb.x;
-                part[4 * q + 1] = filter.y * vb.y;
-                part[4 * q + 2] = filter.z * vb.z;
-                part[4 * q + 3] = filter.w * vb.w;
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    part[8 * c + j] = filter[j] * vb[j];
+                }
             }
             add_runs(reinterpret_cast<float*>(work), tile_first, a.m, half, part);
         }
@@ -364,8 +370,8 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
     Cores cores;
     cores.open(barrier, slot, 128, a.counters, 2);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
-    const uint2* v2 = reinterpret_cast<const uint2*>(a.v);
-    const uint2* gm2 = reinterpret_cast<const uint2*>(a.grad_m);
+    const uint4* v8 = reinterpret_cast<const uint4*>(a.v);
+    const uint4* gm8 = reinterpret_cast<const uint4*>(a.grad_m);
     float4* gv4 = reinterpret_cast<float4*>(a.grad_v);
     __shared__ int tile_first[kTile];
     double w[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
@@ -428,45 +434,40 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
 #pragma unroll
             for (int c = 0; c < 4; ++c)
             {
-                float scaled[8];
+                const int k = 32 * half + 8 * c;
+                float scaled[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                for (int e2 = 0; e2 < 2; ++e2)
+                for (int j = 0; j < 8; ++j)
                 {
-                    const int q = 2 * c + e2;
-                    const int k = 32 * half + 4 * q;
-                    float4 gf = make_float4(0.f, 0.f, 0.f, 0.f);
-                    float4 to_first = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (live)
+                    part[8 * c + j] = 0.0f;
+                }
+                if (live)
+                {
+                    const std::int64_t ga = 8 * static_cast<std::int64_t>(ab.x) + k / 8;
+                    const std::int64_t gb = 8 * static_cast<std::int64_t>(ab.y) + k / 8;
+                    float va[8], vb[8], ma[8], mb[8];
+                    load8(v8, ga, va);
+                    load8(v8, gb, vb);
+                    load8(gm8, ga, ma);
+                    load8(gm8, gb, mb);
+                    float to_second[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
                     {
-                        const std::int64_t ra = 16 * static_cast<std::int64_t>(ab.x) + k / 4;
-                        const std::int64_t rb = 16 * static_cast<std::int64_t>(ab.y) + k / 4;
-                        const float4 va = load4(v2, ra);
-                        const float4 vb = load4(v2, rb);
-                        const float4 ga = load4(gm2, ra);
-                        const float4 gb = load4(gm2, rb);
-                        gf = make_float4(ga.x * vb.x + gb.x * va.x, ga.y * vb.y + gb.y * va.y,
-                                         ga.z * vb.z + gb.z * va.z, ga.w * vb.w + gb.w * va.w);
-                        const float f0 = f[4 * q] + bias2[k];
-                        const float f1 = f[4 * q + 1] + bias2[k + 1];
-                        const float f2 = f[4 * q + 2] + bias2[k + 2];
-                        const float f3 = f[4 * q + 3] + bias2[k + 3];
-                        along += gf.x * f0 + gf.y * f1 + gf.z * f2 + gf.w * f3;
-                        if (gv4 != nullptr)
-                        {
-                            atomicAdd(gv4 + rb, make_float4(f0 * envelope * ga.x, f1 * envelope * ga.y,
-                                                            f2 * envelope * ga.z, f3 * envelope * ga.w));
-                            to_first = make_float4(f0 * envelope * gb.x, f1 * envelope * gb.y,
-                                                   f2 * envelope * gb.z, f3 * envelope * gb.w);
-                        }
+                        const float gf = ma[j] * vb[j] + mb[j] * va[j];
+                        const float raw = f[8 * c + j] + bias2[k + j];
+                        along += gf * raw;
+                        to_second[j] = raw * envelope * ma[j];
+                        part[8 * c + j] = raw * envelope * mb[j];
+                        scaled[j] = gf * envelope;
                     }
-                    part[4 * q] = to_first.x;
-                    part[4 * q + 1] = to_first.y;
-                    part[4 * q + 2] = to_first.z;
-                    part[4 * q + 3] = to_first.w;
-                    scaled[4 * e2] = gf.x * envelope;
-                    scaled[4 * e2 + 1] = gf.y * envelope;
-                    scaled[4 * e2 + 2] = gf.z * envelope;
-                    scaled[4 * e2 + 3] = gf.w * envelope;
+                    if (gv4 != nullptr)
+                    {
+                        atomicAdd(gv4 + 2 * gb, make_float4(to_second[0], to_second[1],
+                                                            to_second[2], to_second[3]));
+                        atomicAdd(gv4 + 2 * gb + 1, make_float4(to_second[4], to_second[5],
+                                                                to_second[6], to_second[7]));
+                    }
                 }
                 umma::store8(work, threadIdx.x, 4 * half + c, scaled);
             }

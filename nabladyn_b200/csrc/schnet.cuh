@@ -118,12 +118,19 @@ __device__ __forceinline__ float sigmoid(float x)
 }
 
 // Feature rows that the pair kernels gather (v = x A^T and Gm) are kept in BF16: 128 B per
-// row. Four consecutive features as one 8-byte word, widened to floats.
-__device__ __forceinline__ float4 load4(const uint2* __restrict__ rows, std::int64_t group)
+// row, read 16 bytes at a time. Eight consecutive features (the word at group = 8 row +
+// feature / 8), widened to floats.
+__device__ __forceinline__ void load8(const uint4* __restrict__ rows, std::int64_t group,
+                                      float (&out)[8])
 {
-    const uint2 word = __ldg(rows + group);
-    return make_float4(__uint_as_float(word.x << 16), __uint_as_float(word.x & 0xFFFF0000u),
-                       __uint_as_float(word.y << 16), __uint_as_float(word.y & 0xFFFF0000u));
+    const uint4 word = __ldg(rows + group);
+    const std::uint32_t w[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        out[2 * i] = __uint_as_float(w[i] << 16);
+        out[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
+    }
 }
 
 __device__ __forceinline__ std::uint32_t pack2(float lo, float hi)

@@ -24,10 +24,11 @@
 // The reverse pass writes every pair's BF16 rows g, g_dot, s, s_dot, z_bar, z_dot_bar, u_bar,
 // u_dot_bar, so the filter weights' gradients, sums over pairs (B1: z_bar^T g + z_dot_bar^T
 // g_dot, B2: u_bar^T s + u_dot_bar^T s_dot, the biases the column sums of z_bar and u_bar), are
-// plain GEMMs for the caller, as are the atom-wise 64 x 64 layers. Each products' pair (value,
-// tangent) runs as two 128 x 64 x 64 BF16 tcgen05 products on one commit; the tiles' rows are
-// pairs in the compacted order of the preceding nd_schnet_energy_force_virial call, whose
-// workspace this pass reads.
+// plain GEMMs for the caller, as are the atom-wise 64 x 64 layers. With fewer than 64
+// Gaussians the g row's last column holds 1, so column 63 of z_bar^T g is the sum of z_bar.
+// Each product runs with its tangent as two 128 x 64 x 64 BF16 tcgen05 products on one commit;
+// the tiles' rows are pairs in the compacted order of the preceding
+// nd_schnet_energy_force_virial call, whose workspace this pass reads.
 
 #include "schnet.cuh"
 
@@ -57,12 +58,12 @@ struct TangentPass
     const float* b2;
     const float* force_adjoint;    // [N][3]
     const double* virial_adjoint;  // [9]
-    const uint2* v;                // [N][64] BF16
-    const uint2* v_dot;
+    const uint4* v;                // [N][64] BF16, 8 features a word
+    const uint4* v_dot;
     float* m;                      // forward: [N][64], added to
     float* m_dot;
-    const uint2* m_bar;            // reverse: [N][64] BF16
-    const uint2* m_dot_bar;
+    const uint4* m_bar;            // reverse: [N][64] BF16
+    const uint4* m_dot_bar;
     float* v_bar;                  // reverse: [N][64], added to
     float* v_dot_bar;
     uint4* rows;                   // reverse: [8][capacity][64] BF16 as 16-byte words
@@ -125,7 +126,8 @@ __device__ __forceinline__ uint4* pair_row(const TangentPass& a, int kind, int p
 }
 
 // g_k = exp(-(t - k)^2 / 2) (zero for k >= K) and g_dot_k = g_k (t - k) scale, scale = -rdot / D,
-// into this thread's row of two tiles, and into HBM rows when given.
+// into this thread's row of two tiles, and into HBM rows when given (there with g_63 = 1 when
+// K < 64).
 __device__ __forceinline__ void store_basis_tangent(unsigned char* tile, unsigned char* tile_dot,
                                                     float t, float scale, int gaussians, bool live,
                                                     uint4* row, uint4* row_dot)
@@ -149,7 +151,17 @@ __device__ __forceinline__ void store_basis_tangent(unsigned char* tile, unsigne
         *reinterpret_cast<uint4*>(tile_dot + umma::image_offset(threadIdx.x, 8 * c)) = word_dot;
         if (row != nullptr)
         {
-            row[c] = word;
+            // With K < 64 the HBM row's column 63 (a zero the products never use) holds 1, so
+            // the sum over pairs of z_bar^T g carries the bias gradient sum(z_bar) there.
+            if (c == 7 && gaussians < 64)
+            {
+                g[7] = 1.0f;
+                row[c] = umma::pack8(g);
+            }
+            else
+            {
+                row[c] = word;
+            }
             row_dot[c] = word_dot;
         }
     }
@@ -262,43 +274,50 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
             float first[32];
             float first_dot[32];
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
+            for (int c = 0; c < 4; ++c)
             {
-                const int k = 32 * half + 4 * q;
-                float f[4];
-                float fd[4];
+                const int k = 32 * half + 8 * c;
+                float f[8];
+                float fd[8];
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
+                for (int j = 0; j < 8; ++j)
                 {
-                    const float raw = u[4 * q + j] + bias2[k + j];
+                    const float raw = u[8 * c + j] + bias2[k + j];
                     f[j] = raw * t.envelope;
-                    fd[j] = ud[4 * q + j] * t.envelope + raw * t.moving;
+                    fd[j] = ud[8 * c + j] * t.envelope + raw * t.moving;
                 }
-                float4 vb = make_float4(0.f, 0.f, 0.f, 0.f);
-                float4 vdb = vb;
+                float vb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                float vdb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 if (t.live)
                 {
-                    const std::int64_t ra = 16 * static_cast<std::int64_t>(t.ab.x) + k / 4;
-                    const std::int64_t rb = 16 * static_cast<std::int64_t>(t.ab.y) + k / 4;
-                    const float4 va = load4(a.v, ra);
-                    const float4 vda = load4(a.v_dot, ra);
-                    vb = load4(a.v, rb);
-                    vdb = load4(a.v_dot, rb);
-                    atomicAdd(m4 + rb, make_float4(f[0] * va.x, f[1] * va.y, f[2] * va.z,
-                                                   f[3] * va.w));
-                    atomicAdd(md4 + rb, make_float4(fd[0] * va.x + f[0] * vda.x,
-                                                    fd[1] * va.y + f[1] * vda.y,
-                                                    fd[2] * va.z + f[2] * vda.z,
-                                                    fd[3] * va.w + f[3] * vda.w));
+                    const std::int64_t ga = 8 * static_cast<std::int64_t>(t.ab.x) + k / 8;
+                    const std::int64_t gb = 8 * static_cast<std::int64_t>(t.ab.y) + k / 8;
+                    float va[8];
+                    float vda[8];
+                    load8(a.v, ga, va);
+                    load8(a.v_dot, ga, vda);
+                    load8(a.v, gb, vb);
+                    load8(a.v_dot, gb, vdb);
+#pragma unroll
+                    for (int h4 = 0; h4 < 2; ++h4)
+                    {
+                        const int o = 4 * h4;
+                        atomicAdd(m4 + 2 * gb + h4,
+                                  make_float4(f[o] * va[o], f[o + 1] * va[o + 1],
+                                              f[o + 2] * va[o + 2], f[o + 3] * va[o + 3]));
+                        atomicAdd(md4 + 2 * gb + h4,
+                                  make_float4(fd[o] * va[o] + f[o] * vda[o],
+                                              fd[o + 1] * va[o + 1] + f[o + 1] * vda[o + 1],
+                                              fd[o + 2] * va[o + 2] + f[o + 2] * vda[o + 2],
+                                              fd[o + 3] * va[o + 3] + f[o + 3] * vda[o + 3]));
+                    }
                 }
-                first[4 * q] = f[0] * vb.x;
-                first[4 * q + 1] = f[1] * vb.y;
-                first[4 * q + 2] = f[2] * vb.z;
-                first[4 * q + 3] = f[3] * vb.w;
-                first_dot[4 * q] = fd[0] * vb.x + f[0] * vdb.x;
-                first_dot[4 * q + 1] = fd[1] * vb.y + f[1] * vdb.y;
-                first_dot[4 * q + 2] = fd[2] * vb.z + f[2] * vdb.z;
-                first_dot[4 * q + 3] = fd[3] * vb.w + f[3] * vdb.w;
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    first[8 * c + j] = f[j] * vb[j];
+                    first_dot[8 * c + j] = fd[j] * vb[j] + f[j] * vdb[j];
+                }
             }
             add_runs(stage, tile_first, a.m, half, first);
             add_runs(stage, tile_first, a.m_dot, half, first_dot);
@@ -376,71 +395,62 @@ __global__ void __launch_bounds__(kTile, 2) tangent_reverse_kernel(TangentPass a
 #pragma unroll
             for (int c = 0; c < 4; ++c)
             {
-                float ub[8];
-                float udb[8];
+                const int k = 32 * half + 8 * c;
+                float f[8];
+                float fd[8];
 #pragma unroll
-                for (int e2 = 0; e2 < 2; ++e2)
+                for (int j = 0; j < 8; ++j)
                 {
-                    const int q = 2 * c + e2;
-                    const int k = 32 * half + 4 * q;
-                    float f[4];
-                    float fd[4];
+                    const float raw = u[8 * c + j] + bias2[k + j];
+                    f[j] = raw * t.envelope;
+                    fd[j] = ud[8 * c + j] * t.envelope + raw * t.moving;
+                }
+                float ub[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                float udb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                    {
-                        const float raw = u[4 * q + j] + bias2[k + j];
-                        f[j] = raw * t.envelope;
-                        fd[j] = ud[4 * q + j] * t.envelope + raw * t.moving;
-                    }
-                    float fb[4] = {0.f, 0.f, 0.f, 0.f};
-                    float fdb[4] = {0.f, 0.f, 0.f, 0.f};
-                    float to_first[4] = {0.f, 0.f, 0.f, 0.f};
-                    float to_first_dot[4] = {0.f, 0.f, 0.f, 0.f};
-                    if (t.live)
-                    {
-                        const std::int64_t ra = 16 * static_cast<std::int64_t>(t.ab.x) + k / 4;
-                        const std::int64_t rb = 16 * static_cast<std::int64_t>(t.ab.y) + k / 4;
-                        const float4 va4 = load4(a.v, ra);
-                        const float4 vb4 = load4(a.v, rb);
-                        const float4 vda4 = load4(a.v_dot, ra);
-                        const float4 vdb4 = load4(a.v_dot, rb);
-                        const float4 ma4 = load4(a.m_bar, ra);
-                        const float4 mb4 = load4(a.m_bar, rb);
-                        const float4 mda4 = load4(a.m_dot_bar, ra);
-                        const float4 mdb4 = load4(a.m_dot_bar, rb);
-                        const float va[4] = {va4.x, va4.y, va4.z, va4.w};
-                        const float vb[4] = {vb4.x, vb4.y, vb4.z, vb4.w};
-                        const float vda[4] = {vda4.x, vda4.y, vda4.z, vda4.w};
-                        const float vdb[4] = {vdb4.x, vdb4.y, vdb4.z, vdb4.w};
-                        const float ma[4] = {ma4.x, ma4.y, ma4.z, ma4.w};
-                        const float mb[4] = {mb4.x, mb4.y, mb4.z, mb4.w};
-                        const float mda[4] = {mda4.x, mda4.y, mda4.z, mda4.w};
-                        const float mdb[4] = {mdb4.x, mdb4.y, mdb4.z, mdb4.w};
-                        float to_second[4];
-                        float to_second_dot[4];
+                for (int j = 0; j < 8; ++j)
+                {
+                    first[8 * c + j] = 0.0f;
+                    first_dot[8 * c + j] = 0.0f;
+                }
+                if (t.live)
+                {
+                    const std::int64_t ga = 8 * static_cast<std::int64_t>(t.ab.x) + k / 8;
+                    const std::int64_t gb = 8 * static_cast<std::int64_t>(t.ab.y) + k / 8;
+                    float va[8], vb[8], vda[8], vdb[8], ma[8], mb[8], mda[8], mdb[8];
+                    load8(a.v, ga, va);
+                    load8(a.v, gb, vb);
+                    load8(a.v_dot, ga, vda);
+                    load8(a.v_dot, gb, vdb);
+                    load8(a.m_bar, ga, ma);
+                    load8(a.m_bar, gb, mb);
+                    load8(a.m_dot_bar, ga, mda);
+                    load8(a.m_dot_bar, gb, mdb);
+                    float to_second[8];
+                    float to_second_dot[8];
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                        {
-                            fb[j] = ma[j] * vb[j] + mb[j] * va[j] + mda[j] * vdb[j] +
-                                    mdb[j] * vda[j];
-                            fdb[j] = mda[j] * vb[j] + mdb[j] * va[j];
-                            to_second[j] = f[j] * ma[j] + fd[j] * mda[j];
-                            to_second_dot[j] = f[j] * mda[j];
-                            to_first[j] = f[j] * mb[j] + fd[j] * mdb[j];
-                            to_first_dot[j] = f[j] * mdb[j];
-                        }
-                        atomicAdd(vbar4 + rb, make_float4(to_second[0], to_second[1],
-                                                          to_second[2], to_second[3]));
-                        atomicAdd(vdbar4 + rb, make_float4(to_second_dot[0], to_second_dot[1],
-                                                           to_second_dot[2], to_second_dot[3]));
+                    for (int j = 0; j < 8; ++j)
+                    {
+                        const float fb = ma[j] * vb[j] + mb[j] * va[j] + mda[j] * vdb[j] +
+                                         mdb[j] * vda[j];
+                        const float fdb = mda[j] * vb[j] + mdb[j] * va[j];
+                        to_second[j] = f[j] * ma[j] + fd[j] * mda[j];
+                        to_second_dot[j] = f[j] * mda[j];
+                        first[8 * c + j] = f[j] * mb[j] + fd[j] * mdb[j];
+                        first_dot[8 * c + j] = f[j] * mdb[j];
+                        ub[j] = fb * t.envelope + fdb * t.moving;
+                        udb[j] = fdb * t.envelope;
                     }
 #pragma unroll
-                    for (int j = 0; j < 4; ++j)
+                    for (int h4 = 0; h4 < 2; ++h4)
                     {
-                        first[4 * q + j] = to_first[j];
-                        first_dot[4 * q + j] = to_first_dot[j];
-                        ub[4 * e2 + j] = fb[j] * t.envelope + fdb[j] * t.moving;
-                        udb[4 * e2 + j] = fdb[j] * t.envelope;
+                        const int o = 4 * h4;
+                        atomicAdd(vbar4 + 2 * gb + h4,
+                                  make_float4(to_second[o], to_second[o + 1], to_second[o + 2],
+                                              to_second[o + 3]));
+                        atomicAdd(vdbar4 + 2 * gb + h4,
+                                  make_float4(to_second_dot[o], to_second_dot[o + 1],
+                                              to_second_dot[o + 2], to_second_dot[o + 3]));
                     }
                 }
                 const int column = 4 * half + c;
@@ -525,6 +535,13 @@ int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction,
     ND_REQUIRE(reinterpret_cast<std::uintptr_t>(s.workspace) % 256 == 0 &&
                    reinterpret_cast<std::uintptr_t>(s.weights) % 256 == 0,
                "weights and workspace must be 256-byte aligned");
+    auto aligned16 = [](const void* pointer) {
+        return reinterpret_cast<std::uintptr_t>(pointer) % 16 == 0;
+    };
+    ND_REQUIRE(aligned16(s.v) && aligned16(s.v_dot) && aligned16(s.m) && aligned16(s.m_dot) &&
+                   aligned16(s.m_bar) && aligned16(s.m_dot_bar) && aligned16(s.v_bar) &&
+                   aligned16(s.v_dot_bar),
+               "feature rows must be 16-byte aligned");
     if (direction == 0)
     {
         ND_REQUIRE(s.m && s.m_dot, "the forward pass needs m and m_dot");
@@ -552,12 +569,12 @@ int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction,
     pass.b2 = reinterpret_cast<const float*>(weights + wl.vectors + (static_cast<std::int64_t>(s.block) * 4 + 1) * kFeatures * 4);
     pass.force_adjoint = s.force_adjoint;
     pass.virial_adjoint = s.virial_adjoint;
-    pass.v = static_cast<const uint2*>(s.v);
-    pass.v_dot = static_cast<const uint2*>(s.v_dot);
+    pass.v = static_cast<const uint4*>(s.v);
+    pass.v_dot = static_cast<const uint4*>(s.v_dot);
     pass.m = s.m;
     pass.m_dot = s.m_dot;
-    pass.m_bar = static_cast<const uint2*>(s.m_bar);
-    pass.m_dot_bar = static_cast<const uint2*>(s.m_dot_bar);
+    pass.m_bar = static_cast<const uint4*>(s.m_bar);
+    pass.m_dot_bar = static_cast<const uint4*>(s.m_dot_bar);
     pass.v_bar = s.v_bar;
     pass.v_dot_bar = s.v_dot_bar;
     pass.rows = static_cast<uint4*>(s.pair_rows);

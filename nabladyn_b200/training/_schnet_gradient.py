@@ -34,6 +34,7 @@ from ..potential import _schnet_kernels as kernels
 _ROWS = 8
 _LN2 = 0.6931471805599453
 _PRODUCT_LOST = 16
+_CHUNK_ROWS = 1024
 
 
 def supported(model) -> bool:
@@ -45,6 +46,21 @@ def supported(model) -> bool:
 
 def _ssp(x: Tensor) -> Tensor:
     return functional.softplus(x) - _LN2
+
+
+def _gram(*terms: tuple[Tensor, Tensor]) -> Tensor:
+    """sum_i a_i^T b_i over [N, p] and [N, q] float32 pairs: one batched GEMM over chunks of
+    1,024 rows and a sum of the chunks (a p x q product with a long reduction would otherwise
+    run on a single CTA)."""
+    a = torch.cat([x for x, _ in terms])
+    b = torch.cat([y for _, y in terms])
+    pad = -a.shape[0] % _CHUNK_ROWS
+    if pad:
+        a = functional.pad(a, (0, 0, 0, pad))
+        b = functional.pad(b, (0, 0, 0, pad))
+    a = a.view(-1, _CHUNK_ROWS, a.shape[1])
+    b = b.view(-1, _CHUNK_ROWS, b.shape[1])
+    return torch.bmm(a.transpose(1, 2), b).sum(dim=0)
 
 
 class _Buffers:
@@ -65,6 +81,7 @@ class _Buffers:
         self.v_bar = torch.empty_like(self.m)
         self.v_dot_bar = torch.empty_like(self.m)
         self.rows = torch.empty((_ROWS, max(columns, 1), 64), dtype=torch.bfloat16, device=device)
+        self.ones = torch.ones((1, max(columns, 1)), dtype=torch.bfloat16, device=device)
 
 
 def _tangent(model, buffers: _Buffers, weights: Tensor, block: int, direction: int,
@@ -143,7 +160,7 @@ def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
     y_dot_bar = -sy * r2
     gradient["readout2.weight"][0] += (e * _ssp(y) - sy * y_dot).sum(dim=0)
     gradient["readout2.bias"][0] += e * model.num_atoms
-    gradient["readout1.weight"] += y_bar.T @ x + y_dot_bar.T @ x_dot
+    gradient["readout1.weight"] += _gram((y_bar, x), (y_dot_bar, x_dot))
     gradient["readout1.bias"] += y_bar.sum(dim=0)
     x_bar, x_dot_bar = y_bar @ r1, y_dot_bar @ r1
     k = model.gaussians
@@ -152,12 +169,12 @@ def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
         name = f"blocks.{b}."
         d2, d1 = w(name + "update2.weight"), w(name + "update1.weight")
         sg = torch.sigmoid(h)
-        gradient[name + "update2.weight"] += x_bar.T @ _ssp(h) + x_dot_bar.T @ (sg * h_dot)
+        gradient[name + "update2.weight"] += _gram((x_bar, _ssp(h)), (x_dot_bar, sg * h_dot))
         gradient[name + "update2.bias"] += x_bar.sum(dim=0)
         ssp_bar, q_bar = x_bar @ d2, x_dot_bar @ d2
         h_bar = ssp_bar * sg + q_bar * h_dot * sg * (1.0 - sg)
         h_dot_bar = q_bar * sg
-        gradient[name + "update1.weight"] += h_bar.T @ m + h_dot_bar.T @ m_dot
+        gradient[name + "update1.weight"] += _gram((h_bar, m), (h_dot_bar, m_dot))
         gradient[name + "update1.bias"] += h_bar.sum(dim=0)
         m_bar = (h_bar @ d1).to(torch.bfloat16)
         m_dot_bar = (h_dot_bar @ d1).to(torch.bfloat16)
@@ -170,14 +187,17 @@ def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
             f32 = torch.float32
             gradient[name + "filter2.weight"] += (torch.mm(u_bar.T, s, out_dtype=f32)
                                                  + torch.mm(u_dot_bar.T, s_dot, out_dtype=f32))
-            gradient[name + "filter2.bias"] += u_bar.sum(dim=0, dtype=f32)
-            gradient[name + "filter1.weight"] += (torch.mm(z_bar.T, g, out_dtype=f32)
-                                                 + torch.mm(z_dot_bar.T, g_dot,
-                                                            out_dtype=f32))[:, :k]
-            gradient[name + "filter1.bias"] += z_bar.sum(dim=0, dtype=f32)
+            gradient[name + "filter2.bias"] += torch.mm(buffers.ones[:, :count], u_bar,
+                                                        out_dtype=f32)[0]
+            filter1 = (torch.mm(z_bar.T, g, out_dtype=f32)
+                       + torch.mm(z_dot_bar.T, g_dot, out_dtype=f32))
+            gradient[name + "filter1.weight"] += filter1[:, :k]
+            # with K < 64 the kernel's g rows carry 1 in column 63: the sum of z_bar
+            gradient[name + "filter1.bias"] += (filter1[:, 63] if k < 64
+                                                else z_bar.sum(dim=0, dtype=f32))
         a = w(name + "atoms.weight")
         v_bar, v_dot_bar = buffers.v_bar, buffers.v_dot_bar
-        gradient[name + "atoms.weight"] += v_bar.T @ x + v_dot_bar.T @ x_dot
+        gradient[name + "atoms.weight"] += _gram((v_bar, x), (v_dot_bar, x_dot))
         x_bar = x_bar + v_bar @ a
         x_dot_bar = x_dot_bar + v_dot_bar @ a
     gradient["embedding"].index_add_(0, model.atom_types, x_bar)
