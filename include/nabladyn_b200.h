@@ -413,7 +413,7 @@ typedef struct nd_schnet_tangent_args {
     float* v_bar;                   /* reverse: [N, 64], added to */
     float* v_dot_bar;               /* reverse: [N, 64], added to */
     void* pair_rows;                /* reverse: [8, capacity, 64] BF16, rows of pairs in the
-                                       compacted order; rows past the pair count untouched */
+                                       compacted order; rows past the pair count set to zero */
     int64_t capacity;               /* at least num_columns */
     int32_t* status;                /* [4], as for nd_schnet_energy_force_virial */
 } nd_schnet_tangent_args;

@@ -510,6 +510,21 @@ __global__ void __launch_bounds__(kTile, 2) tangent_reverse_kernel(TangentPass a
     cores.close(256);
 }
 
+// Rows [count, capacity) of the eight per-pair arrays set to zero, the pair count read from the
+// workspace's counters, so sums over every row of an array equal sums over the pairs.
+__global__ void zero_tail_kernel(uint4* rows, std::int64_t capacity, const int* counters)
+{
+    const std::int64_t count = *reinterpret_cast<const volatile int*>(counters);
+    const std::int64_t words = (capacity - count) * 8;  // 16-byte words past the count, per array
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x;
+         i < 8 * words; i += stride)
+    {
+        const std::int64_t array = i / words;
+        rows[(array * capacity + count) * 8 + i % words] = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
 }  // namespace
 }  // namespace nd
 
@@ -601,6 +616,9 @@ int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction,
     {
         const int grid = pair_grid(reinterpret_cast<const void*>(tangent_reverse_kernel), kTangentReverseShared, 256);
         tangent_reverse_kernel<<<grid, kTile, kTangentReverseShared, stream>>>(pass);
+        ND_LAUNCH_CHECK();
+        zero_tail_kernel<<<std::min<std::int64_t>(1184, blocks_for(s.capacity * 8)), kThreads, 0, stream>>>(
+            pass.rows, s.capacity, pass.counters);
     }
     ND_LAUNCH_CHECK();
     ND_CUDA_TRY(cudaMemcpyAsync(s.status, pass.counters, 4 * sizeof(int), cudaMemcpyDeviceToDevice, stream));

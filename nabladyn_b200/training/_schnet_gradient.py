@@ -16,7 +16,8 @@ The per-pair work of steps 3 and 4 (the filter network with its tangent, the mes
 reverse) runs in the tcgen05 tangent kernels (nd_schnet_tangent); the atom-wise 64 x 64 layers,
 the readout and the sums over pairs of the filter weights' gradients are GEMMs with FP32
 results. Operands of the per-pair products are BF16, as in the E/F/W kernels, so the gradient
-agrees with the float64 definition to the BF16 level, not bitwise.
+agrees with the float64 definition to the BF16 level, not bitwise. One frame's work is one CUDA
+graph over static buffers, replayed frame after frame.
 """
 
 from __future__ import annotations
@@ -33,7 +34,6 @@ from ..potential import _schnet_kernels as kernels
 
 _ROWS = 8
 _LN2 = 0.6931471805599453
-_PRODUCT_LOST = 16
 _CHUNK_ROWS = 1024
 
 
@@ -105,10 +105,10 @@ def _tangent(model, buffers: _Buffers, weights: Tensor, block: int, direction: i
 
 
 def _frame_loss(energy: Tensor, forces: Tensor, virial: Tensor, labels: Mapping[str, Tensor],
-                weights: Mapping[str, float], scales: Mapping[str, float],
-                coefficient: float):
+                weights: Mapping[str, Tensor], scales: Mapping[str, Tensor], coefficient: Tensor):
     """The frame's loss term (float64, on the device) and its adjoints: e_bar (0-d), f_bar
-    [N, 3] float32, w_bar [9] float64 (zeros for channels without a weight)."""
+    [N, 3] float32, w_bar [9] float64 (zeros for channels without a weight). Weights, scales
+    and the frame's coefficient are 0-d float64 device tensors."""
     predicted = {"energy": energy.double().reshape(()), "forces": forces.double(),
                  "virial": virial.double().reshape(3, 3)}
     value = torch.zeros((), dtype=torch.float64, device=forces.device)
@@ -117,17 +117,16 @@ def _frame_loss(energy: Tensor, forces: Tensor, virial: Tensor, labels: Mapping[
         if name not in weights:
             adjoints[name] = torch.zeros_like(x)
             continue
-        scale = float(scales[name])
-        error = (x - labels[name].double().reshape(x.shape)) / scale
+        error = (x - labels[name]) / scales[name]
         value = value + coefficient * weights[name] * error.square().mean()
-        adjoints[name] = coefficient * weights[name] * 2.0 * error / scale / error.numel()
+        adjoints[name] = coefficient * weights[name] * 2.0 * error / scales[name] / error.numel()
     return (value, adjoints["energy"], adjoints["forces"].float().contiguous(),
             adjoints["virial"].reshape(9).contiguous())
 
 
 def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
-                    buffers: _Buffers, count: int, e_bar: Tensor, f_bar: Tensor,
-                    w_bar: Tensor, gradient: dict[str, Tensor]) -> None:
+                    buffers: _Buffers, e_bar: Tensor, f_bar: Tensor, w_bar: Tensor,
+                    gradient: dict[str, Tensor]) -> None:
     """Adds one frame's d(e_bar E - Edot)/dtheta to ``gradient`` (steps 3 and 4)."""
     def w(name: str) -> Tensor:
         return values[name]
@@ -181,26 +180,90 @@ def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
         buffers.v_bar.zero_()
         buffers.v_dot_bar.zero_()
         _tangent(model, buffers, weights_blob, b, 1, f_bar, w_bar, v, v_dot, m_bar, m_dot_bar)
-        if count > 0:
-            rows = buffers.rows[:, :count]
-            g, g_dot, s, s_dot, z_bar, z_dot_bar, u_bar, u_dot_bar = rows.unbind(0)
-            f32 = torch.float32
-            gradient[name + "filter2.weight"] += (torch.mm(u_bar.T, s, out_dtype=f32)
-                                                 + torch.mm(u_dot_bar.T, s_dot, out_dtype=f32))
-            gradient[name + "filter2.bias"] += torch.mm(buffers.ones[:, :count], u_bar,
-                                                        out_dtype=f32)[0]
-            filter1 = (torch.mm(z_bar.T, g, out_dtype=f32)
-                       + torch.mm(z_dot_bar.T, g_dot, out_dtype=f32))
-            gradient[name + "filter1.weight"] += filter1[:, :k]
-            # with K < 64 the kernel's g rows carry 1 in column 63: the sum of z_bar
-            gradient[name + "filter1.bias"] += (filter1[:, 63] if k < 64
-                                                else z_bar.sum(dim=0, dtype=f32))
+        # rows past the pair count are zero, so the sums run over every row
+        g, g_dot, s, s_dot, z_bar, z_dot_bar, u_bar, u_dot_bar = buffers.rows.unbind(0)
+        f32 = torch.float32
+        gradient[name + "filter2.weight"] += (torch.mm(u_bar.T, s, out_dtype=f32)
+                                             + torch.mm(u_dot_bar.T, s_dot, out_dtype=f32))
+        gradient[name + "filter2.bias"] += torch.mm(buffers.ones, u_bar, out_dtype=f32)[0]
+        filter1 = (torch.mm(z_bar.T, g, out_dtype=f32)
+                   + torch.mm(z_dot_bar.T, g_dot, out_dtype=f32))
+        gradient[name + "filter1.weight"] += filter1[:, :k]
+        # with K < 64 the kernel's g rows carry 1 in column 63: the sum of z_bar
+        gradient[name + "filter1.bias"] += (filter1[:, 63] if k < 64
+                                            else z_bar.sum(dim=0, dtype=f32))
         a = w(name + "atoms.weight")
         v_bar, v_dot_bar = buffers.v_bar, buffers.v_dot_bar
         gradient[name + "atoms.weight"] += _gram((v_bar, x), (v_dot_bar, x_dot))
         x_bar = x_bar + v_bar @ a
         x_dot_bar = x_dot_bar + v_dot_bar @ a
     gradient["embedding"].index_add_(0, model.atom_types, x_bar)
+
+
+class _Plan:
+    """Static buffers for one pair-stack width and set of loss channels (parameters, the frame's
+    inputs and labels, the loss weights, the accumulated loss, gradient and status bits) and
+    the CUDA graph of one frame's work over them: the first frame ever runs eagerly (it
+    configures the kernels and the GEMM library), the second is captured, every later one is
+    a replay. Kept on the model for the next call."""
+
+    def __init__(self, model, columns: int, channels: tuple[str, ...]):
+        device = model.device
+        n = model.num_atoms
+        f64 = torch.float64
+        self.key = (columns, channels)
+        self.device = device
+        self.buffers = _Buffers(model, columns)
+        self.values = {name: torch.empty(value.shape, dtype=torch.float32, device=device)
+                       for name, value in model.named_parameters()}
+        self.blob = torch.empty(kernels.weight_bytes(len(model.blocks), model.num_types),
+                                dtype=torch.uint8, device=device)
+        self.positions = torch.empty((n, 3), dtype=torch.float32, device=device)
+        self.cell = torch.empty(3, dtype=torch.float32, device=device)
+        self.index = torch.empty((2, columns), dtype=torch.int32, device=device)
+        shapes = {"energy": (), "forces": (n, 3), "virial": (3, 3)}
+        self.labels = {name: torch.empty(shapes[name], dtype=f64, device=device)
+                       for name in channels}
+        self.weights = {name: torch.empty((), dtype=f64, device=device) for name in channels}
+        self.scales = {name: torch.empty((), dtype=f64, device=device) for name in channels}
+        self.coefficient = torch.empty((), dtype=f64, device=device)
+        self.gradient = {name: torch.zeros_like(value) for name, value in self.values.items()}
+        self.total = torch.zeros((), dtype=f64, device=device)
+        self.bits = torch.zeros((), dtype=torch.int32, device=device)
+        self.warm = False
+        self.graph = None
+
+    def frame(self, model) -> None:
+        """One frame's loss and gradient from the static inputs, added to the accumulators."""
+        b = self.buffers
+        x = torch.remainder(self.positions, self.cell)
+        kernels.launch(model, x, self.cell, self.index, energy=b.energy, forces=b.forces,
+                       virial=b.virial, status=b.status, workspace=b.workspace,
+                       weights=self.blob)
+        value, e_bar, f_bar, w_bar = _frame_loss(b.energy[0], b.forces, b.virial, self.labels,
+                                                 self.weights, self.scales, self.coefficient)
+        self.total += value
+        _frame_gradient(model, self.values, self.blob, b, e_bar, f_bar, w_bar, self.gradient)
+        # the counters hold the frame's E/F/W and tangent bits; the last copy has them all
+        self.bits.bitwise_or_(b.status[1])
+
+    def run(self, model) -> None:
+        if self.graph is not None:
+            self.graph.replay()
+            return
+        if not self.warm:
+            side = torch.cuda.Stream(self.device)
+            side.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(side):
+                self.frame(model)
+            torch.cuda.current_stream(self.device).wait_stream(side)
+            self.warm = True
+            return
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self.frame(model)
+        self.graph = graph
+        graph.replay()
 
 
 def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor, cells: Tensor,
@@ -211,44 +274,50 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
     model's own values for the names not given), for a model with ``supported(model)``.
 
     positions [B, N, 3], cells [B, 3], one [B, 2, C] pair stack; labels of the weighted
-    channels. Syncs with the host once per frame (the pair count). Raises ``RuntimeError``
-    when a kernel reports a pair index out of range or a tensor-core product that did not
-    complete.
+    channels. Each frame is a few input copies and one CUDA-graph replay; the call syncs with
+    the host once, at its end. The buffers (about 1 KB per stack column) and the graph stay on
+    the model for the next call with the same stack width and channels. Raises
+    ``RuntimeError`` when a kernel reports a pair index out of range or a tensor-core product
+    that did not complete.
     """
     if not supported(model):
         raise ValueError("the fused SchNet gradient needs a float32 SchNet on a GPU with 64 "
                          "features and at most 64 Gaussians")
-    values = {name: value.detach().float() for name, value in model.named_parameters()}
-    values.update({name: value.detach().float() for name, value in parameters.items()})
-    blob = kernels.pack(model, values)
     stack = stacks[-1]
     frames, columns = positions.shape[0], stack.shape[-1]
-    buffers = _Buffers(model, columns)
-    gradient = {name: torch.zeros_like(value) for name, value in values.items()}
-    total = torch.zeros((), dtype=torch.float64, device=positions.device)
     channels = tuple(name for name in ("energy", "forces", "virial") if name in weights)
-    tangent_bits = torch.zeros((), dtype=torch.int32, device=positions.device)
-    for f in range(frames):
-        cell = cells[f].float().contiguous()
-        x = torch.remainder(positions[f].float(), cell).contiguous()
-        index = stack[f].to(torch.int32).contiguous()
-        kernels.launch(model, x, cell, index, energy=buffers.energy, forces=buffers.forces,
-                       virial=buffers.virial, status=buffers.status,
-                       workspace=buffers.workspace, weights=blob)
-        count, bits = buffers.status[:2].tolist()
-        if bits:
-            raise RuntimeError(f"SchNet kernels reported status {bits} (1: a pair index out "
-                               "of range; 16: a tensor-core product did not complete)")
-        part = {name: labels[name][f] for name in channels}
-        value, e_bar, f_bar, w_bar = _frame_loss(buffers.energy[0].float(), buffers.forces,
-                                                 buffers.virial.float(), part, weights, scales,
-                                                 1.0 / frames)
-        total = total + value
-        _frame_gradient(model, values, blob, buffers, count, e_bar, f_bar, w_bar, gradient)
-        tangent_bits.bitwise_or_(buffers.status[1])
-    if int(tangent_bits) & _PRODUCT_LOST:
-        raise RuntimeError("a tensor-core product of the SchNet tangent kernels did not complete")
-    return total, {name: gradient[name].to(value.dtype) for name, value in parameters.items()}
+    plan = getattr(model, "_gradient_plan", None)
+    if plan is None or plan.key != (columns, channels):
+        model._gradient_plan = None
+        plan = _Plan(model, columns, channels)
+        model._gradient_plan = plan
+    values = {name: value.detach().float() for name, value in model.named_parameters()}
+    values.update({name: value.detach().float() for name, value in parameters.items()})
+    with torch.no_grad():
+        for name, value in values.items():
+            plan.values[name].copy_(value)
+        plan.blob.copy_(kernels.pack(model, values))
+        for name in channels:
+            plan.weights[name].fill_(float(weights[name]))
+            plan.scales[name].fill_(float(scales[name]))
+        plan.coefficient.fill_(1.0 / frames)
+        plan.total.zero_()
+        plan.bits.zero_()
+        for value in plan.gradient.values():
+            value.zero_()
+        for f in range(frames):
+            plan.positions.copy_(positions[f])
+            plan.cell.copy_(cells[f])
+            plan.index.copy_(stack[f])
+            for name in channels:
+                plan.labels[name].copy_(labels[name][f])
+            plan.run(model)
+    bits = int(plan.bits)
+    if bits:
+        raise RuntimeError(f"SchNet kernels reported status {bits} (1: a pair index out of "
+                           "range; 16: a tensor-core product did not complete)")
+    return plan.total.clone(), {name: plan.gradient[name].to(value.dtype, copy=True)
+                                for name, value in parameters.items()}
 
 
 __all__ = ("supported", "loss_and_gradient")
