@@ -228,11 +228,13 @@ struct PairPass
     int last;                 // reverse: the last pass (block 0) applies forces and virial
 };
 
-// Shared memory of the pair passes: weight images, the basis tile, one work tile, biases.
 // Shared memory of the pair passes: weight images, one row tile (each product's operand
-// replaces the last once that product completed), biases, barrier and tensor-memory slot.
+// replaces the last once that product completed), biases, barrier and tensor-memory slot. The
+// reverse pass's 16 KB run stage overlays its B1 and B1^T images, which only the first and
+// the last product of a tile read; they are copied in again (from L2) after the stage was used,
+// so four CTAs fit an SM.
 constexpr int kPairForwardShared = 2 * umma::kImageBytes + umma::kTileBytes + 2 * 256 + 64;
-constexpr int kPairReverseShared = 4 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
+constexpr int kPairReverseShared = 4 * umma::kImageBytes + umma::kTileBytes + 2 * 256 + 64;
 
 __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
 {
@@ -346,13 +348,13 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
 {
     extern __shared__ __align__(1024) unsigned char shared[];
     unsigned char* image_b1 = shared;
-    unsigned char* image_b2 = image_b1 + umma::kImageBytes;
+    unsigned char* image_b1t = image_b1 + umma::kImageBytes;
+    unsigned char* image_b2 = image_b1t + umma::kImageBytes;
     unsigned char* image_b2t = image_b2 + umma::kImageBytes;
-    unsigned char* image_b1t = image_b2t + umma::kImageBytes;
-    unsigned char* basis = image_b1t + umma::kImageBytes;
+    unsigned char* basis = image_b2t + umma::kImageBytes;
     unsigned char* work = basis;  // each operand replaces the last once its product completed
-    float* stage = reinterpret_cast<float*>(work + umma::kTileBytes);  // Gv runs, 16 KB
-    float* bias1 = stage + kTile * 32;
+    float* stage = reinterpret_cast<float*>(image_b1);  // Gv runs, 16 KB over B1 and B1^T
+    float* bias1 = reinterpret_cast<float*>(work + umma::kTileBytes);
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
     auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
@@ -394,6 +396,11 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
         const float t = g.w / a.width;
         tile_first[threadIdx.x] = live ? ab.x : -1;
         cores.tile_index = tile;
+        if (gv4 != nullptr && tile != blockIdx.x)
+        {
+            // the previous tile's run stage overwrote B1
+            copy_bytes(image_b1, a.images + kB1 * umma::kImageBytes, umma::kImageBytes);
+        }
         store_basis(basis, t, a.gaussians, live);
         if (!cores.run(0, basis, image_b1, 1))
         {
@@ -500,6 +507,11 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
                 }
                 umma::store8(work, threadIdx.x, 4 * half + c, s);
             }
+        }
+        if (gv4 != nullptr)
+        {
+            // this tile's run stage overwrote B1^T
+            copy_bytes(image_b1t, a.images + kB1T * umma::kImageBytes, umma::kImageBytes);
         }
         if (!cores.run(64, work, image_b1t, 4))
         {
