@@ -29,6 +29,10 @@ Fixtures:
 * schnet_fit_gradient.npz — the reference's SchNet training loss over E/F/W on three frames of
   that system (labels from the seed-1 network) and its gradient in four of the seed-0
   network's parameters, by its training predict/loss under torch.func.
+* observables.npz — the reference's kinetic_energy, temperature and pressure
+  (src/nabladyn/observables.py:18-41) on seeded float64 velocities, masses, virials and cells.
+
+``python tests/golden/make_golden.py observables schnet`` writes only the fixtures named.
 """
 
 import os
@@ -48,6 +52,7 @@ from nabladyn.md._ensembles._npt import NPT  # noqa: E402
 from nabladyn.md._ensembles._nvt import NVT  # noqa: E402
 from nabladyn.md._state import _Frame  # noqa: E402
 from nabladyn.neighbors import NeighborPairs  # noqa: E402
+from nabladyn import observables as reference_observables  # noqa: E402
 from nabladyn.observables import kinetic_energy  # noqa: E402
 
 SIGMA, EPSILON, MASS, CUTOFF = 0.34, 0.996, 39.948, 1.0
@@ -332,13 +337,33 @@ def schnet_fit_gradient() -> None:
     np.savez_compressed(OUT / "schnet_fit_gradient.npz", **out)
 
 
+def observables() -> None:
+    generator = torch.Generator().manual_seed(21)
+    out = {}
+    for case, n in enumerate((1, 7, 512)):
+        velocities = torch.randn((n, 3), generator=generator, dtype=torch.float64)
+        masses = 1.0 + 50.0 * torch.rand(n, generator=generator, dtype=torch.float64)
+        virial = 100.0 * torch.randn((3, 3), generator=generator, dtype=torch.float64)
+        cell = 1.0 + 4.0 * torch.rand(3, generator=generator, dtype=torch.float64)
+        kinetic = reference_observables.kinetic_energy(velocities, masses)
+        out[f"{case}:velocities"] = velocities.numpy()
+        out[f"{case}:masses"] = masses.numpy()
+        out[f"{case}:virial"] = virial.numpy()
+        out[f"{case}:cell"] = cell.numpy()
+        out[f"{case}:kinetic"] = kinetic.numpy()
+        out[f"{case}:temperature"] = reference_observables.temperature(
+            kinetic, max(3 * n - 3, 1)).numpy()
+        out[f"{case}:pressure"] = reference_observables.pressure(kinetic, virial, cell).numpy()
+    np.savez_compressed(OUT / "observables.npz", **out)
+
+
+FIXTURES = {"argon": argon, "md": md, "lj_frames": lj_frames, "lj_fit_gradient": lj_fit_gradient,
+            "schnet": schnet, "schnet_fit_gradient": schnet_fit_gradient,
+            "sum_of_models": sum_of_models, "observables": observables}
+
+
 if __name__ == "__main__":
     torch.set_num_threads(os.cpu_count() or 1)
-    argon()
-    md()
-    lj_frames()
-    lj_fit_gradient()
-    schnet()
-    schnet_fit_gradient()
-    sum_of_models()
+    for name in sys.argv[1:] or FIXTURES:
+        FIXTURES[name]()
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
