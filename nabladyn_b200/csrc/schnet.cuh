@@ -120,10 +120,8 @@ __device__ __forceinline__ float sigmoid(float x)
 // Feature rows that the pair kernels gather (v = x A^T and Gm) are kept in BF16: 128 B per
 // row, read 16 bytes at a time. Eight consecutive features (the word at group = 8 row +
 // feature / 8), widened to floats.
-__device__ __forceinline__ void load8(const uint4* __restrict__ rows, std::int64_t group,
-                                      float (&out)[8])
+__device__ __forceinline__ void widen8(const uint4& word, float (&out)[8])
 {
-    const uint4 word = __ldg(rows + group);
     const std::uint32_t w[4] = {word.x, word.y, word.z, word.w};
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -131,6 +129,12 @@ __device__ __forceinline__ void load8(const uint4* __restrict__ rows, std::int64
         out[2 * i] = __uint_as_float(w[i] << 16);
         out[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
     }
+}
+
+__device__ __forceinline__ void load8(const uint4* __restrict__ rows, std::int64_t group,
+                                      float (&out)[8])
+{
+    widen8(__ldg(rows + group), out);
 }
 
 __device__ __forceinline__ std::uint32_t pack2(float lo, float hi)
@@ -258,21 +262,22 @@ __device__ __forceinline__ void store_basis(unsigned char* tile, float r_over_wi
     }
 }
 
-// Adds columns [32 half, 32 half + 32) of every pair's first-atom vector `part` to row
-// first[p] of `target` [N][64]. The tile's pairs keep the list's order, so a first atom's
-// pairs are runs of rows: the rows are staged in shared memory (16 KB, float4 chunks swizzled
-// by row against bank conflicts), each warp sums 32 rows column by column, and one atomic per
-// run and column replaces one per pair. Dead rows carry first = -1.
-__device__ __forceinline__ void add_runs(float* stage, const int* first, float* target, int half,
-                                         const float (&part)[32])
+// Run sums of first-atom rows. Every pair's first-atom vector (32 columns, [32 half,
+// 32 half + 32) of a [N][64] target) is staged in shared memory (16 KB: float4 chunks
+// swizzled by row against bank conflicts); the tile's pairs keep the list's order, so a first
+// atom's pairs are runs of rows: each warp sums 32 rows column by column and adds one atomic
+// per run and column instead of one per pair. Dead rows carry first = -1.
+
+// Stages chunk q (columns 4q .. 4q + 3 of the half) of this thread's row.
+__device__ __forceinline__ void put_run_part(float* stage, int q, float4 value)
 {
-    float4* row = reinterpret_cast<float4*>(stage) + threadIdx.x * 8;
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
-    {
-        row[q ^ (threadIdx.x & 7)] =
-            make_float4(part[4 * q], part[4 * q + 1], part[4 * q + 2], part[4 * q + 3]);
-    }
+    reinterpret_cast<float4*>(stage)[threadIdx.x * 8 + (q ^ (threadIdx.x & 7))] = value;
+}
+
+// Sums the staged rows over runs into `target` (after every thread staged its row).
+__device__ __forceinline__ void sum_runs(const float* stage, const int* first, float* target,
+                                         int half)
+{
     __syncthreads();
     const int column = threadIdx.x & 31;
     const int begin = (threadIdx.x >> 5) * 32;
@@ -292,6 +297,18 @@ __device__ __forceinline__ void add_runs(float* stage, const int* first, float* 
         }
     }
     __syncthreads();
+}
+
+__device__ __forceinline__ void add_runs(float* stage, const int* first, float* target, int half,
+                                         const float (&part)[32])
+{
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+    {
+        put_run_part(stage, q,
+                     make_float4(part[4 * q], part[4 * q + 1], part[4 * q + 2], part[4 * q + 3]));
+    }
+    sum_runs(stage, first, target, half);
 }
 
 // Resident CTAs per SM times the SM count, for a persistent grid: the least of the register

@@ -35,6 +35,9 @@
 namespace nd {
 namespace {
 
+// Feature words (8 features each) the reverse pass gathers before computing on them.
+constexpr int kGatherBatch = 2;
+
 // Per-pair rows of the reverse pass, in this order, [8][capacity][64] BF16.
 enum Row : int
 {
@@ -208,10 +211,10 @@ __device__ __forceinline__ void store_activations(std::uint32_t tmem, const floa
     }
 }
 
-// Shared memory: weight images, two row tiles, (reverse) a 16 KB run stage, biases, barrier
-// and tensor-memory slot.
+// Shared memory: weight images, two row tiles, (reverse) two 16 KB run stages, biases,
+// barrier and tensor-memory slot.
 constexpr int kTangentForwardShared = 2 * umma::kImageBytes + 2 * umma::kTileBytes + 2 * 256 + 64;
-constexpr int kTangentReverseShared = 3 * umma::kImageBytes + 3 * umma::kTileBytes + 2 * 256 + 64;
+constexpr int kTangentReverseShared = 3 * umma::kImageBytes + 4 * umma::kTileBytes + 2 * 256 + 64;
 
 __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a)
 {
@@ -334,8 +337,9 @@ __global__ void __launch_bounds__(kTile, 2) tangent_reverse_kernel(TangentPass a
     unsigned char* image_b2t = image_b2 + umma::kImageBytes;
     unsigned char* tile = image_b2t + umma::kImageBytes;
     unsigned char* tile_dot = tile + umma::kTileBytes;
-    float* stage = reinterpret_cast<float*>(tile_dot + umma::kTileBytes);  // 16 KB
-    float* bias1 = stage + kTile * 32;
+    float* stage = reinterpret_cast<float*>(tile_dot + umma::kTileBytes);  // v_bar runs, 16 KB
+    float* stage_dot = stage + kTile * 32;                                  // v_dot_bar runs
+    float* bias1 = stage_dot + kTile * 32;
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
     auto* slot = reinterpret_cast<std::uint32_t*>(barrier + 1);
@@ -385,88 +389,102 @@ __global__ void __launch_bounds__(kTile, 2) tangent_reverse_kernel(TangentPass a
 #pragma unroll
         for (int half = 0; half < 2; ++half)
         {
-            float u[32];
-            float ud[32];
-            umma::load32(cores.tmem + 128 + 32 * half, u);
-            umma::load32(cores.tmem + 192 + 32 * half, ud);
-            umma::wait_loads();
-            float first[32];
-            float first_dot[32];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int batch = 0; batch < 4; batch += kGatherBatch)
             {
-                const int k = 32 * half + 8 * c;
-                float f[8];
-                float fd[8];
+                // The batch's gathers first (eight rows, kGatherBatch words each), so their
+                // latencies overlap; dead rows read atom 0 and contribute zeros.
+                uint4 raw[kGatherBatch][8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int i = 0; i < kGatherBatch; ++i)
                 {
-                    const float raw = u[8 * c + j] + bias2[k + j];
-                    f[j] = raw * t.envelope;
-                    fd[j] = ud[8 * c + j] * t.envelope + raw * t.moving;
-                }
-                float ub[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                float udb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                {
-                    first[8 * c + j] = 0.0f;
-                    first_dot[8 * c + j] = 0.0f;
-                }
-                if (t.live)
-                {
+                    const int k = 32 * half + 8 * (batch + i);
                     const std::int64_t ga = 8 * static_cast<std::int64_t>(t.ab.x) + k / 8;
                     const std::int64_t gb = 8 * static_cast<std::int64_t>(t.ab.y) + k / 8;
+                    raw[i][0] = __ldg(a.v + ga);
+                    raw[i][1] = __ldg(a.v + gb);
+                    raw[i][2] = __ldg(a.v_dot + ga);
+                    raw[i][3] = __ldg(a.v_dot + gb);
+                    raw[i][4] = __ldg(a.m_bar + ga);
+                    raw[i][5] = __ldg(a.m_bar + gb);
+                    raw[i][6] = __ldg(a.m_dot_bar + ga);
+                    raw[i][7] = __ldg(a.m_dot_bar + gb);
+                }
+#pragma unroll
+                for (int i = 0; i < kGatherBatch; ++i)
+                {
+                    const int c = batch + i;
+                    const int k = 32 * half + 8 * c;
+                    float u[8];
+                    float ud[8];
+                    umma::load8(cores.tmem + 128 + k, u);
+                    umma::load8(cores.tmem + 192 + k, ud);
+                    umma::wait_loads();
                     float va[8], vb[8], vda[8], vdb[8], ma[8], mb[8], mda[8], mdb[8];
-                    load8(a.v, ga, va);
-                    load8(a.v, gb, vb);
-                    load8(a.v_dot, ga, vda);
-                    load8(a.v_dot, gb, vdb);
-                    load8(a.m_bar, ga, ma);
-                    load8(a.m_bar, gb, mb);
-                    load8(a.m_dot_bar, ga, mda);
-                    load8(a.m_dot_bar, gb, mdb);
-                    float to_second[8];
-                    float to_second_dot[8];
+                    widen8(raw[i][0], va);
+                    widen8(raw[i][1], vb);
+                    widen8(raw[i][2], vda);
+                    widen8(raw[i][3], vdb);
+                    widen8(raw[i][4], ma);
+                    widen8(raw[i][5], mb);
+                    widen8(raw[i][6], mda);
+                    widen8(raw[i][7], mdb);
+                    float ub[8], udb[8], first[8], first_dot[8], to_second[8], to_second_dot[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
                     {
+                        const float raw_filter = u[j] + bias2[k + j];
+                        const float f = raw_filter * t.envelope;
+                        const float fd = ud[j] * t.envelope + raw_filter * t.moving;
                         const float fb = ma[j] * vb[j] + mb[j] * va[j] + mda[j] * vdb[j] +
                                          mdb[j] * vda[j];
                         const float fdb = mda[j] * vb[j] + mdb[j] * va[j];
-                        to_second[j] = f[j] * ma[j] + fd[j] * mda[j];
-                        to_second_dot[j] = f[j] * mda[j];
-                        first[8 * c + j] = f[j] * mb[j] + fd[j] * mdb[j];
-                        first_dot[8 * c + j] = f[j] * mdb[j];
+                        to_second[j] = f * ma[j] + fd * mda[j];
+                        to_second_dot[j] = f * mda[j];
+                        first[j] = f * mb[j] + fd * mdb[j];
+                        first_dot[j] = f * mdb[j];
                         ub[j] = fb * t.envelope + fdb * t.moving;
                         udb[j] = fdb * t.envelope;
                     }
-#pragma unroll
-                    for (int h4 = 0; h4 < 2; ++h4)
+                    if (t.live)
                     {
-                        const int o = 4 * h4;
-                        atomicAdd(vbar4 + 2 * gb + h4,
-                                  make_float4(to_second[o], to_second[o + 1], to_second[o + 2],
-                                              to_second[o + 3]));
-                        atomicAdd(vdbar4 + 2 * gb + h4,
-                                  make_float4(to_second_dot[o], to_second_dot[o + 1],
-                                              to_second_dot[o + 2], to_second_dot[o + 3]));
+                        const std::int64_t gb = 8 * static_cast<std::int64_t>(t.ab.y) + k / 8;
+#pragma unroll
+                        for (int h4 = 0; h4 < 2; ++h4)
+                        {
+                            const int o = 4 * h4;
+                            atomicAdd(vbar4 + 2 * gb + h4,
+                                      make_float4(to_second[o], to_second[o + 1],
+                                                  to_second[o + 2], to_second[o + 3]));
+                            atomicAdd(vdbar4 + 2 * gb + h4,
+                                      make_float4(to_second_dot[o], to_second_dot[o + 1],
+                                                  to_second_dot[o + 2], to_second_dot[o + 3]));
+                        }
+                    }
+                    put_run_part(stage, 2 * c, make_float4(first[0], first[1], first[2], first[3]));
+                    put_run_part(stage, 2 * c + 1,
+                                 make_float4(first[4], first[5], first[6], first[7]));
+                    put_run_part(stage_dot, 2 * c,
+                                 make_float4(first_dot[0], first_dot[1], first_dot[2], first_dot[3]));
+                    put_run_part(stage_dot, 2 * c + 1,
+                                 make_float4(first_dot[4], first_dot[5], first_dot[6], first_dot[7]));
+                    const int column = 4 * half + c;
+                    const uint4 word = umma::pack8(ub);
+                    const uint4 word_dot = umma::pack8(udb);
+                    *reinterpret_cast<uint4*>(tile + umma::image_offset(threadIdx.x, 8 * column)) =
+                        word;
+                    *reinterpret_cast<uint4*>(tile_dot +
+                                              umma::image_offset(threadIdx.x, 8 * column)) =
+                        word_dot;
+                    if (row_ub != nullptr)
+                    {
+                        row_ub[column] = word;
+                        row_udb[column] = word_dot;
                     }
                 }
-                const int column = 4 * half + c;
-                const uint4 word = umma::pack8(ub);
-                const uint4 word_dot = umma::pack8(udb);
-                *reinterpret_cast<uint4*>(tile + umma::image_offset(threadIdx.x, 8 * column)) = word;
-                *reinterpret_cast<uint4*>(tile_dot + umma::image_offset(threadIdx.x, 8 * column)) =
-                    word_dot;
-                if (row_ub != nullptr)
-                {
-                    row_ub[column] = word;
-                    row_udb[column] = word_dot;
-                }
             }
-            add_runs(stage, tile_first, a.v_bar, half, first);
-            add_runs(stage, tile_first, a.v_dot_bar, half, first_dot);
+            sum_runs(stage, tile_first, a.v_bar, half);
+            sum_runs(stage_dot, tile_first, a.v_dot_bar, half);
         }
         if (!cores.run2(128, tile, image_b2t, 192, tile_dot, image_b2t, 3))
         {

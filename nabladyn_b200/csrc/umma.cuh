@@ -148,6 +148,22 @@ __device__ __forceinline__ void load32(std::uint32_t tmem, float (&out)[32])
     }
 }
 
+// 8 consecutive 32-bit columns of this thread's lane (follow with wait_loads()).
+__device__ __forceinline__ void load8(std::uint32_t tmem, float (&out)[8])
+{
+    std::uint32_t r[8];
+    __syncwarp();
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7])
+                 : "r"(tmem));
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        out[i] = __uint_as_float(r[i]);
+    }
+}
+
 __device__ __forceinline__ void wait_loads()
 {
     __syncwarp();

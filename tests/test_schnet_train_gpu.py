@@ -152,3 +152,62 @@ def test_fit_on_fused_gradient(cuda, fixture):
     assert report.loss.shape == (4,) and np.isfinite(report.loss).all()
     for name, value in model.named_parameters():
         assert not torch.equal(value.detach(), before[name]), name
+
+
+def compare_with_torch_func(cuda, model, positions, cells, stack, labels, weights):
+    scales = training.scales(**labels)
+    params = {k: v.detach().clone() for k, v in model.named_parameters()}
+    value, gradient = training.loss_and_gradient(model, params, positions, cells, (stack,),
+                                                 labels, weights, scales)
+    expected_value, expected = _generic.torch_func_loss_and_gradient(
+        model, params, positions, cells, (stack,), labels, weights, scales, chunk=1)
+    assert float(value) == pytest.approx(float(expected_value), rel=LOSS_TOL)
+    errors = {name: relative(gradient[name].cpu().numpy(), expected[name].cpu().numpy())
+              for name in expected if float(expected[name].abs().max()) > 0}
+    assert max(errors.values()) <= GRAD_TOL, errors
+    for name in expected:
+        if float(expected[name].abs().max()) == 0:
+            assert float(gradient[name].abs().max()) == 0, name
+
+
+@pytest.mark.parametrize("gaussians, weights", [
+    (64, {"energy": 1.0, "forces": 1.0, "virial": 1.0}),  # no spare basis column
+    (50, {"energy": 1.0}),
+    (50, {"forces": 2.0}),
+    (50, {"virial": 0.5}),
+])
+def test_fused_gradient_sizes_and_channels(cuda, fixture, gaussians, weights):
+    """The 343-bead frames with 64 Gaussians (the filter1 bias summed apart) and with losses
+    over one channel, against the torch.func algorithm on the same float32 model."""
+    golden, fit = fixture
+    n = golden["positions"].shape[0]
+    types = torch.tensor(golden["atom_types"], device=cuda)
+    model = potential.schnet(atom_types=types, num_types=2, cutoff=1.2, gaussians=gaussians,
+                             trainable=True)
+    teacher = potential.schnet(atom_types=types, num_types=2, cutoff=1.2, gaussians=gaussians,
+                               seed=1)
+    positions = torch.tensor(fit["positions"], dtype=torch.float32, device=cuda)
+    cells = torch.tensor(fit["cells"], dtype=torch.float32, device=cuda)
+    first, second = np.triu_indices(n, 1)
+    stack = torch.tensor(np.stack([first, second]), dtype=torch.int32,
+                         device=cuda)[None].expand(positions.shape[0], 2, -1).contiguous()
+    channels = tuple(name for name in CHANNELS if name in weights)
+    predicted = training.predict(teacher, {}, positions, cells, (stack,), channels)
+    labels = {k: v.detach() for k, v in predicted.items()}
+    compare_with_torch_func(cuda, model, positions, cells, stack, labels, weights)
+
+
+def test_fused_gradient_without_pairs(cuda):
+    """Eight beads 2 nm apart in a 16 nm box: no pair within the cutoff, so only the
+    embedding, the atom-wise layers and the readout carry gradient; padding columns only."""
+    grid = np.stack(np.meshgrid(*[np.arange(2)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    positions = torch.tensor(2.0 * grid + 1.0, dtype=torch.float32, device=cuda)[None]
+    cells = torch.full((1, 3), 16.0, dtype=torch.float32, device=cuda)
+    first, second = np.triu_indices(8, 1)
+    stack = torch.tensor(np.stack([first, second]), dtype=torch.int32, device=cuda)[None]
+    types = torch.tensor([0, 1] * 4, device=cuda)
+    model = potential.schnet(atom_types=types, num_types=2, cutoff=1.2, trainable=True)
+    labels = {"energy": torch.tensor([0.5], device=cuda),
+              "forces": torch.zeros((1, 8, 3), device=cuda)}
+    compare_with_torch_func(cuda, model, positions, cells, stack, labels,
+                            {"energy": 1.0, "forces": 1.0})
