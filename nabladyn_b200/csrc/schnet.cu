@@ -303,42 +303,56 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
         {
             break;
         }
+        float* stage = reinterpret_cast<float*>(work);  // free once the second product is done
 #pragma unroll
         for (int half = 0; half < 2; ++half)
         {
-            float f[32];
-            umma::load32(cores.tmem + 32 * half, f);
-            umma::wait_loads();
-            float part[32];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int batch = 0; batch < 4; batch += kGatherBatch)
             {
-                const int k = 32 * half + 8 * c;
-                float filter[8];
+                // The batch's gathers first, so their latencies overlap; dead rows read atom 0
+                // and contribute zeros (their envelope is zero).
+                uint4 raw[kGatherBatch][2];
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int i = 0; i < kGatherBatch; ++i)
                 {
-                    filter[j] = (f[8 * c + j] + bias2[k + j]) * envelope;
-                }
-                float vb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                if (live)
-                {
-                    const std::int64_t gb = 8 * static_cast<std::int64_t>(ab.y) + k / 8;
-                    float va[8];
-                    load8(v8, 8 * static_cast<std::int64_t>(ab.x) + k / 8, va);
-                    load8(v8, gb, vb);
-                    atomicAdd(m4 + 2 * gb, make_float4(filter[0] * va[0], filter[1] * va[1],
-                                                       filter[2] * va[2], filter[3] * va[3]));
-                    atomicAdd(m4 + 2 * gb + 1, make_float4(filter[4] * va[4], filter[5] * va[5],
-                                                           filter[6] * va[6], filter[7] * va[7]));
+                    const int k = 32 * half + 8 * (batch + i);
+                    raw[i][0] = __ldg(v8 + 8 * static_cast<std::int64_t>(ab.x) + k / 8);
+                    raw[i][1] = __ldg(v8 + 8 * static_cast<std::int64_t>(ab.y) + k / 8);
                 }
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int i = 0; i < kGatherBatch; ++i)
                 {
-                    part[8 * c + j] = filter[j] * vb[j];
+                    const int c = batch + i;
+                    const int k = 32 * half + 8 * c;
+                    float f[8];
+                    umma::load8(cores.tmem + k, f);
+                    umma::wait_loads();
+                    float va[8], vb[8], filter[8];
+                    widen8(raw[i][0], va);
+                    widen8(raw[i][1], vb);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                    {
+                        filter[j] = (f[j] + bias2[k + j]) * envelope;
+                    }
+                    if (live)
+                    {
+                        const std::int64_t gb = 8 * static_cast<std::int64_t>(ab.y) + k / 8;
+                        atomicAdd(m4 + 2 * gb, make_float4(filter[0] * va[0], filter[1] * va[1],
+                                                           filter[2] * va[2], filter[3] * va[3]));
+                        atomicAdd(m4 + 2 * gb + 1,
+                                  make_float4(filter[4] * va[4], filter[5] * va[5],
+                                              filter[6] * va[6], filter[7] * va[7]));
+                    }
+                    put_run_part(stage, 2 * c, make_float4(filter[0] * vb[0], filter[1] * vb[1],
+                                                           filter[2] * vb[2], filter[3] * vb[3]));
+                    put_run_part(stage, 2 * c + 1,
+                                 make_float4(filter[4] * vb[4], filter[5] * vb[5],
+                                             filter[6] * vb[6], filter[7] * vb[7]));
                 }
             }
-            add_runs(reinterpret_cast<float*>(work), tile_first, a.m, half, part);
+            sum_runs(stage, tile_first, a.m, half);
         }
     }
     cores.close(64);
@@ -434,53 +448,67 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
 #pragma unroll
         for (int half = 0; half < 2; ++half)
         {
-            float f[32];
-            umma::load32(cores.tmem + 64 + 32 * half, f);
-            umma::wait_loads();
-            float part[32];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int batch = 0; batch < 4; batch += kGatherBatch)
             {
-                const int k = 32 * half + 8 * c;
-                float scaled[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                // The batch's gathers first; dead rows read atom 0 and contribute zeros.
+                uint4 raw[kGatherBatch][4];
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int i = 0; i < kGatherBatch; ++i)
                 {
-                    part[8 * c + j] = 0.0f;
-                }
-                if (live)
-                {
+                    const int k = 32 * half + 8 * (batch + i);
                     const std::int64_t ga = 8 * static_cast<std::int64_t>(ab.x) + k / 8;
                     const std::int64_t gb = 8 * static_cast<std::int64_t>(ab.y) + k / 8;
+                    raw[i][0] = __ldg(v8 + ga);
+                    raw[i][1] = __ldg(v8 + gb);
+                    raw[i][2] = __ldg(gm8 + ga);
+                    raw[i][3] = __ldg(gm8 + gb);
+                }
+#pragma unroll
+                for (int i = 0; i < kGatherBatch; ++i)
+                {
+                    const int c = batch + i;
+                    const int k = 32 * half + 8 * c;
+                    float f[8];
+                    umma::load8(cores.tmem + 64 + k, f);
+                    umma::wait_loads();
                     float va[8], vb[8], ma[8], mb[8];
-                    load8(v8, ga, va);
-                    load8(v8, gb, vb);
-                    load8(gm8, ga, ma);
-                    load8(gm8, gb, mb);
-                    float to_second[8];
+                    widen8(raw[i][0], va);
+                    widen8(raw[i][1], vb);
+                    widen8(raw[i][2], ma);
+                    widen8(raw[i][3], mb);
+                    float scaled[8], to_first[8], to_second[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
                     {
                         const float gf = ma[j] * vb[j] + mb[j] * va[j];
-                        const float raw = f[8 * c + j] + bias2[k + j];
-                        along += gf * raw;
-                        to_second[j] = raw * envelope * ma[j];
-                        part[8 * c + j] = raw * envelope * mb[j];
+                        const float raw_filter = f[j] + bias2[k + j];
+                        along += gf * raw_filter;
+                        to_second[j] = raw_filter * envelope * ma[j];
+                        to_first[j] = raw_filter * envelope * mb[j];
                         scaled[j] = gf * envelope;
                     }
                     if (gv4 != nullptr)
                     {
-                        atomicAdd(gv4 + 2 * gb, make_float4(to_second[0], to_second[1],
-                                                            to_second[2], to_second[3]));
-                        atomicAdd(gv4 + 2 * gb + 1, make_float4(to_second[4], to_second[5],
-                                                                to_second[6], to_second[7]));
+                        if (live)
+                        {
+                            const std::int64_t gb = 8 * static_cast<std::int64_t>(ab.y) + k / 8;
+                            atomicAdd(gv4 + 2 * gb, make_float4(to_second[0], to_second[1],
+                                                                to_second[2], to_second[3]));
+                            atomicAdd(gv4 + 2 * gb + 1, make_float4(to_second[4], to_second[5],
+                                                                    to_second[6], to_second[7]));
+                        }
+                        put_run_part(stage, 2 * c, make_float4(to_first[0], to_first[1],
+                                                               to_first[2], to_first[3]));
+                        put_run_part(stage, 2 * c + 1, make_float4(to_first[4], to_first[5],
+                                                                   to_first[6], to_first[7]));
                     }
+                    umma::store8(work, threadIdx.x, 4 * half + c, scaled);
                 }
-                umma::store8(work, threadIdx.x, 4 * half + c, scaled);
             }
             if (gv4 != nullptr)
             {
-                add_runs(stage, tile_first, a.grad_v, half, part);
+                sum_runs(stage, tile_first, a.grad_v, half);
             }
         }
         if (!cores.run(64, work, image_b2t, 3))

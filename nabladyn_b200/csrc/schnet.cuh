@@ -21,6 +21,7 @@ constexpr int kHidden = 32;      // the readout's hidden layer, features / 2
 constexpr int kTile = 128;       // rows per tensor-core tile = threads per CTA
 constexpr int kImagesPerBlock = 10;
 constexpr float kLn2 = 0.693147180559945309f;
+constexpr int kGatherBatch = 2;  // feature words (8 features) a pair kernel gathers before use
 
 // Status bits of the SchNet status word.
 constexpr int kBadPair = 1;       // a pair index outside [0, N)

@@ -35,9 +35,6 @@
 namespace nd {
 namespace {
 
-// Feature words (8 features each) the reverse pass gathers before computing on them.
-constexpr int kGatherBatch = 2;
-
 // Per-pair rows of the reverse pass, in this order, [8][capacity][64] BF16.
 enum Row : int
 {
@@ -223,7 +220,9 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
     unsigned char* image_b2 = image_b1 + umma::kImageBytes;
     unsigned char* tile = image_b2 + umma::kImageBytes;
     unsigned char* tile_dot = tile + umma::kTileBytes;
-    float* stage = reinterpret_cast<float*>(tile);  // first-atom runs, once the products are done
+    // first-atom runs of m and m_dot, in the row tiles once the products are done
+    float* stage = reinterpret_cast<float*>(tile);
+    float* stage_dot = reinterpret_cast<float*>(tile_dot);
     float* bias1 = reinterpret_cast<float*>(tile_dot + umma::kTileBytes);
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
@@ -269,61 +268,78 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
 #pragma unroll
         for (int half = 0; half < 2; ++half)
         {
-            float u[32];
-            float ud[32];
-            umma::load32(cores.tmem + 32 * half, u);
-            umma::load32(cores.tmem + 64 + 32 * half, ud);
-            umma::wait_loads();
-            float first[32];
-            float first_dot[32];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int batch = 0; batch < 4; batch += kGatherBatch)
             {
-                const int k = 32 * half + 8 * c;
-                float f[8];
-                float fd[8];
+                // The batch's gathers first; dead rows read atom 0 and contribute zeros.
+                uint4 raw[kGatherBatch][4];
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int i = 0; i < kGatherBatch; ++i)
                 {
-                    const float raw = u[8 * c + j] + bias2[k + j];
-                    f[j] = raw * t.envelope;
-                    fd[j] = ud[8 * c + j] * t.envelope + raw * t.moving;
-                }
-                float vb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                float vdb[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                if (t.live)
-                {
+                    const int k = 32 * half + 8 * (batch + i);
                     const std::int64_t ga = 8 * static_cast<std::int64_t>(t.ab.x) + k / 8;
                     const std::int64_t gb = 8 * static_cast<std::int64_t>(t.ab.y) + k / 8;
-                    float va[8];
-                    float vda[8];
-                    load8(a.v, ga, va);
-                    load8(a.v_dot, ga, vda);
-                    load8(a.v, gb, vb);
-                    load8(a.v_dot, gb, vdb);
+                    raw[i][0] = __ldg(a.v + ga);
+                    raw[i][1] = __ldg(a.v + gb);
+                    raw[i][2] = __ldg(a.v_dot + ga);
+                    raw[i][3] = __ldg(a.v_dot + gb);
+                }
+#pragma unroll
+                for (int i = 0; i < kGatherBatch; ++i)
+                {
+                    const int c = batch + i;
+                    const int k = 32 * half + 8 * c;
+                    float u[8];
+                    float ud[8];
+                    umma::load8(cores.tmem + k, u);
+                    umma::load8(cores.tmem + 64 + k, ud);
+                    umma::wait_loads();
+                    float va[8], vb[8], vda[8], vdb[8], f[8], fd[8];
+                    widen8(raw[i][0], va);
+                    widen8(raw[i][1], vb);
+                    widen8(raw[i][2], vda);
+                    widen8(raw[i][3], vdb);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                    {
+                        const float raw_filter = u[j] + bias2[k + j];
+                        f[j] = raw_filter * t.envelope;
+                        fd[j] = ud[j] * t.envelope + raw_filter * t.moving;
+                    }
+                    if (t.live)
+                    {
+                        const std::int64_t gb = 8 * static_cast<std::int64_t>(t.ab.y) + k / 8;
+#pragma unroll
+                        for (int h4 = 0; h4 < 2; ++h4)
+                        {
+                            const int o = 4 * h4;
+                            atomicAdd(m4 + 2 * gb + h4,
+                                      make_float4(f[o] * va[o], f[o + 1] * va[o + 1],
+                                                  f[o + 2] * va[o + 2], f[o + 3] * va[o + 3]));
+                            atomicAdd(md4 + 2 * gb + h4,
+                                      make_float4(fd[o] * va[o] + f[o] * vda[o],
+                                                  fd[o + 1] * va[o + 1] + f[o + 1] * vda[o + 1],
+                                                  fd[o + 2] * va[o + 2] + f[o + 2] * vda[o + 2],
+                                                  fd[o + 3] * va[o + 3] + f[o + 3] * vda[o + 3]));
+                        }
+                    }
 #pragma unroll
                     for (int h4 = 0; h4 < 2; ++h4)
                     {
                         const int o = 4 * h4;
-                        atomicAdd(m4 + 2 * gb + h4,
-                                  make_float4(f[o] * va[o], f[o + 1] * va[o + 1],
-                                              f[o + 2] * va[o + 2], f[o + 3] * va[o + 3]));
-                        atomicAdd(md4 + 2 * gb + h4,
-                                  make_float4(fd[o] * va[o] + f[o] * vda[o],
-                                              fd[o + 1] * va[o + 1] + f[o + 1] * vda[o + 1],
-                                              fd[o + 2] * va[o + 2] + f[o + 2] * vda[o + 2],
-                                              fd[o + 3] * va[o + 3] + f[o + 3] * vda[o + 3]));
+                        put_run_part(stage, 2 * c + h4,
+                                     make_float4(f[o] * vb[o], f[o + 1] * vb[o + 1],
+                                                 f[o + 2] * vb[o + 2], f[o + 3] * vb[o + 3]));
+                        put_run_part(stage_dot, 2 * c + h4,
+                                     make_float4(fd[o] * vb[o] + f[o] * vdb[o],
+                                                 fd[o + 1] * vb[o + 1] + f[o + 1] * vdb[o + 1],
+                                                 fd[o + 2] * vb[o + 2] + f[o + 2] * vdb[o + 2],
+                                                 fd[o + 3] * vb[o + 3] + f[o + 3] * vdb[o + 3]));
                     }
                 }
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                {
-                    first[8 * c + j] = f[j] * vb[j];
-                    first_dot[8 * c + j] = fd[j] * vb[j] + f[j] * vdb[j];
-                }
             }
-            add_runs(stage, tile_first, a.m, half, first);
-            add_runs(stage, tile_first, a.m_dot, half, first_dot);
+            sum_runs(stage, tile_first, a.m, half);
+            sum_runs(stage_dot, tile_first, a.m_dot, half);
         }
     }
     cores.close(128);
