@@ -23,6 +23,7 @@ graph over static buffers, replayed frame after frame.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from collections.abc import Mapping
 
 import torch
@@ -33,6 +34,9 @@ from .._native import SchNetTangentArgs, call, ptr, stream_handle
 from ..potential import _schnet_kernels as kernels
 
 _ROWS = 8
+# Each model's plan (buffers and graph), beside the model rather than on it, so the module
+# still deep-copies and pickles; dropped with the model.
+_PLANS: "weakref.WeakKeyDictionary" = weakref.WeakKeyDictionary()
 _LN2 = 0.6931471805599453
 _CHUNK_ROWS = 1024
 
@@ -205,7 +209,7 @@ class _Plan:
     inputs and labels, the loss weights, the accumulated loss, gradient and status bits) and
     the CUDA graph of one frame's work over them: the first frame ever runs eagerly (it
     configures the kernels and the GEMM library), the second is captured, every later one is
-    a replay. Kept on the model for the next call."""
+    a replay. Kept beside the model for its next call."""
 
     def __init__(self, model, columns: int, channels: tuple[str, ...]):
         device = model.device
@@ -275,8 +279,9 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
 
     positions [B, N, 3], cells [B, 3], one [B, 2, C] pair stack; labels of the weighted
     channels. Each frame is a few input copies and one CUDA-graph replay; the call syncs with
-    the host once, at its end. The buffers (about 1 KB per stack column) and the graph stay on
-    the model for the next call with the same stack width and channels. Raises
+    the host once, at its end. The buffers (about 1 KB per stack column) and the graph stay
+    beside the model (until it is freed) for its next call with the same stack width and
+    channels. Raises
     ``RuntimeError`` when a kernel reports a pair index out of range or a tensor-core product
     that did not complete.
     """
@@ -286,11 +291,11 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
     stack = stacks[-1]
     frames, columns = positions.shape[0], stack.shape[-1]
     channels = tuple(name for name in ("energy", "forces", "virial") if name in weights)
-    plan = getattr(model, "_gradient_plan", None)
+    plan = _PLANS.get(model)
     if plan is None or plan.key != (columns, channels):
-        model._gradient_plan = None
+        _PLANS.pop(model, None)
         plan = _Plan(model, columns, channels)
-        model._gradient_plan = plan
+        _PLANS[model] = plan
     values = {name: value.detach().float() for name, value in model.named_parameters()}
     values.update({name: value.detach().float() for name, value in parameters.items()})
     with torch.no_grad():

@@ -211,3 +211,29 @@ def test_fused_gradient_without_pairs(cuda):
               "forces": torch.zeros((1, 8, 3), device=cuda)}
     compare_with_torch_func(cuda, model, positions, cells, stack, labels,
                             {"energy": 1.0, "forces": 1.0})
+
+
+def test_model_copies_after_fused_gradient(cuda, fixture):
+    """The gradient's buffers and graph live beside the model: it still deep-copies, and the
+    copy's gradient equals the original's to the atomics' summation order."""
+    import copy
+
+    golden, fit = fixture
+    model = potential.schnet(atom_types=torch.tensor(golden["atom_types"], device=cuda),
+                             num_types=2, cutoff=1.2, trainable=True)
+    n = golden["positions"].shape[0]
+    i, j = np.triu_indices(n, 1)
+    stack = torch.tensor(np.stack([i, j]), dtype=torch.int32, device=cuda)[None].contiguous()
+    positions = torch.tensor(fit["positions"][:1], dtype=torch.float32, device=cuda)
+    cells = torch.tensor(fit["cells"][:1], dtype=torch.float32, device=cuda)
+    labels = {"energy": torch.tensor(fit["label:energy"][:1], dtype=torch.float32, device=cuda)}
+    args = (positions, cells, (stack,), labels, {"energy": 1.0}, {"energy": 1.0})
+    params = {k: v.detach().clone() for k, v in model.named_parameters()}
+    value, gradient = training.loss_and_gradient(model, params, *args)
+    twin = copy.deepcopy(model)
+    twin_params = {k: v.detach().clone() for k, v in twin.named_parameters()}
+    twin_value, twin_gradient = training.loss_and_gradient(twin, twin_params, *args)
+    assert float(twin_value) == pytest.approx(float(value), rel=1e-6)
+    for name in gradient:
+        assert relative(twin_gradient[name].cpu().numpy(),
+                        gradient[name].cpu().numpy()) <= GRAD_TOL / 2, name
