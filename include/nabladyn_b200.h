@@ -420,6 +420,41 @@ typedef struct nd_schnet_tangent_args {
 
 int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction, nd_stream_t stream);
 
+/* The atom-wise layers of the same parameter gradient (the embedding, each block's A, D1, d1,
+ * D2, d2 and the readout, src/nabladyn/potential/_schnet/_potential.py:76-88, 190-208) with
+ * their tangents and reverse, in FP32, and the sums over atoms that give those parameters'
+ * gradients (added to `gradient`). Stages, with nd_schnet_tangent between them:
+ *   0 start (x_0 from the table, v_0; clears every block's message and scatter buffers),
+ *   1 block forward after its tangent forward pass (h, x', v' and their tangents),
+ *   2 readout (x_bar, x_dot_bar and the readout's gradients),
+ *   3 block reverse before its tangent reverse pass (m_bar, m_dot_bar; D2, d2, D1, d1),
+ *   4 block reverse after it (x_bar += v_bar A, x_dot_bar += v_dot_bar A; A).
+ * The per-atom arrays live in `workspace` at nd_schnet_atom_offset(N, blocks, kind, block):
+ * FP32 [N, 64] per block: 0 x, 1 x_dot, 2 h, 3 h_dot, 4 m, 5 m_dot, 6 v_bar, 7 v_dot_bar;
+ * FP32: 8 x and 9 x_dot after the last block, 10 x_bar, 11 x_dot_bar (after stage 4 of
+ * block 0: dL/d(embedding rows)); BF16 [N, 64]: 12 v, 13 v_dot per block, 14 m_bar,
+ * 15 m_dot_bar; 16 the per-tile partial sums. No counterpart in the reference. */
+typedef struct nd_schnet_atom_args {
+    int64_t num_atoms;              /* N */
+    int32_t interactions;           /* blocks */
+    int32_t num_types;              /* T */
+    const int64_t* atom_types;      /* [N] in [0, T) */
+    const float* parameters;        /* nd_schnet_atom_parameter_floats floats: per block
+                                       A [64][64], D1 [64][64], d1 [64], D2 [64][64], d2 [64];
+                                       then R1 [32][64], e1 [32], R2 [32], e2 (padded to 32);
+                                       then the embedding [T][64] */
+    float* gradient;                /* the same layout, added to */
+    const double* energy_adjoint;   /* [1] dL/dE */
+    void* workspace;                /* nd_schnet_atom_workspace_bytes, 256-byte aligned */
+} nd_schnet_atom_args;
+
+int64_t nd_schnet_atom_parameter_floats(int32_t interactions, int32_t num_types);
+int64_t nd_schnet_atom_workspace_bytes(int64_t num_atoms, int32_t interactions);
+int64_t nd_schnet_atom_offset(int64_t num_atoms, int32_t interactions, int32_t kind,
+                              int32_t block);
+int nd_schnet_atoms(const nd_schnet_atom_args* args, int32_t stage, int32_t block,
+                    nd_stream_t stream);
+
 /* ---- Integrator of frames in the caller's order ------------------------------------------
  * Velocity Verlet with the Nose-Hoover chain of three (src/nabladyn/md/_ensembles/_nve.py:39-58,
  * _nvt.py:88-129, _chain.py:23-105) and isotropic MTK NPT with chains on the particles and the

@@ -254,6 +254,19 @@ class SchNetTangentArgs(ctypes.Structure):
     ]
 
 
+class SchNetAtomArgs(ctypes.Structure):
+    _fields_ = [
+        ("num_atoms", ctypes.c_int64),
+        ("interactions", ctypes.c_int32),
+        ("num_types", ctypes.c_int32),
+        ("atom_types", ctypes.c_void_p),
+        ("parameters", ctypes.c_void_p),
+        ("gradient", ctypes.c_void_p),
+        ("energy_adjoint", ctypes.c_void_p),
+        ("workspace", ctypes.c_void_p),
+    ]
+
+
 class Integrator(ctypes.Structure):
     _fields_ = [
         ("dtype", ctypes.c_int),
@@ -326,6 +339,8 @@ _SIGNATURES = {
     ],
     "nd_schnet_energy_force_virial": [ctypes.POINTER(SchNetArgs), ctypes.c_void_p],
     "nd_schnet_tangent": [ctypes.POINTER(SchNetTangentArgs), ctypes.c_int32, ctypes.c_void_p],
+    "nd_schnet_atoms": [ctypes.POINTER(SchNetAtomArgs), ctypes.c_int32, ctypes.c_int32,
+                        ctypes.c_void_p],
     "nd_integrate_partial_slots": [ctypes.c_int64, c_int64_p],
     "nd_integrate_open": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],
     "nd_integrate_close": [ctypes.POINTER(Integrator), ctypes.c_int, ctypes.c_void_p],
@@ -336,6 +351,9 @@ _SIGNATURES = {
 _SIZES = {
     "nd_schnet_weight_bytes": [ctypes.c_int32, ctypes.c_int32],
     "nd_schnet_workspace_bytes": [ctypes.c_int64, ctypes.c_int64, ctypes.c_int32],
+    "nd_schnet_atom_parameter_floats": [ctypes.c_int32, ctypes.c_int32],
+    "nd_schnet_atom_workspace_bytes": [ctypes.c_int64, ctypes.c_int32],
+    "nd_schnet_atom_offset": [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
 }
 
 # Every symbol include/nabladyn_b200.h declares.

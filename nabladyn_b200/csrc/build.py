@@ -24,6 +24,7 @@ LIB = PACKAGE / "_lib"
 OBJ = LIB / "obj"
 
 CUDA_SOURCES = ("neighbors.cu", "lj.cu", "md.cu", "serve.cu", "schnet.cu", "schnet_tangent.cu",
+                "schnet_atoms.cu",
                 "integrate.cu")
 CXX_SOURCES = ("abi.cpp",)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

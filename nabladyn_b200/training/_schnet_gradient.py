@@ -13,9 +13,9 @@ parameters, which the reference takes with torch.func through a double backward
    the loss's.
 
 The per-pair work of steps 3 and 4 (the filter network with its tangent, the messages and their
-reverse) runs in the tcgen05 tangent kernels (nd_schnet_tangent); the atom-wise 64 x 64 layers,
-the readout and the sums over pairs of the filter weights' gradients are GEMMs with FP32
-results. Operands of the per-pair products are BF16, as in the E/F/W kernels, so the gradient
+reverse) runs in the tcgen05 tangent kernels (nd_schnet_tangent); the atom-wise layers, the
+readout and their weights' gradients in the FP32 atom kernels (nd_schnet_atoms); the sums over
+pairs of the filter weights' gradients are GEMMs with FP32 results. Operands of the per-pair products are BF16, as in the E/F/W kernels, so the gradient
 agrees with the float64 definition to the BF16 level, not bitwise. One frame's work is one CUDA
 graph over static buffers, replayed frame after frame.
 """
@@ -27,18 +27,26 @@ import weakref
 from collections.abc import Mapping
 
 import torch
-import torch.nn.functional as functional
 from torch import Tensor
 
-from .._native import SchNetTangentArgs, call, ptr, stream_handle
+from .._native import SchNetAtomArgs, SchNetTangentArgs, call, lib, ptr, stream_handle
 from ..potential import _schnet_kernels as kernels
 
 _ROWS = 8
 # Each model's plan (buffers and graph), beside the model rather than on it, so the module
 # still deep-copies and pickles; dropped with the model.
 _PLANS: "weakref.WeakKeyDictionary" = weakref.WeakKeyDictionary()
-_LN2 = 0.6931471805599453
-_CHUNK_ROWS = 1024
+# Per-atom arrays of the atom kernels' workspace (nd_schnet_atom_offset kinds).
+_X, _X_DOT, _H, _H_DOT, _M, _M_DOT, _V_BAR, _V_DOT_BAR = range(8)
+_X_BAR, _X_DOT_BAR, _V, _V_DOT, _M_BAR, _M_DOT_BAR = 10, 11, 12, 13, 14, 15
+# Offsets (floats) of the atom-side parameter block: per block A, D1, d1, D2, d2; readout.
+_BLOCK_FLOATS = 3 * 4096 + 2 * 64
+_BLOCK_PARTS = (("atoms.weight", 0, (64, 64)), ("update1.weight", 4096, (64, 64)),
+                ("update1.bias", 8192, (64,)), ("update2.weight", 8256, (64, 64)),
+                ("update2.bias", 12352, (64,)))
+_READOUT_PARTS = (("readout1.weight", 0, (32, 64)), ("readout1.bias", 2048, (32,)),
+                  ("readout2.weight", 2080, (1, 32)), ("readout2.bias", 2112, (1,)))
+_READOUT_FLOATS = 2048 + 3 * 32
 
 
 def supported(model) -> bool:
@@ -48,64 +56,97 @@ def supported(model) -> bool:
     return isinstance(model, SchNet) and model._fused_kernel
 
 
-def _ssp(x: Tensor) -> Tensor:
-    return functional.softplus(x) - _LN2
-
-
-def _gram(*terms: tuple[Tensor, Tensor]) -> Tensor:
-    """sum_i a_i^T b_i over [N, p] and [N, q] float32 pairs: one batched GEMM over chunks of
-    1,024 rows and a sum of the chunks (a p x q product with a long reduction would otherwise
-    run on a single CTA)."""
-    a = torch.cat([x for x, _ in terms])
-    b = torch.cat([y for _, y in terms])
-    pad = -a.shape[0] % _CHUNK_ROWS
-    if pad:
-        a = functional.pad(a, (0, 0, 0, pad))
-        b = functional.pad(b, (0, 0, 0, pad))
-    a = a.view(-1, _CHUNK_ROWS, a.shape[1])
-    b = b.view(-1, _CHUNK_ROWS, b.shape[1])
-    return torch.bmm(a.transpose(1, 2), b).sum(dim=0)
-
-
 class _Buffers:
     """Device buffers of one model size and pair-list width, reused frame after frame."""
 
     def __init__(self, model, columns: int):
         device = model.device
         n = model.num_atoms
+        blocks = len(model.blocks)
         self.columns = columns
-        self.workspace = torch.empty(kernels.workspace_bytes(n, columns, len(model.blocks)),
+        self.workspace = torch.empty(kernels.workspace_bytes(n, columns, blocks),
                                      dtype=torch.uint8, device=device)
         self.energy = torch.empty(1, dtype=torch.float64, device=device)
         self.forces = torch.empty((n, 3), dtype=torch.float32, device=device)
         self.virial = torch.empty(9, dtype=torch.float64, device=device)
         self.status = torch.empty(4, dtype=torch.int32, device=device)
-        self.m = torch.empty((n, 64), dtype=torch.float32, device=device)
-        self.m_dot = torch.empty_like(self.m)
-        self.v_bar = torch.empty_like(self.m)
-        self.v_dot_bar = torch.empty_like(self.m)
         self.rows = torch.empty((_ROWS, max(columns, 1), 64), dtype=torch.bfloat16, device=device)
         self.ones = torch.ones((1, max(columns, 1)), dtype=torch.bfloat16, device=device)
+        self.atoms = torch.empty(int(lib().nd_schnet_atom_workspace_bytes(n, blocks)),
+                                 dtype=torch.uint8, device=device)
+        self.n, self.blocks = n, blocks
+
+    def view(self, kind: int, block: int = 0) -> Tensor:
+        """Array `kind` (of `block`) of the atom kernels' workspace, [N, 64]."""
+        offset = int(lib().nd_schnet_atom_offset(self.n, self.blocks, kind, block))
+        bf16 = kind >= _V
+        size = self.n * 64 * (2 if bf16 else 4)
+        return self.atoms[offset:offset + size].view(
+            torch.bfloat16 if bf16 else torch.float32).view(self.n, 64)
 
 
 def _tangent(model, buffers: _Buffers, weights: Tensor, block: int, direction: int,
-             force_adjoint: Tensor, virial_adjoint: Tensor, v: Tensor, v_dot: Tensor,
-             m_bar: Tensor | None = None, m_dot_bar: Tensor | None = None) -> None:
+             force_adjoint: Tensor, virial_adjoint: Tensor) -> None:
     reverse = direction == 1
+    view = buffers.view
     args = SchNetTangentArgs(
         num_atoms=model.num_atoms, num_columns=buffers.columns,
         interactions=len(model.blocks), num_types=model.num_types, gaussians=model.gaussians,
         block=block, cutoff=model.cutoff, weights=ptr(weights), workspace=ptr(buffers.workspace),
-        force_adjoint=ptr(force_adjoint), virial_adjoint=ptr(virial_adjoint), v=ptr(v),
-        v_dot=ptr(v_dot), m=None if reverse else ptr(buffers.m),
-        m_dot=None if reverse else ptr(buffers.m_dot),
-        m_bar=ptr(m_bar) if reverse else None, m_dot_bar=ptr(m_dot_bar) if reverse else None,
-        v_bar=ptr(buffers.v_bar) if reverse else None,
-        v_dot_bar=ptr(buffers.v_dot_bar) if reverse else None,
+        force_adjoint=ptr(force_adjoint), virial_adjoint=ptr(virial_adjoint),
+        v=ptr(view(_V, block)), v_dot=ptr(view(_V_DOT, block)),
+        m=None if reverse else ptr(view(_M, block)),
+        m_dot=None if reverse else ptr(view(_M_DOT, block)),
+        m_bar=ptr(view(_M_BAR)) if reverse else None,
+        m_dot_bar=ptr(view(_M_DOT_BAR)) if reverse else None,
+        v_bar=ptr(view(_V_BAR, block)) if reverse else None,
+        v_dot_bar=ptr(view(_V_DOT_BAR, block)) if reverse else None,
         pair_rows=ptr(buffers.rows) if reverse else None, capacity=buffers.rows.shape[1],
         status=ptr(buffers.status),
     )
-    call("nd_schnet_tangent", ctypes.byref(args), direction, stream_handle(v.device))
+    call("nd_schnet_tangent", ctypes.byref(args), direction, stream_handle(force_adjoint.device))
+
+
+def _atoms(model, buffers: _Buffers, parameters: Tensor, gradient: Tensor, e_bar: Tensor,
+           stage: int, block: int) -> None:
+    args = SchNetAtomArgs(
+        num_atoms=model.num_atoms, interactions=len(model.blocks), num_types=model.num_types,
+        atom_types=ptr(model.atom_types), parameters=ptr(parameters), gradient=ptr(gradient),
+        energy_adjoint=ptr(e_bar), workspace=ptr(buffers.atoms),
+    )
+    call("nd_schnet_atoms", ctypes.byref(args), stage, block, stream_handle(gradient.device))
+
+
+def atom_parameters(values: Mapping[str, Tensor], blocks: int) -> Tensor:
+    """The FP32 atom-side parameter block of nd_schnet_atoms from parameters by name."""
+    parts = []
+    for b in range(blocks):
+        parts += [values[f"blocks.{b}.{name}"].reshape(-1) for name, _, _ in _BLOCK_PARTS]
+    parts += [values[name].reshape(-1) for name, _, _ in _READOUT_PARTS]
+    e2 = parts.pop()
+    parts += [e2, e2.new_zeros(31), values["embedding"].reshape(-1)]
+    return torch.cat([part.float() for part in parts])
+
+
+def atom_gradient_views(block: Tensor, blocks: int) -> dict[str, Tensor]:
+    """The parameters' views into a gradient block laid out as atom_parameters."""
+    views = {}
+    for b in range(blocks):
+        for name, offset, shape in _BLOCK_PARTS:
+            start = b * _BLOCK_FLOATS + offset
+            views[f"blocks.{b}.{name}"] = block[start:start + _numel(shape)].view(shape)
+    base = blocks * _BLOCK_FLOATS
+    for name, offset, shape in _READOUT_PARTS:
+        views[name] = block[base + offset:base + offset + _numel(shape)].view(shape)
+    views["embedding"] = block[base + _READOUT_FLOATS:].view(-1, 64)
+    return views
+
+
+def _numel(shape: tuple[int, ...]) -> int:
+    total = 1
+    for size in shape:
+        total *= size
+    return total
 
 
 def _frame_loss(energy: Tensor, forces: Tensor, virial: Tensor, labels: Mapping[str, Tensor],
@@ -128,65 +169,28 @@ def _frame_loss(energy: Tensor, forces: Tensor, virial: Tensor, labels: Mapping[
             adjoints["virial"].reshape(9).contiguous())
 
 
-def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
-                    buffers: _Buffers, e_bar: Tensor, f_bar: Tensor, w_bar: Tensor,
-                    gradient: dict[str, Tensor]) -> None:
-    """Adds one frame's d(e_bar E - Edot)/dtheta to ``gradient`` (steps 3 and 4)."""
-    def w(name: str) -> Tensor:
-        return values[name]
-
+def _frame_gradient(model, plan, e_bar: Tensor, f_bar: Tensor, w_bar: Tensor) -> None:
+    """Adds one frame's d(e_bar E - Edot)/dtheta to the plan's gradient (steps 3 and 4)."""
+    buffers, blob = plan.buffers, plan.blob
     blocks = len(model.blocks)
-    x = w("embedding")[model.atom_types]
-    x_dot = torch.zeros_like(x)
-    saved = []
-    for b in range(blocks):
-        a = w(f"blocks.{b}.atoms.weight")
-        v = (x @ a.T).to(torch.bfloat16)
-        v_dot = (x_dot @ a.T).to(torch.bfloat16)
-        buffers.m.zero_()
-        buffers.m_dot.zero_()
-        _tangent(model, buffers, weights_blob, b, 0, f_bar, w_bar, v, v_dot)
-        m, m_dot = buffers.m.clone(), buffers.m_dot.clone()
-        d1 = w(f"blocks.{b}.update1.weight")
-        h = torch.addmm(w(f"blocks.{b}.update1.bias"), m, d1.T)
-        h_dot = m_dot @ d1.T
-        saved.append((x, x_dot, v, v_dot, m, m_dot, h, h_dot))
-        d2 = w(f"blocks.{b}.update2.weight")
-        x = x + torch.addmm(w(f"blocks.{b}.update2.bias"), _ssp(h), d2.T)
-        x_dot = x_dot + (torch.sigmoid(h) * h_dot) @ d2.T
-    r1, r2 = w("readout1.weight"), w("readout2.weight")[0]
-    y = torch.addmm(w("readout1.bias"), x, r1.T)
-    y_dot = x_dot @ r1.T
-    sy = torch.sigmoid(y)
-    e = e_bar.float()
-    y_bar = (e * sy - sy * (1.0 - sy) * y_dot) * r2
-    y_dot_bar = -sy * r2
-    gradient["readout2.weight"][0] += (e * _ssp(y) - sy * y_dot).sum(dim=0)
-    gradient["readout2.bias"][0] += e * model.num_atoms
-    gradient["readout1.weight"] += _gram((y_bar, x), (y_dot_bar, x_dot))
-    gradient["readout1.bias"] += y_bar.sum(dim=0)
-    x_bar, x_dot_bar = y_bar @ r1, y_dot_bar @ r1
     k = model.gaussians
+
+    def atoms(stage: int, block: int = 0) -> None:
+        _atoms(model, buffers, plan.atom_parameters, plan.atom_gradient, e_bar, stage, block)
+
+    atoms(0)
+    for b in range(blocks):
+        _tangent(model, buffers, blob, b, 0, f_bar, w_bar)
+        atoms(1, b)
+    atoms(2)
+    f32 = torch.float32
     for b in reversed(range(blocks)):
-        x, x_dot, v, v_dot, m, m_dot, h, h_dot = saved[b]
-        name = f"blocks.{b}."
-        d2, d1 = w(name + "update2.weight"), w(name + "update1.weight")
-        sg = torch.sigmoid(h)
-        gradient[name + "update2.weight"] += _gram((x_bar, _ssp(h)), (x_dot_bar, sg * h_dot))
-        gradient[name + "update2.bias"] += x_bar.sum(dim=0)
-        ssp_bar, q_bar = x_bar @ d2, x_dot_bar @ d2
-        h_bar = ssp_bar * sg + q_bar * h_dot * sg * (1.0 - sg)
-        h_dot_bar = q_bar * sg
-        gradient[name + "update1.weight"] += _gram((h_bar, m), (h_dot_bar, m_dot))
-        gradient[name + "update1.bias"] += h_bar.sum(dim=0)
-        m_bar = (h_bar @ d1).to(torch.bfloat16)
-        m_dot_bar = (h_dot_bar @ d1).to(torch.bfloat16)
-        buffers.v_bar.zero_()
-        buffers.v_dot_bar.zero_()
-        _tangent(model, buffers, weights_blob, b, 1, f_bar, w_bar, v, v_dot, m_bar, m_dot_bar)
+        atoms(3, b)
+        _tangent(model, buffers, blob, b, 1, f_bar, w_bar)
         # rows past the pair count are zero, so the sums run over every row
         g, g_dot, s, s_dot, z_bar, z_dot_bar, u_bar, u_dot_bar = buffers.rows.unbind(0)
-        f32 = torch.float32
+        name = f"blocks.{b}."
+        gradient = plan.gradient
         gradient[name + "filter2.weight"] += (torch.mm(u_bar.T, s, out_dtype=f32)
                                              + torch.mm(u_dot_bar.T, s_dot, out_dtype=f32))
         gradient[name + "filter2.bias"] += torch.mm(buffers.ones, u_bar, out_dtype=f32)[0]
@@ -196,12 +200,8 @@ def _frame_gradient(model, values: Mapping[str, Tensor], weights_blob: Tensor,
         # with K < 64 the kernel's g rows carry 1 in column 63: the sum of z_bar
         gradient[name + "filter1.bias"] += (filter1[:, 63] if k < 64
                                             else z_bar.sum(dim=0, dtype=f32))
-        a = w(name + "atoms.weight")
-        v_bar, v_dot_bar = buffers.v_bar, buffers.v_dot_bar
-        gradient[name + "atoms.weight"] += _gram((v_bar, x), (v_dot_bar, x_dot))
-        x_bar = x_bar + v_bar @ a
-        x_dot_bar = x_dot_bar + v_dot_bar @ a
-    gradient["embedding"].index_add_(0, model.atom_types, x_bar)
+        atoms(4, b)
+    plan.gradient["embedding"].index_add_(0, model.atom_types, buffers.view(_X_BAR))
 
 
 class _Plan:
@@ -231,7 +231,14 @@ class _Plan:
         self.weights = {name: torch.empty((), dtype=f64, device=device) for name in channels}
         self.scales = {name: torch.empty((), dtype=f64, device=device) for name in channels}
         self.coefficient = torch.empty((), dtype=f64, device=device)
+        blocks = len(model.blocks)
+        self.atom_parameters = torch.empty(
+            int(lib().nd_schnet_atom_parameter_floats(blocks, model.num_types)),
+            dtype=torch.float32, device=device)
+        self.atom_gradient = torch.zeros_like(self.atom_parameters)
         self.gradient = {name: torch.zeros_like(value) for name, value in self.values.items()}
+        # the atom-side parameters' gradients are views into the atom kernels' gradient block
+        self.gradient.update(atom_gradient_views(self.atom_gradient, blocks))
         self.total = torch.zeros((), dtype=f64, device=device)
         self.bits = torch.zeros((), dtype=torch.int32, device=device)
         self.warm = False
@@ -247,7 +254,7 @@ class _Plan:
         value, e_bar, f_bar, w_bar = _frame_loss(b.energy[0], b.forces, b.virial, self.labels,
                                                  self.weights, self.scales, self.coefficient)
         self.total += value
-        _frame_gradient(model, self.values, self.blob, b, e_bar, f_bar, w_bar, self.gradient)
+        _frame_gradient(model, self, e_bar, f_bar, w_bar)
         # the counters hold the frame's E/F/W and tangent bits; the last copy has them all
         self.bits.bitwise_or_(b.status[1])
 
@@ -302,6 +309,7 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
         for name, value in values.items():
             plan.values[name].copy_(value)
         plan.blob.copy_(kernels.pack(model, values))
+        plan.atom_parameters.copy_(atom_parameters(values, len(model.blocks)))
         for name in channels:
             plan.weights[name].fill_(float(weights[name]))
             plan.scales[name].fill_(float(scales[name]))
@@ -310,6 +318,7 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
         plan.bits.zero_()
         for value in plan.gradient.values():
             value.zero_()
+        plan.atom_gradient.zero_()
         for f in range(frames):
             plan.positions.copy_(positions[f])
             plan.cell.copy_(cells[f])
