@@ -21,7 +21,8 @@
 // y_dot_bar^T x_dot, the biases and R2 column sums). One CTA of 256 threads takes 64 atoms:
 // rows and weights are staged in shared memory (FP32, rows of 68 floats), each thread
 // computes a 4 x 4 block of every 64 x 64 product, and every sum over atoms is written as the
-// tile's partial, then reduced over the tiles in a fixed order and added to the gradient.
+// tile's partial, then summed over 16 ranges of tiles in parallel and added to the gradient
+// (FP32 atomics: the order of those 16 additions varies).
 
 #include "common.cuh"
 
@@ -199,18 +200,31 @@ __device__ __forceinline__ void product(const float* A, const float* M, float (&
             acc[r][j] = 0.0f;
         }
     }
-#pragma unroll 8
-    for (int k = 0; k < 64; ++k)
+#pragma unroll 2
+    for (int k = 0; k < 64; k += 4)
     {
-        const float4 m = *reinterpret_cast<const float4*>(M + k * kRow + q.c0);
+        float a[4][4];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
         {
-            const float a = A[(q.a0 + r) * kRow + k];
-            acc[r][0] = fmaf(a, m.x, acc[r][0]);
-            acc[r][1] = fmaf(a, m.y, acc[r][1]);
-            acc[r][2] = fmaf(a, m.z, acc[r][2]);
-            acc[r][3] = fmaf(a, m.w, acc[r][3]);
+            const float4 row = *reinterpret_cast<const float4*>(A + (q.a0 + r) * kRow + k);
+            a[r][0] = row.x;
+            a[r][1] = row.y;
+            a[r][2] = row.z;
+            a[r][3] = row.w;
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+        {
+            const float4 m = *reinterpret_cast<const float4*>(M + (k + kk) * kRow + q.c0);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+            {
+                acc[r][0] = fmaf(a[r][kk], m.x, acc[r][0]);
+                acc[r][1] = fmaf(a[r][kk], m.y, acc[r][1]);
+                acc[r][2] = fmaf(a[r][kk], m.z, acc[r][2]);
+                acc[r][3] = fmaf(a[r][kk], m.w, acc[r][3]);
+            }
         }
     }
 }
@@ -659,16 +673,21 @@ struct Segments
     float* dst[4];
 };
 
+constexpr int kReduceSlices = 16;  // tile ranges summed in parallel, then added atomically
+
 __global__ void reduce_kernel(const float* __restrict__ partials, std::int64_t tiles, Segments s)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const std::int64_t per_slice = (tiles + kReduceSlices - 1) / kReduceSlices;
+    const std::int64_t begin = blockIdx.y * per_slice;
+    const std::int64_t end = min(tiles, begin + per_slice);
     for (int k = 0; k < s.count; ++k)
     {
         if (j < s.length[k])
         {
             float sums[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            std::int64_t t = 0;
-            for (; t + 4 <= tiles; t += 4)
+            std::int64_t t = begin;
+            for (; t + 4 <= end; t += 4)
             {
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
@@ -676,11 +695,14 @@ __global__ void reduce_kernel(const float* __restrict__ partials, std::int64_t t
                     sums[u] += partials[(t + u) * kPartialFloats + s.src[k] + j];
                 }
             }
-            for (; t < tiles; ++t)
+            for (; t < end; ++t)
             {
                 sums[0] += partials[t * kPartialFloats + s.src[k] + j];
             }
-            s.dst[k][j] += (sums[0] + sums[1]) + (sums[2] + sums[3]);
+            if (begin < end)
+            {
+                atomicAdd(s.dst[k] + j, (sums[0] + sums[1]) + (sums[2] + sums[3]));
+            }
             return;
         }
         j -= s.length[k];
@@ -785,7 +807,8 @@ int nd_schnet_atoms(const nd_schnet_atom_args* args, int32_t stage, int32_t bloc
         {
             total += segments.length[k];
         }
-        reduce_kernel<<<blocks_for(total), kThreads, 0, stream>>>(p.partials, layout.tiles, segments);
+        const dim3 grid(blocks_for(total), kReduceSlices);
+        reduce_kernel<<<grid, kThreads, 0, stream>>>(p.partials, layout.tiles, segments);
         ND_LAUNCH_CHECK();
         return ND_OK;
     };
