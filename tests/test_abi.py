@@ -119,3 +119,42 @@ def test_torch_ops_load_first_in_a_fresh_process():
                           timeout=120)
     assert done.returncode == 0, done.stderr
     assert done.stdout.strip() == "True"
+
+
+def test_schnet_training_entry_points_check_arguments():
+    """nd_schnet_tangent and nd_schnet_atoms reject null buffers, bad stages and directions
+    before any launch; the atom workspace's arrays are 256-byte aligned and in order."""
+    library = _native.lib()
+    tangent = _native.SchNetTangentArgs(num_atoms=100, num_columns=10, interactions=3,
+                                        num_types=1, gaussians=50, block=0, cutoff=1.2,
+                                        capacity=10)
+    assert library.nd_schnet_tangent(ctypes.byref(tangent), 0, None) == _native.ND_EINVAL
+    assert b"null" in library.nd_last_error()
+    assert library.nd_schnet_tangent(ctypes.byref(tangent), 2, None) == _native.ND_EINVAL
+    assert b"direction" in library.nd_last_error()
+    atoms = _native.SchNetAtomArgs(num_atoms=100, interactions=3, num_types=2)
+    assert library.nd_schnet_atoms(ctypes.byref(atoms), 0, 0, None) == _native.ND_EINVAL
+    assert b"null" in library.nd_last_error()
+    assert library.nd_schnet_atoms(ctypes.byref(atoms), 5, 0, None) == _native.ND_EINVAL
+    assert b"stage" in library.nd_last_error()
+    assert library.nd_schnet_atoms(ctypes.byref(atoms), 1, 3, None) == _native.ND_EINVAL
+    assert library.nd_schnet_atom_parameter_floats(3, 2) == 3 * (3 * 4096 + 128) + 2144 + 128
+    offsets = [library.nd_schnet_atom_offset(100, 3, kind, 2 if kind < 8 else 0)
+               for kind in range(17)]
+    assert all(offset >= 0 and offset % 256 == 0 for offset in offsets)
+    assert library.nd_schnet_atom_workspace_bytes(100, 3) > max(offsets)
+    assert library.nd_schnet_atom_offset(100, 3, 17, 0) == -1
+
+
+def test_schnet_tangent_rejects_small_row_capacity():
+    """The reverse pass needs pair rows for every column: a smaller capacity is refused before
+    anything is launched (the pointers here are never dereferenced)."""
+    library = _native.lib()
+    fake = ctypes.c_void_p(1 << 20)
+    tangent = _native.SchNetTangentArgs(
+        num_atoms=100, num_columns=10, interactions=3, num_types=1, gaussians=50, block=0,
+        cutoff=1.2, weights=fake, workspace=fake, force_adjoint=fake, virial_adjoint=fake,
+        v=fake, v_dot=fake, m=fake, m_dot=fake, m_bar=fake, m_dot_bar=fake, v_bar=fake,
+        v_dot_bar=fake, pair_rows=fake, capacity=5, status=fake)
+    assert library.nd_schnet_tangent(ctypes.byref(tangent), 1, None) == _native.ND_EINVAL
+    assert b"capacity" in library.nd_last_error()

@@ -141,3 +141,22 @@ def test_oracle_parameter_gradient_matches_reference(golden):
             name = key[len("grad:"):]
             np.testing.assert_allclose(gradient[name], fit[key], rtol=1e-8,
                                        atol=1e-8 * np.abs(fit[key]).max(), err_msg=name)
+
+
+def test_atom_parameter_block_layout():
+    """The FP32 atom-side parameter block the training kernels read (every block's A, D1, d1,
+    D2, d2, then the readout and the embedding) has the library's size, and the gradient views
+    over the same layout land on exactly those parameters."""
+    from nabladyn_b200 import _native
+    from nabladyn_b200.training import _schnet_gradient
+
+    model = potential.schnet(atom_types=torch.tensor([0, 1, 1]), num_types=2, cutoff=1.2,
+                             trainable=True)
+    values = {name: value.detach() for name, value in model.named_parameters()}
+    block = _schnet_gradient.atom_parameters(values, 3)
+    assert block.numel() == _native.lib().nd_schnet_atom_parameter_floats(3, 2)
+    views = _schnet_gradient.atom_gradient_views(block, 3)
+    for name, view in views.items():
+        assert torch.equal(view, values[name].float()), name
+    covered = set(views)
+    assert covered == {name for name in values if "filter" not in name}
