@@ -237,3 +237,35 @@ def test_model_copies_after_fused_gradient(cuda, fixture):
     for name in gradient:
         assert relative(twin_gradient[name].cpu().numpy(),
                         gradient[name].cpu().numpy()) <= GRAD_TOL / 2, name
+
+
+def test_fit_matches_torch_func_fit(cuda, fixture, monkeypatch):
+    """training.fit, four plain SGD updates over the fixture's frames, on the fused gradient
+    against the same fit on the reference's torch.func gradient (same start, seed and batches):
+    the losses and every parameter tensor's total change agree to the gradient's bound."""
+    golden, fit = fixture
+    types = torch.tensor(golden["atom_types"], device=cuda)
+    data = training.Dataset(fit["positions"].astype(np.float32), fit["cells"].astype(np.float32),
+                            energy=fit["label:energy"].astype(np.float32),
+                            forces=fit["label:forces"].astype(np.float32),
+                            virial=fit["label:virial"].astype(np.float32))
+
+    def run(fused: bool):
+        model = potential.schnet(atom_types=types, num_types=2, cutoff=1.2, trainable=True)
+        start = {k: v.detach().clone() for k, v in model.named_parameters()}
+        optimizer = torch.optim.SGD(model.parameters(), lr=1e-8)
+        with monkeypatch.context() as patch:
+            if not fused:
+                patch.setattr(_schnet_gradient, "supported", lambda m: False)
+            report = training.fit(model, data, optimizer, updates=4, batch_size=2, energy=1.0,
+                                  forces=1.0, virial=1.0, seed=3)
+        change = {k: (v.detach() - start[k]).double().cpu().numpy()
+                  for k, v in model.named_parameters()}
+        return report, change
+
+    fused_report, fused_change = run(True)
+    reference_report, reference_change = run(False)
+    np.testing.assert_allclose(fused_report.loss, reference_report.loss, rtol=LOSS_TOL)
+    errors = {name: relative(fused_change[name], reference_change[name])
+              for name in reference_change}
+    assert max(errors.values()) <= GRAD_TOL, errors
