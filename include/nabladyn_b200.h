@@ -385,7 +385,8 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
 /* The per-pair passes of SchNet's parameter gradient of a training loss over E, F and W, by
  * forward-over-reverse along the loss's adjoints: one block's filter network with its
  * derivative along each pair's rate rdot = (d . (dL/dF_a - dL/dF_b) + d^T dL/dW d) / r.
- * direction 0 (forward) adds the block's messages m and m_dot; direction 1 (reverse) adds
+ * direction 0 (forward) writes the block's messages m (those of the E/F/W call, from its
+ * workspace) and adds their tangent m_dot; direction 1 (reverse) adds
  * v_bar and v_dot_bar and writes every pair's BF16 rows (g, g_dot, s, s_dot, z_bar, z_dot_bar,
  * u_bar, u_dot_bar), from which the filter weights' gradients are sums over pairs. Reads the
  * compacted pairs in `workspace` of the nd_schnet_energy_force_virial call just made with the
@@ -406,7 +407,7 @@ typedef struct nd_schnet_tangent_args {
     const double* virial_adjoint;   /* [9] dL/dW, row-major */
     const void* v;                  /* [N, 64] BF16: this block's x A^T */
     const void* v_dot;              /* [N, 64] BF16: its derivative along the direction */
-    float* m;                       /* forward: [N, 64], added to */
+    float* m;                       /* forward: [N, 64], written */
     float* m_dot;                   /* forward: [N, 64], added to */
     const void* m_bar;              /* reverse: [N, 64] BF16 */
     const void* m_dot_bar;          /* reverse: [N, 64] BF16 */

@@ -1049,7 +1049,7 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
     auto* x = reinterpret_cast<float*>(at(ws.x));
     auto v = [&](int b) { return reinterpret_cast<float*>(at(ws.v + b * row_bytes)); };
     auto h = [&](int b) { return reinterpret_cast<float*>(at(ws.h + b * row_bytes)); };
-    auto* m = reinterpret_cast<float*>(at(ws.m));
+    auto m = [&](int b) { return reinterpret_cast<float*>(at(ws.m + b * row_bytes)); };
     auto* grad = reinterpret_cast<float*>(at(ws.grad));
     auto* grad_m = reinterpret_cast<float*>(at(ws.grad_m));
     auto* grad_v = reinterpret_cast<float*>(at(ws.grad_v));
@@ -1113,12 +1113,12 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
     for (int b = 0; b < s.interactions; ++b)
     {
         const bool last = b == s.interactions - 1;
-        ND_CUDA_TRY(cudaMemsetAsync(m, 0, s.num_atoms * kFeatures * 4, stream));
+        ND_CUDA_TRY(cudaMemsetAsync(m(b), 0, s.num_atoms * kFeatures * 4, stream));
         pass.images = block_images(b);
         pass.b1 = block_vector(b, 0);
         pass.b2 = block_vector(b, 1);
         pass.v = v(b);
-        pass.m = m;
+        pass.m = m(b);
         pair_forward_kernel<<<forward_grid, kTile, kPairForwardShared, stream>>>(pass);
         ND_LAUNCH_CHECK();
         AtomPass atoms{};
@@ -1127,7 +1127,7 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
         atoms.next_images = last ? nullptr : block_images(b + 1);
         atoms.d1 = block_vector(b, 2);
         atoms.d2 = block_vector(b, 3);
-        atoms.m = m;
+        atoms.m = m(b);
         atoms.h = h(b);
         atoms.x = x;
         atoms.v_next = last ? nullptr : v(b + 1);

@@ -85,8 +85,8 @@ struct Workspace
         x = geometry + align256(columns * 16);
         v = x + align256(row);
         h = v + blocks * align256(row);
-        m = h + blocks * align256(row);
-        grad = m + align256(row);
+        m = h + blocks * align256(row);  // one message buffer per block (the tangent pass reuses them)
+        grad = m + blocks * align256(row);
         grad_m = grad + align256(row);
         grad_v = grad_m + align256(row);
         dedr = grad_v + align256(row);

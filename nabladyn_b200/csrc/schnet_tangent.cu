@@ -12,7 +12,8 @@
 //   forward:  g, g_dot = g * (-(r / D - k) / D) rdot;  z, z_dot = (g, g_dot) B1^T (+ b1 on z);
 //             s = ssp(z), s_dot = sigmoid(z) z_dot;  u, u_dot = (s, s_dot) B2^T (+ b2 on u);
 //             f = u C, f_dot = u_dot C + u C' rdot;
-//             m_a += f v_b, m_b += f v_a, m_dot_a += f_dot v_b + f v_dot_b, m_dot_b likewise;
+//             m_dot_a += f_dot v_b + f v_dot_b, m_dot_b likewise (m itself, f v of the other
+//             atom, is the E/F/W call's, copied from its workspace);
 //   reverse, given m_bar and m_dot_bar from the atom-wise layers:
 //             fb = m_bar_a v_b + m_bar_b v_a + m_dot_bar_a v_dot_b + m_dot_bar_b v_dot_a,
 //             fdb = m_dot_bar_a v_b + m_dot_bar_b v_a;
@@ -220,9 +221,8 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
     unsigned char* image_b2 = image_b1 + umma::kImageBytes;
     unsigned char* tile = image_b2 + umma::kImageBytes;
     unsigned char* tile_dot = tile + umma::kTileBytes;
-    // first-atom runs of m and m_dot, in the row tiles once the products are done
-    float* stage = reinterpret_cast<float*>(tile);
-    float* stage_dot = reinterpret_cast<float*>(tile_dot);
+    // first-atom runs of m_dot, in a row tile once the products are done
+    float* stage_dot = reinterpret_cast<float*>(tile);
     float* bias1 = reinterpret_cast<float*>(tile_dot + umma::kTileBytes);
     float* bias2 = bias1 + kFeatures;
     auto* barrier = reinterpret_cast<std::uint64_t*>(bias2 + kFeatures);
@@ -245,7 +245,6 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
     Cores cores;
     cores.open(barrier, slot, 128, a.counters, 5);
     const int count = *reinterpret_cast<volatile int*>(a.counters);
-    float4* m4 = reinterpret_cast<float4*>(a.m);
     float4* md4 = reinterpret_cast<float4*>(a.m_dot);
 
     for (int index = blockIdx.x; index * kTile < count; index += gridDim.x)
@@ -313,9 +312,6 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
                         for (int h4 = 0; h4 < 2; ++h4)
                         {
                             const int o = 4 * h4;
-                            atomicAdd(m4 + 2 * gb + h4,
-                                      make_float4(f[o] * va[o], f[o + 1] * va[o + 1],
-                                                  f[o + 2] * va[o + 2], f[o + 3] * va[o + 3]));
                             atomicAdd(md4 + 2 * gb + h4,
                                       make_float4(fd[o] * va[o] + f[o] * vda[o],
                                                   fd[o + 1] * va[o + 1] + f[o + 1] * vda[o + 1],
@@ -327,9 +323,6 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
                     for (int h4 = 0; h4 < 2; ++h4)
                     {
                         const int o = 4 * h4;
-                        put_run_part(stage, 2 * c + h4,
-                                     make_float4(f[o] * vb[o], f[o + 1] * vb[o + 1],
-                                                 f[o + 2] * vb[o + 2], f[o + 3] * vb[o + 3]));
                         put_run_part(stage_dot, 2 * c + h4,
                                      make_float4(fd[o] * vb[o] + f[o] * vdb[o],
                                                  fd[o + 1] * vb[o + 1] + f[o + 1] * vdb[o + 1],
@@ -338,7 +331,6 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
                     }
                 }
             }
-            sum_runs(stage, tile_first, a.m, half);
             sum_runs(stage_dot, tile_first, a.m_dot, half);
         }
     }
@@ -643,6 +635,11 @@ int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction,
     }
     if (direction == 0)
     {
+        // The messages m are the E/F/W call's for this block; only their tangent is computed.
+        const std::int64_t row_bytes = align256(s.num_atoms * kFeatures * 4);
+        ND_CUDA_TRY(cudaMemcpyAsync(s.m, base + ws.m + s.block * row_bytes,
+                                    s.num_atoms * kFeatures * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, stream));
         const int grid = pair_grid(reinterpret_cast<const void*>(tangent_forward_kernel), kTangentForwardShared, 128);
         tangent_forward_kernel<<<grid, kTile, kTangentForwardShared, stream>>>(pass);
     }
