@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
                                              filter[6] * vb[6], filter[7] * vb[7]));
                 }
             }
-            sum_runs(stage, tile_first, a.m, half);
+            sum_runs(stage, tile_first, a.m, half, half == 1);  // the next basis overwrites it
         }
     }
     cores.close(64);
@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
             }
             if (gv4 != nullptr)
             {
-                sum_runs(stage, tile_first, a.grad_v, half);
+                sum_runs(stage, tile_first, a.grad_v, half, half == 1);  // B1^T is copied over it
             }
         }
         if (!cores.run(64, work, image_b2t, 3))

@@ -265,9 +265,10 @@ __device__ __forceinline__ void store_basis(unsigned char* tile, float r_over_wi
 
 // Run sums of first-atom rows. Every pair's first-atom vector (32 columns, [32 half,
 // 32 half + 32) of a [N][64] target) is staged in shared memory (16 KB: float4 chunks
-// swizzled by row against bank conflicts); the tile's pairs keep the list's order, so a first
-// atom's pairs are runs of rows: each warp sums 32 rows column by column and adds one atomic
-// per run and column instead of one per pair. Dead rows carry first = -1.
+// swizzled by row against bank conflicts; thread t stages row t); the tile's pairs keep the
+// list's order, so a first atom's pairs are runs of rows: each warp sums its 32 rows column
+// by column and adds one atomic per run and column instead of one per pair. Dead rows carry
+// first = -1.
 
 // Stages chunk q (columns 4q .. 4q + 3 of the half) of this thread's row.
 __device__ __forceinline__ void put_run_part(float* stage, int q, float4 value)
@@ -275,11 +276,13 @@ __device__ __forceinline__ void put_run_part(float* stage, int q, float4 value)
     reinterpret_cast<float4*>(stage)[threadIdx.x * 8 + (q ^ (threadIdx.x & 7))] = value;
 }
 
-// Sums the staged rows over runs into `target` (after every thread staged its row).
+// Sums the staged rows over runs into `target`. Each warp sums the 32 rows its own threads
+// staged, so a warp barrier orders the staging; `block_barrier` ends with a block barrier,
+// for callers whose next writes to the stage's bytes come from other warps.
 __device__ __forceinline__ void sum_runs(const float* stage, const int* first, float* target,
-                                         int half)
+                                         int half, bool block_barrier)
 {
-    __syncthreads();
+    __syncwarp();
     const int column = threadIdx.x & 31;
     const int begin = (threadIdx.x >> 5) * 32;
     float sum = 0.0f;
@@ -297,19 +300,14 @@ __device__ __forceinline__ void sum_runs(const float* stage, const int* first, f
             sum = 0.0f;
         }
     }
-    __syncthreads();
-}
-
-__device__ __forceinline__ void add_runs(float* stage, const int* first, float* target, int half,
-                                         const float (&part)[32])
-{
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
+    if (block_barrier)
     {
-        put_run_part(stage, q,
-                     make_float4(part[4 * q], part[4 * q + 1], part[4 * q + 2], part[4 * q + 3]));
+        __syncthreads();
     }
-    sum_runs(stage, first, target, half);
+    else
+    {
+        __syncwarp();
+    }
 }
 
 // Resident CTAs per SM times the SM count, for a persistent grid: the least of the register

@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kTile, 3) tangent_forward_kernel(TangentPass a
                     }
                 }
             }
-            sum_runs(stage_dot, tile_first, a.m_dot, half);
+            sum_runs(stage_dot, tile_first, a.m_dot, half, half == 1);  // the next basis overwrites it
         }
     }
     cores.close(128);
@@ -491,8 +491,9 @@ __global__ void __launch_bounds__(kTile, 2) tangent_reverse_kernel(TangentPass a
                     }
                 }
             }
-            sum_runs(stage, tile_first, a.v_bar, half);
-            sum_runs(stage_dot, tile_first, a.v_dot_bar, half);
+            // the stages are this kernel's own: only this warp writes their rows again
+            sum_runs(stage, tile_first, a.v_bar, half, false);
+            sum_runs(stage_dot, tile_first, a.v_dot_bar, half, false);
         }
         if (!cores.run2(128, tile, image_b2t, 192, tile_dot, image_b2t, 3))
         {
