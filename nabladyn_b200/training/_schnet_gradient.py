@@ -15,9 +15,10 @@ parameters, which the reference takes with torch.func through a double backward
 The per-pair work of steps 3 and 4 (the filter network with its tangent, the messages and their
 reverse) runs in the tcgen05 tangent kernels (nd_schnet_tangent); the atom-wise layers, the
 readout and their weights' gradients in the FP32 atom kernels (nd_schnet_atoms); the sums over
-pairs of the filter weights' gradients are GEMMs with FP32 results. Operands of the per-pair products are BF16, as in the E/F/W kernels, so the gradient
-agrees with the float64 definition to the BF16 level, not bitwise. One frame's work is one CUDA
-graph over static buffers, replayed frame after frame.
+pairs of the filter weights' gradients are GEMMs with FP32 results. Operands of the per-pair
+products are BF16, as in the E/F/W kernels, so the gradient agrees with the float64 definition
+to the BF16 level, not bitwise. One frame's work is one CUDA graph over static buffers,
+replayed frame after frame.
 """
 
 from __future__ import annotations
@@ -36,9 +37,10 @@ _ROWS = 8
 # Each model's plan (buffers and graph), beside the model rather than on it, so the module
 # still deep-copies and pickles; dropped with the model.
 _PLANS: "weakref.WeakKeyDictionary" = weakref.WeakKeyDictionary()
-# Per-atom arrays of the atom kernels' workspace (nd_schnet_atom_offset kinds).
-_X, _X_DOT, _H, _H_DOT, _M, _M_DOT, _V_BAR, _V_DOT_BAR = range(8)
-_X_BAR, _X_DOT_BAR, _V, _V_DOT, _M_BAR, _M_DOT_BAR = 10, 11, 12, 13, 14, 15
+# The atom kernels' per-atom arrays the host hands on (nd_schnet_atom_offset kinds): per block
+# m, m_dot, v_bar, v_dot_bar (FP32) and v, v_dot (BF16); x_bar (FP32); m_bar, m_dot_bar (BF16).
+_M, _M_DOT, _V_BAR, _V_DOT_BAR = 4, 5, 6, 7
+_X_BAR, _V, _V_DOT, _M_BAR, _M_DOT_BAR = 10, 12, 13, 14, 15
 # Offsets (floats) of the atom-side parameter block: per block A, D1, d1, D2, d2; readout.
 _BLOCK_FLOATS = 3 * 4096 + 2 * 64
 _BLOCK_PARTS = (("atoms.weight", 0, (64, 64)), ("update1.weight", 4096, (64, 64)),
