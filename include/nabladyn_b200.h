@@ -274,6 +274,15 @@ int nd_md_step(const nd_md_system* system, int thermostat, int virial, nd_stream
 int nd_md_step_phase(const nd_md_system* system, int phase, int thermostat, int virial,
                      nd_stream_t stream);
 
+/* `steps` whole steps of a small-box system (fewer than three cells on an axis, at most 4,096
+ * atoms), as many calls of nd_md_step without the virial would make them, in one launch of one
+ * thread-block cluster (up to 8 CTAs, each owning a range of atoms, phases separated by cluster
+ * barriers): a small box's step is a few microseconds of work over six launches, so the
+ * launches bound it. After a failure (a status bit) the list is no longer rebuilt, as in
+ * nd_md_step. The totals' float64 sums run in another fixed order than nd_md_step's. No
+ * counterpart in the reference (its small-box step is the same graph as any other). */
+int nd_md_run_small(const nd_md_system* system, int thermostat, int steps, nd_stream_t stream);
+
 /* The number of kernels one nd_md_step launches. */
 int nd_md_step_launches(const nd_md_system* system, int64_t* launches);
 

@@ -319,6 +319,7 @@ _SIGNATURES = {
     "nd_md_rebuild": [ctypes.POINTER(MDSystem), ctypes.c_void_p],
     "nd_md_forces": [ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_void_p],
     "nd_md_step": [ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_int, ctypes.c_void_p],
+    "nd_md_run_small": [ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_int, ctypes.c_void_p],
     "nd_md_step_phase": [
         ctypes.POINTER(MDSystem), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
     ],

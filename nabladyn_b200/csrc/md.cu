@@ -34,6 +34,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <type_traits>
@@ -1426,6 +1427,309 @@ std::int64_t step_launches(const nd_md_system* m)
     return 1 + rebuild + 2;  // drift, rebuild, forces and their finalize
 }
 
+// ---------------------------------------------------------------------------------------
+// Small boxes in one thread-block cluster: many whole steps per launch.
+//
+// A small box's step is a few microseconds of work spread over six launches (drift, the three
+// gated rebuild launches, forces, finalize), so the launches bound it. Here one cluster of up
+// to kRunCluster CTAs runs `steps` steps back to back, each CTA owning a contiguous range of
+// atoms, the phases separated by cluster barriers (release/acquire at cluster scope), on the
+// same arrays and with the same arithmetic as those kernels: the chain's opening half step
+// and the drift with the reuse check; on a rebuild the wrap and each CTA's centers' lists over
+// all atoms; the forces with the second half kick (each atom's list over kSmallLanes lanes);
+// the CTAs' float64 E and K summed in CTA order, then the chain's closing half step. Every CTA
+// keeps the chain's state and closes it from the same sums (CTA 0 stores it), and the reuse
+// flag carries the step's stamp instead of being cleared, so a step needs two cluster barriers
+// (three with a rebuild). Every branch around a cluster barrier is decided from values all
+// CTAs read after the same barrier, so every CTA takes the same barriers. A failure (a status
+// bit) stops the rebuilds, as in the per-step path; the host reads it.
+
+constexpr int kRunThreads = 512;
+constexpr int kRunMaxAtoms = 4096;
+constexpr int kRunCluster = 8;
+
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <typename T, bool kMulti, bool kThermostat>
+__global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int steps)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
+    __shared__ PairParams<T> params[36];
+    __shared__ double warp_sums[kRunThreads / kWarp][2];
+    __shared__ T scales[2];
+    __shared__ int rebuild;
+    const int rows = s.num_types * (s.num_types + 1) / 2;
+    for (int k = threadIdx.x; k < rows; k += blockDim.x)
+    {
+        params[k] = pair_params(s.sigma[k], s.epsilon[k], s.cutoff_squared);
+    }
+    const int n = s.n;
+    const int ctas = gridDim.x;
+    const int rank = blockIdx.x;  // the grid is one cluster
+    const int first = static_cast<int>(static_cast<std::int64_t>(n) * rank / ctas);
+    const int last = static_cast<int>(static_cast<std::int64_t>(n) * (rank + 1) / ctas);
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    // The chain's state after the last closing half step, kept by thread 0 of every CTA: each
+    // closes the chain from the same partials in the same order, so the copies agree.
+    double chain_q[3] = {0, 0, 0}, chain_p[3] = {0, 0, 0}, chain_kinetic = 0, pending = 1;
+    if (kThermostat && threadIdx.x == 0)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            chain_q[k] = s.thermo[kChainA + k];
+            chain_p[k] = s.thermo[kChainA + 3 + k];
+        }
+        chain_kinetic = s.thermo[kKineticA];
+        pending = s.thermo[kPendingScale];
+    }
+    for (int step = 0; step < steps; ++step)
+    {
+        // The chain's opening half step (as every drift block computes it; CTA 0 stores it).
+        if (kThermostat && threadIdx.x == 0)
+        {
+            const double* th = s.thermo;
+            const double factor = chain_half_step(chain_kinetic, chain_q, chain_p, th + kChainMass,
+                                                  th[kDegrees], th[kThermalEnergy], th[kTimestep]);
+            scales[0] = static_cast<T>(pending);
+            scales[1] = static_cast<T>(factor);
+            if (rank == 0)
+            {
+                double* out = s.thermo;
+                for (int k = 0; k < 3; ++k)
+                {
+                    out[kChainB + k] = chain_q[k];
+                    out[kChainB + 3 + k] = chain_p[k];
+                }
+                out[kKineticB] = chain_kinetic;
+                out[kOpenScale] = factor;
+            }
+        }
+        __syncthreads();
+        for (int i = first + threadIdx.x; i < last; i += blockDim.x)
+        {
+            T* v = s.vel + 3LL * i;
+            const T* f = s.force + 3LL * i;
+            const T kick = s.half_dt * s.inv_mass[i];
+            T vx = v[0], vy = v[1], vz = v[2];
+            if (kThermostat)
+            {
+                vx = (vx * scales[0]) * scales[1];
+                vy = (vy * scales[0]) * scales[1];
+                vz = (vz * scales[0]) * scales[1];
+            }
+            vx = fma(kick, f[0], vx);
+            vy = fma(kick, f[1], vy);
+            vz = fma(kick, f[2], vz);
+            Pos4<T> p = s.pos[i];
+            p.x = fma(s.dt, vx, p.x);
+            p.y = fma(s.dt, vy, p.y);
+            p.z = fma(s.dt, vz, p.z);
+            v[0] = vx;
+            v[1] = vy;
+            v[2] = vz;
+            s.pos[i] = p;
+            if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
+            {
+                atomicOr(s.status, kNonFinite);
+                continue;
+            }
+            const Pos4<T> r = s.ref_pos[i];
+            if (squared_norm(p.x - r.x, p.y - r.y, p.z - r.z) >= s.threshold_squared)
+            {
+                s.rebuild[0] = step + 1;  // this step's stamp; every writer stores the same
+            }
+        }
+        cluster_barrier();
+        // Every CTA reads the same stamp and status here: this step's writers are all before
+        // the barrier, the next step's all after the next one.
+        if (threadIdx.x == 0)
+        {
+            rebuild = (s.rebuild[0] == step + 1 && s.status[0] == 0) ? 1 : 0;
+        }
+        __syncthreads();
+        if (rebuild)
+        {
+            for (int i = first + threadIdx.x; i < last; i += blockDim.x)
+            {
+                Pos4<T> p = s.pos[i];
+                long long cx, cy, cz;
+                p.x = wrap_axis(p.x, s.length[0], cx);
+                p.y = wrap_axis(p.y, s.length[1], cy);
+                p.z = wrap_axis(p.z, s.length[2], cz);
+                if (cx | cy | cz)
+                {
+                    long long* image = s.images + 3LL * i;
+                    image[0] += cx;
+                    image[1] += cy;
+                    image[2] += cz;
+                }
+                s.pos[i] = p;
+                s.ref_pos[i] = p;
+            }
+            if (rank == 0 && threadIdx.x == 0)
+            {
+                ++s.rebuild_count[0];
+            }
+            cluster_barrier();
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            tile[i] = s.pos[i];
+        }
+        if (threadIdx.x == 0)
+        {
+            tile[s.sentinel] = far_atom<T>();
+        }
+        __syncthreads();
+        if (rebuild)
+        {
+            const T r2max = s.radius_squared;
+            for (int center = first + threadIdx.x; center < last; center += blockDim.x)
+            {
+                const Pos4<T> c = tile[center];
+                ListWriter list(s.nbr, s.width, center, s.sentinel);
+                for (int k = 0; k < n; ++k)
+                {
+                    if (k == center)
+                    {
+                        continue;
+                    }
+                    const Pos4<T> p = tile[k];
+                    const T dx = min_image(c.x, p.x, s.length[0]);
+                    const T dy = min_image(c.y, p.y, s.length[1]);
+                    const T dz = min_image(c.z, p.z, s.length[2]);
+                    if (squared_norm(dx, dy, dz) < r2max)
+                    {
+                        list.add(k);
+                    }
+                }
+                list.finish();
+                s.nbr_count[center] = list.count;
+                if (list.count > s.width)
+                {
+                    flag_overflow(s.status, 1, list.count);
+                }
+            }
+            __syncthreads();
+        }
+        // This CTA's centers: forces with the second half kick, kSmallLanes lanes per center.
+        double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const int tasks = (last - first) * kSmallLanes;
+        for (int base = 0; base < tasks; base += blockDim.x)
+        {
+            const int task = base + threadIdx.x;
+            const int center = task < tasks ? first + task / kSmallLanes : n;  // n: no center
+            force_center_split<T, kMulti, false, true, kThermostat>(s, tile, params, center,
+                                                                    task % kSmallLanes, sums);
+        }
+        const double e = warp_sum(sums[0]);
+        const double k = warp_sum(sums[1]);
+        if (lane == 0)
+        {
+            warp_sums[warp][0] = e;
+            warp_sums[warp][1] = k;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double energy = 0.0, kinetic = 0.0;
+            for (int w = 0; w < kRunThreads / kWarp; ++w)
+            {
+                energy += warp_sums[w][0];
+                kinetic += warp_sums[w][1];
+            }
+            s.partials[2 * rank] = energy;
+            s.partials[2 * rank + 1] = kinetic;
+        }
+        cluster_barrier();
+        // Every CTA: the totals in CTA order and the chain's closing half step
+        // (finalize_kernel's); CTA 0 stores them. The next step's partials are written only
+        // after its drift barrier, which every CTA reaches after reading these.
+        if (threadIdx.x == 0)
+        {
+            double energy = 0.0, kinetic = 0.0;
+            for (int c = 0; c < ctas; ++c)
+            {
+                energy += s.partials[2 * c];
+                kinetic += s.partials[2 * c + 1];
+            }
+            if (kThermostat)
+            {
+                const double* th = s.thermo;
+                chain_kinetic = kinetic;
+                pending = chain_half_step(chain_kinetic, chain_q, chain_p, th + kChainMass,
+                                          th[kDegrees], th[kThermalEnergy], th[kTimestep]);
+            }
+            if (rank == 0)
+            {
+                s.totals[0] = energy;
+                s.totals[1] = kinetic;
+                for (int r = 2; r < kReduced; ++r)
+                {
+                    s.totals[r] = 0.0;
+                }
+                if (kThermostat)
+                {
+                    double* out = s.thermo;
+                    for (int r = 0; r < 3; ++r)
+                    {
+                        out[kChainA + r] = chain_q[r];
+                        out[kChainA + 3 + r] = chain_p[r];
+                    }
+                    out[kKineticA] = chain_kinetic;
+                    out[kPendingScale] = pending;
+                }
+            }
+        }
+    }
+    // Every CTA read the last stamp before the last barrier: the flag starts clean next time.
+    if (rank == 0 && threadIdx.x == 0)
+    {
+        s.rebuild[0] = 0;
+    }
+}
+
+template <typename T>
+int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t stream)
+{
+    const std::size_t bytes = tile_bytes(s);
+    // Up to kRunCluster CTAs, no more than the partial slots hold two sums each.
+    const int slots = static_cast<int>(s.force_blocks) * kReduced;
+    const int ctas = std::max(1, std::min(std::min(kRunCluster, slots / 2), static_cast<int>(s.n)));
+    cudaLaunchConfig_t config = {};
+    config.gridDim = dim3(ctas);
+    config.blockDim = dim3(kRunThreads);
+    config.dynamicSmemBytes = bytes;
+    config.stream = stream;
+    cudaLaunchAttribute attribute[1];
+    attribute[0].id = cudaLaunchAttributeClusterDimension;
+    attribute[0].val.clusterDim.x = ctas;
+    attribute[0].val.clusterDim.y = 1;
+    attribute[0].val.clusterDim.z = 1;
+    config.attrs = attribute;
+    config.numAttrs = 1;
+#define ND_RUN_CASE(MULTI, THERMO)                                                 \
+    if ((s.num_types > 1) == MULTI && (thermostat != 0) == THERMO)                 \
+    {                                                                              \
+        auto kernel = small_run_kernel<T, MULTI, THERMO>;                          \
+        static std::size_t granted = 0;                                            \
+        ND_CUDA_TRY(allow_shared(kernel, bytes, granted));                         \
+        ND_CUDA_TRY(cudaLaunchKernelEx(&config, kernel, s, steps));                \
+        return ND_OK;                                                              \
+    }
+    ND_RUN_CASE(false, false)
+    ND_RUN_CASE(false, true)
+    ND_RUN_CASE(true, false)
+    ND_RUN_CASE(true, true)
+#undef ND_RUN_CASE
+    return ND_OK;
+}
+
 // Sets the rebuild branch of a step graph from the device flag the drift kernel wrote.
 __global__ void rebuild_condition_kernel(cudaGraphConditionalHandle handle,
                                          const index_t* rebuild, const index_t* status)
@@ -1636,6 +1940,24 @@ int nd_md_step_phase(const nd_md_system* system, int phase, int thermostat, int 
     const std::int64_t cells =
         static_cast<std::int64_t>(system->dims[0]) * system->dims[1] * system->dims[2];
     return ND_MD_DISPATCH(system, nd::launch_step(s, cells, thermostat, virial, phase, st));
+}
+
+int nd_md_run_small(const nd_md_system* system, int thermostat, int steps, nd_stream_t stream)
+{
+    const int rc = nd::check_system(system);
+    if (rc != ND_OK)
+    {
+        return rc;
+    }
+    ND_REQUIRE(system->small, "only small-box systems (fewer than three cells on an axis) run in one launch");
+    ND_REQUIRE(system->num_atoms <= nd::kRunMaxAtoms, "a one-launch run takes at most 4096 atoms");
+    ND_REQUIRE(steps >= 0, "steps must be nonnegative");
+    if (steps == 0)
+    {
+        return ND_OK;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    return ND_MD_DISPATCH(system, nd::launch_small_run(s, thermostat, steps, st));
 }
 
 int nd_md_step_launches(const nd_md_system* system, int64_t* launches)

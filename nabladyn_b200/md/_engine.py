@@ -278,6 +278,20 @@ class Engine:
         with torch.cuda.device(self.device):
             call("nd_md_step", self.system, int(thermostat), 0, self._stream())
 
+    # Small boxes up to this many atoms run many steps per launch (nd_md_run_small).
+    ONE_LAUNCH_MAX_ATOMS = 4096
+
+    @property
+    def runs_in_one_launch(self) -> bool:
+        """Whether ``run_steps`` applies: a small box of at most ONE_LAUNCH_MAX_ATOMS atoms."""
+        return bool(self.small) and self.num_atoms <= self.ONE_LAUNCH_MAX_ATOMS
+
+    def run_steps(self, thermostat: bool, steps: int) -> None:
+        """``steps`` steps of a small box in one launch of one thread-block cluster
+        (nd_md_run_small), as many ``step`` calls would make them."""
+        with torch.cuda.device(self.device):
+            call("nd_md_run_small", self.system, int(thermostat), int(steps), self._stream())
+
     def step_phase(self, phase: int, thermostat: bool) -> None:
         with torch.cuda.device(self.device):
             call("nd_md_step_phase", self.system, int(phase), int(thermostat), 0, self._stream())

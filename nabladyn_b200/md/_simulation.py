@@ -397,6 +397,12 @@ class Simulation:
         return graphs
 
     def _advance(self, steps: int) -> None:
+        engine = self._engine
+        if isinstance(engine, Engine) and engine.runs_in_one_launch:
+            # A small box runs whole stretches of steps in one launch; its step is a few
+            # microseconds of work, which per-step launches would bound.
+            engine.run_steps(self._thermostat, steps)
+            return
         chunks, rest = divmod(steps, _CHUNK)
         for _ in range(chunks):
             self._graphs[_CHUNK].replay()

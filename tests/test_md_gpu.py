@@ -65,6 +65,39 @@ def test_trajectory_matches_reference(argon, argon_md, cuda, ensemble, tag):
                                        argon_md[f"{key}_chain_momenta"], atol=1e-9)
 
 
+@pytest.mark.parametrize("ensemble", ["NVE", "NVT"])
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_one_launch_run_matches_step_graphs(argon, cuda, monkeypatch, ensemble, tag):
+    """The 512-atom box's one-launch runs (nd_md_run_small, the small-box path) against the same
+    300 steps from the per-step graphs, with rebuilds on the way: the same trajectory and
+    panel. Only the float64 order of the totals differs, which the thermostat's factor sees:
+    float64 to 1e-9, float32 NVE exactly, float32 NVT to 1e-4 nm."""
+    from nabladyn_b200.md._engine import Engine
+
+    dtype = torch.float64 if tag == "f64" else torch.float32
+
+    def run(one_launch: bool):
+        with monkeypatch.context() as patch:
+            if not one_launch:
+                patch.setattr(Engine, "ONE_LAUNCH_MAX_ATOMS", 0)
+            simulation = build(ensemble, *argon_system(argon, dtype, cuda))
+            assert simulation._engine.runs_in_one_launch == one_launch
+            panel = simulation.run(300, sample_every=100)
+            return simulation.state(), panel
+
+    state, panel = run(True)
+    expected, expected_panel = run(False)
+    atol = 1e-9 if tag == "f64" else (0.0 if ensemble == "NVE" else 1e-4)
+    np.testing.assert_allclose(state.positions.cpu().numpy(),
+                               expected.positions.cpu().numpy(), atol=atol, rtol=0)
+    np.testing.assert_allclose(state.velocities.cpu().numpy(),
+                               expected.velocities.cpu().numpy(), atol=10 * atol, rtol=0)
+    np.testing.assert_array_equal(state.images.cpu().numpy(), expected.images.cpu().numpy())
+    for name, values in expected_panel.items():
+        np.testing.assert_allclose(panel[name].numpy(), values.numpy(),
+                                   rtol=1e-9 if tag == "f64" else 1e-4, err_msg=name)
+
+
 def test_resume_from_state_is_the_same_run(argon, cuda):
     model, x, v, masses, cell = argon_system(argon, torch.float64, cuda)
     straight = build("NVT", model, x, v, masses, cell)
