@@ -1454,6 +1454,105 @@ __device__ __forceinline__ void cluster_barrier()
                  "barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
+// One center's pair loop on the small-box path, its lanes' sums met in force_center_split's
+// shuffle tree and with its arithmetic, the list's first word loaded with its length; returns
+// the force (lane `part` 0 only) and adds half the pair energy to `energy`.
+template <typename T, bool kMulti>
+__device__ __forceinline__ void run_center_forces(const System<T>& s,
+                                                  const Pos4<T>* __restrict__ tile,
+                                                  const PairParams<T>* __restrict__ params,
+                                                  int center, int part, T (&force)[3],
+                                                  double& energy)
+{
+    CenterSums<T> c{};
+    const bool real = center < s.n;
+    const Pos4<T> me = real ? tile[center] : far_atom<T>();
+    if (real)
+    {
+        const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
+        const int stored_chunks = s.width / kChunk;
+        uint4 next = part < stored_chunks ? chunks[static_cast<std::int64_t>(part) * kWarp]
+                                          : make_uint4(0, 0, 0, 0);
+        const int count = s.nbr_count[center];
+        const int used = count < s.width ? count : s.width;
+        const int num_chunks = (used + kChunk - 1) / kChunk;
+        const T cutoff_squared = s.cutoff_squared;
+        const T s2 = params[0].s2;
+        for (int chunk = part; chunk < num_chunks; chunk += kSmallLanes)
+        {
+            const uint4 word = next;
+            if (chunk + kSmallLanes < num_chunks)
+            {
+                next = chunks[static_cast<std::int64_t>(chunk + kSmallLanes) * kWarp];
+            }
+            const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+            for (int r = 0; r < kChunk; ++r)
+            {
+                const Pos4<T> p = tile[(packed[r / 2] >> (16 * (r % 2))) & 0xffffu];
+                const T dx = min_image(me.x, p.x, s.length[0]);
+                const T dy = min_image(me.y, p.y, s.length[1]);
+                const T dz = min_image(me.z, p.z, s.length[2]);
+                const T r2 = squared_norm(dx, dy, dz);
+                const bool inside = r2 < cutoff_squared;
+                const T inv_r2 = fast_reciprocal(r2);
+                PairParams<T> pp;
+                if (kMulti)
+                {
+                    pp = params[type_pair_row(static_cast<int>(me.w), static_cast<int>(p.w),
+                                              s.num_types)];
+                }
+                const T q = (kMulti ? pp.s2 : s2) * inv_r2;
+                const T p6 = q * q * q;
+                const T mask = inside ? T(1) : T(0);
+                T fs = mask * (inv_r2 * (p6 * fma(T(2), p6, T(-1))));
+                const T u = fma(p6, p6, -p6);
+                if (kMulti)
+                {
+                    fs *= pp.e24;
+                    c.energy = fma(mask, fma(pp.e4, u, -pp.shift), c.energy);
+                }
+                else
+                {
+                    c.energy = fma(mask, u, c.energy);
+                    c.inside += mask;
+                }
+                c.fx = fma(fs, dx, c.fx);
+                c.fy = fma(fs, dy, c.fy);
+                c.fz = fma(fs, dz, c.fz);
+            }
+        }
+    }
+#pragma unroll
+    for (int offset = kSmallLanes / 2; offset > 0; offset /= 2)
+    {
+        c.fx += __shfl_xor_sync(kFullMask, c.fx, offset);
+        c.fy += __shfl_xor_sync(kFullMask, c.fy, offset);
+        c.fz += __shfl_xor_sync(kFullMask, c.fz, offset);
+        c.energy += __shfl_xor_sync(kFullMask, c.energy, offset);
+        c.inside += __shfl_xor_sync(kFullMask, c.inside, offset);
+    }
+    if (!real || part != 0)
+    {
+        return;
+    }
+    T scale = T(1);
+    double e;
+    if (kMulti)
+    {
+        e = double(c.energy);
+    }
+    else
+    {
+        scale = params[0].e24;
+        e = double(params[0].e4) * double(c.energy) - double(params[0].shift) * double(c.inside);
+    }
+    force[0] = c.fx * scale;
+    force[1] = c.fy * scale;
+    force[2] = c.fz * scale;
+    energy += 0.5 * e;
+}
+
 template <typename T, bool kMulti, bool kThermostat>
 __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int steps)
 {
@@ -1461,6 +1560,7 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
     __shared__ PairParams<T> params[36];
     __shared__ double warp_sums[kRunThreads / kWarp][2];
+    __shared__ T forces[kRunThreads][3];  // this step's force on each owned atom
     __shared__ T scales[2];
     __shared__ int rebuild;
     const int rows = s.num_types * (s.num_types + 1) / 2;
@@ -1474,8 +1574,25 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     const int first = static_cast<int>(static_cast<std::int64_t>(n) * rank / ctas);
     const int last = static_cast<int>(static_cast<std::int64_t>(n) * (rank + 1) / ctas);
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
-    // The chain's state after the last closing half step, kept by thread 0 of every CTA: each
-    // closes the chain from the same partials in the same order, so the copies agree.
+    // Thread t owns atom first + t (at most kRunThreads per CTA): its state stays in registers
+    // for the whole launch and is stored back at the end.
+    const int mine = first + static_cast<int>(threadIdx.x);
+    const bool owner = mine < last;
+    Pos4<T> position{}, reference{};
+    T velocity[3] = {T(0), T(0), T(0)};
+    T inv_mass = T(0), mass = T(0);
+    if (owner)
+    {
+        position = s.pos[mine];
+        reference = s.ref_pos[mine];
+        for (int a = 0; a < 3; ++a)
+        {
+            velocity[a] = s.vel[3LL * mine + a];
+            forces[threadIdx.x][a] = s.force[3LL * mine + a];
+        }
+        inv_mass = s.inv_mass[mine];
+        mass = s.mass[mine];
+    }
     double chain_q[3] = {0, 0, 0}, chain_p[3] = {0, 0, 0}, chain_kinetic = 0, pending = 1;
     if (kThermostat && threadIdx.x == 0)
     {
@@ -1487,6 +1604,7 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         chain_kinetic = s.thermo[kKineticA];
         pending = s.thermo[kPendingScale];
     }
+    const T kick = s.half_dt * inv_mass;
     for (int step = 0; step < steps; ++step)
     {
         // The chain's opening half step (as every drift block computes it; CTA 0 stores it).
@@ -1510,84 +1628,78 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
             }
         }
         __syncthreads();
-        for (int i = first + threadIdx.x; i < last; i += blockDim.x)
+        // The drift of the owned atom, from registers and this CTA's forces.
+        if (owner)
         {
-            T* v = s.vel + 3LL * i;
-            const T* f = s.force + 3LL * i;
-            const T kick = s.half_dt * s.inv_mass[i];
-            T vx = v[0], vy = v[1], vz = v[2];
+            T vx = velocity[0], vy = velocity[1], vz = velocity[2];
             if (kThermostat)
             {
                 vx = (vx * scales[0]) * scales[1];
                 vy = (vy * scales[0]) * scales[1];
                 vz = (vz * scales[0]) * scales[1];
             }
-            vx = fma(kick, f[0], vx);
-            vy = fma(kick, f[1], vy);
-            vz = fma(kick, f[2], vz);
-            Pos4<T> p = s.pos[i];
-            p.x = fma(s.dt, vx, p.x);
-            p.y = fma(s.dt, vy, p.y);
-            p.z = fma(s.dt, vz, p.z);
-            v[0] = vx;
-            v[1] = vy;
-            v[2] = vz;
-            s.pos[i] = p;
-            if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
+            vx = fma(kick, forces[threadIdx.x][0], vx);
+            vy = fma(kick, forces[threadIdx.x][1], vy);
+            vz = fma(kick, forces[threadIdx.x][2], vz);
+            position.x = fma(s.dt, vx, position.x);
+            position.y = fma(s.dt, vy, position.y);
+            position.z = fma(s.dt, vz, position.z);
+            velocity[0] = vx;
+            velocity[1] = vy;
+            velocity[2] = vz;
+            s.pos[mine] = position;
+            if (!(isfinite(position.x) && isfinite(position.y) && isfinite(position.z)))
             {
                 atomicOr(s.status, kNonFinite);
-                continue;
             }
-            const Pos4<T> r = s.ref_pos[i];
-            if (squared_norm(p.x - r.x, p.y - r.y, p.z - r.z) >= s.threshold_squared)
+            else if (squared_norm(position.x - reference.x, position.y - reference.y,
+                                  position.z - reference.z) >= s.threshold_squared)
             {
                 s.rebuild[0] = step + 1;  // this step's stamp; every writer stores the same
             }
         }
         cluster_barrier();
-        // Every CTA reads the same stamp and status here: this step's writers are all before
-        // the barrier, the next step's all after the next one.
+        // Every CTA reads the same stamp and status here (this step's writers are all before
+        // the barrier, the next step's all after the next one), the tile beside it.
         if (threadIdx.x == 0)
         {
             rebuild = (s.rebuild[0] == step + 1 && s.status[0] == 0) ? 1 : 0;
+            tile[s.sentinel] = far_atom<T>();
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            tile[i] = s.pos[i];
         }
         __syncthreads();
         if (rebuild)
         {
-            for (int i = first + threadIdx.x; i < last; i += blockDim.x)
+            if (owner)
             {
-                Pos4<T> p = s.pos[i];
                 long long cx, cy, cz;
-                p.x = wrap_axis(p.x, s.length[0], cx);
-                p.y = wrap_axis(p.y, s.length[1], cy);
-                p.z = wrap_axis(p.z, s.length[2], cz);
+                position.x = wrap_axis(position.x, s.length[0], cx);
+                position.y = wrap_axis(position.y, s.length[1], cy);
+                position.z = wrap_axis(position.z, s.length[2], cz);
                 if (cx | cy | cz)
                 {
-                    long long* image = s.images + 3LL * i;
+                    long long* image = s.images + 3LL * mine;
                     image[0] += cx;
                     image[1] += cy;
                     image[2] += cz;
                 }
-                s.pos[i] = p;
-                s.ref_pos[i] = p;
+                reference = position;
+                s.pos[mine] = position;
+                s.ref_pos[mine] = position;
             }
             if (rank == 0 && threadIdx.x == 0)
             {
                 ++s.rebuild_count[0];
             }
             cluster_barrier();
-        }
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
-        {
-            tile[i] = s.pos[i];
-        }
-        if (threadIdx.x == 0)
-        {
-            tile[s.sentinel] = far_atom<T>();
-        }
-        __syncthreads();
-        if (rebuild)
-        {
+            for (int i = threadIdx.x; i < n; i += blockDim.x)
+            {
+                tile[i] = s.pos[i];
+            }
+            __syncthreads();
             const T r2max = s.radius_squared;
             for (int center = first + threadIdx.x; center < last; center += blockDim.x)
             {
@@ -1617,15 +1729,40 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
             }
             __syncthreads();
         }
-        // This CTA's centers: forces with the second half kick, kSmallLanes lanes per center.
-        double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
+        // This CTA's centers over kSmallLanes lanes each; the forces meet in shared memory.
+        double sums[2] = {0.0, 0.0};
         const int tasks = (last - first) * kSmallLanes;
         for (int base = 0; base < tasks; base += blockDim.x)
         {
             const int task = base + threadIdx.x;
             const int center = task < tasks ? first + task / kSmallLanes : n;  // n: no center
-            force_center_split<T, kMulti, false, true, kThermostat>(s, tile, params, center,
-                                                                    task % kSmallLanes, sums);
+            T force[3];
+            run_center_forces<T, kMulti>(s, tile, params, center, task % kSmallLanes, force,
+                                         sums[0]);
+            if (center < n && task % kSmallLanes == 0)
+            {
+                const int local = center - first;
+                for (int a = 0; a < 3; ++a)
+                {
+                    forces[local][a] = force[a];
+                    s.force[3LL * center + a] = force[a];
+                }
+            }
+        }
+        __syncthreads();
+        // The second half kick of the owned atom, and its kinetic energy.
+        if (owner)
+        {
+            const T vx = fma(kick, forces[threadIdx.x][0], velocity[0]);
+            const T vy = fma(kick, forces[threadIdx.x][1], velocity[1]);
+            const T vz = fma(kick, forces[threadIdx.x][2], velocity[2]);
+            velocity[0] = vx;
+            velocity[1] = vy;
+            velocity[2] = vz;
+            if (kThermostat)
+            {
+                sums[1] += 0.5 * double(mass) * (double(vx) * vx + double(vy) * vy + double(vz) * vz);
+            }
         }
         const double e = warp_sum(sums[0]);
         const double k = warp_sum(sums[1]);
@@ -1685,6 +1822,13 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
                     out[kPendingScale] = pending;
                 }
             }
+        }
+    }
+    if (owner)
+    {
+        for (int a = 0; a < 3; ++a)
+        {
+            s.vel[3LL * mine + a] = velocity[a];
         }
     }
     // Every CTA read the last stamp before the last barrier: the flag starts clean next time.
