@@ -1059,18 +1059,19 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
     const int atom_tiles = static_cast<int>((s.num_atoms + kTile - 1) / kTile);
     const bool reverse = s.forces != nullptr || s.virial != nullptr;
 
-    static bool configured = false;
-    if (!configured)
-    {
-        ND_CUDA_TRY(cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairForwardShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairReverseShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(atom_forward_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(atom_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(atom_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-        configured = true;
-    }
+    // The kernels' attributes, set once (a function-local static starts once, thread-safely).
+    static const cudaError_t configured = [] {
+        cudaError_t rc = cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairForwardShared);
+        auto then = [&rc](cudaError_t next) { rc = rc != cudaSuccess ? rc : next; };
+        then(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairReverseShared));
+        then(cudaFuncSetAttribute(atom_forward_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        then(cudaFuncSetAttribute(atom_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        then(cudaFuncSetAttribute(atom_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kAtomShared));
+        then(cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+        then(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+        return rc;
+    }();
+    ND_CUDA_TRY(configured);
     const int forward_grid = pair_grid(reinterpret_cast<const void*>(pair_forward_kernel), kPairForwardShared, 64);
     const int reverse_grid = std::min(kVirialSlots, pair_grid(reinterpret_cast<const void*>(pair_reverse_kernel), kPairReverseShared, 128));
 

@@ -791,16 +791,17 @@ int nd_schnet_atoms(const nd_schnet_atom_args* args, int32_t stage, int32_t bloc
     p.x_dot_bar = f32(kXDotBar, 0);
     const unsigned tiles = static_cast<unsigned>(layout.tiles);
 
-    static bool configured = false;
-    if (!configured)
-    {
-        ND_CUDA_TRY(cudaFuncSetAttribute(start_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStartShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kForwardShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(readout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReadoutShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReverseShared));
-        ND_CUDA_TRY(cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterShared));
-        configured = true;
-    }
+    // The kernels' attributes, set once (a function-local static starts once, thread-safely).
+    static const cudaError_t configured = [] {
+        cudaError_t rc = cudaFuncSetAttribute(start_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStartShared);
+        auto then = [&rc](cudaError_t next) { rc = rc != cudaSuccess ? rc : next; };
+        then(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kForwardShared));
+        then(cudaFuncSetAttribute(readout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReadoutShared));
+        then(cudaFuncSetAttribute(reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReverseShared));
+        then(cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterShared));
+        return rc;
+    }();
+    ND_CUDA_TRY(configured);
     auto reduce = [&](const Segments& segments) -> int {
         int total = 0;
         for (int k = 0; k < segments.count; ++k)
