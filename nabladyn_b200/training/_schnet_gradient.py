@@ -206,6 +206,13 @@ def _frame_gradient(model, plan, e_bar: Tensor, f_bar: Tensor, w_bar: Tensor) ->
     plan.gradient["embedding"].index_add_(0, model.atom_types, buffers.view(_X_BAR))
 
 
+def _plan_key(model, columns: int, channels: tuple[str, ...]) -> tuple:
+    """What a plan's buffers and captured graph depend on besides the parameter values (copied
+    in at every call): the stack width, the channels, the device and the atom-type buffer."""
+    types = model.atom_types
+    return (columns, channels, str(model.device), types.data_ptr(), types._version)
+
+
 class _Plan:
     """Static buffers for one pair-stack width and set of loss channels (parameters, the frame's
     inputs and labels, the loss weights, the accumulated loss, gradient and status bits) and
@@ -217,7 +224,7 @@ class _Plan:
         device = model.device
         n = model.num_atoms
         f64 = torch.float64
-        self.key = (columns, channels)
+        self.key = _plan_key(model, columns, channels)
         self.device = device
         self.buffers = _Buffers(model, columns)
         self.values = {name: torch.empty(value.shape, dtype=torch.float32, device=device)
@@ -301,7 +308,7 @@ def loss_and_gradient(model, parameters: Mapping[str, Tensor], positions: Tensor
     frames, columns = positions.shape[0], stack.shape[-1]
     channels = tuple(name for name in ("energy", "forces", "virial") if name in weights)
     plan = _PLANS.get(model)
-    if plan is None or plan.key != (columns, channels):
+    if plan is None or plan.key != _plan_key(model, columns, channels):
         _PLANS.pop(model, None)
         plan = _Plan(model, columns, channels)
         _PLANS[model] = plan
