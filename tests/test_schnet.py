@@ -160,3 +160,36 @@ def test_atom_parameter_block_layout():
         assert torch.equal(view, values[name].float()), name
     covered = set(views)
     assert covered == {name for name in values if "filter" not in name}
+
+
+@pytest.mark.parametrize("channels", [("energy",), ("forces",), ("virial",),
+                                      ("energy", "forces", "virial")])
+def test_frame_loss_adjoints_match_oracle(channels):
+    """The fused gradient's per-frame loss term and its adjoints dL/dE, dL/dF, dL/dW (the
+    inputs of the tangent passes) against the oracle's restatement of the reference's loss."""
+    from nabladyn_b200.training import _schnet_gradient
+
+    rng = np.random.default_rng(5)
+    n = 11
+    predicted = {"energy": rng.normal(), "forces": rng.normal(size=(n, 3)),
+                 "virial": rng.normal(size=(3, 3))}
+    labels = {"energy": rng.normal(), "forces": rng.normal(size=(n, 3)),
+              "virial": rng.normal(size=(3, 3))}
+    weights = {name: float(w) for name, w in zip(channels, (0.5, 2.0, 1.5))}
+    scales = {"energy": 3.0, "forces": 0.7, "virial": 5.0}
+    coefficient = 0.25
+    device_scalar = lambda v: torch.tensor(v, dtype=torch.float64)  # noqa: E731
+    value, e_bar, f_bar, w_bar = _schnet_gradient._frame_loss(
+        torch.tensor(predicted["energy"], dtype=torch.float64),
+        torch.tensor(predicted["forces"], dtype=torch.float32),
+        torch.tensor(predicted["virial"].reshape(9), dtype=torch.float64),
+        {name: torch.tensor(labels[name], dtype=torch.float64) for name in channels},
+        {name: device_scalar(w) for name, w in weights.items()},
+        {name: device_scalar(scales[name]) for name in channels}, device_scalar(coefficient))
+    forces32 = torch.tensor(predicted["forces"], dtype=torch.float32).double().numpy()
+    expected = oracle.loss_adjoints({**predicted, "forces": forces32}, labels, weights, scales,
+                                    coefficient)
+    assert float(value) == pytest.approx(expected[0], rel=1e-12)
+    assert float(e_bar) == pytest.approx(expected[1], rel=1e-12, abs=1e-15)
+    np.testing.assert_allclose(f_bar.double().numpy(), expected[2], rtol=1e-6, atol=1e-12)
+    np.testing.assert_allclose(w_bar.numpy().reshape(3, 3), expected[3], rtol=1e-12, atol=1e-15)
