@@ -135,6 +135,45 @@ def build_system(torch, device, seed: int):
     return simulation, host, n
 
 
+def frame_accuracy(simulation) -> dict:
+    """The current frame's float32 forces, energy and virial against a float64 evaluation of
+    the same coordinates (the engine's cell-order positions, unwrapped as the kernels used
+    them): this package's float64 LJ kernels over a float64 neighbor list of all atoms, which
+    the tests pin to the float64 oracle (to 1e-9, and on a 4,096-atom sample of this box)."""
+    import torch
+
+    from nabladyn_b200 import neighbors, potential, quantity, space
+
+    panel = simulation.sample()  # forces and virial of the current frame, float32
+    engine = simulation._engine
+    device = engine.device
+    x32 = engine.tensors["positions"][:, :3]
+    f32 = engine.tensors["forces"].double()
+    totals = engine.totals.tolist()
+    w32 = torch.tensor([[totals[2], totals[5], totals[6]], [totals[5], totals[3], totals[7]],
+                        [totals[6], totals[7], totals[4]]], dtype=torch.float64)
+    n = x32.shape[0]
+    cell64 = engine.cell.double()
+    x64, _ = space.wrap(x32.double(), cell64)
+    exact = potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64, device=device),
+        sigma=torch.tensor([SIGMA], dtype=torch.float64, device=device),
+        epsilon=torch.tensor([EPSILON], dtype=torch.float64, device=device), cutoff=CUTOFF)
+    listing = neighbors.NeighborList(CUTOFF, skin=0.0)
+    listing.allocate(x64, cell64)
+    e64, f64, w64 = quantity.energy_force_virial(exact)(x64, cell64, listing.tensors())
+    w64 = w64.cpu()
+    out = {
+        "force_error_vs_fp64": float((f32 - f64).norm() / f64.norm()),
+        "energy_error_vs_fp64": abs(float(panel["potential_energy"]) - float(e64)) / abs(float(e64)),
+        "virial_error_vs_fp64": float((w32 - w64).norm() / w64.norm()),
+        "measure": "||x32 - x64|| / ||x64|| on the last timed frame, all atoms",
+    }
+    del listing, f64
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_port_rate(steps: int = 3, cells: int = 24, threads: int | None = None) -> dict:
     """The oracle port of the reference's step on the host: pairs by the C restatement of the
     neighbor operator (one thread), LJ and velocity Verlet in float64 numpy with the pairs
@@ -718,6 +757,7 @@ def run_ours(args) -> None:
     elapsed_ms = max_over_ranks(start.elapsed_time(end))
     rebuilds = simulation._rebuild_count - rebuilds_before
     value = world * n * args.steps / (elapsed_ms / 1e3)
+    accuracy = frame_accuracy(simulation)
 
     # Roofline of the dominant kernel: the same steps run eagerly, each phase between events.
     phases = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
@@ -794,6 +834,7 @@ def run_ours(args) -> None:
                 "l2": "working set > L2 (126 MB); no flush",
                 "rebuilds_in_timed_steps": rebuilds,
             },
+            "accuracy": accuracy,
             "roofline": {
                 "kernel": "force_kernel (forces, second half kick, float64 tail)",
                 "bound": "hbm",

@@ -17,8 +17,8 @@
 //
 // Bricks and tiles. Cells of at least the list radius are grouped along x into bricks of a few
 // cells. One CTA per brick stages the brick's 3 x 3 rows of neighbor cells (x extended by one
-// cell each way) into shared memory, each cell already shifted by its periodic image, with
-// coalesced 16-B loads. The neighbor list is a full list (both directions, no atomics) of
+// cell each way) into shared memory, each cell already shifted by its periodic image and the
+// brick's frame (brick_frame: every displacement rounds once), with coalesced 16-B loads. The neighbor list is a full list (both directions, no atomics) of
 // uint16 tile-local indices, interleaved by warps of 32 cell-order slots:
 //     entry (i, k) lives at ((i / 32) * width + k) * 32 + i % 32.
 // The force kernel re-stages the same tile from the current positions and reads every
@@ -182,6 +182,37 @@ __device__ __forceinline__ bool barrier_wait_bounded(std::uint64_t* barrier)
 // ---------------------------------------------------------------------------------------
 // Tiles.
 
+// The brick's frame: an offset per axis, 0 or -L, added to every coordinate of its tile and
+// to its centers, so that each displacement is rounded once, as the reference's image rule
+// does (src/nabladyn/neighbors/csrc/common/traversal.cuh:9-28). A tile cell past the upper
+// face needs +L: x + L rounds at the ulp of L (1.9e-6 nm at L = 36.8 nm, which alone gives a
+// force error of 1.2e-5 of FP64 on the 1M-atom box). So a brick whose tile crosses only the
+// upper face along an axis moves its frame by -L there: its own cells then take x - L, exact
+// by Sterbenz's lemma for x >= L/2, and the cells past the face keep x unchanged. A brick that
+// crosses only the lower face (shift -L, x near L, exact) or no face keeps offset 0; a brick
+// crossing both (a row of one brick) keeps 0 and rounds its +L cells.
+template <typename T>
+struct BrickFrame
+{
+    T x, y, z;
+};
+
+template <typename T>
+__device__ __forceinline__ BrickFrame<T> brick_frame(const System<T>& s, int brick)
+{
+    const int nx = s.dims[0], ny = s.dims[1], nz = s.dims[2];
+    const int bx = brick % s.bricks_x;
+    const int y = (brick / s.bricks_x) % ny;
+    const int z = brick / (s.bricks_x * ny);
+    const int x0 = bx * nx / s.bricks_x;
+    const int x1 = (bx + 1) * nx / s.bricks_x;
+    BrickFrame<T> frame;
+    frame.x = (x1 == nx && x0 > 0) ? -s.length[0] : T(0);
+    frame.y = (y == ny - 1 && y > 0) ? -s.length[1] : T(0);
+    frame.z = (z == nz - 1 && z > 0) ? -s.length[2] : T(0);
+    return frame;
+}
+
 // Stages one brick's tile. The tile cells of a row are consecutive cells of the cell order
 // (apart from a wrap along x), so each maximal run of cells whose atoms are adjacent in memory
 // is one bulk copy, issued by the first warp; every thread then waits on the barrier, and the
@@ -302,14 +333,15 @@ __device__ __forceinline__ TileShape stage_brick(
         shape.size = s.tile_cap + 1;
         return shape;
     }
-    // The image shifts of cells across a periodic boundary, one warp per such cell.
+    // Each cell's image shift plus the brick's frame, one warp per cell that moves.
+    const BrickFrame<T> frame = brick_frame(s, brick);
     for (int t = warp; t < cells; t += kWarpsPerBlock)
     {
         const int r = t / per_row, c = t % per_row;
         const int cx = x0 - 1 + c, cy = y + r % 3 - 1, cz = z + r / 3 - 1;
-        const T sx = cx < 0 ? -s.length[0] : (cx >= nx ? s.length[0] : T(0));
-        const T sy = cy < 0 ? -s.length[1] : (cy >= ny ? s.length[1] : T(0));
-        const T sz = cz < 0 ? -s.length[2] : (cz >= nz ? s.length[2] : T(0));
+        const T sx = (cx < 0 ? -s.length[0] : (cx >= nx ? s.length[0] : T(0))) + frame.x;
+        const T sy = (cy < 0 ? -s.length[1] : (cy >= ny ? s.length[1] : T(0))) + frame.y;
+        const T sz = (cz < 0 ? -s.length[2] : (cz >= nz ? s.length[2] : T(0))) + frame.z;
         if (sx != T(0) || sy != T(0) || sz != T(0))
         {
             for (int k = start[t] + lane; k < start[t + 1]; k += kWarp)
@@ -550,11 +582,16 @@ __device__ __forceinline__ void force_center(
     const System<T>& s,
     const Pos4<T>* __restrict__ tile,
     const PairParams<T>* __restrict__ params,
+    const BrickFrame<T>& frame,
     int center,
     double* sums
 )
 {
-    const Pos4<T> me = s.pos[center];
+    // The center in the brick's frame, by the same additions its tile copy took.
+    Pos4<T> me = s.pos[center];
+    me.x += frame.x;
+    me.y += frame.y;
+    me.z += frame.z;
     CenterSums<T> c = pair_loop<T, kSmall, kMulti, kVirial>(s, tile, params, me, center);
     T scale = T(1);  // kJ/mol/nm per unit of the accumulated force
     double energy;
@@ -893,11 +930,12 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
         const TileShape shape = stage_brick(s, blockIdx.x, s.pos, tile, start, first);
         if (shape.size <= s.tile_cap)
         {
+            const BrickFrame<T> frame = brick_frame(s, blockIdx.x);
             for (int center = shape.home_first + threadIdx.x; center < shape.home_end;
                  center += blockDim.x)
             {
-                force_center<T, false, kMulti, kVirial, kKickStep, kThermostat>(s, tile, params,
-                                                                               center, sums);
+                force_center<T, false, kMulti, kVirial, kKickStep, kThermostat>(
+                    s, tile, params, frame, center, sums);
             }
         }
         else if (threadIdx.x == 0)

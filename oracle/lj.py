@@ -68,3 +68,33 @@ def energy_force_virial(positions, cell, first, second, sigma, epsilon, cutoff, 
     np.add.at(dsigma, rows, 24 * e / s * (2 * p6 * p6 - p6 - 2 * pc6 * pc6 + pc6))
     np.add.at(depsilon, rows, 4 * (p6 * p6 - p6) - 4 * (pc6 * pc6 - pc6))
     return energy, forces, virial, dsigma, depsilon
+
+
+def sample_forces(positions, cell, centers, sigma, epsilon, cutoff):
+    """float64 forces on the atoms ``centers`` only, each with its complete neighbor set.
+
+    For boxes too large for an all-atom evaluation here: positions [N, 3] anywhere (wrapped in
+    float64 first), neighbors within the cutoff found by a periodic k-d tree, each unordered
+    pair listed once, then ``energy_force_virial`` over those pairs (one atom type).
+    """
+    from scipy.spatial import cKDTree
+
+    cell = np.asarray(cell, dtype=np.float64)
+    x = np.asarray(positions, dtype=np.float64)
+    x = x - np.floor(x / cell) * cell
+    x = np.where(x >= cell, x - cell, x)
+    centers = np.asarray(centers, dtype=np.int64)
+    tree = cKDTree(x, boxsize=cell)
+    found = tree.query_ball_point(x[centers], cutoff)
+    sampled = np.zeros(len(x), dtype=bool)
+    sampled[centers] = True
+    first, second = [], []
+    for center, neighbors in zip(centers, found):
+        neighbors = np.asarray(neighbors, dtype=np.int64)
+        # A pair of two sampled atoms is listed from its lower index only.
+        keep = (neighbors != center) & ~(sampled[neighbors] & (neighbors < center))
+        second.append(neighbors[keep])
+        first.append(np.full(int(keep.sum()), center, dtype=np.int64))
+    first, second = np.concatenate(first), np.concatenate(second)
+    _, forces, _ = energy_force_virial(x, cell, first, second, sigma, epsilon, cutoff)
+    return forces[centers]
