@@ -61,6 +61,15 @@ class Ranks:
         dist.all_reduce(tensor, op=dist.ReduceOp.SUM)
         return float(tensor)
 
+    def gather(self, rows: list) -> list:
+        """Every rank's ``rows`` (picklable items), concatenated in rank order, on every rank.
+        Host objects only: per-request results of a shard, not device data."""
+        if not self._joined:
+            return list(rows)
+        parts: list = [None] * self.world
+        dist.all_gather_object(parts, list(rows))
+        return [row for part in parts for row in part]
+
     def close(self) -> None:
         if self._joined:
             dist.destroy_process_group()

@@ -5,7 +5,8 @@ frames prepared once with their pair stacks, batches from one seeded shuffle per
 batch's loss gradient written into ``.grad`` and ``optimizer.step()``, rows the model does not
 train held, RMS errors before and after. The gradient of a Lennard-Jones model comes from the
 batched kernels and their hand-written parameter backward in one pass over the batch; any
-other model's from the reference's torch.func algorithm in chunks of frames.
+other model's from the reference's torch.func algorithm in chunks of frames. Given a process
+group, the frames of each batch are split over its ranks (``_parallel``).
 """
 
 from __future__ import annotations
@@ -20,6 +21,7 @@ from torch import Tensor
 
 from ..potential import Potential
 from ..potential._lennard_jones import LennardJones
+from . import _parallel
 from ._generic import loss_and_gradient
 from ._loss import CHANNELS, loss as batch_loss, scales as label_scales
 from ._predict import predict
@@ -127,7 +129,24 @@ def _errors(model, prepared, channels, size: int) -> dict[str, float]:
     return {name: math.sqrt(squares[name] / labels[name].numel()) for name in channels}
 
 
-def _gradient(model, trained, prepared, frames, weights, scales, channels, chunk):
+def _gradient(model, trained, prepared, frames, weights, scales, channels, chunk,
+              process_group=None):
+    """The batch's loss and gradient; with a process group, each rank differentiates its share
+    of the frames and one all-reduce sums the frame-weighted shares."""
+    if process_group is None:
+        return _share_gradient(model, trained, prepared, frames, weights, scales, channels,
+                               chunk)
+    mine = _parallel.share(frames, process_group)
+    if len(mine) > 0:
+        value, grads = _share_gradient(model, trained, prepared, mine, weights, scales,
+                                       channels, chunk)
+    else:
+        value = torch.zeros((), dtype=torch.float64, device=prepared[0].device)
+        grads = {name: torch.zeros_like(tensor) for name, tensor in trained.items()}
+    return _parallel.reduce(value, grads, len(mine) / len(frames), process_group)
+
+
+def _share_gradient(model, trained, prepared, frames, weights, scales, channels, chunk):
     positions, cells, stack, labels = prepared
     index = frames.to(positions.device)
     part = {name: labels[name][index] for name in channels}
@@ -148,7 +167,8 @@ def _gradient(model, trained, prepared, frames, weights, scales, channels, chunk
 def fit(model: Potential, train: Dataset, optimizer: torch.optim.Optimizer, *, updates: Integral,
         batch_size: Integral, energy: Real | None = None, forces: Real | None = None,
         virial: Real | None = None, validation: Dataset | None = None, seed: Integral = 0,
-        scheduler=None, echo_every: Integral | None = None, chunk: Integral = 4) -> Report:
+        scheduler=None, echo_every: Integral | None = None, chunk: Integral = 4,
+        process_group=None) -> Report:
     """Fit the model's trainable parameters to the training labels; return a ``Report``.
 
     A channel enters the loss when its weight is given: w mean(((X - X*) / s)^2), s from the
@@ -156,7 +176,10 @@ def fit(model: Potential, train: Dataset, optimizer: torch.optim.Optimizer, *, u
     writes the gradient of the batch's loss into ``.grad`` and steps the optimizer (and the
     ``scheduler`` after it); rows the model does not train keep their values. ``chunk`` bounds
     the frames a non-LJ model differentiates at once. With ``echo_every`` = k, prints the
-    mean loss and terms every k updates. Syncs with the host.
+    mean loss and terms every k updates. With ``process_group`` (torch.distributed, one rank
+    per GPU, every rank calling ``fit`` with the same arguments), each update's frames are
+    split over the ranks and their gradients summed by one all-reduce, so every rank takes
+    the same step. Syncs with the host.
 
     Raises ``TypeError`` for a model that is not a Potential and ``ValueError`` for weights
     or counts out of range, no trainable parameter, or sets with another atom count or
@@ -204,7 +227,7 @@ def fit(model: Potential, train: Dataset, optimizer: torch.optim.Optimizer, *, u
         print("update loss", flush=True)
     for update, frames in enumerate(batches(len(train), batch_size, updates, seed)):
         value, gradient = _gradient(model, trained, prepared["training"], frames, weights,
-                                    scales, channels, int(chunk))
+                                    scales, channels, int(chunk), process_group)
         optimizer.zero_grad()
         for name, parameter in trained.items():
             parameter.grad = gradient[name].to(parameter.dtype)

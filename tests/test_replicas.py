@@ -1,7 +1,8 @@
 """The multi-rank plumbing of bench.py and serving on the host: two gloo ranks on the CPU
 (one process each, rendezvous on 127.0.0.1) join, meet at a barrier, agree on the maximum and
-the sum of their values, compute the same request shards, and leave; shards cover every
-request once and stay within one request of the average."""
+the sum of their values, compute the same request shards, gather every shard's results on
+every rank (the sharded serve's p50/p99 come from them), and leave; shards cover every request
+once and stay within one request of the average."""
 
 import os
 import socket
@@ -25,10 +26,13 @@ def _rank_main(rank: int, world: int, port: int, queue) -> None:
     ranks.barrier()
     largest = ranks.max(rank + 1.5)
     total = ranks.sum(rank + 1.0)
-    shards = shard_requests([float(k % 7 + 1) for k in range(23)], ranks.world)
+    work = [float(k % 7 + 1) for k in range(23)]
+    shards = shard_requests(work, ranks.world)
+    # A sharded serve: each rank "serves" its share and every rank gathers all results.
+    served = ranks.gather([(k, work[k] * 10.0) for k in shards[rank]])
     ranks.barrier()
     ranks.close()
-    queue.put((rank, largest, total, shards))
+    queue.put((rank, largest, total, shards, served))
 
 
 def test_two_gloo_ranks_agree():
@@ -46,6 +50,10 @@ def test_two_gloo_ranks_agree():
     assert [r[1] for r in results] == [2.5, 2.5]
     assert [r[2] for r in results] == [3.0, 3.0]
     assert results[0][3] == results[1][3]
+    for result in results:  # every request's result reaches every rank exactly once
+        served = result[4]
+        assert sorted(k for k, _ in served) == list(range(23))
+        assert all(latency == (k % 7 + 1) * 10.0 for k, latency in served)
 
 
 @pytest.mark.parametrize("world", [1, 2, 3, 8])
@@ -61,5 +69,6 @@ def test_single_rank_needs_no_group():
     ranks = Ranks("gloo")
     assert (ranks.rank, ranks.world) == (0, 1)
     assert ranks.max(4.0) == 4.0 and ranks.sum(2.0) == 2.0
+    assert ranks.gather([1, 2]) == [1, 2]
     ranks.barrier()
     ranks.close()
