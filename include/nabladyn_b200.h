@@ -117,8 +117,10 @@ int nd_neighbors_update(int dtype, const void* positions, const void* cell, int6
  * passes only the inputs and the outputs: positions [N, 3] wrapped into [0, L) and cell [3]
  * (device), the grid dims[3] and bin widths[3] (host values, as allocate chooses them), and
  * pairs [2, capacity], pair_total [1], status [2] (device). Limits: N <= 16384 and at most
- * 16384 bins; with at most three bins per axis (the all-pairs path) N <= 2048; larger inputs
- * return ND_EINVAL. The first call on a device looks up the array's address with
+ * 16384 bins; with at most three bins per axis (the all-pairs path) N <= 2048; larger inputs,
+ * and widths that are not finite, not positive or narrower than the radius, return ND_EINVAL.
+ * The kernels bin with width L / dims (the cell on the device) and, should that be narrower
+ * than the radius, build nothing and set ND_STATUS_INVALID_CELL. The first call on a device looks up the array's address with
  * cudaGetSymbolAddress, so make it before any stream capture. Every call shares the array and
  * leaves the last call's contents in it: calls that overlap on the GPU (other streams, other
  * threads) race and must be serialized by the caller. */

@@ -1,21 +1,36 @@
 // The neighbor operator: a cell-list half list of the pairs closer than the list radius,
 // with the on-GPU skin-reuse check, behind the C-ABI of include/nabladyn_b200.h.
 //
-// The operator keeps the reference's contract exactly (src/nabladyn/neighbors/csrc/ops.h:12-89,
-// entry_points.cu:284-508): the same buffers, the same status bits, the same pair set (each
-// pair found once, from the lower sorted index), padding columns k holding (k mod N, k mod N),
-// and every rebuild kernel gated by a device flag so one CUDA Graph holds the whole update.
+// The contract is the reference's (src/nabladyn/neighbors/csrc/ops.h:12-89,
+// runtime/entry_points.cu:284-508): the same 15 buffers, the same status bits, the same pair
+// set (each pair once, listed from the atom earlier in bin order), pair columns grouped by that
+// atom from its offset in the scan of the counts, padding column k = (k mod N, k mod N), and
+// every rebuild kernel gated by a device flag so one CUDA Graph holds a whole update. Two
+// rules decide the pair set bit for bit and are kept: the grid (bins of width L / n_a, atoms
+// ordered by bin, then by id) and the rounding of a displacement and its square (one rounding
+// per difference, r^2 = fma(dz, dz, fma(dx, dx, dy * dy))).
 //
-// What differs is how a build runs on the GPU:
-//   * binning takes its in-bin slot from the counting atomic, so the scatter needs no atomics;
-//   * one warp per bin orders the bin by atom id with register shuffles and gathers the sorted
-//     positions in the same pass (the reference ranks from global memory, then gathers);
-//   * the scans are our own gated kernels (scan.cuh), so an update that reuses its pairs runs
-//     no scan at all;
-//   * the pair total and the padding share one launch.
+// How the GPU builds it is this file's own design:
+//   * binning takes each atom's in-bin slot from the counting atomic, and one warp per bin
+//     orders the bin by id with shuffles while gathering the sorted positions;
+//   * the pairs are built per HOME BIN, one CTA each. Every candidate of a home bin's atoms
+//     sits in the home bin itself (after the atom) or in a stencil bin that comes later in bin
+//     order; the CTA stages exactly those bins into shared memory as 16-B (x, y, z, id) slots,
+//     each bin's coordinates already moved by its image where the move is exact. A warp then
+//     takes one center at a time and its 32 lanes take 32 candidates: one ballot per 32
+//     tests, pair counts from popcounts, and the fill's columns from a prefix popcount, so
+//     each warp writes a center's pairs as contiguous, coalesced columns;
+//   * small boxes (at most three bins per axis) keep a word-major bit matrix: one thread per
+//     (center, 32-candidate word) with the word's candidates staged in shared memory, so
+//     threads of a block store consecutive words;
+//   * the update opens with one warp that checks the cell and sets the grid and the reuse
+//     threshold, checks reuse with one atomic per warp, and commits the new reference frame
+//     inside the fill; the scans are our own gated kernels (scan.cuh), so an update that
+//     reuses its pairs runs no scan; the pair total and the padding share one launch.
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -26,122 +41,22 @@
 
 namespace nd {
 
-// ---------------------------------------------------------------------------------------
-// The traversal.
-
-// One neighbor bin along one axis of a 27-bin stencil: its index and the image split of its
-// shift s in {-L, 0, L}: the difference is (center - lead) - (other + trail), where lead = s
-// when s > 0 and trail = s when s < 0, so each side moves by an exact multiple of L and the
-// difference rounds once (reference: traversal.cuh:9-28, 40-57).
+// A staged candidate: coordinates in the list's dtype and the atom id in the fourth word.
 template <typename T>
-struct StencilAxis
+struct alignas(4 * sizeof(T)) Slot
 {
-    index_t bin[3];
-    T lead[3];   // center - lead, per step -1, 0, +1
-    T trail[3];  // other + trail
-
-    __device__ __forceinline__ StencilAxis(index_t home, index_t count, T center, T length)
-    {
-#pragma unroll
-        for (int s = 0; s < 3; ++s)
-        {
-            const index_t raw = home + s - 1;
-            const T shift = raw < 0 ? -length : (raw >= count ? length : T(0));
-            bin[s] = raw < 0 ? raw + count : (raw >= count ? raw - count : raw);
-            lead[s] = shift > T(0) ? center - shift : center;
-            trail[s] = shift < T(0) ? shift : T(0);
-        }
-    }
+    T x, y, z, w;
 };
 
-// Calls visit(k) for every sorted atom k > center, in the 27 (or, on short axes, all) bins
-// around the center's bin, that lies closer than sqrt(radius_squared). With three or more bins
-// on every axis each stencil bin has a fixed image; otherwise every candidate takes its minimum
-// image. The visiting order (z, y, x bins; ascending sorted index) fixes the fill order.
-template <typename T, typename Visit>
-__device__ __forceinline__ void visit_listed(
-    const T* __restrict__ sorted_positions,
-    const index_t* __restrict__ sorted_ids,
-    const index_t* __restrict__ atom_bin,
-    const index_t* __restrict__ bin_offsets,
-    const index_t* __restrict__ dims,
-    const T* __restrict__ cell,
-    T radius_squared,
-    index_t center,
-    Visit& visit
-)
+__device__ __forceinline__ float id_word(float, index_t id) { return __int_as_float(id); }
+__device__ __forceinline__ double id_word(double, index_t id)
 {
-    const T cx = sorted_positions[3LL * center];
-    const T cy = sorted_positions[3LL * center + 1];
-    const T cz = sorted_positions[3LL * center + 2];
-    const index_t nx = dims[0], ny = dims[1], nz = dims[2];
-    const index_t home = atom_bin[sorted_ids[center]];
-    const index_t hx = home % nx, hy = (home / nx) % ny, hz = home / (nx * ny);
-    if (nx >= 3 && ny >= 3 && nz >= 3)
-    {
-        const StencilAxis<T> ax(hx, nx, cx, cell[0]);
-        const StencilAxis<T> ay(hy, ny, cy, cell[1]);
-        const StencilAxis<T> az(hz, nz, cz, cell[2]);
-#pragma unroll
-        for (int sz = 0; sz < 3; ++sz)
-        {
-#pragma unroll
-            for (int sy = 0; sy < 3; ++sy)
-            {
-                const index_t row = nx * (ay.bin[sy] + ny * az.bin[sz]);
-#pragma unroll
-                for (int sx = 0; sx < 3; ++sx)
-                {
-                    const index_t bin = ax.bin[sx] + row;
-                    const index_t first = bin_offsets[bin];
-                    const index_t end = bin_offsets[bin + 1];
-                    for (index_t k = first > center ? first : center + 1; k < end; ++k)
-                    {
-                        const T* p = sorted_positions + 3LL * k;
-                        const T dx = ax.lead[sx] - (p[0] + ax.trail[sx]);
-                        const T dy = ay.lead[sy] - (p[1] + ay.trail[sy]);
-                        const T dz = az.lead[sz] - (p[2] + az.trail[sz]);
-                        if (squared_norm(dx, dy, dz) < radius_squared)
-                        {
-                            visit(k);
-                        }
-                    }
-                }
-            }
-        }
-        return;
-    }
-    // An axis with fewer than three bins is searched whole; one with three or more, around home.
-    const int span_x = nx >= 3 ? 3 : nx, span_y = ny >= 3 ? 3 : ny, span_z = nz >= 3 ? 3 : nz;
-    auto around = [](index_t h, int step, index_t count) {
-        const index_t raw = h + step - 1;
-        return raw < 0 ? raw + count : (raw >= count ? raw - count : raw);
-    };
-    for (int iz = 0; iz < span_z; ++iz)
-    {
-        const index_t bz = nz >= 3 ? around(hz, iz, nz) : iz;
-        for (int iy = 0; iy < span_y; ++iy)
-        {
-            const index_t by = ny >= 3 ? around(hy, iy, ny) : iy;
-            for (int ix = 0; ix < span_x; ++ix)
-            {
-                const index_t bin = (nx >= 3 ? around(hx, ix, nx) : ix) + nx * (by + ny * bz);
-                const index_t first = bin_offsets[bin];
-                const index_t end = bin_offsets[bin + 1];
-                for (index_t k = first > center ? first : center + 1; k < end; ++k)
-                {
-                    const T* p = sorted_positions + 3LL * k;
-                    const T dx = min_image(cx, p[0], cell[0]);
-                    const T dy = min_image(cy, p[1], cell[1]);
-                    const T dz = min_image(cz, p[2], cell[2]);
-                    if (squared_norm(dx, dy, dz) < radius_squared)
-                    {
-                        visit(k);
-                    }
-                }
-            }
-        }
-    }
+    return __longlong_as_double(static_cast<long long>(id));
+}
+__device__ __forceinline__ index_t word_id(float w) { return __float_as_int(w); }
+__device__ __forceinline__ index_t word_id(double w)
+{
+    return static_cast<index_t>(__double_as_longlong(w));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -248,181 +163,489 @@ __global__ void order_bins_kernel(
 }
 
 // ---------------------------------------------------------------------------------------
-// Pairs on the grid path.
+// Pairs on the grid path: one CTA per home bin.
 
-struct CountVisit
-{
-    index_t count;
-    __device__ __forceinline__ void operator()(index_t) { ++count; }
-};
+constexpr int kHoodThreads = 128;
+constexpr int kHoodWarps = kHoodThreads / kWarp;
+constexpr int kHoodBins = 27;  // the home bin and its stencil, at most
 
-// Writes (center id, neighbor id) from the center's first column; columns at or past the
-// capacity are counted but not written.
-struct FillVisit
-{
-    const index_t* __restrict__ sorted_ids;
-    index_t center_id;
-    std::int64_t column;
-    std::int64_t capacity;
-    index_t* __restrict__ pairs;
-
-    __device__ __forceinline__ void operator()(index_t neighbor)
-    {
-        if (column < capacity)
-        {
-            pairs[column] = center_id;
-            pairs[capacity + column] = sorted_ids[neighbor];
-        }
-        ++column;
-    }
-};
-
+// Shared-memory slots of one neighborhood: 32 KB in either dtype. A neighborhood with more
+// candidates (dense or very wide bins) is read from global memory instead, with the same
+// arithmetic.
 template <typename T>
-__global__ void count_pairs_kernel(
-    const T* __restrict__ sorted_positions,
-    const index_t* __restrict__ sorted_ids,
-    const index_t* __restrict__ atom_bin,
-    const index_t* __restrict__ bin_offsets,
+struct HoodSlots
+{
+    static constexpr int value = 32768 / static_cast<int>(sizeof(Slot<T>));
+};
+
+// The part of a home bin's stencil that holds candidates: the home bin (its atoms after the
+// center) and each stencil bin that comes later in bin order (all its atoms). With three or
+// more bins per axis each bin has a fixed image: `ahead` marks the axes on which the bin lies
+// past the upper face, where the center moves by -L (the rounding of center - L, then of the
+// difference), `behind` those on which it lies past the lower face, where the candidate moves
+// by -L when staged. Otherwise every candidate takes the minimum image per axis.
+struct Hood
+{
+    int count;                    // bins kept, the home bin first
+    int total;                    // candidates in them
+    int first[kHoodBins];         // sorted index of each bin's first atom
+    int size[kHoodBins];          // atoms per bin
+    int slot[kHoodBins + 1];      // first slot of each bin in the staged list
+    unsigned char ahead[kHoodBins];
+    unsigned char behind[kHoodBins];
+};
+
+// One warp lists the home bin's stencil. Lane s takes stencil bin s; the kept bins follow the
+// home bin in stencil order, placed by a ballot.
+__device__ __forceinline__ void plan_hood(
+    Hood& hood,
+    index_t home,
     const index_t* __restrict__ dims,
-    const T* __restrict__ cell,
-    T radius_squared,
-    index_t num_atoms,
-    index_t* __restrict__ pair_counts,
-    const index_t* __restrict__ rebuild,
-    const index_t* __restrict__ status
+    const index_t* __restrict__ bin_offsets,
+    bool fixed_images
 )
 {
-    const std::int64_t center = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (center >= num_atoms || !rebuilding(rebuild, status))
+    const int lane = threadIdx.x % kWarp;
+    const index_t n[3] = {dims[0], dims[1], dims[2]};
+    const index_t h[3] = {home % n[0], (home / n[0]) % n[1], home / (n[0] * n[1])};
+    // Stencil bins per axis: three around home, or the whole axis when it has fewer bins.
+    int span[3];
+    for (int a = 0; a < 3; ++a)
     {
-        return;
+        span[a] = n[a] >= 3 ? 3 : n[a];
     }
-    CountVisit visit{0};
-    visit_listed(sorted_positions, sorted_ids, atom_bin, bin_offsets, dims, cell, radius_squared,
-                 static_cast<index_t>(center), visit);
-    pair_counts[center] = visit.count;
+    bool keep = false;
+    index_t bin = 0;
+    unsigned ahead = 0, behind = 0;
+    if (lane < span[0] * span[1] * span[2])
+    {
+        const int s[3] = {lane % span[0], (lane / span[0]) % span[1], lane / (span[0] * span[1])};
+        index_t b[3];
+        for (int a = 0; a < 3; ++a)
+        {
+            if (n[a] >= 3)
+            {
+                const index_t raw = h[a] + s[a] - 1;
+                b[a] = raw < 0 ? raw + n[a] : (raw >= n[a] ? raw - n[a] : raw);
+                if (fixed_images)
+                {
+                    ahead |= raw >= n[a] ? 1u << a : 0u;
+                    behind |= raw < 0 ? 1u << a : 0u;
+                }
+            }
+            else
+            {
+                b[a] = s[a];
+            }
+        }
+        bin = b[0] + n[0] * (b[1] + n[1] * b[2]);
+        keep = bin > home;
+    }
+    const unsigned kept = __ballot_sync(kFullMask, keep);
+    const int count = 1 + __popc(kept);
+    if (keep)
+    {
+        const int at = 1 + __popc(kept & ((1u << lane) - 1u));
+        const index_t begin = bin_offsets[bin];
+        hood.first[at] = begin;
+        hood.size[at] = bin_offsets[bin + 1] - begin;
+        hood.ahead[at] = static_cast<unsigned char>(ahead);
+        hood.behind[at] = static_cast<unsigned char>(behind);
+    }
+    if (lane == 0)
+    {
+        const index_t begin = bin_offsets[home];
+        hood.first[0] = begin;
+        hood.size[0] = bin_offsets[home + 1] - begin;
+        hood.ahead[0] = 0;
+        hood.behind[0] = 0;
+        hood.count = count;
+    }
+    __syncwarp();
+    // Slots: an exclusive scan of the kept bins' sizes, in their order.
+    const int value = lane < count ? hood.size[lane] : 0;
+    int inclusive = value;
+#pragma unroll
+    for (int offset = 1; offset < kWarp; offset *= 2)
+    {
+        const int up = __shfl_up_sync(kFullMask, inclusive, offset);
+        inclusive += lane >= offset ? up : 0;
+    }
+    if (lane < count)
+    {
+        hood.slot[lane] = inclusive - value;
+    }
+    if (lane == count - 1)
+    {
+        hood.slot[count] = inclusive;
+        hood.total = inclusive;
+    }
 }
 
+// Candidate `k` of kept bin `g`, in the list's arithmetic: the coordinate moved by -L on the
+// axes where the bin lies past the lower face (an exact move), and the atom id.
 template <typename T>
-__global__ void fill_pairs_kernel(
+__device__ __forceinline__ Slot<T> hood_candidate(
+    const Hood& hood, int g, int k,
     const T* __restrict__ sorted_positions,
     const index_t* __restrict__ sorted_ids,
-    const index_t* __restrict__ atom_bin,
+    T lx, T ly, T lz
+)
+{
+    const std::int64_t atom = hood.first[g] + k;
+    const T* p = sorted_positions + 3 * atom;
+    const unsigned behind = hood.behind[g];
+    Slot<T> out;
+    out.x = (behind & 1u) ? p[0] + (-lx) : p[0];
+    out.y = (behind & 2u) ? p[1] + (-ly) : p[1];
+    out.z = (behind & 4u) ? p[2] + (-lz) : p[2];
+    out.w = id_word(T(0), sorted_ids[atom]);
+    return out;
+}
+
+// What a warp does with one center's candidates: count them, or write them as columns.
+struct CountSink
+{
+    index_t count = 0;
+    __device__ __forceinline__ void take(unsigned hits, bool, index_t) { count += __popc(hits); }
+};
+
+struct FillSink
+{
+    index_t* __restrict__ pairs;
+    std::int64_t capacity;
+    std::int64_t column;  // the next column of this center
+    index_t center_id;
+    __device__ __forceinline__ void take(unsigned hits, bool hit, index_t other)
+    {
+        if (hit)
+        {
+            const int lane = threadIdx.x % kWarp;
+            const std::int64_t at = column + __popc(hits & ((1u << lane) - 1u));
+            if (at < capacity)
+            {
+                pairs[at] = center_id;
+                pairs[capacity + at] = other;
+            }
+        }
+        column += __popc(hits);
+    }
+};
+
+// One warp, one center: its candidates 32 at a time, per kept bin.
+template <typename T, bool kFixed, bool kStaged, typename Sink>
+__device__ __forceinline__ void visit_center(
+    const Hood& hood,
+    const Slot<T>* __restrict__ staged,
+    const T* __restrict__ sorted_positions,
+    const index_t* __restrict__ sorted_ids,
+    int h,
+    T lx, T ly, T lz,
+    T radius_squared,
+    Sink& sink
+)
+{
+    const int lane = threadIdx.x % kWarp;
+    const Slot<T> c = kStaged ? staged[h]
+                              : hood_candidate(hood, 0, h, sorted_positions, sorted_ids, lx, ly,
+                                               lz);
+    // The center past the lower face of a later bin's image: center - L, rounded once.
+    const T cx_ahead = c.x - lx, cy_ahead = c.y - ly, cz_ahead = c.z - lz;
+    for (int g = 0; g < hood.count; ++g)
+    {
+        const unsigned ahead = hood.ahead[g];
+        const T ax = (ahead & 1u) ? cx_ahead : c.x;
+        const T ay = (ahead & 2u) ? cy_ahead : c.y;
+        const T az = (ahead & 4u) ? cz_ahead : c.z;
+        const int begin = g == 0 ? h + 1 : 0;
+        const int end = hood.size[g];
+        for (int base = begin; base < end; base += kWarp)
+        {
+            const int k = base + lane;
+            const bool valid = k < end;
+            Slot<T> p;
+            if (valid)
+            {
+                p = kStaged ? staged[hood.slot[g] + k]
+                            : hood_candidate(hood, g, k, sorted_positions, sorted_ids, lx, ly,
+                                             lz);
+            }
+            else
+            {
+                p = Slot<T>{ax, ay, az, T(0)};
+            }
+            T dx, dy, dz;
+            if (kFixed)
+            {
+                dx = ax - p.x;
+                dy = ay - p.y;
+                dz = az - p.z;
+            }
+            else
+            {
+                dx = min_image(c.x, p.x, lx);
+                dy = min_image(c.y, p.y, ly);
+                dz = min_image(c.z, p.z, lz);
+            }
+            const bool hit = valid && squared_norm(dx, dy, dz) < radius_squared;
+            const unsigned hits = __ballot_sync(kFullMask, hit);
+            sink.take(hits, hit, word_id(p.w));
+        }
+    }
+}
+
+// Counts (kFill false) or writes (kFill true) the pairs of one home bin per CTA. The fill
+// of an update also stores the frame it was built from: each CTA its home atoms' positions,
+// CTA 0 the cell and the rebuild count.
+template <typename T, bool kFill>
+__global__ void __launch_bounds__(kHoodThreads) hood_pairs_kernel(
+    const T* __restrict__ sorted_positions,
+    const index_t* __restrict__ sorted_ids,
     const index_t* __restrict__ bin_offsets,
     const index_t* __restrict__ dims,
     const T* __restrict__ cell,
-    const index_t* __restrict__ pair_offsets,
     T radius_squared,
-    index_t num_atoms,
+    index_t* __restrict__ pair_counts,
+    const index_t* __restrict__ pair_offsets,
     index_t capacity,
     index_t* __restrict__ pairs,
+    const T* __restrict__ positions,
+    T* __restrict__ reference_positions,
+    T* __restrict__ reference_cell,
+    index_t* __restrict__ rebuild_count,
     const index_t* __restrict__ rebuild,
     const index_t* __restrict__ status
 )
 {
-    const std::int64_t center = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (center >= num_atoms || !rebuilding(rebuild, status))
+    if (!rebuilding(rebuild, status))
     {
         return;
     }
-    FillVisit visit{sorted_ids, sorted_ids[center], pair_offsets[center], capacity, pairs};
-    visit_listed(sorted_positions, sorted_ids, atom_bin, bin_offsets, dims, cell, radius_squared,
-                 static_cast<index_t>(center), visit);
+    __shared__ Hood hood;
+    __shared__ Slot<T> staged[HoodSlots<T>::value];
+    const index_t home = blockIdx.x;
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const bool fixed = dims[0] >= 3 && dims[1] >= 3 && dims[2] >= 3;
+    const T lx = cell[0], ly = cell[1], lz = cell[2];
+    if (warp == 0)
+    {
+        plan_hood(hood, home, dims, bin_offsets, fixed);
+    }
+    __syncthreads();
+    const int homes = hood.size[0];
+    if (kFill && reference_positions != nullptr)
+    {
+        for (int k = threadIdx.x; k < 3 * homes; k += blockDim.x)
+        {
+            const std::int64_t id = sorted_ids[hood.first[0] + k / 3];
+            reference_positions[3 * id + k % 3] = positions[3 * id + k % 3];
+        }
+        if (home == 0 && threadIdx.x < 3)
+        {
+            reference_cell[threadIdx.x] = cell[threadIdx.x];
+        }
+        if (home == 0 && threadIdx.x == 0)
+        {
+            ++rebuild_count[0];
+        }
+    }
+    if (homes == 0)
+    {
+        return;
+    }
+    const bool stage = hood.total <= HoodSlots<T>::value;
+    if (stage)
+    {
+        for (int g = warp; g < hood.count; g += kHoodWarps)
+        {
+            for (int k = lane; k < hood.size[g]; k += kWarp)
+            {
+                staged[hood.slot[g] + k] =
+                    hood_candidate(hood, g, k, sorted_positions, sorted_ids, lx, ly, lz);
+            }
+        }
+        __syncthreads();
+    }
+    for (int h = warp; h < homes; h += kHoodWarps)
+    {
+        const index_t center = hood.first[0] + h;
+        auto run = [&](auto& sink) {
+            if (fixed)
+            {
+                stage ? visit_center<T, true, true>(hood, staged, sorted_positions, sorted_ids, h,
+                                                    lx, ly, lz, radius_squared, sink)
+                      : visit_center<T, true, false>(hood, staged, sorted_positions, sorted_ids,
+                                                     h, lx, ly, lz, radius_squared, sink);
+            }
+            else
+            {
+                stage ? visit_center<T, false, true>(hood, staged, sorted_positions, sorted_ids,
+                                                     h, lx, ly, lz, radius_squared, sink)
+                      : visit_center<T, false, false>(hood, staged, sorted_positions,
+                                                      sorted_ids, h, lx, ly, lz, radius_squared,
+                                                      sink);
+            }
+        };
+        if (kFill)
+        {
+            FillSink sink{pairs, capacity, pair_offsets[center], sorted_ids[center]};
+            run(sink);
+        }
+        else
+        {
+            CountSink sink;
+            run(sink);
+            if (lane == 0)
+            {
+                pair_counts[center] = sink.count;
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------
 // The all-pairs path, for lists whose first grid has at most three bins on every axis.
+//
+// The hits live in a word-major bit matrix: word w of atom i, bits[w * N + i], holds bit b for
+// atom 32 w + b, set when that atom comes after i and lies closer than the radius (minimum
+// image per axis). Words that hold no atom after i are never written nor read.
 
 __host__ __device__ __forceinline__ std::int64_t bit_words(std::int64_t num_atoms)
 {
     return (num_atoms + kWarp - 1) / kWarp;
 }
 
-constexpr int kAllPairsThreads = 128;
+constexpr int kWordThreads = 128;
 
-// One warp per atom: every atom with a higher id is tested once, 32 per ballot, and the hits
-// are kept as the atom's bit row, so the fill computes no distance again.
+// Grid (centers / 128, words): the block stages word w's 32 candidates in shared memory and
+// each thread builds one center's word from them.
 template <typename T>
-__global__ void test_all_pairs_kernel(
+__global__ void __launch_bounds__(kWordThreads) pair_words_kernel(
     const T* __restrict__ positions,
     const T* __restrict__ cell,
     T radius_squared,
     index_t num_atoms,
     std::uint32_t* __restrict__ bits,
+    const index_t* __restrict__ rebuild,
+    const index_t* __restrict__ status
+)
+{
+    const std::int64_t word = blockIdx.y;
+    const std::int64_t first_center = static_cast<std::int64_t>(blockIdx.x) * kWordThreads;
+    if (first_center >= 32 * (word + 1) - 1 || !rebuilding(rebuild, status))
+    {
+        return;  // every center of the block comes at or after the word's last atom
+    }
+    __shared__ T candidates[3][kWarp];
+    if (threadIdx.x < kWarp)
+    {
+        const std::int64_t j = 32 * word + threadIdx.x;
+        const bool real = j < num_atoms;
+        for (int a = 0; a < 3; ++a)
+        {
+            candidates[a][threadIdx.x] = real ? positions[3 * j + a] : T(0);
+        }
+    }
+    __syncthreads();
+    const std::int64_t center = first_center + threadIdx.x;
+    if (center >= num_atoms || center >= 32 * (word + 1) - 1)
+    {
+        return;
+    }
+    const T cx = positions[3 * center], cy = positions[3 * center + 1],
+            cz = positions[3 * center + 2];
+    const T lx = cell[0], ly = cell[1], lz = cell[2];
+    std::uint32_t hits = 0;
+#pragma unroll 8
+    for (int b = 0; b < kWarp; ++b)
+    {
+        const std::int64_t j = 32 * word + b;
+        const T dx = min_image(cx, candidates[0][b], lx);
+        const T dy = min_image(cy, candidates[1][b], ly);
+        const T dz = min_image(cz, candidates[2][b], lz);
+        const bool hit = j > center && j < num_atoms && squared_norm(dx, dy, dz) < radius_squared;
+        hits |= hit ? 1u << b : 0u;
+    }
+    bits[word * num_atoms + center] = hits;
+}
+
+// One thread per center: its pair count from its words.
+__global__ void row_counts_kernel(
+    const std::uint32_t* __restrict__ bits,
+    index_t num_atoms,
     index_t* __restrict__ pair_counts,
     const index_t* __restrict__ rebuild,
     const index_t* __restrict__ status
 )
 {
-    const std::int64_t thread = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const std::int64_t center = thread / kWarp;
+    const std::int64_t center = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (center >= num_atoms || !rebuilding(rebuild, status))
     {
         return;
     }
-    const int lane = static_cast<int>(thread % kWarp);
     const std::int64_t words = bit_words(num_atoms);
-    const T cx = positions[3 * center], cy = positions[3 * center + 1],
-            cz = positions[3 * center + 2];
-    const T lx = cell[0], ly = cell[1], lz = cell[2];
     index_t count = 0;
-    for (std::int64_t word = (center + 1) / kWarp; word < words; ++word)
+    for (std::int64_t w = (center + 1) / kWarp; w < words; ++w)
     {
-        const std::int64_t other = word * kWarp + lane;
-        bool hit = false;
-        if (other > center && other < num_atoms)
-        {
-            const T* p = positions + 3 * other;
-            hit = squared_norm(min_image(cx, p[0], lx), min_image(cy, p[1], ly),
-                               min_image(cz, p[2], lz)) < radius_squared;
-        }
-        const unsigned hits = __ballot_sync(kFullMask, hit);
-        if (lane == 0)
-        {
-            bits[center * words + word] = hits;
-        }
-        count += __popc(hits);
+        count += __popc(bits[w * num_atoms + center]);
     }
-    if (lane == 0)
-    {
-        pair_counts[center] = count;
-    }
+    pair_counts[center] = count;
 }
 
-// Writes each atom's pairs from its bit row, from its first column on, in lane order.
-__global__ void fill_all_pairs_kernel(
+// One thread per center: its pairs from its words, in atom order, from its first column. The
+// fill of an update also stores the center's position, and thread 0 the cell and the count.
+template <typename T>
+__global__ void row_fill_kernel(
     const std::uint32_t* __restrict__ bits,
     const index_t* __restrict__ pair_offsets,
     index_t num_atoms,
     index_t capacity,
     index_t* __restrict__ pairs,
+    const T* __restrict__ positions,
+    const T* __restrict__ cell,
+    T* __restrict__ reference_positions,
+    T* __restrict__ reference_cell,
+    index_t* __restrict__ rebuild_count,
     const index_t* __restrict__ rebuild,
     const index_t* __restrict__ status
 )
 {
-    const std::int64_t thread = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const std::int64_t center = thread / kWarp;
+    const std::int64_t center = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (center >= num_atoms || !rebuilding(rebuild, status))
     {
         return;
     }
-    const int lane = static_cast<int>(thread % kWarp);
-    const unsigned below = (1u << lane) - 1u;
+    if (reference_positions != nullptr)
+    {
+        for (int a = 0; a < 3; ++a)
+        {
+            reference_positions[3 * center + a] = positions[3 * center + a];
+        }
+        if (center == 0)
+        {
+            for (int a = 0; a < 3; ++a)
+            {
+                reference_cell[a] = cell[a];
+            }
+            ++rebuild_count[0];
+        }
+    }
     const std::int64_t words = bit_words(num_atoms);
     std::int64_t column = pair_offsets[center];
-    for (std::int64_t word = (center + 1) / kWarp; word < words; ++word)
+    for (std::int64_t w = (center + 1) / kWarp; w < words; ++w)
     {
-        const unsigned hits = bits[center * words + word];
-        if ((hits >> lane) & 1u)
+        std::uint32_t hits = bits[w * num_atoms + center];
+        while (hits != 0)
         {
-            const std::int64_t slot = column + __popc(hits & below);
-            if (slot < capacity)
+            const int b = __ffs(hits) - 1;
+            hits &= hits - 1;
+            if (column < capacity)
             {
-                pairs[slot] = static_cast<index_t>(center);
-                pairs[capacity + slot] = static_cast<index_t>(word * kWarp + lane);
+                pairs[column] = static_cast<index_t>(center);
+                pairs[capacity + column] = static_cast<index_t>(32 * w + b);
             }
+            ++column;
         }
-        column += __popc(hits);
     }
 }
 
@@ -468,18 +691,19 @@ __global__ void total_and_pad_kernel(
 }
 
 // ---------------------------------------------------------------------------------------
-// The update: the cell check, the reuse rule and the commit of a rebuild
-// (reference: src/nabladyn/neighbors/csrc/update/update.cuh:21-145).
+// The update's gate (the rule of src/nabladyn/neighbors/csrc/update/update.cuh:13-20).
 //
-// A rebuild stores the wrapped positions x0 and the cell L0. In a cell L, with s = L / L0 per
+// A build stores the wrapped positions x0 and the cell L0. In a cell L, with s = L / L0 per
 // axis, atom i has moved d_i = min image of x_i - s x0_i; the pairs are reused while every
-// |d_i|^2 < ((R min(s) - cutoff - 32 eps L_max) / 2)^2.
+// |d_i|^2 < ((R min(s) - cutoff - 32 eps L_max) / 2)^2. Entries of `reuse`: the squared
+// threshold, then s per axis.
 
-constexpr int kThresholdSquared = 0;
-constexpr int kScale = 1;
-
+// One warp: lane a < 3 checks axis a of the cell and sets its grid (at most the first grid's
+// bins, each wider than the radius with a margin of a few roundings of L) and its scale; lane 0
+// then sets the threshold, or asks for a rebuild when there is no room to move. A list whose
+// status holds an error stays as it is until it is allocated again.
 template <typename T>
-__global__ void prepare_update_kernel(
+__global__ void open_update_kernel(
     const T* __restrict__ cell,
     const T* __restrict__ reference_cell,
     T cutoff,
@@ -493,43 +717,63 @@ __global__ void prepare_update_kernel(
     index_t* __restrict__ status
 )
 {
-    rebuild[0] = 0;
-    if (status[0] != 0)
+    const int lane = threadIdx.x;
+    const bool sound = status[0] == 0;
+    if (lane == 0)
+    {
+        rebuild[0] = 0;
+    }
+    const int axis = lane < 3 ? lane : 0;
+    const T length = cell[axis];
+    const T scale = length / reference_cell[axis];
+    const bool valid = isfinite(length) && length > 2 * cutoff;
+    const bool all_valid = __all_sync(kFullMask, valid);
+    if (!sound)
     {
         return;
     }
-    T smallest = cell[0] / reference_cell[0];
-    T longest = cell[0];
-    for (int axis = 0; axis < 3; ++axis)
+    if (!all_valid)
     {
-        const T length = cell[axis];
-        if (!(isfinite(length) && length > 2 * cutoff))
+        if (lane == 0)
         {
             status[0] |= kInvalidCell;
-            return;
         }
-        const T scale = length / reference_cell[axis];
-        reuse[kScale + axis] = scale;
-        smallest = scale < smallest ? scale : smallest;
-        longest = length > longest ? length : longest;
-        // Each bin keeps a margin of a few roundings of L.
+        return;
+    }
+    if (lane < 3)
+    {
+        reuse[1 + axis] = scale;
         const T fit = floor(length / fma(T(4) * epsilon, length, radius));
         const index_t count =
             fit < 1 ? 1 : (fit > limits[axis] ? limits[axis] : static_cast<index_t>(fit));
         dims[axis] = count;
         widths[axis] = length / count;
     }
-    const T allowance = fma(-(T(32) * epsilon), longest, fma(radius, smallest, -cutoff));
-    if (allowance <= 0)
+    // The smallest scale and the longest length, over the three axes in lane order.
+    const T s0 = __shfl_sync(kFullMask, scale, 0), s1 = __shfl_sync(kFullMask, scale, 1),
+            s2 = __shfl_sync(kFullMask, scale, 2);
+    const T l0 = __shfl_sync(kFullMask, length, 0), l1 = __shfl_sync(kFullMask, length, 1),
+            l2 = __shfl_sync(kFullMask, length, 2);
+    if (lane == 0)
     {
-        rebuild[0] = 1;
-        return;
+        T smallest = s0 < s1 ? s0 : s1;
+        smallest = s2 < smallest ? s2 : smallest;
+        T longest = l1 > l0 ? l1 : l0;
+        longest = l2 > longest ? l2 : longest;
+        const T allowance = fma(-(T(32) * epsilon), longest, fma(radius, smallest, -cutoff));
+        if (allowance <= 0)
+        {
+            rebuild[0] = 1;
+            return;
+        }
+        reuse[0] = allowance * allowance / 4;
     }
-    reuse[kThresholdSquared] = allowance * allowance / 4;
 }
 
+// One thread per atom, one atomic per warp: the non-finite bit, then the rebuild request when
+// an atom has moved past the threshold.
 template <typename T>
-__global__ void check_reuse_kernel(
+__global__ void reuse_check_kernel(
     const T* __restrict__ positions,
     const T* __restrict__ reference_positions,
     const T* __restrict__ cell,
@@ -540,58 +784,34 @@ __global__ void check_reuse_kernel(
 )
 {
     const std::int64_t atom = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (atom >= num_atoms || status[0] != 0)
+    if (status[0] != 0)
     {
-        return;
+        return;  // uniform: the open's verdict, read after its launch
     }
-    const T* x = positions + 3 * atom;
-    const T* x0 = reference_positions + 3 * atom;
-    if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2])))
+    const int lane = threadIdx.x % kWarp;
+    bool bad = false, moved_far = false;
+    if (atom < num_atoms)
+    {
+        const T* x = positions + 3 * atom;
+        const T* x0 = reference_positions + 3 * atom;
+        bad = !(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]));
+        T moved = 0;
+        for (int axis = 0; axis < 3; ++axis)
+        {
+            const T d = min_image(x[axis], reuse[1 + axis] * x0[axis], cell[axis]);
+            moved = fma(d, d, moved);
+        }
+        moved_far = !bad && moved >= reuse[0];
+    }
+    const unsigned bad_lanes = __ballot_sync(kFullMask, bad);
+    const unsigned far_lanes = __ballot_sync(kFullMask, moved_far);
+    if (lane == 0 && bad_lanes != 0)
     {
         atomicOr(status, kNonFinite);
-        return;
     }
-    if (rebuild[0] != 0)
-    {
-        return;
-    }
-    T moved = 0;
-    for (int axis = 0; axis < 3; ++axis)
-    {
-        const T d = min_image(x[axis], reuse[kScale + axis] * x0[axis], cell[axis]);
-        moved = fma(d, d, moved);
-    }
-    if (moved >= reuse[kThresholdSquared])
+    if (lane == 0 && far_lanes != 0)
     {
         rebuild[0] = 1;  // every writer stores the same value
-    }
-}
-
-template <typename T>
-__global__ void commit_rebuild_kernel(
-    const T* __restrict__ positions,
-    const T* __restrict__ cell,
-    index_t num_atoms,
-    T* __restrict__ reference_positions,
-    T* __restrict__ reference_cell,
-    index_t* __restrict__ rebuild_count,
-    const index_t* __restrict__ rebuild,
-    const index_t* __restrict__ status
-)
-{
-    const std::int64_t index = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (index >= 3LL * num_atoms || !rebuilding(rebuild, status))
-    {
-        return;
-    }
-    reference_positions[index] = positions[index];
-    if (index < 3)
-    {
-        reference_cell[index] = cell[index];
-    }
-    if (index == 0)
-    {
-        ++rebuild_count[0];
     }
 }
 
@@ -604,7 +824,16 @@ struct List
     const index_t* rebuild;  // null: a build from allocate, which always runs
 
     bool all_pairs() const { return b->bits_numel > 0; }
-    index_t* status() const { return b->status; }
+};
+
+// Where an update's fill stores the frame it was built from; all null for allocate.
+template <typename T>
+struct Commit
+{
+    const T* positions = nullptr;
+    T* reference_positions = nullptr;
+    T* reference_cell = nullptr;
+    index_t* rebuild_count = nullptr;
 };
 
 template <typename T>
@@ -630,6 +859,20 @@ int launch_grid(const T* positions, std::int64_t n, const List& list, cudaStream
     return ND_OK;
 }
 
+template <typename T, bool kFill>
+void launch_hood(const T* cell, double radius, const List& list, const Commit<T>& commit,
+                 cudaStream_t stream)
+{
+    const nd_neighbor_buffers& b = *list.b;
+    const T r = static_cast<T>(radius);
+    hood_pairs_kernel<T, kFill><<<static_cast<unsigned>(b.num_bin_slots - 1), kHoodThreads, 0,
+                                  stream>>>(
+        static_cast<const T*>(b.sorted_positions), b.sorted_ids, b.bin_offsets, b.dims, cell,
+        r * r, b.pair_counts, b.pair_offsets, static_cast<index_t>(b.capacity), b.pairs,
+        commit.positions, commit.reference_positions, commit.reference_cell,
+        commit.rebuild_count, list.rebuild, b.status);
+}
+
 template <typename T>
 int launch_count(const T* positions, const T* cell, std::int64_t n, double radius,
                  const List& list, cudaStream_t stream)
@@ -639,16 +882,18 @@ int launch_count(const T* positions, const T* cell, std::int64_t n, double radiu
     const T r = static_cast<T>(radius);
     if (list.all_pairs())
     {
-        test_all_pairs_kernel<T><<<blocks_for(n * kWarp, kAllPairsThreads), kAllPairsThreads, 0,
-                                   stream>>>(
-            positions, cell, r * r, num_atoms, reinterpret_cast<std::uint32_t*>(b.bits),
-            b.pair_counts, list.rebuild, b.status);
+        auto* bits = reinterpret_cast<std::uint32_t*>(b.bits);
+        const dim3 grid(blocks_for(n, kWordThreads), static_cast<unsigned>(bit_words(n)));
+        pair_words_kernel<T><<<grid, kWordThreads, 0, stream>>>(positions, cell, r * r,
+                                                               num_atoms, bits, list.rebuild,
+                                                               b.status);
+        ND_LAUNCH_CHECK();
+        row_counts_kernel<<<blocks_for(n), kThreads, 0, stream>>>(bits, num_atoms, b.pair_counts,
+                                                                  list.rebuild, b.status);
     }
     else
     {
-        count_pairs_kernel<T><<<blocks_for(n), kThreads, 0, stream>>>(
-            static_cast<const T*>(b.sorted_positions), b.sorted_ids, b.atom_bin, b.bin_offsets,
-            b.dims, cell, r * r, num_atoms, b.pair_counts, list.rebuild, b.status);
+        launch_hood<T, false>(cell, radius, list, Commit<T>{}, stream);
     }
     ND_LAUNCH_CHECK();
     ND_CUDA_TRY(scan_exclusive(b.pair_counts, b.pair_offsets, n, b.scan_temp, list.rebuild,
@@ -658,25 +903,21 @@ int launch_count(const T* positions, const T* cell, std::int64_t n, double radiu
 
 template <typename T>
 int launch_fill(const T* cell, std::int64_t n, double radius, const List& list,
-                cudaStream_t stream)
+                const Commit<T>& commit, cudaStream_t stream)
 {
     const nd_neighbor_buffers& b = *list.b;
     const auto num_atoms = static_cast<index_t>(n);
     const auto capacity = static_cast<index_t>(b.capacity);
-    const T r = static_cast<T>(radius);
     if (list.all_pairs())
     {
-        fill_all_pairs_kernel<<<blocks_for(n * kWarp, kAllPairsThreads), kAllPairsThreads, 0,
-                                stream>>>(
+        row_fill_kernel<T><<<blocks_for(n), kThreads, 0, stream>>>(
             reinterpret_cast<const std::uint32_t*>(b.bits), b.pair_offsets, num_atoms, capacity,
-            b.pairs, list.rebuild, b.status);
+            b.pairs, commit.positions, cell, commit.reference_positions, commit.reference_cell,
+            commit.rebuild_count, list.rebuild, b.status);
     }
     else
     {
-        fill_pairs_kernel<T><<<blocks_for(n), kThreads, 0, stream>>>(
-            static_cast<const T*>(b.sorted_positions), b.sorted_ids, b.atom_bin, b.bin_offsets,
-            b.dims, cell, b.pair_offsets, r * r, num_atoms, capacity, b.pairs, list.rebuild,
-            b.status);
+        launch_hood<T, true>(cell, radius, list, commit, stream);
     }
     ND_LAUNCH_CHECK();
     total_and_pad_kernel<<<blocks_for(b.capacity), kThreads, 0, stream>>>(
@@ -696,6 +937,8 @@ int check_buffers(int dtype, std::int64_t n, const nd_neighbor_buffers* b)
     ND_REQUIRE(b->capacity >= 1 && b->capacity <= INT32_MAX, "pairs must be [2, C] with int32 C");
     ND_REQUIRE(b->bits_numel == 0 || b->bits_numel == n * bit_words(n),
                "bits must be empty or hold N rows of ceil(N / 32) words");
+    ND_REQUIRE(b->bits_numel == 0 || bit_words(n) <= 65535,
+               "the all-pairs path takes at most 2,097,120 atoms");
     const std::int64_t need = scan_scratch_bytes(b->num_bin_slots > n ? b->num_bin_slots : n);
     ND_REQUIRE(b->scan_temp_bytes >= need, "scan_temp is smaller than scan_temp_bytes asks");
     ND_REQUIRE(b->dims && b->widths && b->atom_bin && b->bin_counts && b->bin_offsets &&
@@ -731,12 +974,12 @@ int update(const void* positions, const void* cell, std::int64_t n, double cutof
     const auto* x = static_cast<const T*>(positions);
     const auto* box = static_cast<const T*>(cell);
     const auto num_atoms = static_cast<index_t>(n);
-    prepare_update_kernel<T><<<1, 1, 0, stream>>>(
+    open_update_kernel<T><<<1, kWarp, 0, stream>>>(
         box, static_cast<const T*>(r->reference_cell), static_cast<T>(cutoff),
         static_cast<T>(radius), std::numeric_limits<T>::epsilon(), r->limits, b->dims,
         static_cast<T*>(b->widths), static_cast<T*>(r->reuse), r->rebuild, b->status);
     ND_LAUNCH_CHECK();
-    check_reuse_kernel<T><<<blocks_for(n), kThreads, 0, stream>>>(
+    reuse_check_kernel<T><<<blocks_for(n), kThreads, 0, stream>>>(
         x, static_cast<const T*>(r->reference_positions), box, static_cast<const T*>(r->reuse),
         num_atoms, r->rebuild, b->status);
     ND_LAUNCH_CHECK();
@@ -749,15 +992,12 @@ int update(const void* positions, const void* cell, std::int64_t n, double cutof
     {
         return rc;
     }
-    if ((rc = launch_fill<T>(box, n, radius, list, stream)) != ND_OK)
-    {
-        return rc;
-    }
-    commit_rebuild_kernel<T><<<blocks_for(3 * n), kThreads, 0, stream>>>(
-        x, box, num_atoms, static_cast<T*>(r->reference_positions),
-        static_cast<T*>(r->reference_cell), r->rebuild_count, r->rebuild, b->status);
-    ND_LAUNCH_CHECK();
-    return ND_OK;
+    Commit<T> commit;
+    commit.positions = x;
+    commit.reference_positions = static_cast<T*>(r->reference_positions);
+    commit.reference_cell = static_cast<T*>(r->reference_cell);
+    commit.rebuild_count = r->rebuild_count;
+    return launch_fill<T>(box, n, radius, list, commit, stream);
 }
 
 }  // namespace nd
@@ -804,9 +1044,10 @@ int nd_neighbors_fill_first_frame(int dtype, const void* positions, const void* 
     const nd::List list{buffers, nullptr};
     auto s = static_cast<cudaStream_t>(stream);
     return dtype == ND_FLOAT32
-               ? nd::launch_fill<float>(static_cast<const float*>(cell), num_atoms, radius, list, s)
+               ? nd::launch_fill<float>(static_cast<const float*>(cell), num_atoms, radius, list,
+                                        nd::Commit<float>{}, s)
                : nd::launch_fill<double>(static_cast<const double*>(cell), num_atoms, radius,
-                                         list, s);
+                                         list, nd::Commit<double>{}, s);
 }
 
 int nd_neighbors_update(int dtype, const void* positions, const void* cell,
@@ -839,7 +1080,7 @@ int nd_neighbors_update(int dtype, const void* positions, const void* cell,
 // Graph capture or memory pool, plugins whose host forbids allocation, or embedded drivers
 // with a fixed memory map. For them, nd_neighbors_build_no_alloc builds one frame's pair list
 // with every intermediate buffer (bins, sorted ids and positions, counts, offsets, scan tiles,
-// the all-pairs bit rows) in one file-scope device array of fixed size, kNoAllocBytes, which
+// the all-pairs bit matrix) in one file-scope device array of fixed size, kNoAllocBytes, which
 // every GPU that loads this library holds until the process exits. The caller passes only
 // the positions, the cell and the outputs.
 
@@ -858,6 +1099,7 @@ constexpr std::int64_t round_up_256(std::int64_t bytes)
 struct NoAllocLayout
 {
     static constexpr std::int64_t dims = 0;
+    static constexpr std::int64_t go = 128;      // the build's gate, set by store_grid_kernel
     static constexpr std::int64_t widths = 256;  // three doubles at most
     static constexpr std::int64_t atom_bin = 512;
     static constexpr std::int64_t bin_counts = atom_bin + round_up_256(4 * kNoAllocMaxAtoms);
@@ -883,41 +1125,51 @@ constexpr std::int64_t kNoAllocBytes = NoAllocLayout::size;
 // address comes from cudaGetSymbolAddress, per device.
 static __device__ __align__(256) unsigned char no_alloc_scratch[kNoAllocBytes];
 
+// The grid of the frame: the caller's bins per axis, each of width L / n as allocate chooses.
+// A bin narrower than the radius would lose pairs: the build is then not run and the status
+// reports an invalid cell. `go` gates the build's kernels as an update's rebuild flag does.
 template <typename T>
-__global__ void store_grid_kernel(index_t* dims, T* widths, int nx, int ny, int nz, double wx,
-                                  double wy, double wz)
+__global__ void store_grid_kernel(index_t* dims, T* widths, const T* cell, T radius, int nx,
+                                  int ny, int nz, index_t* go, index_t* status)
 {
-    dims[0] = nx;
-    dims[1] = ny;
-    dims[2] = nz;
-    widths[0] = static_cast<T>(wx);
-    widths[1] = static_cast<T>(wy);
-    widths[2] = static_cast<T>(wz);
+    const int n[3] = {nx, ny, nz};
+    bool narrow = false;
+    for (int a = 0; a < 3; ++a)
+    {
+        dims[a] = n[a];
+        widths[a] = cell[a] / n[a];
+        narrow = narrow || !(widths[a] >= radius);
+    }
+    go[0] = 1;
+    status[0] = narrow ? kInvalidCell : 0;
+    status[1] = 0;
 }
 
-// The array's device address on the current device, looked up once per device.
+// The array's device address on the current device, looked up once per device; concurrent
+// first calls from several host threads store the same address.
 int no_alloc_scratch_address(unsigned char** address)
 {
     constexpr int kMaxDevices = 64;
-    static unsigned char* addresses[kMaxDevices] = {};
+    static std::atomic<unsigned char*> addresses[kMaxDevices] = {};
     int device = 0;
     ND_CUDA_TRY(cudaGetDevice(&device));
     ND_REQUIRE(device >= 0 && device < kMaxDevices, "the device index is out of range");
-    if (addresses[device] == nullptr)
+    unsigned char* known = addresses[device].load(std::memory_order_acquire);
+    if (known == nullptr)
     {
         void* found = nullptr;
         ND_CUDA_TRY(cudaGetSymbolAddress(&found, no_alloc_scratch));
-        addresses[device] = static_cast<unsigned char*>(found);
+        known = static_cast<unsigned char*>(found);
+        addresses[device].store(known, std::memory_order_release);
     }
-    *address = addresses[device];
+    *address = known;
     return ND_OK;
 }
 
 template <typename T>
 int build_no_alloc(const void* positions, const void* cell, std::int64_t n, double radius,
-                   const std::int32_t* dims, const double* widths, std::int32_t* pairs,
-                   std::int64_t capacity, std::int32_t* pair_total, std::int32_t* status,
-                   cudaStream_t stream)
+                   const std::int32_t* dims, std::int32_t* pairs, std::int64_t capacity,
+                   std::int32_t* pair_total, std::int32_t* status, cudaStream_t stream)
 {
     unsigned char* base = nullptr;
     const int found = no_alloc_scratch_address(&base);
@@ -948,20 +1200,28 @@ int build_no_alloc(const void* positions, const void* cell, std::int64_t n, doub
     b.bits = all_pairs ? reinterpret_cast<std::int32_t*>(base + NoAllocLayout::bits) : nullptr;
     b.bits_numel = all_pairs ? n * bit_words(n) : 0;
     // What must start at zero: the bin counts (a build returns them to zero, but an earlier
-    // call may have stopped short), the outputs' total and status.
+    // call may have stopped short) and the total; the grid kernel sets the status and the gate.
+    auto* go = reinterpret_cast<std::int32_t*>(base + NoAllocLayout::go);
     ND_CUDA_TRY(cudaMemsetAsync(b.bin_counts, 0, sizeof(std::int32_t) * (bins + 1), stream));
     ND_CUDA_TRY(cudaMemsetAsync(pair_total, 0, sizeof(std::int32_t), stream));
-    ND_CUDA_TRY(cudaMemsetAsync(status, 0, 2 * sizeof(std::int32_t), stream));
-    store_grid_kernel<T><<<1, 1, 0, stream>>>(b.dims, static_cast<T*>(b.widths), dims[0], dims[1],
-                                              dims[2], widths[0], widths[1], widths[2]);
+    store_grid_kernel<T><<<1, 1, 0, stream>>>(b.dims, static_cast<T*>(b.widths),
+                                              static_cast<const T*>(cell),
+                                              static_cast<T>(radius), dims[0], dims[1], dims[2],
+                                              go, status);
     ND_LAUNCH_CHECK();
-    const int counted = count_first_frame<T>(positions, cell, n, radius, &b, stream);
-    if (counted != ND_OK)
+    const List list{&b, go};
+    const auto* x = static_cast<const T*>(positions);
+    const auto* box = static_cast<const T*>(cell);
+    int rc = ND_OK;
+    if (!all_pairs && (rc = launch_grid<T>(x, n, list, stream)) != ND_OK)
     {
-        return counted;
+        return rc;
     }
-    const List list{&b, nullptr};
-    return launch_fill<T>(static_cast<const T*>(cell), n, radius, list, stream);
+    if ((rc = launch_count<T>(x, box, n, radius, list, stream)) != ND_OK)
+    {
+        return rc;
+    }
+    return launch_fill<T>(box, n, radius, list, Commit<T>{}, stream);
 }
 
 }  // namespace nd
@@ -978,7 +1238,14 @@ extern "C" int nd_neighbors_build_no_alloc(int dtype, const void* positions, con
                "a required pointer is null");
     ND_REQUIRE(num_atoms >= 1 && num_atoms <= nd::kNoAllocMaxAtoms,
                "nd_neighbors_build_no_alloc takes at most 16384 atoms");
+    ND_REQUIRE(std::isfinite(radius) && radius > 0, "the radius must be positive and finite");
     ND_REQUIRE(dims[0] >= 1 && dims[1] >= 1 && dims[2] >= 1, "dims must be positive");
+    for (int a = 0; a < 3; ++a)
+    {
+        ND_REQUIRE(std::isfinite(widths[a]) && widths[a] > 0,
+                   "widths must be positive and finite");
+        ND_REQUIRE(widths[a] >= radius, "a bin must be at least the radius wide");
+    }
     const std::int64_t bins = static_cast<std::int64_t>(dims[0]) * dims[1] * dims[2];
     ND_REQUIRE(bins <= nd::kNoAllocMaxBins, "nd_neighbors_build_no_alloc takes at most 16384 bins");
     const bool all_pairs = dims[0] <= 3 && dims[1] <= 3 && dims[2] <= 3;
@@ -988,8 +1255,8 @@ extern "C" int nd_neighbors_build_no_alloc(int dtype, const void* positions, con
     ND_REQUIRE(capacity >= 1 && capacity <= INT32_MAX, "pairs must be [2, C] with int32 C");
     auto s = static_cast<cudaStream_t>(stream);
     return dtype == ND_FLOAT32
-               ? nd::build_no_alloc<float>(positions, cell, num_atoms, radius, dims, widths, pairs,
+               ? nd::build_no_alloc<float>(positions, cell, num_atoms, radius, dims, pairs,
                                            capacity, pair_total, status, s)
-               : nd::build_no_alloc<double>(positions, cell, num_atoms, radius, dims, widths,
-                                            pairs, capacity, pair_total, status, s);
+               : nd::build_no_alloc<double>(positions, cell, num_atoms, radius, dims, pairs,
+                                            capacity, pair_total, status, s);
 }

@@ -22,7 +22,7 @@ from torch import Tensor
 from .. import _native, quantity
 from .._native import Integrator, call, dtype_code, ptr, stream_handle
 from ..neighbors import NeighborList
-from ..neighbors._neighbor_list import check_cell_lengths
+from ..neighbors._neighbor_list import check_cell_lengths, status_causes
 from ..potential._schnet import SchNet
 from ..units import BOLTZMANN
 from ._engine import (
@@ -236,12 +236,8 @@ class PairEngine:
         return self.neighbors._rebuild_count
 
     def _list_tensors(self) -> dict[str, Tensor]:
-        listing = self.neighbors
-        out = {f"list.{name}": getattr(listing._buffers, name)
-               for name in listing._buffers.__slots__}
-        out.update({f"reuse.{name}": getattr(listing._reuse, name)
-                    for name in listing._reuse.__slots__})
-        return out
+        return {f"list.{name}": tensor
+                for name, tensor in self.neighbors._device_tensors().items()}
 
     def snapshot(self) -> dict[str, Tensor]:
         saved = {name: tensor.clone() for name, tensor in self.tensors.items()}
@@ -259,15 +255,10 @@ class PairEngine:
         causes = []
         if int(self.tensors["status"][0]) & _native.NON_FINITE:
             causes.append("positions must be finite")
-        flags, needed = self.neighbors._buffers.status.tolist()
-        if flags & _native.INVALID_CELL:
-            causes.append("every cell length must be finite and above twice the cutoff")
-        if flags & _native.NON_FINITE and "positions must be finite" not in causes:
-            causes.append("positions must be finite")
-        if flags & _native.OVERFLOW:
-            causes.append(
-                f"the pair capacity {self.neighbors.pair_capacity} is too small: the frame has "
-                f"{needed} pairs within {self.radius} nm; raise capacity_multiplier")
+        flags, needed = self.neighbors._device_tensors()["status"].tolist()
+        for cause in status_causes(flags, needed, self.neighbors.pair_capacity, self.radius):
+            if cause not in causes:
+                causes.append(cause)
         if self._fused:
             model_flags = self.tensors["model_status"].tolist()
             if model_flags[1] & 1:

@@ -1,8 +1,12 @@
 """Per-frame pair stacks for training, built by the GPU neighbor operator.
 
-The rule of src/nabladyn/training/_fit.py:190-242: a zero-skin list counts each frame's pairs,
-one sized for the densest frame builds every row, and rows are padded with self-pairs
-(k mod N, k mod N) to a common width.
+A stack is the reference's training input (src/nabladyn/training/_fit.py:190-242): int32
+[F, 2, C] holding each frame's pairs within the cutoff (zero skin) in its first columns and
+self-pairs (k mod N, k mod N) after them, C being the densest frame's pair capacity rounded up
+by ``width``. Here one zero-skin list counts every frame on the device (its status cleared
+between frames, so an overflow of one frame does not stop the count of the next) with a single
+host read of all counts at the end; a second list, sized for the densest frame, then builds
+each frame and its pairs are copied into the stack on the device.
 """
 
 import torch
@@ -11,12 +15,14 @@ from torch import Tensor
 from .. import space
 from .._native import OVERFLOW
 from ..neighbors import NeighborList
+from ..neighbors._neighbor_list import status_causes
 
 
 def width(count: int) -> int:
-    """``count`` rounded up to a multiple of 1/8 of its leading power of two."""
-    step = 1 << max(0, count.bit_length() - 4)
-    return -(-count // step) * step
+    """``count`` rounded up to a multiple of 2^(bits - 4), bits being its bit length: at most
+    1/8 of padding, and few distinct widths across data sets."""
+    shift = max(0, count.bit_length() - 4)
+    return ((count + (1 << shift) - 1) >> shift) << shift
 
 
 def pair_stack(positions: Tensor, cells: Tensor, cutoff: float) -> Tensor:
@@ -26,33 +32,38 @@ def pair_stack(positions: Tensor, cells: Tensor, cutoff: float) -> Tensor:
     a non-finite coordinate.
     """
     frames, atoms = positions.shape[:2]
+    device = positions.device
     wrapped = space.wrap(positions.detach(), cells.detach()[:, None])[0].contiguous()
     cells = cells.detach().contiguous()
-    totals = torch.empty(frames, dtype=torch.int32, device=positions.device)
-    densest = 0
-    while True:
-        counter = NeighborList(cutoff, capacity_multiplier=2.0)
-        counter.allocate(wrapped[densest], cells[densest])
-        for frame in range(frames):
-            counter._rebuild_wrapped(wrapped[frame], cells[frame])
-            totals[frame:frame + 1].copy_(counter._buffers.pair_total)
-        status = counter._buffers.status[0]
-        flags, densest = torch.stack([status, totals.argmax().to(status.dtype)]).tolist()
-        if flags & ~OVERFLOW:
-            counter._check_status()
-        if not flags & OVERFLOW:
-            break
-    neighbors = NeighborList(cutoff, capacity_multiplier=1.0)
-    neighbors.allocate(wrapped[densest], cells[densest])
-    capacity = neighbors.pair_capacity
-    columns = width(capacity)
-    fill = torch.arange(columns, dtype=torch.int32, device=positions.device) % atoms
-    stack = fill.expand(frames, 2, columns).contiguous()
-    pairs = neighbors.tensors().index
+
+    # Counting: every frame rebuilt into a list sized for frame 0; totals and error flags
+    # gathered on the device.
+    counter = NeighborList(cutoff, capacity_multiplier=1.0)
+    counter.allocate(wrapped[0], cells[0])
+    status = counter._device_tensors()["status"]
+    totals = torch.empty(frames, dtype=torch.int32, device=device)
+    errors = torch.zeros(1, dtype=torch.int32, device=device)
     for frame in range(frames):
-        neighbors._rebuild_wrapped(wrapped[frame], cells[frame])
+        status.zero_()
+        counter._rebuild_wrapped(wrapped[frame], cells[frame])
+        totals[frame:frame + 1].copy_(counter._device_tensors()["pair_total"])
+        errors.bitwise_or_(status[:1] & ~OVERFLOW)
+    flags, densest = torch.cat([errors, totals.argmax().reshape(1).int()]).tolist()
+    if flags:
+        raise ValueError("; ".join(status_causes(flags, 0, 0, counter.radius)))
+
+    # Building: a list sized for the densest frame, each frame's pairs copied into its row.
+    builder = NeighborList(cutoff, capacity_multiplier=1.0)
+    builder.allocate(wrapped[densest], cells[densest])
+    capacity = builder.pair_capacity
+    columns = width(capacity)
+    stack = (torch.arange(columns, dtype=torch.int32, device=device) % atoms).expand(
+        frames, 2, columns).contiguous()
+    pairs = builder.tensors().index
+    for frame in range(frames):
+        builder._rebuild_wrapped(wrapped[frame], cells[frame])
         stack[frame, :, :capacity].copy_(pairs)
-    neighbors._check_status()
+    builder._check_status()
     return stack
 
 

@@ -195,3 +195,53 @@ def test_engine_forces_on_grid_path(cuda, dtype):
     _, f64, _ = lj.energy_force_virial(wrapped, cell, first, second, [0.34], [0.996], 1.0)
     error = np.linalg.norm(state.forces.cpu().double().numpy() - f64) / np.linalg.norm(f64)
     assert error < (1e-5 if dtype == torch.float32 else 1e-12)
+
+
+def test_two_types_on_grid_path_match_oracle(cuda):
+    """A 50/50 two-type mixture on the brick-tile path (2,048 atoms, 4 cells per axis), float64:
+    20 NVE steps of md.nve against the oracle's velocity Verlet (positions to 1e-9 nm), then
+    the panel's potential energy and pressure of the last frame against the oracle's E and
+    virial (1e-9 relative): the multi-type force kernel and the grid path's virial."""
+    from oracle import integrator
+
+    positions, cell = lattice.fcc(8, 8 * 0.5745, 0.02, seed=23)
+    n = positions.shape[0]
+    types = np.random.default_rng(23).permutation(np.arange(n) % 2)
+    sigma, epsilon = [0.34, 0.32, 0.30], [0.996, 0.8, 0.6]
+    dtype = torch.float64
+    model = potential.lennard_jones(
+        atom_types=torch.tensor(types, device=cuda),
+        sigma=torch.tensor(sigma, dtype=dtype, device=cuda),
+        epsilon=torch.tensor(epsilon, dtype=dtype, device=cuda),
+        cutoff=1.0,
+    )
+    masses = torch.full((n,), 39.948, dtype=dtype, device=cuda)
+    velocities = md.maxwell_boltzmann(masses, 120.0, seed=23)
+    simulation = md.nve(model, torch.tensor(positions, dtype=dtype, device=cuda), velocities,
+                        masses, torch.tensor(cell, dtype=dtype, device=cuda), timestep=0.004)
+    assert not simulation._engine.small and simulation._engine.num_types == 2
+    simulation.run(20)
+    state = simulation.state()
+
+    def evaluate(frame):
+        first, second, _ = on.pairs(frame, cell, 1.0)
+        energy, forces, _ = lj.energy_force_virial(frame, cell, first, second, sigma, epsilon,
+                                                   1.0, atom_types=types)
+        return energy, forces
+
+    want = integrator.run(positions, velocities.cpu().numpy(), np.full(n, 39.948), cell, sigma,
+                          epsilon, 1.0, 0.004, 20, evaluate=evaluate)
+    np.testing.assert_allclose(state.positions.cpu().numpy(), want["positions"], rtol=0,
+                               atol=1e-9)
+    np.testing.assert_allclose(state.velocities.cpu().numpy(), want["velocities"], rtol=0,
+                               atol=1e-8)
+    panel = simulation.sample()
+    x = state.positions.cpu().numpy()
+    first, second, _ = on.pairs(x, cell, 1.0)
+    energy, _, virial = lj.energy_force_virial(x, cell, first, second, sigma, epsilon, 1.0,
+                                               atom_types=types)
+    v = state.velocities.cpu().numpy()
+    kinetic = 0.5 * 39.948 * float((v * v).sum())
+    pressure = (2 * kinetic + np.trace(virial)) / (3 * float(np.prod(cell)))
+    assert float(panel["potential_energy"]) == pytest.approx(energy, rel=1e-9)
+    assert float(panel["pressure"]) == pytest.approx(pressure, rel=1e-9)

@@ -99,6 +99,25 @@ def test_boundary_pairs_bit_exact(cuda, tag):
 
 
 @pytest.mark.parametrize("tag", ["f32", "f64"])
+@pytest.mark.parametrize("length, path", [(6.0, "grid"), (3.2, "all")])
+def test_designed_rounding_frames_bit_exact(cuda, tag, length, path):
+    """Pairs within 0.6 ulp of the squared radius (tests/boundary_frames.py): the kernels list
+    exactly the pairs that r^2 = fma(dz, dz, fma(dx, dx, dy * dy)) lists."""
+    import boundary_frames as bf
+
+    torch_dtype, np_dtype = DTYPES[tag]
+    positions, cell, first, second = bf.designed_frame(length, 1200 if path == "grid" else 300,
+                                                       1.1, np_dtype, seed=4)
+    neighbor_list, found = check_against_oracle(positions, cell, 1.1, torch_dtype, cuda)
+    assert found == path
+    index, total = listed(neighbor_list)
+    listed_here = bf.designed_listed(on.pair_set(index[0, :total], index[1, :total]), first,
+                                     second)
+    np.testing.assert_array_equal(
+        listed_here, bf.listed_under(bf.PINNED, positions, first, second, 1.1))
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
 def test_update_reuses_then_rebuilds(cuda, tag):
     torch_dtype, np_dtype = DTYPES[tag]
     positions, cell = lattice.simple_cubic(14, 5.2, 0.02, seed=9)

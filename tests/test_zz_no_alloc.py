@@ -116,3 +116,26 @@ def test_no_alloc_rejects_sizes_beyond_its_array():
     box = torch.tensor(cell, dtype=torch.float32, device=device)
     with pytest.raises(_native.NativeError, match="at most 16384 atoms"):
         no_alloc_build(x, box, cell, 1.1, on.grid_dims(cell, 1.1, np.float32), 10)
+
+
+@pytest.mark.parametrize("widths, message", [
+    ((1.0, 2.0, 2.0), "at least the radius wide"),      # narrower than the radius
+    ((0.0, 2.0, 2.0), "positive and finite"),
+    ((float("nan"), 2.0, 2.0), "positive and finite"),
+])
+def test_no_alloc_rejects_bad_widths(widths, message):
+    """Bins narrower than the radius would drop pairs: such widths return ND_EINVAL before
+    anything is launched."""
+    device = torch.device("cuda", 0)
+    positions, cell = lattice.random_box(100, (6.0, 6.0, 6.0), seed=35)
+    x = torch.tensor(positions, dtype=torch.float32, device=device)
+    box = torch.tensor(cell, dtype=torch.float32, device=device)
+    ints = {"dtype": torch.int32, "device": device}
+    pairs, total, status = (torch.zeros((2, 64), **ints), torch.zeros(1, **ints),
+                            torch.zeros(2, **ints))
+    rc = _native.lib().nd_neighbors_build_no_alloc(
+        _native.ND_FLOAT32, x.data_ptr(), box.data_ptr(), 100, ctypes.c_double(1.1),
+        (ctypes.c_int32 * 3)(3, 3, 3), (ctypes.c_double * 3)(*widths), pairs.data_ptr(), 64,
+        total.data_ptr(), status.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
+    assert rc == 1  # ND_EINVAL
+    assert message in _native.lib().nd_last_error().decode()
