@@ -229,14 +229,77 @@ def cpu_port_rate(steps: int = 3, cells: int = 24, threads: int | None = None) -
     }
 
 
+REFERENCE_TREE = ROOT / "baseline" / "_ref"
+
+
+def reference_cpu_rate(steps: int = 3, cells: int = 24, threads: int | None = None) -> dict:
+    """The reference's own CPU path (installed in baseline/_ref): per step its
+    quantity.energy_force_virial of its LennardJones on CPU float32 tensors (torch.func, with
+    ``threads`` host threads, all of them by default), the two half kicks and the drift with its
+    space.wrap. The reference builds pairs only on CUDA, so the pairs come from the oracle's C
+    restatement of its operator, once per sample at the list radius (untimed; the atoms move
+    well under half the skin in these steps).
+
+    Sample: a cells^3-cell FCC block of the workload's density (4 cells^3 atoms).
+    """
+    import torch
+
+    if str(REFERENCE_TREE) not in sys.path:
+        sys.path.insert(0, str(REFERENCE_TREE))
+    from nabladyn import potential, quantity, space  # the reference package
+    from nabladyn.neighbors import NeighborPairs
+
+    from nabladyn_b200 import lattice
+    from oracle import neighbors as on
+
+    threads = threads or os.cpu_count() or 1
+    previous = torch.get_num_threads()
+    torch.set_num_threads(threads)
+    length = LENGTH * cells / ATOMS_PER_SIDE_CELLS
+    positions, cell = lattice.fcc(cells, length, 0.02, seed=1)
+    n = positions.shape[0]
+    box = torch.tensor(cell, dtype=torch.float32)
+    x, _ = space.wrap(torch.tensor(positions, dtype=torch.float32), box)
+    first, second, _ = on.pairs(x.numpy(), box.numpy(), CUTOFF + SKIN)
+    pairs = NeighborPairs(torch.tensor(np.stack([first, second]), dtype=torch.int64), n, CUTOFF)
+    model = potential.lennard_jones(atom_types=torch.zeros(n, dtype=torch.int64),
+                                    sigma=torch.tensor([SIGMA]), epsilon=torch.tensor([EPSILON]),
+                                    cutoff=CUTOFF)
+    evaluate = quantity.energy_force_virial(model)
+    generator = torch.Generator().manual_seed(1)
+    v = torch.randn((n, 3), generator=generator) * math.sqrt(0.00831446261815324 * TEMPERATURE / MASS)
+    _, f, _ = evaluate(x, box, pairs)
+    start = time.perf_counter()
+    for _ in range(steps):
+        v = v + (0.5 * TIMESTEP / MASS) * f
+        x, _ = space.wrap(x + TIMESTEP * v, box)
+        _, f, _ = evaluate(x, box, pairs)
+        v = v + (0.5 * TIMESTEP / MASS) * f
+    elapsed = time.perf_counter() - start
+    torch.set_num_threads(previous)
+    return {
+        "value": n * steps / elapsed,
+        "unit": "atom-steps/s",
+        "cores": threads,
+        "kind": "reference",
+        "sample": f"{steps} NVE steps of a {cells}^3-cell FCC block ({n} atoms, same density): "
+                  f"the reference's quantity.energy_force_virial (torch.func, float32, "
+                  f"{threads} threads) + velocity Verlet on CPU tensors; pairs from the oracle's "
+                  f"C restatement of its operator, untimed",
+        "seconds": elapsed,
+    }
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     steps = max(1, args.steps)
-    # Each bench step is one port step of the sample; warm-up steps run untimed.
-    cpu_port_rate(steps=max(1, args.warmup), cells=12)
-    baseline = cpu_port_rate(steps=min(steps, 5), cells=24)
+    # Each bench step is one CPU step of the sample; warm-up steps run untimed. The reference's
+    # own torch CPU path when baseline/_ref holds it, else the oracle port.
+    rate = reference_cpu_rate if (REFERENCE_TREE / "nabladyn").exists() else cpu_port_rate
+    rate(steps=max(1, min(args.warmup, 3)), cells=12)
+    baseline = rate(steps=min(steps, 5), cells=24)
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -249,7 +312,7 @@ def run_reference(args) -> None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32" if baseline["kind"] == "reference" else "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": baseline["sample"]},
         "cpu_baseline": baseline,
@@ -259,32 +322,64 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_serving(device, requests: int, plain_sample: int, rate: float | None) -> dict:
-    """The serving workload: ``requests`` independent argon NVT replicas (64-16,384 atoms,
-    500 steps) through the replica server with Poisson arrivals at ``rate`` per second (None:
-    all at once, over-subscribed), against the plain path: a sample of the same requests one
-    at a time through md.nvt (construction, capture and run)."""
+def serve_requests(device, ranks, requests: int, rate: float | None, seed: int = 7) -> dict:
+    """``requests`` independent argon NVT replicas (64-16,384 atoms, 500 steps each) through
+    the replica server, Poisson arrivals at ``rate`` per second (None: all at t = 0). With N
+    ranks each serves its share (replicas.shard_requests by atom-steps) on its own GPU with no
+    collective on the data path; the wall time is the slowest rank's, the latencies are
+    gathered from every rank for p50/p99."""
     import torch
 
-    from nabladyn_b200 import md, potential
+    from nabladyn_b200.replicas import shard_requests
     from nabladyn_b200.serving import ReplicaServer, serving_requests
 
-    work = serving_requests(requests, seed=7, rate=rate)
+    work = serving_requests(requests, seed=seed, rate=rate)
+    mine = shard_requests([r.steps * r.positions.shape[0] for r in work], ranks.world)[ranks.rank]
     server = ReplicaServer(device=device, budget_bytes=16 << 30, max_slots=2048)
     server.serve(serving_requests(8, seed=99, steps=20), realtime=False)  # warm-up
     torch.cuda.synchronize(device)
+    ranks.barrier()
     start = time.perf_counter()
-    results = server.serve(work, realtime=rate is not None)
-    wall = time.perf_counter() - start
-    latencies = np.array([r.latency for r in results])
-    replica_steps = sum(r.steps for r in results)
-    atom_steps = sum(r.steps * r.num_atoms for r in results)
-    failed = sum(1 for r in results if r.status != 0)
-    # Plain: the same requests one at a time through md.nvt, on a seeded sample.
-    sample = [work[k] for k in np.random.default_rng(1).choice(len(work), plain_sample, replace=False)]
-    plain_total = plain_run = 0.0
-    plain_steps = 0
-    for request in sample:
+    results = server.serve([work[k] for k in mine], realtime=rate is not None)
+    wall = ranks.max(time.perf_counter() - start)
+    rows = ranks.gather([(r.latency, r.steps, r.steps * r.num_atoms, int(r.status != 0))
+                         for r in results])
+    latencies = np.array([row[0] for row in rows])
+    replica_steps = sum(row[1] for row in rows)
+    atom_steps = sum(row[2] for row in rows)
+    peaks = load_peaks()
+    achieved = atom_steps / wall * STEP_BYTES_PER_ATOM / 1e9
+    return {
+        "workload": f"{requests} LJ argon NVT replicas, N log-uniform 64-16384, 500 steps, fp32, "
+                    f"arrivals {'Poisson ' + str(rate) + '/s' if rate else 'all at t=0'}, "
+                    f"{ranks.world} GPU(s)",
+        "replica_steps_per_s": replica_steps / wall,
+        "atom_steps_per_s": atom_steps / wall,
+        "wall_s": wall,
+        "latency_p50_s": float(np.percentile(latencies, 50)),
+        "latency_p99_s": float(np.percentile(latencies, 99)),
+        "failed": sum(row[3] for row in rows),
+        # The step's algorithmic bytes per atom-step (as the headline's step roofline) at the
+        # served atom-step rate, against the measured HBM copy bandwidth.
+        "roofline": {"bound": "hbm", "bytes_per_atom_step": STEP_BYTES_PER_ATOM,
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"]},
+    }
+
+
+def plain_requests(device, requests: int, sample: int, seed: int = 7) -> dict:
+    """The plain path for the serving workload: a seeded sample of the same requests one at a
+    time through md.nvt; with setup (model, simulation, capture) and run only."""
+    import torch
+
+    from nabladyn_b200 import md, potential
+    from nabladyn_b200.serving import serving_requests
+
+    work = serving_requests(requests, seed=seed)
+    picked = np.random.default_rng(1).choice(len(work), sample, replace=False)
+    total = run = 0.0
+    steps = 0
+    for request in (work[k] for k in picked):
         t0 = time.perf_counter()
         n = request.positions.shape[0]
         model = potential.lennard_jones(
@@ -298,30 +393,33 @@ def run_serving(device, requests: int, plain_sample: int, rate: float | None) ->
             torch.tensor(request.cell, dtype=torch.float32, device=device),
             timestep=request.timestep, temperature=request.temperature,
             thermostat_timescale=request.thermostat_timescale, skin=request.skin)
+        torch.cuda.synchronize(device)
         t1 = time.perf_counter()
         simulation.run(request.steps)
         simulation.state()
         torch.cuda.synchronize(device)
         t2 = time.perf_counter()
-        plain_total += t2 - t0
-        plain_run += t2 - t1
-        plain_steps += request.steps
-    served_rate = replica_steps / wall
-    plain_rate = plain_steps / plain_total
-    return {
-        "workload": f"{requests} LJ argon NVT replicas, N log-uniform 64-16384, 500 steps, "
-                    f"fp32, arrivals {'Poisson ' + str(rate) + '/s' if rate else 'all at t=0'}",
-        "replica_steps_per_s": served_rate,
-        "atom_steps_per_s": atom_steps / wall,
-        "wall_s": wall,
-        "latency_p50_s": float(np.percentile(latencies, 50)),
-        "latency_p99_s": float(np.percentile(latencies, 99)),
-        "failed": failed,
-        "plain_replica_steps_per_s": plain_rate,
-        "plain_run_only_replica_steps_per_s": plain_steps / plain_run,
-        "plain_sample": plain_sample,
-        "vs_plain": served_rate / plain_rate,
-    }
+        total += t2 - t0
+        run += t2 - t1
+        steps += request.steps
+    return {"sample": sample, "replica_steps_per_s_with_setup": steps / total,
+            "replica_steps_per_s_run_only": steps / run}
+
+
+def run_serving(device, ranks, requests: int, plain_sample: int,
+                rates: tuple[float | None, ...]) -> dict:
+    """The serving workload at each arrival rate, against the plain path (rank 0 only)."""
+    legs = {f"rate_{rate if rate else 'all_at_t0'}": serve_requests(device, ranks, requests, rate)
+            for rate in rates}
+    out = {"legs": legs}
+    if ranks.rank == 0 and plain_sample:
+        plain = plain_requests(device, requests, plain_sample)
+        out["plain"] = plain
+        out["vs_plain"] = {
+            name: {"with_setup": leg["replica_steps_per_s"] / plain["replica_steps_per_s_with_setup"],
+                   "run_only": leg["replica_steps_per_s"] / plain["replica_steps_per_s_run_only"]}
+            for name, leg in legs.items()}
+    return out
 
 
 def small_system(module, device, dtype):
@@ -650,6 +748,12 @@ def run_reference_cuda(args) -> None:
     from nabladyn_b200 import lattice
 
     device = torch.device("cuda", 0)
+    if args.workload == "neighbors":
+        import nabladyn
+
+        print(json.dumps(run_neighbors(nabladyn, device, args.steps, args.warmup,
+                                       "reference-cuda")), flush=True)
+        return
     if args.workload == "small":
         import nabladyn
 
@@ -723,6 +827,86 @@ def run_reference_cuda(args) -> None:
         "pair_capacity": simulation._neighbors.pair_capacity,
         "config": {"workload": WORKLOAD},
     }), flush=True)
+
+
+NEIGHBOR_SYSTEMS = {
+    "lj_1m": "1,048,576 LJ atoms (64^3-cell FCC, L=36.77 nm), cutoff 1.0 nm, skin 0.1 nm, fp32",
+    "beads_32k": "32,768 beads (32^3 lattice, 10/nm^3, L=14.86 nm), cutoff 1.2 nm, skin 0.1 nm, fp32",
+}
+
+
+def neighbor_frames(name: str):
+    """Positions (wrapped), cell, cutoff and skin of a neighbor-operator workload."""
+    from nabladyn_b200 import lattice
+
+    if name == "lj_1m":
+        positions, cell = lattice.fcc(ATOMS_PER_SIDE_CELLS, LENGTH, 0.02, 2024)
+        return positions % cell, cell, CUTOFF, SKIN
+    n_side = 32
+    length = (n_side**3 / 10.0) ** (1.0 / 3.0)
+    positions, cell = lattice.simple_cubic(n_side, length, 0.02, seed=n_side**3)
+    return positions % cell, cell, 1.2, SKIN
+
+
+def run_neighbors(module, device, steps: int, warmup: int, label: str) -> dict:
+    """The neighbor operator alone through ``module``'s NeighborList (this package's, or the
+    reference's own from baseline/_ref): per system, the first build (allocate), then
+    ``steps`` forced rebuilds of the same frame and ``steps`` updates that reuse the pairs,
+    each timed by CUDA events after ``warmup``."""
+    import torch
+
+    out = {"impl": label, "workload": "neighbor operator: rebuild and reuse", "systems": {}}
+    for name, description in NEIGHBOR_SYSTEMS.items():
+        positions, cell, cutoff, skin = neighbor_frames(name)
+        x = torch.tensor(positions, dtype=torch.float32, device=device)
+        box = torch.tensor(cell, dtype=torch.float32, device=device)
+        listing = module.neighbors.NeighborList(cutoff, skin=skin)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        listing.allocate(x, box)
+        torch.cuda.synchronize(device)
+        allocate_s = time.perf_counter() - t0
+        events = []
+        for mode in ("rebuild", "reuse"):
+            step = listing._rebuild_wrapped if mode == "rebuild" else listing._update_wrapped
+            for _ in range(max(1, warmup)):
+                step(x, box)
+            torch.cuda.synchronize(device)
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(steps):
+                step(x, box)
+            end.record()
+            torch.cuda.synchronize(device)
+            events.append(start.elapsed_time(end) / steps)
+        out["systems"][name] = {
+            "system": description, "atoms": int(x.shape[0]), "pairs": listing.num_pairs,
+            "rebuilds_counted": listing._rebuild_count, "allocate_s": allocate_s,
+            "ms_per_rebuild": events[0], "ms_per_reuse_update": events[1],
+        }
+        del listing
+        torch.cuda.empty_cache()
+    return out
+
+
+# Serving legs of the default line: arrivals over-subscribing the server (about three times
+# what it completes) and a moderate rate, both Poisson.
+SERVING_RATES = (2000.0, 400.0)
+
+
+def spawn_reference_cuda(args) -> dict | None:
+    """The reference's own CUDA path on this GPU for the same workload, seeds, steps and
+    warm-up (bench.py --impl reference-cuda, in a process of its own: it registers the same
+    operator namespace); None when baseline/_ref holds no reference build."""
+    if not any((REFERENCE_TREE / "nabladyn" / "neighbors").glob("_C*.so")):
+        return None
+    command = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference-cuda",
+               "--steps", str(args.steps), "--warmup", str(args.warmup)]
+    try:
+        done = subprocess.run(command, capture_output=True, text=True, timeout=900, check=True)
+        return json.loads(done.stdout.strip().splitlines()[-1])
+    except (subprocess.SubprocessError, ValueError, IndexError) as error:
+        return {"unavailable": f"{type(error).__name__}: {str(error).splitlines()[0][:200]}"}
 
 
 def run_ours(args) -> None:
@@ -806,10 +990,15 @@ def run_ours(args) -> None:
     h2d = 2 * n * 3 * 4 / chunk
     d2h = (3 * n * 3 * 4 + n * 3 * 8) / chunk
 
-    cpu = cpu_port_rate() if (rank == 0 and world == 1) else None
+    cpu = port = reference_cuda = None
+    if rank == 0 and world == 1:
+        port = cpu_port_rate()
+        cpu = reference_cpu_rate() if (REFERENCE_TREE / "nabladyn").exists() else port
+        reference_cuda = spawn_reference_cuda(args) if args.reference_cuda == "auto" else None
     serving = None
-    if args.serving and rank == 0:
-        serving = run_serving(device, args.serving, plain_sample=16, rate=None)
+    if args.serving:
+        serving = run_serving(device, ranks, args.serving, plain_sample=16 if rank == 0 else 0,
+                              rates=SERVING_RATES)
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -863,6 +1052,12 @@ def run_ours(args) -> None:
                              if not engine.small else engine.step_launches * args.steps),
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "cpu_port": port,
+            "reference_cuda": reference_cuda,
+            "vs_reference_cuda": (value / reference_cuda["value"]
+                                  if reference_cuda and reference_cuda.get("value") else None),
+            "e2e_vs_reference_cuda": (e2e_value / reference_cuda["value"]
+                                      if reference_cuda and reference_cuda.get("value") else None),
             "serving": serving,
         }
         print(json.dumps(line), flush=True)
@@ -879,9 +1074,11 @@ def main() -> None:
                         help="requests of the serving workload (0 skips it)")
     parser.add_argument("--serving-rate", type=float, default=None,
                         help="with --workload serving: Poisson arrivals per second")
+    parser.add_argument("--reference-cuda", choices=("auto", "off"), default="auto",
+                        help="auto: time the reference's CUDA path beside ours when installed")
     parser.add_argument("--workload",
                         choices=("large", "serving", "small", "schnet", "gradient",
-                                 "schnet-train"),
+                                 "schnet-train", "neighbors"),
                         default="large")
     args = parser.parse_args()
     if args.warmup < 3:
@@ -910,6 +1107,28 @@ def main() -> None:
         print(json.dumps(run_schnet(nabladyn_b200, torch.device("cuda", 0), args.steps,
                                     args.warmup, "ours")), flush=True)
         return
+    if args.workload == "neighbors" and args.impl == "ours":
+        import torch
+
+        import nabladyn_b200
+
+        result = run_neighbors(nabladyn_b200, torch.device("cuda", 0), args.steps, args.warmup,
+                               "ours")
+        if args.reference_cuda == "auto" and any(
+                (REFERENCE_TREE / "nabladyn" / "neighbors").glob("_C*.so")):
+            command = [sys.executable, str(ROOT / "bench.py"), "--workload", "neighbors",
+                       "--impl", "reference-cuda", "--steps", str(args.steps), "--warmup",
+                       str(args.warmup)]
+            done = subprocess.run(command, capture_output=True, text=True, timeout=900)
+            lines = [l for l in done.stdout.splitlines() if l.startswith("{")]
+            reference = json.loads(lines[-1]) if lines else {"unavailable": done.stderr[-300:]}
+            result["reference_cuda"] = reference
+            if "systems" in reference:
+                result["rebuild_speedup"] = {
+                    name: reference["systems"][name]["ms_per_rebuild"] / mine["ms_per_rebuild"]
+                    for name, mine in result["systems"].items()}
+        print(json.dumps(result), flush=True)
+        return
     if args.workload == "small" and args.impl == "ours":
         import torch
 
@@ -921,9 +1140,17 @@ def main() -> None:
     if args.workload == "serving":
         import torch
 
-        device = torch.device("cuda", 0)
-        print(json.dumps(run_serving(device, args.serving, plain_sample=16,
-                                     rate=args.serving_rate)), flush=True)
+        from nabladyn_b200.replicas import Ranks
+
+        device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(device)
+        ranks = Ranks("nccl", device, timeout_s=300)
+        rates = (args.serving_rate,) if args.serving_rate else SERVING_RATES
+        result = run_serving(device, ranks, args.serving, plain_sample=16 if ranks.rank == 0 else 0,
+                             rates=rates)
+        if ranks.rank == 0:
+            print(json.dumps(result), flush=True)
+        ranks.close()
         return
     if args.impl == "reference":
         run_reference(args)

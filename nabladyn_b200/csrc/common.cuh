@@ -9,8 +9,11 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "nabladyn_b200.h"
@@ -62,6 +65,119 @@ const char* last_error();
     } while (0)
 
 #define ND_LAUNCH_CHECK() ND_CUDA_TRY(cudaGetLastError())
+
+// Kernel attributes (dynamic shared-memory limits, carveouts) and device properties belong to
+// one device: a library used from several GPUs in one process sets and reads them per device.
+constexpr int kMaxDevices = 64;
+
+// Runs a setup once per device (the current one), under a lock; a setup that failed is run
+// again by the next call instead of being remembered.
+class DeviceOnce
+{
+public:
+    template <typename Setup>
+    cudaError_t run(Setup setup)
+    {
+        int device = 0;
+        cudaError_t rc = cudaGetDevice(&device);
+        if (rc != cudaSuccess)
+        {
+            return rc;
+        }
+        if (device < 0 || device >= kMaxDevices)
+        {
+            return cudaErrorInvalidDevice;
+        }
+        if (done_[device].load(std::memory_order_acquire))
+        {
+            return cudaSuccess;
+        }
+        std::lock_guard<std::mutex> lock(mutex_);
+        if (done_[device].load(std::memory_order_relaxed))
+        {
+            return cudaSuccess;
+        }
+        rc = setup();
+        if (rc == cudaSuccess)
+        {
+            done_[device].store(true, std::memory_order_release);
+        }
+        return rc;
+    }
+
+private:
+    std::mutex mutex_;
+    std::atomic<bool> done_[kMaxDevices] = {};
+};
+
+// The dynamic shared memory one kernel may use on each device: raised when a launch needs more
+// than any launch before it on that device (launches up to 48 KB need no raise).
+class DeviceGrant
+{
+public:
+    template <typename Kernel>
+    cudaError_t allow(Kernel kernel, std::size_t bytes)
+    {
+        if (bytes <= 48 * 1024)
+        {
+            return cudaSuccess;
+        }
+        int device = 0;
+        cudaError_t rc = cudaGetDevice(&device);
+        if (rc != cudaSuccess)
+        {
+            return rc;
+        }
+        if (device < 0 || device >= kMaxDevices)
+        {
+            return cudaErrorInvalidDevice;
+        }
+        std::lock_guard<std::mutex> lock(mutex_);
+        if (bytes <= granted_[device])
+        {
+            return cudaSuccess;
+        }
+        rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(bytes));
+        if (rc == cudaSuccess)
+        {
+            granted_[device] = bytes;
+        }
+        return rc;
+    }
+
+private:
+    std::mutex mutex_;
+    std::size_t granted_[kMaxDevices] = {};
+};
+
+// The current device's multiprocessor count, looked up once per device.
+inline cudaError_t multiprocessors(int* count)
+{
+    static std::atomic<int> known[kMaxDevices] = {};
+    int device = 0;
+    cudaError_t rc = cudaGetDevice(&device);
+    if (rc != cudaSuccess)
+    {
+        return rc;
+    }
+    if (device < 0 || device >= kMaxDevices)
+    {
+        return cudaErrorInvalidDevice;
+    }
+    int value = known[device].load(std::memory_order_relaxed);
+    if (value == 0)
+    {
+        rc = cudaDeviceGetAttribute(&value, cudaDevAttrMultiProcessorCount, device);
+        if (rc != cudaSuccess)
+        {
+            return rc;
+        }
+        known[device].store(value, std::memory_order_relaxed);
+    }
+    *count = value;
+    return cudaSuccess;
+}
 
 // Whether a gated rebuild kernel does work: a build from allocate passes no flag and always
 // runs; an update runs only when the reuse check asked for a rebuild and no error latched.

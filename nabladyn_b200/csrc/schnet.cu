@@ -1059,8 +1059,9 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
     const int atom_tiles = static_cast<int>((s.num_atoms + kTile - 1) / kTile);
     const bool reverse = s.forces != nullptr || s.virial != nullptr;
 
-    // The kernels' attributes, set once (a function-local static starts once, thread-safely).
-    static const cudaError_t configured = [] {
+    // The kernels' attributes, set once per device (they belong to its instance of a kernel).
+    static DeviceOnce configured;  // per device, retried after a failure
+    ND_CUDA_TRY(configured.run([] {
         cudaError_t rc = cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairForwardShared);
         auto then = [&rc](cudaError_t next) { rc = rc != cudaSuccess ? rc : next; };
         then(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairReverseShared));
@@ -1070,8 +1071,7 @@ int nd_schnet_energy_force_virial(const nd_schnet_args* args, nd_stream_t stream
         then(cudaFuncSetAttribute(pair_forward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
         then(cudaFuncSetAttribute(pair_reverse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
         return rc;
-    }();
-    ND_CUDA_TRY(configured);
+    }));
     const int forward_grid = pair_grid(reinterpret_cast<const void*>(pair_forward_kernel), kPairForwardShared, 64);
     const int reverse_grid = std::min(kVirialSlots, pair_grid(reinterpret_cast<const void*>(pair_reverse_kernel), kPairReverseShared, 128));
 

@@ -315,13 +315,8 @@ __device__ __forceinline__ void sum_runs(const float* stage, const int* first, f
 // columns) over one CTA's needs.
 int pair_grid(const void* kernel, int shared_bytes, int tmem_columns)
 {
-    static int sms = 0;
-    if (sms == 0)
-    {
-        int device = 0;
-        cudaGetDevice(&device);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    }
+    int sms = 148;
+    multiprocessors(&sms);
     int per_sm = 1;
     cudaFuncAttributes attributes{};
     if (cudaFuncGetAttributes(&attributes, kernel) == cudaSuccess)

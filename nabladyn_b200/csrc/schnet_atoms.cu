@@ -791,8 +791,9 @@ int nd_schnet_atoms(const nd_schnet_atom_args* args, int32_t stage, int32_t bloc
     p.x_dot_bar = f32(kXDotBar, 0);
     const unsigned tiles = static_cast<unsigned>(layout.tiles);
 
-    // The kernels' attributes, set once (a function-local static starts once, thread-safely).
-    static const cudaError_t configured = [] {
+    // The kernels' attributes, set once per device (they belong to its instance of a kernel).
+    static DeviceOnce configured;  // per device, retried after a failure
+    ND_CUDA_TRY(configured.run([] {
         cudaError_t rc = cudaFuncSetAttribute(start_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStartShared);
         auto then = [&rc](cudaError_t next) { rc = rc != cudaSuccess ? rc : next; };
         then(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kForwardShared));
@@ -800,8 +801,7 @@ int nd_schnet_atoms(const nd_schnet_atom_args* args, int32_t stage, int32_t bloc
         then(cudaFuncSetAttribute(reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReverseShared));
         then(cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterShared));
         return rc;
-    }();
-    ND_CUDA_TRY(configured);
+    }));
     auto reduce = [&](const Segments& segments) -> int {
         int total = 0;
         for (int k = 0; k < segments.count; ++k)

@@ -625,16 +625,16 @@ int nd_schnet_tangent(const nd_schnet_tangent_args* args, int32_t direction,
     pass.phase = static_cast<float>(3.14159265358979323846 / s.cutoff);
     pass.gaussians = s.gaussians;
 
-    // The kernels' attributes, set once (a function-local static starts once, thread-safely).
-    static const cudaError_t configured = [] {
+    // The kernels' attributes, set once per device (they belong to its instance of a kernel).
+    static DeviceOnce configured;  // per device, retried after a failure
+    ND_CUDA_TRY(configured.run([] {
         cudaError_t rc = cudaFuncSetAttribute(tangent_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTangentForwardShared);
         auto then = [&rc](cudaError_t next) { rc = rc != cudaSuccess ? rc : next; };
         then(cudaFuncSetAttribute(tangent_reverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTangentReverseShared));
         then(cudaFuncSetAttribute(tangent_forward_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
         then(cudaFuncSetAttribute(tangent_reverse_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
         return rc;
-    }();
-    ND_CUDA_TRY(configured);
+    }));
     if (direction == 0)
     {
         // The messages m are the E/F/W call's for this block; only their tangent is computed.

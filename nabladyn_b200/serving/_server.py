@@ -5,11 +5,14 @@ Each request is an independent one-type Lennard-Jones NVT simulation (the refere
 
 * admits a request when a slot and room in the HBM budget are free (first fit over the pool's
   atom ranges), uploads its frame and has the replica kernel build its list and first forces;
+  the host work of an admission (the slot record, the frame in pinned memory) is done ahead,
+  while the device runs the previous round, and the upload itself needs no host sync;
 * every round launches the replica kernel once over all active slots, each slot with a budget
   of steps inversely proportional to its size, so a round costs about the same on every SM and
   small replicas are not held back by large ones;
-* harvests replicas whose steps are done, hands back their frame and frees their room, so
-  requests that arrived meanwhile are admitted in the next round.
+* harvests replicas whose steps are done (their frames read back together, in one copy),
+  hands back their frame and frees their room, so requests that arrived meanwhile are
+  admitted in the next round.
 
 Replicas never interact on the device: each is advanced by its own CTA, so a replica's result
 does not depend on which others share its rounds.
@@ -34,6 +37,7 @@ _ALIGN = 32          # atoms per allocation unit (one warp of list chunks)
 _MAX_CELLS = 4096    # kServeMaxCells in serve.cu
 _WIDTH = 192         # list slots per atom: room for ~1.5x the mean count at 22 atoms/nm^3
 _BYTES_PER_ATOM = 16 + 12 + 12 + 4 + 4 + 24 + 16 + 2 * _WIDTH + 4 + 4 + 4
+_STAGE_AHEAD = 256   # arrived requests made ready on the host while a round runs
 _CHAIN_A, _KINETIC_A, _PENDING, _CHAIN_MASS, _KT, _DEGREES, _TIMESTEP = 0, 6, 14, 16, 19, 20, 21
 
 
@@ -92,6 +96,16 @@ class _Active:
     units: int
     admitted: float
     steps_left: int = field(default=0)
+    staged: object = None  # the pinned host frame of its upload, kept until the copy is done
+
+
+@dataclass
+class _Staged:
+    """A request made ready on the host while the device runs a round: its slot record (all
+    but the offsets) and its frame in pinned memory, uploaded without a host sync."""
+
+    record: Replica
+    frame: torch.Tensor  # [n, 9] float32: x, y, z, 0, vx, vy, vz, m, 1/m
 
 
 class ReplicaServer:
@@ -213,26 +227,41 @@ class ReplicaServer:
         record.thermostat[_TIMESTEP] = request.timestep
         return record, velocities32
 
-    def _write_record(self, slot: int, record: Replica) -> None:
+    def _stage(self, request: ReplicaRequest) -> _Staged:
+        """The host part of an admission: the record and the frame in pinned memory."""
+        record, velocities32 = self._describe(request, 0, 0)
+        n = record.num_atoms
+        frame = torch.empty((n, 9), dtype=torch.float32).pin_memory()
+        masses = np.asarray(request.masses, dtype=np.float32)
+        host = frame.numpy()
+        host[:, :3] = np.asarray(request.positions, dtype=np.float32)
+        host[:, 3] = 0.0
+        host[:, 4:7] = velocities32
+        host[:, 7] = masses
+        host[:, 8] = 1.0 / masses
+        return _Staged(record, frame)
+
+    def _place(self, staged: _Staged, slot: int, offset: int) -> None:
+        """The device part: the frame's pinned rows copied into the pool (no host sync) and the
+        slot record written with its offsets."""
+        record = staged.record
+        n = record.num_atoms
+        record.atom_offset = offset
+        record.list_offset = offset * _WIDTH
+        record.cell_offset = slot * (_MAX_CELLS + 1)
+        rows = staged.frame.to(self.device, non_blocking=True)
+        b = self.buffers
+        b["positions"][offset:offset + n].copy_(rows[:, :4])
+        b["velocities"][offset:offset + n].copy_(rows[:, 4:7])
+        b["forces"][offset:offset + n].zero_()
+        b["masses"][offset:offset + n].copy_(rows[:, 7])
+        b["inverse_masses"][offset:offset + n].copy_(rows[:, 8])
+        b["images"][offset:offset + n].zero_()
         size = ctypes.sizeof(Replica)
         raw = torch.frombuffer(bytearray(ctypes.string_at(ctypes.addressof(record), size)),
-                               dtype=torch.uint8)
-        self.table[slot * size:(slot + 1) * size].copy_(raw)
-
-    def _upload(self, request: ReplicaRequest, slot: int, offset: int) -> None:
-        record, velocities32 = self._describe(request, slot, offset)
-        n = record.num_atoms
-        b = self.buffers
-        positions = torch.zeros((n, 4), dtype=torch.float32)
-        positions[:, :3] = torch.from_numpy(np.asarray(request.positions, dtype=np.float32))
-        masses = torch.from_numpy(np.asarray(request.masses, dtype=np.float32))
-        b["positions"][offset:offset + n].copy_(positions)
-        b["velocities"][offset:offset + n].copy_(torch.from_numpy(velocities32))
-        b["forces"][offset:offset + n].zero_()
-        b["masses"][offset:offset + n].copy_(masses)
-        b["inverse_masses"][offset:offset + n].copy_(1.0 / masses)
-        b["images"][offset:offset + n].zero_()
-        self._write_record(slot, record)
+                               dtype=torch.uint8).pin_memory()
+        self.table[slot * size:(slot + 1) * size].copy_(raw, non_blocking=True)
+        staged.raw = raw  # the pinned record stays alive with the staged frame
 
     def _launch(self, slots: list[int], budgets: list[int] | None, mode: int) -> None:
         if not slots:
@@ -255,11 +284,24 @@ class ReplicaServer:
         offset = getattr(Replica, name).offset
         return np.ascontiguousarray(raw[:, offset:offset + 4]).view(np.int32)[:, 0]
 
-    def _harvest(self, active: _Active, raw: np.ndarray, now: float) -> ReplicaResult:
-        record = Replica.from_buffer_copy(raw.tobytes())
-        n, offset = record.num_atoms, active.offset
-        cell = torch.tensor(list(record.cell), dtype=torch.float32, device=self.device)
-        unwrapped = self.buffers["positions"][offset:offset + n, :3]
+    def _harvest(self, done: list[tuple[_Active, np.ndarray]], now: float) -> list[ReplicaResult]:
+        """Finished replicas' frames (positions wrapped as space.wrap does, pending chain factor
+        applied to the velocities, images with the last crossings): computed on the device for
+        all of them together and read back in one copy; their room is freed."""
+        if not done:
+            return []
+        rows, cells, scales, sizes = [], [], [], []
+        for active, raw in done:
+            record = Replica.from_buffer_copy(raw.tobytes())
+            n, offset = record.num_atoms, active.offset
+            rows.append(torch.arange(offset, offset + n, device=self.device))
+            cells.append(torch.tensor(list(record.cell), dtype=torch.float32).expand(n, 3))
+            scales.append(np.full(n, np.float32(record.thermostat[_PENDING]), dtype=np.float32))
+            sizes.append((record, n))
+        index = torch.cat(rows)
+        cell = torch.cat(cells).to(self.device, non_blocking=True)
+        scale = torch.from_numpy(np.concatenate(scales)).to(self.device, non_blocking=True)
+        unwrapped = self.buffers["positions"][index, :3]
         crossings = torch.floor(unwrapped / cell)
         wrapped = unwrapped - crossings * cell
         below = wrapped < 0
@@ -268,26 +310,31 @@ class ReplicaServer:
         above = wrapped >= cell
         wrapped = torch.where(above, wrapped - cell, wrapped)
         crossings = torch.where(above, crossings + 1, crossings)
-        scale = np.float32(record.thermostat[_PENDING])
-        velocities = self.buffers["velocities"][offset:offset + n] * float(scale)
-        images = self.buffers["images"][offset:offset + n] + crossings.to(torch.int64)
-        result = ReplicaResult(
-            name=active.request.name,
-            positions=wrapped.cpu().numpy(),
-            velocities=velocities.cpu().numpy(),
-            images=images.cpu().numpy(),
-            energy=float(record.energy),
-            status=int(record.status),
-            rebuilds=int(record.rebuild_count),
-            arrival=float(active.request.arrival),
-            admitted=active.admitted,
-            finished=now,
-            num_atoms=n,
-            steps=int(active.request.steps) - int(record.steps_left),
-        )
-        self._give(active.offset // _ALIGN, active.units)
-        self._free_slots.append(active.slot)
-        return result
+        velocities = self.buffers["velocities"][index] * scale[:, None]
+        images = self.buffers["images"][index] + crossings.to(torch.int64)
+        frame = torch.cat([wrapped, velocities], dim=1).cpu().numpy()
+        images = images.cpu().numpy()
+        results, begin = [], 0
+        for (active, _), (record, n) in zip(done, sizes):
+            end = begin + n
+            results.append(ReplicaResult(
+                name=active.request.name,
+                positions=frame[begin:end, :3].copy(),
+                velocities=frame[begin:end, 3:].copy(),
+                images=images[begin:end].copy(),
+                energy=float(record.energy),
+                status=int(record.status),
+                rebuilds=int(record.rebuild_count),
+                arrival=float(active.request.arrival),
+                admitted=active.admitted,
+                finished=now,
+                num_atoms=n,
+                steps=int(active.request.steps) - int(record.steps_left),
+            ))
+            begin = end
+            self._give(active.offset // _ALIGN, active.units)
+            self._free_slots.append(active.slot)
+        return results
 
     # -- the loop ------------------------------------------------------------------------
 
@@ -305,7 +352,17 @@ class ReplicaServer:
                 raise ValueError(f"a replica of {n} atoms exceeds the server's budget")
         active: dict[int, _Active] = {}
         results: list[ReplicaResult] = []
+        staged: dict[int, _Staged] = {}  # by id(request): host work done ahead of admission
         start = time.perf_counter()
+
+        def stage_ahead(now: float) -> None:
+            # Host preparation of the requests that have arrived, a bounded number ahead.
+            for request in list(pending)[:_STAGE_AHEAD]:
+                if realtime and request.arrival > now:
+                    break
+                if id(request) not in staged:
+                    staged[id(request)] = self._stage(request)
+
         while pending or active:
             now = time.perf_counter() - start
             admitted = []
@@ -320,8 +377,10 @@ class ReplicaServer:
                 pending.popleft()
                 slot = self._free_slots.pop()
                 offset = first * _ALIGN
-                self._upload(request, slot, offset)
-                active[slot] = _Active(request, slot, offset, units, now, int(request.steps))
+                ready = staged.pop(id(request), None) or self._stage(request)
+                self._place(ready, slot, offset)
+                active[slot] = _Active(request, slot, offset, units, now, int(request.steps),
+                                       ready)
                 admitted.append(slot)
             self._launch(admitted, None, 0)
             if not active:
@@ -333,15 +392,19 @@ class ReplicaServer:
                                   -(-self.round_atom_steps // active[s].request.positions.shape[0])))
                        for s in slots]
             self._launch(slots, budgets, 1)
+            # While the round runs: the next admissions' host work.
+            stage_ahead(time.perf_counter() - start)
             raw = self._records()
             now = time.perf_counter() - start
             steps_left_all = self._int_field(raw, "steps_left")
             status_all = self._int_field(raw, "status")
+            done = []
             for slot in slots:
                 steps_left, status = int(steps_left_all[slot]), int(status_all[slot])
                 active[slot].steps_left = steps_left
                 if steps_left == 0 or status != 0:
-                    results.append(self._harvest(active.pop(slot), raw[slot], now))
+                    done.append((active.pop(slot), raw[slot]))
+            results.extend(self._harvest(done, now))
         return results
 
 

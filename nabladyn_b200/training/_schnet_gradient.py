@@ -208,9 +208,12 @@ def _frame_gradient(model, plan, e_bar: Tensor, f_bar: Tensor, w_bar: Tensor) ->
 
 def _plan_key(model, columns: int, channels: tuple[str, ...]) -> tuple:
     """What a plan's buffers and captured graph depend on besides the parameter values (copied
-    in at every call): the stack width, the channels, the device and the atom-type buffer."""
+    in at every call): the stack width, the channels, the device, the sizes (atoms, types,
+    blocks) and the atom-type buffer (a new buffer at a freed address has other sizes or a
+    new version)."""
     types = model.atom_types
-    return (columns, channels, str(model.device), types.data_ptr(), types._version)
+    return (columns, channels, str(model.device), model.num_atoms, model.num_types,
+            len(model.blocks), tuple(types.shape), types.data_ptr(), types._version)
 
 
 class _Plan:
