@@ -24,6 +24,7 @@ from ..potential import Potential
 from ..potential._lennard_jones import LennardJones
 from ..units import BOLTZMANN
 from ._engine import CHAIN_A, CHAIN_MASS, DEGREES, PENDING_SCALE, THERMAL_ENERGY, Engine
+from ._output import FRAME, SampleWriter
 from ._pair_engine import PairEngine
 from ._state import BarostatState, ChainState, State
 
@@ -234,9 +235,11 @@ class Simulation:
         With ``sample_every``, returns the panel at each step that is a multiple of it, as host
         tensors [S] under the names of the fields and ``step`` [S] int64; otherwise None.
         ``echo`` (True for stdout, or a text stream) prints a header and one row per sample.
-        Syncs with the host every 1,000 steps, at each sample and at the end. Raises
-        ``ValueError`` for settings out of range and when the status reports a failure (which
-        fails the simulation); ``RuntimeError`` after a failure.
+        ``sample_file`` names an HDF5 file, overwritten, holding each sample's frame and panel
+        (``read_sample_file``; h5py is needed only then). Syncs with the host every 1,000
+        steps, at each sample and at the end. Raises ``ValueError`` for settings out of range
+        and when the status reports a failure (which fails the simulation; the file keeps the
+        samples written before it); ``RuntimeError`` after a failure.
         """
         steps = _count("steps", steps)
         if sample_every is not None and _count("sample_every", sample_every) == 0:
@@ -245,8 +248,6 @@ class Simulation:
             raise ValueError("echo must be True, False or a text stream")
         if (echo is not False or sample_file is not None) and sample_every is None:
             raise ValueError("echo and sample_file need sample_every")
-        if sample_file is not None:
-            raise NotImplementedError("HDF5 sample files are not part of this build")
         self._require()
         start = self._step
         due: list[int] = []
@@ -257,6 +258,30 @@ class Simulation:
         if stream is not None:
             stream.write("".join(f"{name:>20}" for name in ("step", "time", *self._fields)) + "\n")
         rows = []
+        writer = None
+        if sample_file is not None:
+            writer = SampleWriter(
+                sample_file, masses=self._masses.cpu().numpy(), fields=self._fields,
+                attributes={**self._settings, "timestep": self._timestep,
+                            "cutoff": self._model.cutoff})
+        try:
+            self._run_stops(start, steps, due, rows, stream, writer)
+        finally:
+            if writer is not None:
+                writer.close()
+        self._step = start + steps
+        if sample_every is None:
+            return None
+        table = torch.tensor(rows, dtype=torch.float64).reshape(len(due), len(self._fields))
+        samples = {"step": torch.tensor(due, dtype=torch.int64)}
+        samples.update(
+            {name: table[:, k].to(self._model.dtype) for k, name in enumerate(self._fields)}
+        )
+        return samples
+
+    def _run_stops(self, start: int, steps: int, due: list[int], rows: list, stream,
+                   writer) -> None:
+        """The steps of ``run`` between its stops: samples, status reads, the end."""
         # Stops: samples, status reads every 1,000 steps and the end.
         stops = sorted(
             set(due)
@@ -271,23 +296,19 @@ class Simulation:
             if stop in due:
                 values = self._panel_values()
                 rows.append(values)
+                if stream is not None or writer is not None:
+                    self._check(stop)  # no sample of a failed run is echoed or written
                 if stream is not None:
-                    self._check(stop)
                     stream.write(
                         "".join(f"{v:>20.6g}" for v in (stop, stop * self._timestep, *values))
                         + "\n",
                     )
+                if writer is not None:
+                    state = self.state()
+                    frame = {name: getattr(state, name).cpu().numpy() for name in FRAME}
+                    writer.write(stop, stop * self._timestep, frame, values)
             if (stop - start) % _STATUS_INTERVAL == 0 or stop == start + steps:
                 self._check(stop)
-        self._step = start + steps
-        if sample_every is None:
-            return None
-        table = torch.tensor(rows, dtype=torch.float64).reshape(len(due), len(self._fields))
-        samples = {"step": torch.tensor(due, dtype=torch.int64)}
-        samples.update(
-            {name: table[:, k].to(self._model.dtype) for k, name in enumerate(self._fields)}
-        )
-        return samples
 
     @property
     def model(self) -> Potential:
