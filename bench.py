@@ -322,7 +322,8 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def serve_requests(device, ranks, requests: int, rate: float | None, seed: int = 7) -> dict:
+def serve_requests(device, ranks, requests: int, rate: float | None, seed: int = 7,
+                   stage_ahead: int = 32) -> dict:
     """``requests`` independent argon NVT replicas (64-16,384 atoms, 500 steps each) through
     the replica server, Poisson arrivals at ``rate`` per second (None: all at t = 0). With N
     ranks each serves its share (replicas.shard_requests by atom-steps) on its own GPU with no
@@ -335,7 +336,8 @@ def serve_requests(device, ranks, requests: int, rate: float | None, seed: int =
 
     work = serving_requests(requests, seed=seed, rate=rate)
     mine = shard_requests([r.steps * r.positions.shape[0] for r in work], ranks.world)[ranks.rank]
-    server = ReplicaServer(device=device, budget_bytes=16 << 30, max_slots=2048)
+    server = ReplicaServer(device=device, budget_bytes=16 << 30, max_slots=2048,
+                           stage_ahead=stage_ahead)
     server.serve(serving_requests(8, seed=99, steps=20), realtime=False)  # warm-up
     torch.cuda.synchronize(device)
     ranks.barrier()
@@ -359,6 +361,7 @@ def serve_requests(device, ranks, requests: int, rate: float | None, seed: int =
         "latency_p50_s": float(np.percentile(latencies, 50)),
         "latency_p99_s": float(np.percentile(latencies, 99)),
         "failed": sum(row[3] for row in rows),
+        "stage_ahead": stage_ahead,
         # The step's algorithmic bytes per atom-step (as the headline's step roofline) at the
         # served atom-step rate, against the measured HBM copy bandwidth.
         "roofline": {"bound": "hbm", "bytes_per_atom_step": STEP_BYTES_PER_ATOM,
@@ -407,9 +410,10 @@ def plain_requests(device, requests: int, sample: int, seed: int = 7) -> dict:
 
 
 def run_serving(device, ranks, requests: int, plain_sample: int,
-                rates: tuple[float | None, ...]) -> dict:
+                rates: tuple[float | None, ...], stage_ahead: int = 32) -> dict:
     """The serving workload at each arrival rate, against the plain path (rank 0 only)."""
-    legs = {f"rate_{rate if rate else 'all_at_t0'}": serve_requests(device, ranks, requests, rate)
+    legs = {f"rate_{rate if rate else 'all_at_t0'}": serve_requests(device, ranks, requests, rate,
+                                                                    stage_ahead=stage_ahead)
             for rate in rates}
     out = {"legs": legs}
     if ranks.rank == 0 and plain_sample:
@@ -1074,6 +1078,8 @@ def main() -> None:
                         help="requests of the serving workload (0 skips it)")
     parser.add_argument("--serving-rate", type=float, default=None,
                         help="with --workload serving: Poisson arrivals per second")
+    parser.add_argument("--stage-ahead", type=int, default=32,
+                        help="serving: arrived requests made ready on the host during a round")
     parser.add_argument("--reference-cuda", choices=("auto", "off"), default="auto",
                         help="auto: time the reference's CUDA path beside ours when installed")
     parser.add_argument("--workload",
@@ -1147,7 +1153,7 @@ def main() -> None:
         ranks = Ranks("nccl", device, timeout_s=300)
         rates = (args.serving_rate,) if args.serving_rate else SERVING_RATES
         result = run_serving(device, ranks, args.serving, plain_sample=16 if ranks.rank == 0 else 0,
-                             rates=rates)
+                             rates=rates, stage_ahead=args.stage_ahead)
         if ranks.rank == 0:
             print(json.dumps(result), flush=True)
         ranks.close()

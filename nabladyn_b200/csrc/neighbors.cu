@@ -13,13 +13,13 @@
 // How the GPU builds it is this file's own design:
 //   * binning takes each atom's in-bin slot from the counting atomic, and one warp per bin
 //     orders the bin by id with shuffles while gathering the sorted positions;
-//   * the pairs are built per HOME BIN, one CTA each. Every candidate of a home bin's atoms
+//   * the pairs are built per HOME BIN, one warp each. Every candidate of a home bin's atoms
 //     sits in the home bin itself (after the atom) or in a stencil bin that comes later in bin
-//     order; the CTA stages exactly those bins into shared memory as 16-B (x, y, z, id) slots,
-//     each bin's coordinates already moved by its image where the move is exact. A warp then
-//     takes one center at a time and its 32 lanes take 32 candidates: one ballot per 32
-//     tests, pair counts from popcounts, and the fill's columns from a prefix popcount, so
-//     each warp writes a center's pairs as contiguous, coalesced columns;
+//     order; the warp stages exactly those bins into shared memory as 16-B (x, y, z, id) slots,
+//     each bin's coordinates already moved by its image where the move is exact. The lanes are
+//     the home bin's atoms: each staged candidate is read once (a broadcast) and tested against
+//     all of them, and a lane sets one bit per hit in a word of 32 candidates, so the count is
+//     a popcount per word and only the fill's writes diverge;
 //   * small boxes (at most three bins per axis) keep a word-major bit matrix: one thread per
 //     (center, 32-candidate word) with the word's candidates staged in shared memory, so
 //     threads of a block store consecutive words;
@@ -163,19 +163,19 @@ __global__ void order_bins_kernel(
 }
 
 // ---------------------------------------------------------------------------------------
-// Pairs on the grid path: one CTA per home bin.
+// Pairs on the grid path: one warp per home bin.
 
-constexpr int kHoodThreads = 128;
-constexpr int kHoodWarps = kHoodThreads / kWarp;
-constexpr int kHoodBins = 27;  // the home bin and its stencil, at most
+constexpr int kHoodWarps = 4;                 // bins per CTA, one per warp
+constexpr int kHoodThreads = kHoodWarps * kWarp;
+constexpr int kHoodBins = 27;                 // the home bin and its stencil, at most
 
-// Shared-memory slots of one neighborhood: 32 KB in either dtype. A neighborhood with more
-// candidates (dense or very wide bins) is read from global memory instead, with the same
-// arithmetic.
+// Shared-memory slots of one warp's neighborhood: 8 KB in either dtype (512 float32 or 256
+// float64 candidates; a liquid at 21 atoms/nm^3 with 1.1 nm bins needs about 410). A larger
+// neighborhood is read from global memory instead, with the same arithmetic.
 template <typename T>
 struct HoodSlots
 {
-    static constexpr int value = 32768 / static_cast<int>(sizeof(Slot<T>));
+    static constexpr int value = 8192 / static_cast<int>(sizeof(Slot<T>));
 };
 
 // The part of a home bin's stencil that holds candidates: the home bin (its atoms after the
@@ -280,6 +280,7 @@ __device__ __forceinline__ void plan_hood(
         hood.slot[count] = inclusive;
         hood.total = inclusive;
     }
+    __syncwarp();
 }
 
 // Candidate `k` of kept bin `g`, in the list's arithmetic: the coordinate moved by -L on the
@@ -303,100 +304,136 @@ __device__ __forceinline__ Slot<T> hood_candidate(
     return out;
 }
 
-// What a warp does with one center's candidates: count them, or write them as columns.
-struct CountSink
+// One word of the lane's center against 32 consecutive candidates of kept bin `g` (each read
+// once for the whole warp): bit j is set when candidate base + j is closer than the radius.
+template <typename T, bool kFixed, bool kStaged>
+__device__ __forceinline__ unsigned hit_word(
+    const Hood& hood, const Slot<T>* __restrict__ staged,
+    const T* __restrict__ sorted_positions, const index_t* __restrict__ sorted_ids,
+    int g, int base, int size, const Slot<T>& c, T ax, T ay, T az, T lx, T ly, T lz,
+    T radius_squared)
 {
-    index_t count = 0;
-    __device__ __forceinline__ void take(unsigned hits, bool, index_t) { count += __popc(hits); }
-};
-
-struct FillSink
-{
-    index_t* __restrict__ pairs;
-    std::int64_t capacity;
-    std::int64_t column;  // the next column of this center
-    index_t center_id;
-    __device__ __forceinline__ void take(unsigned hits, bool hit, index_t other)
-    {
-        if (hit)
+    auto test = [&](int j) {
+        const int k = base + j;
+        const Slot<T> p = kStaged ? staged[hood.slot[g] + k]
+                                  : hood_candidate(hood, g, k, sorted_positions, sorted_ids,
+                                                   lx, ly, lz);
+        T dx, dy, dz;
+        if (kFixed)
         {
-            const int lane = threadIdx.x % kWarp;
-            const std::int64_t at = column + __popc(hits & ((1u << lane) - 1u));
-            if (at < capacity)
-            {
-                pairs[at] = center_id;
-                pairs[capacity + at] = other;
-            }
+            dx = ax - p.x;
+            dy = ay - p.y;
+            dz = az - p.z;
         }
-        column += __popc(hits);
+        else
+        {
+            dx = min_image(c.x, p.x, lx);
+            dy = min_image(c.y, p.y, ly);
+            dz = min_image(c.z, p.z, lz);
+        }
+        return squared_norm(dx, dy, dz) < radius_squared;
+    };
+    unsigned hits = 0;
+    if (size == kWarp)
+    {
+#pragma unroll
+        for (int j = 0; j < kWarp; ++j)
+        {
+            hits |= test(j) ? 1u << j : 0u;
+        }
     }
-};
+    else
+    {
+        for (int j = 0; j < size; ++j)
+        {
+            hits |= test(j) ? 1u << j : 0u;
+        }
+    }
+    return hits;
+}
 
-// One warp, one center: its candidates 32 at a time, per kept bin.
-template <typename T, bool kFixed, bool kStaged, typename Sink>
-__device__ __forceinline__ void visit_center(
-    const Hood& hood,
-    const Slot<T>* __restrict__ staged,
-    const T* __restrict__ sorted_positions,
-    const index_t* __restrict__ sorted_ids,
-    int h,
-    T lx, T ly, T lz,
-    T radius_squared,
-    Sink& sink
-)
+// One warp, one home bin: the lanes are the bin's atoms (32 at a time), every candidate is
+// read once per warp and tested against all of them. Each lane keeps a word of hits per 32
+// candidates: the count adds its popcount; the fill writes its set bits from the lane's next
+// column (only the writes diverge).
+template <typename T, bool kFill, bool kFixed, bool kStaged>
+__device__ __forceinline__ void hood_lanes(
+    const Hood& hood, const Slot<T>* __restrict__ staged,
+    const T* __restrict__ sorted_positions, const index_t* __restrict__ sorted_ids,
+    T lx, T ly, T lz, T radius_squared,
+    index_t* __restrict__ pair_counts, const index_t* __restrict__ pair_offsets,
+    std::int64_t capacity, index_t* __restrict__ pairs)
 {
     const int lane = threadIdx.x % kWarp;
-    const Slot<T> c = kStaged ? staged[h]
-                              : hood_candidate(hood, 0, h, sorted_positions, sorted_ids, lx, ly,
-                                               lz);
-    // The center past the lower face of a later bin's image: center - L, rounded once.
-    const T cx_ahead = c.x - lx, cy_ahead = c.y - ly, cz_ahead = c.z - lz;
-    for (int g = 0; g < hood.count; ++g)
+    const int homes = hood.size[0];
+    for (int group = 0; group < homes; group += kWarp)
     {
-        const unsigned ahead = hood.ahead[g];
-        const T ax = (ahead & 1u) ? cx_ahead : c.x;
-        const T ay = (ahead & 2u) ? cy_ahead : c.y;
-        const T az = (ahead & 4u) ? cz_ahead : c.z;
-        const int begin = g == 0 ? h + 1 : 0;
-        const int end = hood.size[g];
-        for (int base = begin; base < end; base += kWarp)
+        const int h = group + lane;
+        const bool active = h < homes;
+        const Slot<T> c = !active ? Slot<T>{T(0), T(0), T(0), T(0)}
+                          : kStaged ? staged[h]
+                                    : hood_candidate(hood, 0, h, sorted_positions, sorted_ids,
+                                                     lx, ly, lz);
+        // The center past the lower face of a later bin's image: center - L, rounded once.
+        const T cx_ahead = c.x - lx, cy_ahead = c.y - ly, cz_ahead = c.z - lz;
+        const index_t center = hood.first[0] + h;
+        index_t count = 0;
+        std::int64_t column = kFill && active ? pair_offsets[center] : 0;
+        const index_t center_id = kFill && active ? sorted_ids[center] : 0;
+        // The home bin's candidates start after the group's first center.
+        for (int g = 0; g < hood.count; ++g)
         {
-            const int k = base + lane;
-            const bool valid = k < end;
-            Slot<T> p;
-            if (valid)
+            const unsigned ahead = hood.ahead[g];
+            const T ax = (ahead & 1u) ? cx_ahead : c.x;
+            const T ay = (ahead & 2u) ? cy_ahead : c.y;
+            const T az = (ahead & 4u) ? cz_ahead : c.z;
+            const int end = hood.size[g];
+            for (int base = g == 0 ? group + 1 : 0; base < end; base += kWarp)
             {
-                p = kStaged ? staged[hood.slot[g] + k]
-                            : hood_candidate(hood, g, k, sorted_positions, sorted_ids, lx, ly,
-                                             lz);
+                const int size = end - base < kWarp ? end - base : kWarp;
+                unsigned hits = hit_word<T, kFixed, kStaged>(hood, staged, sorted_positions,
+                                                             sorted_ids, g, base, size, c, ax,
+                                                             ay, az, lx, ly, lz, radius_squared);
+                if (g == 0)
+                {
+                    // Only candidates after the lane's own center: bits above h - base.
+                    const int above = h - base + 1;
+                    hits &= above <= 0 ? ~0u : (above >= kWarp ? 0u : ~0u << above);
+                }
+                hits = active ? hits : 0u;
+                if (kFill)
+                {
+                    while (hits != 0)
+                    {
+                        const int j = __ffs(hits) - 1;
+                        hits &= hits - 1;
+                        if (column < capacity)
+                        {
+                            const index_t other =
+                                kStaged ? word_id(staged[hood.slot[g] + base + j].w)
+                                        : sorted_ids[hood.first[g] + base + j];
+                            pairs[column] = center_id;
+                            pairs[capacity + column] = other;
+                        }
+                        ++column;
+                    }
+                }
+                else
+                {
+                    count += __popc(hits);
+                }
             }
-            else
-            {
-                p = Slot<T>{ax, ay, az, T(0)};
-            }
-            T dx, dy, dz;
-            if (kFixed)
-            {
-                dx = ax - p.x;
-                dy = ay - p.y;
-                dz = az - p.z;
-            }
-            else
-            {
-                dx = min_image(c.x, p.x, lx);
-                dy = min_image(c.y, p.y, ly);
-                dz = min_image(c.z, p.z, lz);
-            }
-            const bool hit = valid && squared_norm(dx, dy, dz) < radius_squared;
-            const unsigned hits = __ballot_sync(kFullMask, hit);
-            sink.take(hits, hit, word_id(p.w));
+        }
+        if (!kFill && active)
+        {
+            pair_counts[center] = count;
         }
     }
 }
 
-// Counts (kFill false) or writes (kFill true) the pairs of one home bin per CTA. The fill
-// of an update also stores the frame it was built from: each CTA its home atoms' positions,
-// CTA 0 the cell and the rebuild count.
+// Counts (kFill false) or writes (kFill true) the pairs of one home bin per warp. The fill of
+// an update also stores the frame it was built from: each warp its home atoms' positions, the
+// first warp the cell and the rebuild count.
 template <typename T, bool kFill>
 __global__ void __launch_bounds__(kHoodThreads) hood_pairs_kernel(
     const T* __restrict__ sorted_positions,
@@ -405,6 +442,7 @@ __global__ void __launch_bounds__(kHoodThreads) hood_pairs_kernel(
     const index_t* __restrict__ dims,
     const T* __restrict__ cell,
     T radius_squared,
+    std::int64_t num_bins,
     index_t* __restrict__ pair_counts,
     const index_t* __restrict__ pair_offsets,
     index_t capacity,
@@ -417,34 +455,32 @@ __global__ void __launch_bounds__(kHoodThreads) hood_pairs_kernel(
     const index_t* __restrict__ status
 )
 {
-    if (!rebuilding(rebuild, status))
-    {
-        return;
-    }
-    __shared__ Hood hood;
-    __shared__ Slot<T> staged[HoodSlots<T>::value];
-    const index_t home = blockIdx.x;
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const std::int64_t home = static_cast<std::int64_t>(blockIdx.x) * kHoodWarps + warp;
+    if (home >= num_bins || !rebuilding(rebuild, status))
+    {
+        return;  // whole warps; no block barrier follows
+    }
+    __shared__ Hood hoods[kHoodWarps];
+    __shared__ Slot<T> tiles[kHoodWarps][HoodSlots<T>::value];
+    Hood& hood = hoods[warp];
+    Slot<T>* staged = tiles[warp];
     const bool fixed = dims[0] >= 3 && dims[1] >= 3 && dims[2] >= 3;
     const T lx = cell[0], ly = cell[1], lz = cell[2];
-    if (warp == 0)
-    {
-        plan_hood(hood, home, dims, bin_offsets, fixed);
-    }
-    __syncthreads();
+    plan_hood(hood, static_cast<index_t>(home), dims, bin_offsets, fixed);
     const int homes = hood.size[0];
     if (kFill && reference_positions != nullptr)
     {
-        for (int k = threadIdx.x; k < 3 * homes; k += blockDim.x)
+        for (int k = lane; k < 3 * homes; k += kWarp)
         {
             const std::int64_t id = sorted_ids[hood.first[0] + k / 3];
             reference_positions[3 * id + k % 3] = positions[3 * id + k % 3];
         }
-        if (home == 0 && threadIdx.x < 3)
+        if (home == 0 && lane < 3)
         {
-            reference_cell[threadIdx.x] = cell[threadIdx.x];
+            reference_cell[lane] = cell[lane];
         }
-        if (home == 0 && threadIdx.x == 0)
+        if (home == 0 && lane == 0)
         {
             ++rebuild_count[0];
         }
@@ -456,7 +492,7 @@ __global__ void __launch_bounds__(kHoodThreads) hood_pairs_kernel(
     const bool stage = hood.total <= HoodSlots<T>::value;
     if (stage)
     {
-        for (int g = warp; g < hood.count; g += kHoodWarps)
+        for (int g = 0; g < hood.count; ++g)
         {
             for (int k = lane; k < hood.size[g]; k += kWarp)
             {
@@ -464,42 +500,26 @@ __global__ void __launch_bounds__(kHoodThreads) hood_pairs_kernel(
                     hood_candidate(hood, g, k, sorted_positions, sorted_ids, lx, ly, lz);
             }
         }
-        __syncthreads();
+        __syncwarp();
     }
-    for (int h = warp; h < homes; h += kHoodWarps)
+    const std::int64_t cap = capacity;
+    if (fixed)
     {
-        const index_t center = hood.first[0] + h;
-        auto run = [&](auto& sink) {
-            if (fixed)
-            {
-                stage ? visit_center<T, true, true>(hood, staged, sorted_positions, sorted_ids, h,
-                                                    lx, ly, lz, radius_squared, sink)
-                      : visit_center<T, true, false>(hood, staged, sorted_positions, sorted_ids,
-                                                     h, lx, ly, lz, radius_squared, sink);
-            }
-            else
-            {
-                stage ? visit_center<T, false, true>(hood, staged, sorted_positions, sorted_ids,
-                                                     h, lx, ly, lz, radius_squared, sink)
-                      : visit_center<T, false, false>(hood, staged, sorted_positions,
-                                                      sorted_ids, h, lx, ly, lz, radius_squared,
-                                                      sink);
-            }
-        };
-        if (kFill)
-        {
-            FillSink sink{pairs, capacity, pair_offsets[center], sorted_ids[center]};
-            run(sink);
-        }
-        else
-        {
-            CountSink sink;
-            run(sink);
-            if (lane == 0)
-            {
-                pair_counts[center] = sink.count;
-            }
-        }
+        stage ? hood_lanes<T, kFill, true, true>(hood, staged, sorted_positions, sorted_ids, lx,
+                                                 ly, lz, radius_squared, pair_counts,
+                                                 pair_offsets, cap, pairs)
+              : hood_lanes<T, kFill, true, false>(hood, staged, sorted_positions, sorted_ids, lx,
+                                                  ly, lz, radius_squared, pair_counts,
+                                                  pair_offsets, cap, pairs);
+    }
+    else
+    {
+        stage ? hood_lanes<T, kFill, false, true>(hood, staged, sorted_positions, sorted_ids, lx,
+                                                  ly, lz, radius_squared, pair_counts,
+                                                  pair_offsets, cap, pairs)
+              : hood_lanes<T, kFill, false, false>(hood, staged, sorted_positions, sorted_ids,
+                                                   lx, ly, lz, radius_squared, pair_counts,
+                                                   pair_offsets, cap, pairs);
     }
 }
 
@@ -865,10 +885,11 @@ void launch_hood(const T* cell, double radius, const List& list, const Commit<T>
 {
     const nd_neighbor_buffers& b = *list.b;
     const T r = static_cast<T>(radius);
-    hood_pairs_kernel<T, kFill><<<static_cast<unsigned>(b.num_bin_slots - 1), kHoodThreads, 0,
-                                  stream>>>(
+    const std::int64_t bins = b.num_bin_slots - 1;
+    hood_pairs_kernel<T, kFill><<<static_cast<unsigned>((bins + kHoodWarps - 1) / kHoodWarps),
+                                  kHoodThreads, 0, stream>>>(
         static_cast<const T*>(b.sorted_positions), b.sorted_ids, b.bin_offsets, b.dims, cell,
-        r * r, b.pair_counts, b.pair_offsets, static_cast<index_t>(b.capacity), b.pairs,
+        r * r, bins, b.pair_counts, b.pair_offsets, static_cast<index_t>(b.capacity), b.pairs,
         commit.positions, commit.reference_positions, commit.reference_cell,
         commit.rebuild_count, list.rebuild, b.status);
 }

@@ -37,7 +37,6 @@ _ALIGN = 32          # atoms per allocation unit (one warp of list chunks)
 _MAX_CELLS = 4096    # kServeMaxCells in serve.cu
 _WIDTH = 192         # list slots per atom: room for ~1.5x the mean count at 22 atoms/nm^3
 _BYTES_PER_ATOM = 16 + 12 + 12 + 4 + 4 + 24 + 16 + 2 * _WIDTH + 4 + 4 + 4
-_STAGE_AHEAD = 256   # arrived requests made ready on the host while a round runs
 _CHAIN_A, _KINETIC_A, _PENDING, _CHAIN_MASS, _KT, _DEGREES, _TIMESTEP = 0, 6, 14, 16, 19, 20, 21
 
 
@@ -112,12 +111,15 @@ class ReplicaServer:
     """Resident replicas in one device pool, advanced in rounds by the replica kernel.
 
     ``budget_bytes`` bounds the pool (about 0.5 kB per atom); ``max_slots`` bounds the replicas
-    resident at once; ``round_atom_steps`` is the work a slot gets per round, in atom-steps.
+    resident at once; ``round_atom_steps`` is the work a slot gets per round, in atom-steps;
+    ``stage_ahead`` is how many arrived requests the host makes ready (slot record, frame in
+    pinned memory) while a round runs on the device (0: each at its admission).
     """
 
     def __init__(self, *, device: torch.device | str = "cuda", budget_bytes: int = 4 << 30,
-                 max_slots: int = 2048, round_atom_steps: int = 200_000):
+                 max_slots: int = 2048, round_atom_steps: int = 200_000, stage_ahead: int = 32):
         self.device = torch.device(device)
+        self.stage_ahead = int(stage_ahead)
         self.max_slots = int(max_slots)
         self.round_atom_steps = int(round_atom_steps)
         self.capacity = max(_ALIGN, (int(budget_bytes) // _BYTES_PER_ATOM) // _ALIGN * _ALIGN)
@@ -227,11 +229,13 @@ class ReplicaServer:
         record.thermostat[_TIMESTEP] = request.timestep
         return record, velocities32
 
-    def _stage(self, request: ReplicaRequest) -> _Staged:
-        """The host part of an admission: the record and the frame in pinned memory."""
+    def _stage(self, request: ReplicaRequest, pinned: bool = True) -> _Staged:
+        """The host part of an admission: the record and the frame, in pinned memory when the
+        upload is to overlap a round (staged ahead), else in ordinary memory."""
         record, velocities32 = self._describe(request, 0, 0)
         n = record.num_atoms
-        frame = torch.empty((n, 9), dtype=torch.float32).pin_memory()
+        frame = torch.empty((n, 9), dtype=torch.float32)
+        frame = frame.pin_memory() if pinned else frame
         masses = np.asarray(request.masses, dtype=np.float32)
         host = frame.numpy()
         host[:, :3] = np.asarray(request.positions, dtype=np.float32)
@@ -259,7 +263,8 @@ class ReplicaServer:
         b["images"][offset:offset + n].zero_()
         size = ctypes.sizeof(Replica)
         raw = torch.frombuffer(bytearray(ctypes.string_at(ctypes.addressof(record), size)),
-                               dtype=torch.uint8).pin_memory()
+                               dtype=torch.uint8)
+        raw = raw.pin_memory() if staged.frame.is_pinned() else raw
         self.table[slot * size:(slot + 1) * size].copy_(raw, non_blocking=True)
         staged.raw = raw  # the pinned record stays alive with the staged frame
 
@@ -357,7 +362,7 @@ class ReplicaServer:
 
         def stage_ahead(now: float) -> None:
             # Host preparation of the requests that have arrived, a bounded number ahead.
-            for request in list(pending)[:_STAGE_AHEAD]:
+            for request in list(pending)[:self.stage_ahead]:
                 if realtime and request.arrival > now:
                     break
                 if id(request) not in staged:
@@ -377,7 +382,7 @@ class ReplicaServer:
                 pending.popleft()
                 slot = self._free_slots.pop()
                 offset = first * _ALIGN
-                ready = staged.pop(id(request), None) or self._stage(request)
+                ready = staged.pop(id(request), None) or self._stage(request, pinned=False)
                 self._place(ready, slot, offset)
                 active[slot] = _Active(request, slot, offset, units, now, int(request.steps),
                                        ready)
@@ -393,7 +398,8 @@ class ReplicaServer:
                        for s in slots]
             self._launch(slots, budgets, 1)
             # While the round runs: the next admissions' host work.
-            stage_ahead(time.perf_counter() - start)
+            if self.stage_ahead:
+                stage_ahead(time.perf_counter() - start)
             raw = self._records()
             now = time.perf_counter() - start
             steps_left_all = self._int_field(raw, "steps_left")

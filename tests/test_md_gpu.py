@@ -245,3 +245,28 @@ def test_two_types_on_grid_path_match_oracle(cuda):
     pressure = (2 * kinetic + np.trace(virial)) / (3 * float(np.prod(cell)))
     assert float(panel["potential_energy"]) == pytest.approx(energy, rel=1e-9)
     assert float(panel["pressure"]) == pytest.approx(pressure, rel=1e-9)
+
+
+def test_run_writes_sample_file(argon, cuda, monkeypatch, tmp_path):
+    """run(..., sample_file=) writes each sample's frame and panel (through the in-memory h5py
+    stand-in of tests/fake_h5py.py): the samples equal run's returned panel and the last
+    frame equals state()."""
+    import sys
+
+    import fake_h5py
+
+    monkeypatch.setitem(sys.modules, "h5py", fake_h5py)
+    simulation = build("NVT", *argon_system(argon, torch.float32, cuda))
+    path = tmp_path / "run.h5"
+    samples = simulation.run(20, sample_every=10, sample_file=path)
+    state = simulation.state()
+    data, attributes = md.read_sample_file(path)
+    assert data["step"].tolist() == [10, 20]
+    np.testing.assert_allclose(data["time"], [0.04, 0.08])
+    np.testing.assert_array_equal(data["positions"][-1], state.positions.cpu().numpy())
+    np.testing.assert_array_equal(data["images"][-1], state.images.cpu().numpy())
+    for name, values in samples.items():
+        if name != "step":
+            np.testing.assert_array_equal(data[name], values.numpy(), err_msg=name)
+    assert attributes["ensemble"] == "NVT" and attributes["timestep"] == 0.004
+    assert attributes["cutoff"] == 1.0 and attributes["schema"] == "nabladyn.samples"
