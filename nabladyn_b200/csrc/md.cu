@@ -18,8 +18,9 @@
 // Bricks and tiles. Cells of at least the list radius are grouped along x into bricks of a few
 // cells. One CTA per brick stages the brick's 3 x 3 rows of neighbor cells (x extended by one
 // cell each way) into shared memory, each cell already shifted by its periodic image and the
-// brick's frame (brick_frame: every displacement rounds once), with coalesced 16-B loads. The neighbor list is a full list (both directions, no atomics) of
-// uint16 tile-local indices, interleaved by warps of 32 cell-order slots:
+// brick's frame (brick_frame: every displacement rounds once), with coalesced 16-B loads. The
+// neighbor list is a full list (both directions, no atomics) of uint16 tile-local indices,
+// interleaved by warps of 32 cell-order slots:
 //     entry (i, k) lives at ((i / 32) * width + k) * 32 + i % 32.
 // The force kernel re-stages the same tile from the current positions and reads every
 // neighbor from shared memory, so the only per-pair global traffic is the 2-B index.
@@ -324,7 +325,13 @@ __device__ __forceinline__ TileShape stage_brick(
     // One decision for the whole block, so every thread takes the same path below.
     if (!__syncthreads_and(barrier_wait_bounded(&copied)))
     {
-        // Lost copies: flag it, give them one more bounded wait, and compute nothing.
+        // Lost copies: flag it, give them one more bounded wait, and compute nothing. The
+        // copies write only this CTA's own tile, so a copy still in flight after both waits
+        // (a second, then another 0.5 s) can reach no other CTA's data; but a CTA that exits
+        // with one outstanding leaves its shared memory to a late write, which is undefined.
+        // That point means the copy engine has stopped: the status bit fails the run at its
+        // next host read and no later result is used; an unbounded wait here would instead
+        // hang the GPU, so the CTA leaves after the second bound.
         if (threadIdx.x == 0)
         {
             atomicOr(s.status, kStageTimeout);
@@ -431,7 +438,9 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
         return;
     }
     // One warp per home cell: the lanes are the cell's atoms and share its candidate rows, so
-    // every candidate is one broadcast read of shared memory and the loops do not diverge.
+    // every candidate is one broadcast read of shared memory and the tests do not diverge.
+    // A lane first sets one bit per hit in a word of 32 candidates, then appends the word's
+    // hits: the appends (about 15 % of the candidates) diverge, the tests do not.
     const int per_row = shape.cells_per_row;
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     for (int c = 1 + warp; c < per_row - 1; c += kMDThreads / kWarp)
@@ -451,13 +460,64 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             {
                 const int begin = start[r * per_row + c - 1];
                 const int end = start[r * per_row + c + 2];
-                for (int k = begin; k < end; ++k)
+                for (int word = begin; word < end; word += kWarp)
                 {
-                    const Pos4<T> p = tile[k];
-                    if (active && k != self &&
-                        squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max)
+                    const int size = end - word < kWarp ? end - word : kWarp;
+                    unsigned hits = 0;
+                    if constexpr (std::is_same_v<T, float>)
                     {
-                        list.add(k);
+                        if (size == kWarp)
+                        {
+                            // Two candidates per packed instruction (sm_100 f32x2): each half
+                            // rounds as the scalar test, p - x being the exact negative of
+                            // x - p, so the bits are the same.
+                            const float2 nx = make_float2(-me.x, -me.x);
+                            const float2 ny = make_float2(-me.y, -me.y);
+                            const float2 nz = make_float2(-me.z, -me.z);
+#pragma unroll
+                            for (int j = 0; j < kWarp; j += 2)
+                            {
+                                const Pos4<T> a = tile[word + j];
+                                const Pos4<T> b = tile[word + j + 1];
+                                const float2 dx = __fadd2_rn(make_float2(a.x, b.x), nx);
+                                const float2 dy = __fadd2_rn(make_float2(a.y, b.y), ny);
+                                const float2 dz = __fadd2_rn(make_float2(a.z, b.z), nz);
+                                const float2 r2 =
+                                    __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+                                hits |= r2.x < r2max ? 1u << j : 0u;
+                                hits |= r2.y < r2max ? 2u << j : 0u;
+                            }
+                        }
+                    }
+                    if (!std::is_same_v<T, float> && size == kWarp)
+                    {
+#pragma unroll
+                        for (int j = 0; j < kWarp; ++j)
+                        {
+                            const Pos4<T> p = tile[word + j];
+                            hits |= squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max
+                                        ? 1u << j
+                                        : 0u;
+                        }
+                    }
+                    else if (size < kWarp)
+                    {
+                        for (int j = 0; j < size; ++j)
+                        {
+                            const Pos4<T> p = tile[word + j];
+                            hits |= squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max
+                                        ? 1u << j
+                                        : 0u;
+                        }
+                    }
+                    const unsigned offset = static_cast<unsigned>(self - word);
+                    hits &= offset < kWarp ? ~(1u << offset) : ~0u;  // not the atom itself
+                    hits = active ? hits : 0u;
+                    while (hits != 0)
+                    {
+                        const int j = __ffs(hits) - 1;
+                        hits &= hits - 1;
+                        list.add(word + j);
                     }
                 }
             }
@@ -491,7 +551,7 @@ struct CenterSums
 // shared memory, no bounds checks (partial chunks are padded with the far sentinel) and no
 // branch on the cutoff (outside pairs contribute an exact zero). With one atom type the
 // constants 24 eps, 4 eps and u(r_c) are applied once per center, not per pair.
-template <typename T, bool kSmall, bool kMulti, bool kVirial>
+template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kEnergy>
 __device__ __forceinline__ CenterSums<T> pair_loop(
     const System<T>& s,
     const Pos4<T>* __restrict__ tile,
@@ -549,16 +609,22 @@ __device__ __forceinline__ CenterSums<T> pair_loop(
             const T p6 = q * q * q;
             const T mask = inside ? T(1) : T(0);
             T fs = mask * (inv_r2 * (p6 * fma(T(2), p6, T(-1))));
-            const T u = fma(p6, p6, -p6);
             if (kMulti)
             {
                 fs *= pp.e24;
-                out.energy = fma(mask, fma(pp.e4, u, -pp.shift), out.energy);
             }
-            else
+            if (kEnergy)
             {
-                out.energy = fma(mask, u, out.energy);
-                out.inside += mask;
+                const T u = fma(p6, p6, -p6);
+                if (kMulti)
+                {
+                    out.energy = fma(mask, fma(pp.e4, u, -pp.shift), out.energy);
+                }
+                else
+                {
+                    out.energy = fma(mask, u, out.energy);
+                    out.inside += mask;
+                }
             }
             out.fx = fma(fs, dx, out.fx);
             out.fy = fma(fs, dy, out.fy);
@@ -592,7 +658,9 @@ __device__ __forceinline__ void force_center(
     me.x += frame.x;
     me.y += frame.y;
     me.z += frame.z;
-    CenterSums<T> c = pair_loop<T, kSmall, kMulti, kVirial>(s, tile, params, me, center);
+    // A step needs no energy (its finalize uses only K); a frame's evaluation does.
+    constexpr bool kEnergy = !kKickStep;
+    CenterSums<T> c = pair_loop<T, kSmall, kMulti, kVirial, kEnergy>(s, tile, params, me, center);
     T scale = T(1);  // kJ/mol/nm per unit of the accumulated force
     double energy;
     if (kMulti)
@@ -606,7 +674,10 @@ __device__ __forceinline__ void force_center(
     }
     const T fx = c.fx * scale, fy = c.fy * scale, fz = c.fz * scale;
     // Each pair is listed from both ends: half of the energy and virial per end.
-    sums[0] += 0.5 * energy;
+    if (kEnergy)
+    {
+        sums[0] += 0.5 * energy;
+    }
     if (kVirial)
     {
 #pragma unroll
@@ -1327,30 +1398,12 @@ std::size_t tile_bytes(const System<T>& s)
     return static_cast<std::size_t>(s.sentinel + 1) * sizeof(Pos4<T>);
 }
 
-// Raises a kernel's dynamic shared-memory limit when a launch needs more than any before; the
-// first launch of every kernel happens outside graph capture (allocation, warm-up).
-template <typename Kernel>
-cudaError_t allow_shared(Kernel kernel, std::size_t bytes, std::size_t& granted)
-{
-    if (bytes <= granted || bytes <= 48 * 1024)
-    {
-        return cudaSuccess;
-    }
-    const cudaError_t rc = cudaFuncSetAttribute(
-        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-    if (rc == cudaSuccess)
-    {
-        granted = bytes;
-    }
-    return rc;
-}
-
 template <typename T>
 int launch_build(const System<T>& s, int gated, cudaStream_t stream)
 {
     const std::size_t bytes = tile_bytes(s);
-    static std::size_t granted = 0;
-    ND_CUDA_TRY(allow_shared(build_list_kernel<T>, bytes, granted));
+    static DeviceGrant grant;  // per device; the first launch happens outside graph capture
+    ND_CUDA_TRY(grant.allow(build_list_kernel<T>, bytes));
     build_list_kernel<T><<<s.num_bricks, kMDThreads, bytes, stream>>>(s, gated);
     ND_LAUNCH_CHECK();
     return ND_OK;
@@ -1389,8 +1442,8 @@ int launch_force_variant(const System<T>& s, cudaStream_t stream)
     if (s.small == SMALL && multi == MULTI)                                                 \
     {                                                                                       \
         auto kernel = force_kernel<T, SMALL, MULTI, kVirial, kKickStep, kThermostat>;       \
-        static std::size_t granted = 0;                                                     \
-        ND_CUDA_TRY(allow_shared(kernel, bytes, granted));                                  \
+        static DeviceGrant grant;                                                           \
+        ND_CUDA_TRY(grant.allow(kernel, bytes));                                            \
         kernel<<<s.force_blocks, kMDThreads, bytes, stream>>>(s);                           \
         ND_LAUNCH_CHECK();                                                                  \
         finalize_kernel<kThermostat, kKickStep><<<1, kFinalizeThreads, 0, stream>>>(        \
@@ -1899,8 +1952,8 @@ int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t
     if ((s.num_types > 1) == MULTI && (thermostat != 0) == THERMO)                 \
     {                                                                              \
         auto kernel = small_run_kernel<T, MULTI, THERMO>;                          \
-        static std::size_t granted = 0;                                            \
-        ND_CUDA_TRY(allow_shared(kernel, bytes, granted));                         \
+        static DeviceGrant grant;                                                  \
+        ND_CUDA_TRY(grant.allow(kernel, bytes));                                   \
         ND_CUDA_TRY(cudaLaunchKernelEx(&config, kernel, s, steps));                \
         return ND_OK;                                                              \
     }
