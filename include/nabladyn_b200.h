@@ -214,7 +214,7 @@ typedef struct nd_md_system {
     int32_t small;           /* 1: one tile holds the whole system, minimum image per pair */
     int32_t dims[3];         /* cells per axis (>= 3 each unless small) */
     int32_t bricks_x;        /* bricks per row of cells along x */
-    int32_t width;           /* neighbor-list slots per atom, a multiple of 8 */
+    int32_t width;           /* neighbor-list slots per list row, a multiple of 8 */
     int32_t tile_capacity;   /* atoms per brick tile, at most */
     double cell[3];          /* orthorhombic cell lengths, fixed */
     double widths[3];        /* cell widths, L / dims, rounded to T */
@@ -243,8 +243,11 @@ typedef struct nd_md_system {
     int32_t* unordered;      /* [N] */
     int32_t* order;          /* [N] */
     void* scan_temp;         /* nd_neighbors_scan_temp_bytes(cells + 1) bytes */
-    uint16_t* neighbors;     /* [ceil(N / 32) * 32 * width] */
-    int32_t* neighbor_counts; /* [N] */
+    uint16_t* neighbors;     /* [ceil(rows / 32) * 32 * width]; rows = N when small, else
+                              * N + 2 * bricks + 2 (bricks = bricks_x * dims[1] * dims[2]):
+                              * two rows per center pair, the halves of the pair's list */
+    int32_t* neighbor_counts; /* [rows] */
+    int32_t* pair_order;     /* [rows / 2]: each brick's center pairs, longest lists first */
     int32_t* rebuild;        /* [1] */
     int32_t* rebuild_count;  /* [1] */
     int32_t* status;         /* [4]: flags, most neighbors needed, largest tile needed, largest tile built */

@@ -152,6 +152,7 @@ class MDSystem(ctypes.Structure):
         ("scan_temp", ctypes.c_void_p),
         ("neighbors", ctypes.c_void_p),
         ("neighbor_counts", ctypes.c_void_p),
+        ("pair_order", ctypes.c_void_p),
         ("rebuild", ctypes.c_void_p),
         ("rebuild_count", ctypes.c_void_p),
         ("status", ctypes.c_void_p),

@@ -19,9 +19,13 @@
 // cells. One CTA per brick stages the brick's 3 x 3 rows of neighbor cells (x extended by one
 // cell each way) into shared memory, each cell already shifted by its periodic image and the
 // brick's frame (brick_frame: every displacement rounds once), with coalesced 16-B loads. The
-// neighbor list is a full list (both directions, no atomics) of uint16 tile-local indices,
-// interleaved by warps of 32 cell-order slots:
-//     entry (i, k) lives at ((i / 32) * width + k) * 32 + i % 32.
+// neighbor list is a full list (both directions, no atomics) of uint16 tile-local indices, kept
+// per PAIR of centers: consecutive centers of a brick share one list of the tile atoms closer
+// than the radius to either of them (166 entries per pair on the 1M-atom argon box, against
+// 2 x 125 for two lists), split into two halves, one per lane, and every neighbor read from
+// shared memory is evaluated against both centers, the two as the halves of packed f32x2
+// instructions. The halves are list rows, interleaved by warps of 32 rows:
+//     entry (row, k) lives at ((row / 32) * width + k) * 32 + row % 32.
 // The force kernel re-stages the same tile from the current positions and reads every
 // neighbor from shared memory, so the only per-pair global traffic is the 2-B index.
 //
@@ -82,6 +86,7 @@ struct System
     void* scan_temp;
     std::uint16_t* nbr;
     index_t* nbr_count;
+    index_t* pair_order;
     index_t* rebuild;
     index_t* rebuild_count;
     index_t* status;
@@ -199,18 +204,12 @@ struct BrickFrame
 };
 
 template <typename T>
-__device__ __forceinline__ BrickFrame<T> brick_frame(const System<T>& s, int brick)
+__device__ __forceinline__ BrickFrame<T> brick_frame(const System<T>& s, const TileShape& shape)
 {
-    const int nx = s.dims[0], ny = s.dims[1], nz = s.dims[2];
-    const int bx = brick % s.bricks_x;
-    const int y = (brick / s.bricks_x) % ny;
-    const int z = brick / (s.bricks_x * ny);
-    const int x0 = bx * nx / s.bricks_x;
-    const int x1 = (bx + 1) * nx / s.bricks_x;
     BrickFrame<T> frame;
-    frame.x = (x1 == nx && x0 > 0) ? -s.length[0] : T(0);
-    frame.y = (y == ny - 1 && y > 0) ? -s.length[1] : T(0);
-    frame.z = (z == nz - 1 && z > 0) ? -s.length[2] : T(0);
+    frame.x = (shape.x1 == s.dims[0] && shape.x0 > 0) ? -s.length[0] : T(0);
+    frame.y = (shape.y == s.dims[1] - 1 && shape.y > 0) ? -s.length[1] : T(0);
+    frame.z = (shape.z == s.dims[2] - 1 && shape.z > 0) ? -s.length[2] : T(0);
     return frame;
 }
 
@@ -218,30 +217,35 @@ __device__ __forceinline__ BrickFrame<T> brick_frame(const System<T>& s, int bri
 // (apart from a wrap along x), so each maximal run of cells whose atoms are adjacent in memory
 // is one bulk copy, issued by the first warp; every thread then waits on the barrier, and the
 // cells across a periodic boundary get their image shift in shared memory.
-template <typename T>
+//
+// `between(shape)` runs on every thread after the copies are issued and before the wait (only
+// when the tile fits): work that needs the brick's shape but not its tile, such as the loads a
+// CTA's first pass over its centers starts with, overlaps the copies.
+template <typename T, typename Between>
 __device__ __forceinline__ TileShape stage_brick(
     const System<T>& s,
     int brick,
     const Pos4<T>* __restrict__ positions,
     Pos4<T>* tile,
     int* start,
-    int* first
+    int* first,
+    Between&& between
 )
 {
     __shared__ std::uint64_t copied;
     const int nx = s.dims[0], ny = s.dims[1], nz = s.dims[2];
     const int bx = brick % s.bricks_x;
-    const int y = (brick / s.bricks_x) % ny;
-    const int z = brick / (s.bricks_x * ny);
     const int x0 = bx * nx / s.bricks_x;
     const int x1 = (bx + 1) * nx / s.bricks_x;
-    const int per_row = x1 - x0 + 2;
-    const int cells = 9 * per_row;
+    const int y = (brick / s.bricks_x) % ny;
+    const int z = brick / (s.bricks_x * ny);
     if (threadIdx.x == 0)
     {
         tile[s.sentinel] = far_atom<T>();
         barrier_init(&copied);
     }
+    const int per_row = x1 - x0 + 2;
+    const int cells = 9 * per_row;
     // Per tile cell: its cell-order range.
     for (int t = threadIdx.x; t < cells; t += blockDim.x)
     {
@@ -287,6 +291,10 @@ __device__ __forceinline__ TileShape stage_brick(
     TileShape shape;
     shape.cells_per_row = per_row;
     shape.size = start[cells];
+    shape.x0 = x0;
+    shape.x1 = x1;
+    shape.y = y;
+    shape.z = z;
     const int home_row = 4 * per_row;
     shape.home_first = first[home_row + 1];
     shape.home_end = first[home_row + per_row - 2] + (start[home_row + per_row - 1] -
@@ -322,8 +330,13 @@ __device__ __forceinline__ TileShape stage_brick(
             }
         }
     }
-    // One decision for the whole block, so every thread takes the same path below.
-    if (!__syncthreads_and(barrier_wait_bounded(&copied)))
+    between(static_cast<const TileShape&>(shape));
+    // The first warp polls the barrier while the others wait at the block barrier (no issue
+    // slots spent polling); then every warp observes the completed phase once, which makes
+    // the copied bytes visible to it. One decision for the whole block, so every thread takes
+    // the same path below.
+    const bool arrived = warp != 0 || barrier_wait_bounded(&copied);
+    if (!__syncthreads_and(arrived) || !barrier_try_wait(&copied, 0))
     {
         // Lost copies: flag it, give them one more bounded wait, and compute nothing. The
         // copies write only this CTA's own tile, so a copy still in flight after both waits
@@ -341,10 +354,15 @@ __device__ __forceinline__ TileShape stage_brick(
         return shape;
     }
     // Each cell's image shift plus the brick's frame, one warp per cell that moves.
-    const BrickFrame<T> frame = brick_frame(s, brick);
+    const BrickFrame<T> frame = brick_frame(s, shape);
+    int r = 0, c = warp;  // tile cell t = r * per_row + c, stepped without a division
+    while (c >= per_row)
+    {
+        c -= per_row;
+        ++r;
+    }
     for (int t = warp; t < cells; t += kWarpsPerBlock)
     {
-        const int r = t / per_row, c = t % per_row;
         const int cx = x0 - 1 + c, cy = y + r % 3 - 1, cz = z + r / 3 - 1;
         const T sx = (cx < 0 ? -s.length[0] : (cx >= nx ? s.length[0] : T(0))) + frame.x;
         const T sy = (cy < 0 ? -s.length[1] : (cy >= ny ? s.length[1] : T(0))) + frame.y;
@@ -358,15 +376,61 @@ __device__ __forceinline__ TileShape stage_brick(
                 tile[k].z += sz;
             }
         }
+        c += kWarpsPerBlock;
+        while (c >= per_row)
+        {
+            c -= per_row;
+            ++r;
+        }
     }
     __syncthreads();
     return shape;
+}
+
+template <typename T>
+__device__ __forceinline__ TileShape stage_brick(const System<T>& s, int brick,
+                                                 const Pos4<T>* __restrict__ positions,
+                                                 Pos4<T>* tile, int* start, int* first)
+{
+    return stage_brick(s, brick, positions, tile, start, first, [](const TileShape&) {});
 }
 
 __device__ __forceinline__ void flag_overflow(index_t* status, int word, int needed)
 {
     atomicOr(status, kOverflow);
     atomicMax(status + word, needed);
+}
+
+// Center pairs. On the brick path a brick's centers, cell-order slots [home_first, home_end),
+// are taken two at a time: pair q holds slots home_first + 2q and home_first + 2q + 1 (the
+// second missing when the count is odd). Pair q of brick b is P = home_first / 2 + b + q, and
+// its list has two halves, rows 2P and 2P + 1. Bricks come in cell order, so brick b's pairs
+// end at or before the next brick's first (ceil(n / 2) <= n / 2 + 1 makes up for the rounded
+// halves), and the rows of a system are fewer than N + 2 bricks + 2.
+__device__ __forceinline__ int pair_row(int home_first, int brick, int q, int part)
+{
+    return 2 * (home_first / 2 + brick + q) + part;
+}
+
+// Whether p lies closer than sqrt(r2max) to center a or to center b.
+template <typename T>
+__device__ __forceinline__ bool pair_hit(const Pos4<T>& a, const Pos4<T>& b, const Pos4<T>& p,
+                                         T r2max)
+{
+    return squared_norm(a.x - p.x, a.y - p.y, a.z - p.z) < r2max ||
+           squared_norm(b.x - p.x, b.y - p.y, b.z - p.z) < r2max;
+}
+
+// The same test with the two centers as the halves of packed f32x2 instructions (sm_100):
+// each half rounds as the scalar test, p - x being the exact negative of x - p.
+__device__ __forceinline__ bool pair_hit(const Pos4<float>& a, const Pos4<float>& b,
+                                         const Pos4<float>& p, float r2max)
+{
+    const float2 dx = __fadd2_rn(make_float2(p.x, p.x), make_float2(-a.x, -b.x));
+    const float2 dy = __fadd2_rn(make_float2(p.y, p.y), make_float2(-a.y, -b.y));
+    const float2 dz = __fadd2_rn(make_float2(p.z, p.z), make_float2(-a.z, -b.z));
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+    return r2.x < r2max || r2.y < r2max;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -437,100 +501,114 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
         }
         return;
     }
-    // One warp per home cell: the lanes are the cell's atoms and share its candidate rows, so
-    // every candidate is one broadcast read of shared memory and the tests do not diverge.
-    // A lane first sets one bit per hit in a word of 32 candidates, then appends the word's
-    // hits: the appends (about 15 % of the candidates) diverge, the tests do not.
+    // Pair lists. The brick's centers are taken two at a time in cell order (see pair_row);
+    // a pair's list holds every tile atom closer than the radius to either center, the two
+    // centers themselves excepted, in two halves: candidates at even and at odd offsets of a
+    // 32-candidate word. A warp builds the lists of 16 pairs (32 centers, one or two home
+    // cells): lanes 0-15 the even halves, lanes 16-31 the odd ones. Every candidate row is
+    // the x-run of tile cells around the warp's home cells, so a candidate is one broadcast
+    // read per half-warp (the two half-warps read adjacent slots) and the tests do not
+    // diverge; a lane tests its candidate against both of its centers and keeps one bit per
+    // hit in a word, then appends the word's hits.
     const int per_row = shape.cells_per_row;
+    const int home_row = 4 * per_row;
+    const int home_first = shape.home_first, home_end = shape.home_end;
+    const int pairs = (home_end - home_first + 1) / 2;
+    const int tile_home = start[home_row + 1];  // the tile slot of center home_first
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    for (int c = 1 + warp; c < per_row - 1; c += kMDThreads / kWarp)
+    const int part = lane >> 4;
+    const Pos4<T> far = far_atom<T>();
+    for (int group = warp; group * 16 < pairs; group += kWarpsPerBlock)
     {
-        const int home = 4 * per_row + c;
-        const int cell_first = first[home];
-        const int tile_first = start[home];
-        const int cell_count = start[home + 1] - tile_first;
-        for (int base = 0; base < cell_count; base += kWarp)
+        const int q = group * 16 + (lane & 15);
+        const bool active = q < pairs;
+        const int first_center = home_first + 2 * q;
+        const bool second = active && first_center + 1 < home_end;
+        const int self_a = active ? tile_home + 2 * q : -1;
+        const int self_b = second ? self_a + 1 : -1;
+        const Pos4<T> a = active ? tile[self_a] : far;
+        const Pos4<T> b = second ? tile[self_b] : far;
+        // The home cells (tile columns) of the group's first and last centers.
+        const int group_first = home_first + 32 * group;
+        const int group_last = min(group_first + 32, home_end) - 1;
+        int column_a = 1, column_b = 1;
+        for (int c = 1; c < per_row - 1; ++c)
         {
-            const bool active = base + lane < cell_count;
-            const int self = tile_first + (active ? base + lane : 0);
-            const int center = cell_first + base + lane;
-            const Pos4<T> me = tile[self];
-            StagedListWriter list(s.nbr, lane_slots[threadIdx.x], s.width, center);
-            for (int r = 0; r < 9; ++r)
+            const int f = first[home_row + c];
+            column_a = f <= group_first ? c : column_a;
+            column_b = f <= group_last ? c : column_b;
+        }
+        const std::int64_t row = pair_row(home_first, blockIdx.x, q, part);
+        StagedListWriter list(s.nbr, lane_slots[threadIdx.x], s.width, row);
+        for (int r = 0; r < 9; ++r)
+        {
+            const int begin = start[r * per_row + column_a - 1];
+            const int end = start[r * per_row + column_b + 2];
+            for (int word = begin; word < end; word += kWarp)
             {
-                const int begin = start[r * per_row + c - 1];
-                const int end = start[r * per_row + c + 2];
-                for (int word = begin; word < end; word += kWarp)
+                const int size = end - word < kWarp ? end - word : kWarp;
+                unsigned hits = 0;
+                if (size == kWarp)
                 {
-                    const int size = end - word < kWarp ? end - word : kWarp;
-                    unsigned hits = 0;
-                    if constexpr (std::is_same_v<T, float>)
-                    {
-                        if (size == kWarp)
-                        {
-                            // Two candidates per packed instruction (sm_100 f32x2): each half
-                            // rounds as the scalar test, p - x being the exact negative of
-                            // x - p, so the bits are the same.
-                            const float2 nx = make_float2(-me.x, -me.x);
-                            const float2 ny = make_float2(-me.y, -me.y);
-                            const float2 nz = make_float2(-me.z, -me.z);
 #pragma unroll
-                            for (int j = 0; j < kWarp; j += 2)
-                            {
-                                const Pos4<T> a = tile[word + j];
-                                const Pos4<T> b = tile[word + j + 1];
-                                const float2 dx = __fadd2_rn(make_float2(a.x, b.x), nx);
-                                const float2 dy = __fadd2_rn(make_float2(a.y, b.y), ny);
-                                const float2 dz = __fadd2_rn(make_float2(a.z, b.z), nz);
-                                const float2 r2 =
-                                    __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
-                                hits |= r2.x < r2max ? 1u << j : 0u;
-                                hits |= r2.y < r2max ? 2u << j : 0u;
-                            }
-                        }
-                    }
-                    if (!std::is_same_v<T, float> && size == kWarp)
+                    for (int j = 0; j < kWarp; j += 2)
                     {
-#pragma unroll
-                        for (int j = 0; j < kWarp; ++j)
-                        {
-                            const Pos4<T> p = tile[word + j];
-                            hits |= squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max
-                                        ? 1u << j
-                                        : 0u;
-                        }
-                    }
-                    else if (size < kWarp)
-                    {
-                        for (int j = 0; j < size; ++j)
-                        {
-                            const Pos4<T> p = tile[word + j];
-                            hits |= squared_norm(me.x - p.x, me.y - p.y, me.z - p.z) < r2max
-                                        ? 1u << j
-                                        : 0u;
-                        }
-                    }
-                    const unsigned offset = static_cast<unsigned>(self - word);
-                    hits &= offset < kWarp ? ~(1u << offset) : ~0u;  // not the atom itself
-                    hits = active ? hits : 0u;
-                    while (hits != 0)
-                    {
-                        const int j = __ffs(hits) - 1;
-                        hits &= hits - 1;
-                        list.add(word + j);
+                        hits |= pair_hit(a, b, tile[word + j + part], r2max) ? 1u << (j + part)
+                                                                            : 0u;
                     }
                 }
-            }
-            if (active)
-            {
-                list.finish(s.sentinel);
-                s.nbr_count[center] = list.count;
-                if (list.count > s.width)
+                else
                 {
-                    flag_overflow(s.status, 1, list.count);
+                    for (int j = part; j < size; j += 2)
+                    {
+                        hits |= pair_hit(a, b, tile[word + j], r2max) ? 1u << j : 0u;
+                    }
+                }
+                const unsigned off_a = static_cast<unsigned>(self_a - word);
+                const unsigned off_b = static_cast<unsigned>(self_b - word);
+                hits &= off_a < kWarp ? ~(1u << off_a) : ~0u;  // not the centers themselves
+                hits &= off_b < kWarp ? ~(1u << off_b) : ~0u;
+                hits = active ? hits : 0u;
+                while (hits != 0)
+                {
+                    const int j = __ffs(hits) - 1;
+                    hits &= hits - 1;
+                    list.add(word + j);
                 }
             }
         }
+        if (active)
+        {
+            list.finish(s.sentinel);
+            s.nbr_count[row] = list.count;
+            if (list.count > s.width)
+            {
+                flag_overflow(s.status, 1, list.count);
+            }
+        }
+    }
+    // The order in which the force kernel takes the pairs: longest list first (ties by q), so
+    // the lanes of a warp walk lists of about one length. The tile's memory is free now.
+    __syncthreads();
+    auto* lengths = reinterpret_cast<int*>(smem_raw);
+    const int first_pair = home_first / 2 + static_cast<int>(blockIdx.x);
+    for (int q = threadIdx.x; q < pairs; q += blockDim.x)
+    {
+        const int row = pair_row(home_first, blockIdx.x, q, 0);
+        const int even = s.nbr_count[row], odd = s.nbr_count[row + 1];
+        lengths[q] = even > odd ? even : odd;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < pairs; q += blockDim.x)
+    {
+        const int mine = lengths[q];
+        int rank = 0;
+        for (int other = 0; other < pairs; ++other)
+        {
+            const int length = lengths[other];
+            rank += length > mine || (length == mine && other < q);
+        }
+        s.pair_order[first_pair + rank] = q;
     }
 }
 
@@ -547,29 +625,76 @@ struct CenterSums
     T w[6];        // like the force
 };
 
-// Loops one center's list: 8 neighbors per 16-B word, every neighbor read from the tile in
-// shared memory, no bounds checks (partial chunks are padded with the far sentinel) and no
-// branch on the cutoff (outside pairs contribute an exact zero). With one atom type the
-// constants 24 eps, 4 eps and u(r_c) are applied once per center, not per pair.
-template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kEnergy>
-__device__ __forceinline__ CenterSums<T> pair_loop(
-    const System<T>& s,
-    const Pos4<T>* __restrict__ tile,
-    const PairParams<T>* __restrict__ params,
-    const Pos4<T>& me,
-    int center
-)
+// One pair term, center `me` against neighbor p, added to the center's sums: no branch on the
+// cutoff (a pair outside contributes an exact zero). With one atom type the constants 24 eps,
+// 4 eps and u(r_c) are applied once per center, not per pair.
+template <typename T, bool kMulti, bool kVirial, bool kEnergy>
+__device__ __forceinline__ void add_pair_term(CenterSums<T>& c, const Pos4<T>& me,
+                                              const Pos4<T>& p,
+                                              const PairParams<T>* __restrict__ params, T s2,
+                                              T cutoff_squared, int num_types)
 {
-    CenterSums<T> out{};
-    const int count = s.nbr_count[center];
+    const T dx = me.x - p.x;
+    const T dy = me.y - p.y;
+    const T dz = me.z - p.z;
+    const T r2 = squared_norm(dx, dy, dz);
+    const bool inside = r2 < cutoff_squared;
+    const T inv_r2 = fast_reciprocal(r2);
+    PairParams<T> pp;
+    if (kMulti)
+    {
+        pp = params[type_pair_row(static_cast<int>(me.w), static_cast<int>(p.w), num_types)];
+    }
+    const T q = (kMulti ? pp.s2 : s2) * inv_r2;
+    const T p6 = q * q * q;
+    const T mask = inside ? T(1) : T(0);
+    T fs = mask * (inv_r2 * (p6 * fma(T(2), p6, T(-1))));
+    if (kMulti)
+    {
+        fs *= pp.e24;
+    }
+    if (kEnergy)
+    {
+        const T u = fma(p6, p6, -p6);
+        if (kMulti)
+        {
+            c.energy = fma(mask, fma(pp.e4, u, -pp.shift), c.energy);
+        }
+        else
+        {
+            c.energy = fma(mask, u, c.energy);
+            c.inside += mask;
+        }
+    }
+    c.fx = fma(fs, dx, c.fx);
+    c.fy = fma(fs, dy, c.fy);
+    c.fz = fma(fs, dz, c.fz);
+    if (kVirial)
+    {
+        c.w[0] = fma(fs * dx, dx, c.w[0]);
+        c.w[1] = fma(fs * dy, dy, c.w[1]);
+        c.w[2] = fma(fs * dz, dz, c.w[2]);
+        c.w[3] = fma(fs * dx, dy, c.w[3]);
+        c.w[4] = fma(fs * dx, dz, c.w[4]);
+        c.w[5] = fma(fs * dy, dz, c.w[5]);
+    }
+}
+
+// Walks one half of a pair's list (8 neighbors per 16-B word, every neighbor read from the
+// tile in shared memory, two words in flight since the list streams from HBM; partial chunks
+// are padded with the far sentinel), each neighbor against both centers.
+template <typename T, bool kMulti, bool kVirial, bool kEnergy>
+__device__ __forceinline__ void half_list(const System<T>& s, const Pos4<T>* __restrict__ tile,
+                                          const PairParams<T>* __restrict__ params,
+                                          const Pos4<T>& a, const Pos4<T>& b, int row, int count,
+                                          uint4 next, uint4 after, CenterSums<T>& ca,
+                                          CenterSums<T>& cb)
+{
     const int used = count < s.width ? count : s.width;
     const int num_chunks = (used + kChunk - 1) / kChunk;
-    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
+    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(row, 0, s.width);
     const T cutoff_squared = s.cutoff_squared;
     const T s2 = params[0].s2;
-    // Two words in flight ahead of the one being computed: the list streams from HBM.
-    uint4 next = num_chunks > 0 ? chunks[0] : make_uint4(0, 0, 0, 0);
-    uint4 after = num_chunks > 1 ? chunks[kWarp] : make_uint4(0, 0, 0, 0);
     for (int chunk = 0; chunk < num_chunks; ++chunk)
     {
         const uint4 word = next;
@@ -583,97 +708,280 @@ __device__ __forceinline__ CenterSums<T> pair_loop(
         for (int r = 0; r < kChunk; ++r)
         {
             const Pos4<T> p = tile[(packed[r / 2] >> (16 * (r % 2))) & 0xffffu];
-            T dx, dy, dz;
-            if (kSmall)
-            {
-                dx = min_image(me.x, p.x, s.length[0]);
-                dy = min_image(me.y, p.y, s.length[1]);
-                dz = min_image(me.z, p.z, s.length[2]);
-            }
-            else
-            {
-                dx = me.x - p.x;
-                dy = me.y - p.y;
-                dz = me.z - p.z;
-            }
-            const T r2 = squared_norm(dx, dy, dz);
-            const bool inside = r2 < cutoff_squared;
-            const T inv_r2 = fast_reciprocal(r2);
-            PairParams<T> pp;
-            if (kMulti)
-            {
-                pp = params[type_pair_row(static_cast<int>(me.w), static_cast<int>(p.w),
-                                          s.num_types)];
-            }
-            const T q = (kMulti ? pp.s2 : s2) * inv_r2;
-            const T p6 = q * q * q;
-            const T mask = inside ? T(1) : T(0);
-            T fs = mask * (inv_r2 * (p6 * fma(T(2), p6, T(-1))));
-            if (kMulti)
-            {
-                fs *= pp.e24;
-            }
-            if (kEnergy)
-            {
-                const T u = fma(p6, p6, -p6);
-                if (kMulti)
-                {
-                    out.energy = fma(mask, fma(pp.e4, u, -pp.shift), out.energy);
-                }
-                else
-                {
-                    out.energy = fma(mask, u, out.energy);
-                    out.inside += mask;
-                }
-            }
-            out.fx = fma(fs, dx, out.fx);
-            out.fy = fma(fs, dy, out.fy);
-            out.fz = fma(fs, dz, out.fz);
-            if (kVirial)
-            {
-                out.w[0] = fma(fs * dx, dx, out.w[0]);
-                out.w[1] = fma(fs * dy, dy, out.w[1]);
-                out.w[2] = fma(fs * dz, dz, out.w[2]);
-                out.w[3] = fma(fs * dx, dy, out.w[3]);
-                out.w[4] = fma(fs * dx, dz, out.w[4]);
-                out.w[5] = fma(fs * dy, dz, out.w[5]);
-            }
+            add_pair_term<T, kMulti, kVirial, kEnergy>(ca, a, p, params, s2, cutoff_squared,
+                                                       s.num_types);
+            add_pair_term<T, kMulti, kVirial, kEnergy>(cb, b, p, params, s2, cutoff_squared,
+                                                       s.num_types);
         }
     }
-    return out;
 }
 
-template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
-__device__ __forceinline__ void force_center(
+// One 16-B tile slot by a single 128-bit shared load, at a shared-window byte address.
+__device__ __forceinline__ float4 load_slot(unsigned address)
+{
+    float4 v;
+    asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "r"(address));
+    return v;
+}
+
+// The step's half-list walk for one float32 atom type (forces only: a step needs neither
+// energy nor virial). The two centers are the two halves of every packed f32x2 instruction
+// (sm_100): a neighbor is read once and its displacement to both centers is three packed adds,
+// its r^2 three packed products, the force factor a packed chain and the force sums three
+// packed FMAs. The displacement is taken as p - me, the exact negative of me - p, and the
+// sums are negated back, so each term is add_pair_term's up to the order of the force sums.
+__device__ __forceinline__ void step_half_list(const System<float>& s,
+                                               const Pos4<float>* __restrict__ tile,
+                                               const PairParams<float>* __restrict__ params,
+                                               const Pos4<float>& a, const Pos4<float>& b,
+                                               int row, int count, uint4 next, uint4 after,
+                                               CenterSums<float>& ca, CenterSums<float>& cb)
+{
+    const int used = count < s.width ? count : s.width;
+    const int num_chunks = (used + kChunk - 1) / kChunk;
+    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(row, 0, s.width);
+    const float cutoff_squared = s.cutoff_squared;
+    const float2 s2 = make_float2(params[0].s2, params[0].s2);
+    const float2 two = make_float2(2.0f, 2.0f), minus_one = make_float2(-1.0f, -1.0f);
+    const float2 back_x = make_float2(-a.x, -b.x);
+    const float2 back_y = make_float2(-a.y, -b.y);
+    const float2 back_z = make_float2(-a.z, -b.z);
+    const unsigned base = shared_address(tile);
+    float2 gx = make_float2(0.0f, 0.0f), gy = gx, gz = gx;  // sums of fs (p - me)
+    for (int chunk = 0; chunk < num_chunks; ++chunk)
+    {
+        const uint4 word = next;
+        next = after;
+        if (chunk + 2 < num_chunks)
+        {
+            after = chunks[static_cast<std::int64_t>(chunk + 2) * kWarp];
+        }
+        const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+        for (int r = 0; r < kChunk; ++r)
+        {
+            const unsigned index = (packed[r / 2] >> (16 * (r % 2))) & 0xffffu;
+            const float4 p = load_slot(base + (index << 4));
+            const float2 dx = __fadd2_rn(make_float2(p.x, p.x), back_x);
+            const float2 dy = __fadd2_rn(make_float2(p.y, p.y), back_y);
+            const float2 dz = __fadd2_rn(make_float2(p.z, p.z), back_z);
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+            const float2 inv = make_float2(fast_reciprocal(r2.x), fast_reciprocal(r2.y));
+            const float2 inside = make_float2(r2.x < cutoff_squared ? 1.0f : 0.0f,
+                                              r2.y < cutoff_squared ? 1.0f : 0.0f);
+            const float2 q = __fmul2_rn(__fmul2_rn(inv, s2), inside);  // zero outside
+            const float2 p6 = __fmul2_rn(__fmul2_rn(q, q), q);
+            const float2 fs = __fmul2_rn(inv, __fmul2_rn(p6, __ffma2_rn(two, p6, minus_one)));
+            gx = __ffma2_rn(fs, dx, gx);
+            gy = __ffma2_rn(fs, dy, gy);
+            gz = __ffma2_rn(fs, dz, gz);
+        }
+    }
+    ca.fx -= gx.x;
+    ca.fy -= gy.x;
+    ca.fz -= gz.x;
+    cb.fx -= gx.y;
+    cb.fy -= gy.y;
+    cb.fz -= gz.y;
+}
+
+// The stand-in for the missing second center of a brick's last pair (an odd number of
+// centers): far from every tile atom and from the far sentinel alike, so every one of its
+// terms is an exact zero.
+template <typename T>
+__device__ __forceinline__ Pos4<T> absent_center()
+{
+    return Pos4<T>{T(-1e18), T(-1e18), T(-1e18), T(0)};
+}
+
+// What the second half kick of a center needs, loaded before its list is walked so that the
+// loads' latency hides behind the pair work.
+template <typename T>
+struct KickInputs
+{
+    T vx, vy, vz, inverse_mass, mass;
+};
+
+template <typename T, bool kKickStep, bool kThermostat>
+__device__ __forceinline__ KickInputs<T> load_kick(const System<T>& s, int center, bool valid)
+{
+    KickInputs<T> k{};
+    if (kKickStep && valid)
+    {
+        const T* v = s.vel + 3LL * center;
+        k.vx = v[0];
+        k.vy = v[1];
+        k.vz = v[2];
+        k.inverse_mass = s.inv_mass[center];
+        if (kThermostat)
+        {
+            k.mass = s.mass[center];
+        }
+    }
+    return k;
+}
+
+// Writes a center's force, kicks its velocity (steps) and adds its kinetic energy (NVT).
+template <typename T, bool kKickStep, bool kThermostat>
+__device__ __forceinline__ void finish_center(const System<T>& s, int center,
+                                              const KickInputs<T>& in, T fx, T fy, T fz,
+                                              double* sums)
+{
+    T* f = s.force + 3LL * center;
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = fz;
+    if (kKickStep)
+    {
+        const T kick = s.half_dt * in.inverse_mass;
+        T* v = s.vel + 3LL * center;
+        const T vx = fma(kick, fx, in.vx);
+        const T vy = fma(kick, fy, in.vy);
+        const T vz = fma(kick, fz, in.vz);
+        v[0] = vx;
+        v[1] = vy;
+        v[2] = vz;
+        if (kThermostat)
+        {
+            sums[1] += 0.5 * double(in.mass) * (double(vx) * vx + double(vy) * vy + double(vz) * vz);
+        }
+    }
+}
+
+// What a lane needs before walking its half of a pair's list: the pair (from the brick's
+// longest-first order), its half's length and its first two list words. None of it needs the
+// tile, so a CTA's first pass loads it while the tile's copies are in flight.
+struct PairStart
+{
+    int q;
+    bool live;  // the lane has a pair
+    int count;
+    uint4 first_word, second_word;
+};
+
+template <typename T>
+__device__ __forceinline__ PairStart pair_start(const System<T>& s, const TileShape& shape,
+                                                int lane_index)
+{
+    PairStart p;
+    const int lanes = (shape.home_end - shape.home_first + 1) & ~1;  // two per pair
+    p.live = lane_index < lanes;
+    p.q = p.live ? s.pair_order[shape.home_first / 2 + blockIdx.x + (lane_index >> 1)] : 0;
+    const int row = pair_row(shape.home_first, blockIdx.x, p.q, lane_index & 1);
+    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(row, 0, s.width);
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    // A row holds width / 8 >= 1 words; the first two are loaded without waiting for the count.
+    p.count = p.live ? s.nbr_count[row] : 0;
+    p.first_word = p.live ? chunks[0] : zero;
+    p.second_word = p.live && s.width > kChunk ? chunks[kWarp] : zero;
+    return p;
+}
+
+// One center pair of a brick, one half of its list per lane: lanes 2k and 2k + 1 of a warp
+// hold the two halves of pair q, add their force sums with one shuffle each, add the term
+// between the two centers (kept out of the list) and write one center each. Every lane of the
+// warp calls this, `live` false past the brick's last pair, so the shuffles see a full warp.
+// Energy and virial: each pair of atoms is met from both ends, half from each; the term
+// between the two centers is added, whole, by lane 2k alone.
+template <typename T, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
+__device__ __forceinline__ void force_pair(
     const System<T>& s,
     const Pos4<T>* __restrict__ tile,
     const PairParams<T>* __restrict__ params,
     const BrickFrame<T>& frame,
-    int center,
+    int home_first,
+    int home_end,
+    const PairStart& start,
+    int part,
     double* sums
 )
 {
-    // The center in the brick's frame, by the same additions its tile copy took.
-    Pos4<T> me = s.pos[center];
-    me.x += frame.x;
-    me.y += frame.y;
-    me.z += frame.z;
-    // A step needs no energy (its finalize uses only K); a frame's evaluation does.
-    constexpr bool kEnergy = !kKickStep;
-    CenterSums<T> c = pair_loop<T, kSmall, kMulti, kVirial, kEnergy>(s, tile, params, me, center);
+    constexpr bool kEnergy = !kKickStep;  // a step needs no energy; a frame's evaluation does
+    const bool live = start.live;
+    const int q = start.q;
+    const int center_a = home_first + 2 * q;
+    const bool has_b = live && center_a + 1 < home_end;
+    // The centers in the brick's frame, by the same additions their tile copies took.
+    Pos4<T> a = live ? s.pos[center_a] : absent_center<T>();
+    Pos4<T> b = has_b ? s.pos[center_a + 1] : absent_center<T>();
+    if (live)
+    {
+        a.x += frame.x;
+        a.y += frame.y;
+        a.z += frame.z;
+    }
+    if (has_b)
+    {
+        b.x += frame.x;
+        b.y += frame.y;
+        b.z += frame.z;
+    }
+    // The center this lane finishes: the first for lane 2k, the second for lane 2k + 1.
+    const KickInputs<T> kick =
+        load_kick<T, kKickStep, kThermostat>(s, center_a + part, part == 0 ? live : has_b);
+    CenterSums<T> ca{}, cb{};
+    if (live)
+    {
+        const int row = pair_row(home_first, blockIdx.x, q, part);
+        if constexpr (std::is_same_v<T, float> && !kMulti && !kVirial && !kEnergy)
+        {
+            step_half_list(s, tile, params, a, b, row, start.count, start.first_word,
+                           start.second_word, ca, cb);
+        }
+        else
+        {
+            half_list<T, kMulti, kVirial, kEnergy>(s, tile, params, a, b, row, start.count,
+                                                   start.first_word, start.second_word, ca,
+                                                   cb);
+        }
+    }
+    ca.fx += __shfl_xor_sync(kFullMask, ca.fx, 1);
+    ca.fy += __shfl_xor_sync(kFullMask, ca.fy, 1);
+    ca.fz += __shfl_xor_sync(kFullMask, ca.fz, 1);
+    cb.fx += __shfl_xor_sync(kFullMask, cb.fx, 1);
+    cb.fy += __shfl_xor_sync(kFullMask, cb.fy, 1);
+    cb.fz += __shfl_xor_sync(kFullMask, cb.fz, 1);
+    if (!live)
+    {
+        return;
+    }
+    if (has_b)
+    {
+        // The term between the two centers: the forces in both lanes, energy and virial once.
+        CenterSums<T> ab{};
+        add_pair_term<T, kMulti, kVirial, kEnergy>(ab, a, b, params, params[0].s2,
+                                                   s.cutoff_squared, s.num_types);
+        ca.fx += ab.fx;
+        ca.fy += ab.fy;
+        ca.fz += ab.fz;
+        cb.fx -= ab.fx;
+        cb.fy -= ab.fy;
+        cb.fz -= ab.fz;
+        if (part == 0)
+        {
+            ca.energy += T(2) * ab.energy;
+            ca.inside += T(2) * ab.inside;
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+            {
+                ca.w[k] += T(2) * ab.w[k];
+            }
+        }
+    }
     T scale = T(1);  // kJ/mol/nm per unit of the accumulated force
     double energy;
     if (kMulti)
     {
-        energy = double(c.energy);
+        energy = double(ca.energy) + double(cb.energy);
     }
     else
     {
         scale = params[0].e24;
-        energy = double(params[0].e4) * double(c.energy) - double(params[0].shift) * double(c.inside);
+        energy = double(params[0].e4) * (double(ca.energy) + double(cb.energy)) -
+                 double(params[0].shift) * (double(ca.inside) + double(cb.inside));
     }
-    const T fx = c.fx * scale, fy = c.fy * scale, fz = c.fz * scale;
-    // Each pair is listed from both ends: half of the energy and virial per end.
     if (kEnergy)
     {
         sums[0] += 0.5 * energy;
@@ -683,28 +991,18 @@ __device__ __forceinline__ void force_center(
 #pragma unroll
         for (int k = 0; k < 6; ++k)
         {
-            sums[2 + k] += 0.5 * double(c.w[k] * scale);
+            sums[2 + k] += 0.5 * (double(ca.w[k] * scale) + double(cb.w[k] * scale));
         }
     }
-    T* f = s.force + 3LL * center;
-    f[0] = fx;
-    f[1] = fy;
-    f[2] = fz;
-    if (kKickStep)
+    if (part == 0)
     {
-        const T kick = s.half_dt * s.inv_mass[center];
-        T* v = s.vel + 3LL * center;
-        const T vx = fma(kick, fx, v[0]);
-        const T vy = fma(kick, fy, v[1]);
-        const T vz = fma(kick, fz, v[2]);
-        v[0] = vx;
-        v[1] = vy;
-        v[2] = vz;
-        if (kThermostat)
-        {
-            sums[1] += 0.5 * double(s.mass[center]) *
-                       (double(vx) * vx + double(vy) * vy + double(vz) * vz);
-        }
+        finish_center<T, kKickStep, kThermostat>(s, center_a, kick, ca.fx * scale,
+                                                 ca.fy * scale, ca.fz * scale, sums);
+    }
+    else if (has_b)
+    {
+        finish_center<T, kKickStep, kThermostat>(s, center_a + 1, kick, cb.fx * scale,
+                                                 cb.fy * scale, cb.fz * scale, sums);
     }
 }
 
@@ -712,6 +1010,8 @@ __device__ __forceinline__ void force_center(
 // block's last warp adds the warps' sums in a fixed order into the block's slot of `partials`.
 // No block barrier: a warp leaves as soon as its own centers are done. `arrivals` starts at
 // zero and is made visible by a barrier before any warp arrives.
+// Only the sums in kMask (bit k for sums[k]) are reduced; the others are stored as zeros.
+template <unsigned kMask = 0xffu>
 __device__ __forceinline__ void block_partial(const double* sums, double* partials,
                                               unsigned* arrivals,
                                               double (*warp_sums)[kReduced])
@@ -720,7 +1020,7 @@ __device__ __forceinline__ void block_partial(const double* sums, double* partia
 #pragma unroll
     for (int k = 0; k < kReduced; ++k)
     {
-        const double v = warp_sum(sums[k]);
+        const double v = (kMask >> k) & 1u ? warp_sum(sums[k]) : 0.0;
         if (lane == 0)
         {
             warp_sums[warp][k] = v;
@@ -755,12 +1055,22 @@ constexpr int kFinalizeThreads = 1024;
 // One block: the fixed-order sum of the block slots into `totals`, then the scalar tail of a
 // step: the rebuild flag cleared for the next check and, for NVT, the closing half step of the
 // chain against this step's K, whose factor the next drift (or a frame read) applies.
-template <bool kThermostat, bool kStep>
+// kSums false: the force kernel reduced nothing (an NVE step without the virial), so only
+// the rebuild flag is cleared and `totals` keep their last values.
+template <bool kThermostat, bool kStep, bool kSums = true>
 __global__ void __launch_bounds__(kFinalizeThreads) finalize_kernel(const double* partials,
                                                                     int blocks, double* totals,
                                                                     double* thermo,
                                                                     index_t* rebuild)
 {
+    if constexpr (!kSums)
+    {
+        if (threadIdx.x == 0)
+        {
+            rebuild[0] = 0;  // the next step's check starts clean
+        }
+        return;
+    }
     __shared__ double warp_sums[kFinalizeThreads / kWarp][kReduced];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     double mine[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -961,8 +1271,17 @@ __device__ __forceinline__ void force_center_split(const System<T>& s,
     }
 }
 
+// Float32 steps are held to 64 registers, so four CTAs share an SM (as their shared memory
+// allows); the other forms keep the registers they need.
+template <typename T, bool kKickStep>
+constexpr int force_blocks_per_sm()
+{
+    return std::is_same_v<T, float> && kKickStep ? 4 : 1;
+}
+
 template <typename T, bool kSmall, bool kMulti, bool kVirial, bool kKickStep, bool kThermostat>
-__global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
+__global__ void __launch_bounds__(kMDThreads, force_blocks_per_sm<T, kKickStep>())
+    force_kernel(System<T> s)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
@@ -998,15 +1317,25 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
     }
     else
     {
-        const TileShape shape = stage_brick(s, blockIdx.x, s.pos, tile, start, first);
+        PairStart prefetched{};
+        const TileShape shape =
+            stage_brick(s, blockIdx.x, s.pos, tile, start, first, [&](const TileShape& planned) {
+                prefetched = pair_start(s, planned, threadIdx.x);
+            });
         if (shape.size <= s.tile_cap)
         {
-            const BrickFrame<T> frame = brick_frame(s, blockIdx.x);
-            for (int center = shape.home_first + threadIdx.x; center < shape.home_end;
-                 center += blockDim.x)
+            const BrickFrame<T> frame = brick_frame(s, shape);
+            const int lanes = (shape.home_end - shape.home_first + 1) & ~1;  // two per pair
+            for (int base = 0; base < lanes; base += blockDim.x)
             {
-                force_center<T, false, kMulti, kVirial, kKickStep, kThermostat>(
-                    s, tile, params, frame, center, sums);
+                if (base + (threadIdx.x & ~(kWarp - 1)) >= lanes)
+                {
+                    break;  // the whole warp is past the last pair
+                }
+                const int t = base + threadIdx.x;
+                const PairStart pair = base == 0 ? prefetched : pair_start(s, shape, t);
+                force_pair<T, kMulti, kVirial, kKickStep, kThermostat>(
+                    s, tile, params, frame, shape.home_first, shape.home_end, pair, t & 1, sums);
             }
         }
         else if (threadIdx.x == 0)
@@ -1014,7 +1343,17 @@ __global__ void __launch_bounds__(kMDThreads) force_kernel(System<T> s)
             flag_overflow(s.status, 2, shape.size);
         }
     }
-    block_partial(sums, s.partials, &arrivals, warp_sums);
+    // A step reduces only what its tail reads: K for NVT, the virial when asked; an NVE step
+    // without the virial reduces nothing (its finalize only clears the rebuild flag).
+    if constexpr (!kKickStep)
+    {
+        block_partial(sums, s.partials, &arrivals, warp_sums);
+    }
+    else if constexpr (kThermostat || kVirial)
+    {
+        block_partial<(kThermostat ? 0x2u : 0u) | (kVirial ? 0xfcu : 0u)>(sums, s.partials,
+                                                                          &arrivals, warp_sums);
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1358,6 +1697,7 @@ System<T> view(const nd_md_system* m)
     s.scan_temp = m->scan_temp;
     s.nbr = m->neighbors;
     s.nbr_count = m->neighbor_counts;
+    s.pair_order = m->pair_order;
     s.rebuild = m->rebuild;
     s.rebuild_count = m->rebuild_count;
     s.status = m->status;
@@ -1446,7 +1786,8 @@ int launch_force_variant(const System<T>& s, cudaStream_t stream)
         ND_CUDA_TRY(grant.allow(kernel, bytes));                                            \
         kernel<<<s.force_blocks, kMDThreads, bytes, stream>>>(s);                           \
         ND_LAUNCH_CHECK();                                                                  \
-        finalize_kernel<kThermostat, kKickStep><<<1, kFinalizeThreads, 0, stream>>>(        \
+        finalize_kernel<kThermostat, kKickStep, !kKickStep || kThermostat || kVirial>        \
+            <<<1, kFinalizeThreads, 0, stream>>>(                                           \
             s.partials, s.force_blocks, s.totals, s.thermo, s.rebuild);                     \
         ND_LAUNCH_CHECK();                                                                  \
         return ND_OK;                                                                       \

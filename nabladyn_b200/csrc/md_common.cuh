@@ -100,6 +100,7 @@ struct TileShape
     int size;
     int home_first;  // cell-order slots [home_first, home_end) are the brick's centers
     int home_end;
+    int x0, x1, y, z;  // the brick: home cells x0 <= x < x1 of row (y, z)
 };
 
 // The list stores each center's entries in chunks of kChunk uint16 indices, one 16-B word per

@@ -128,7 +128,12 @@ class Engine:
         call("nd_neighbors_scan_temp_bytes", num_cells + 1,
              _native.ctypes.cast(scan_bytes.data_ptr(), _native.c_int64_p))
         t["scan_temp"] = torch.zeros(int(scan_bytes), dtype=torch.uint8, device=device)
-        t["neighbor_counts"] = torch.zeros(n, **ints)
+        # List rows: one per atom on the small-box path; on the brick path two per center pair
+        # (the halves of the pair's list), fewer than N + 2 bricks + 2.
+        bricks = bricks_x * dims[1] * dims[2] if not small else 0
+        self.list_rows = n if small else n + 2 * bricks + 2
+        t["neighbor_counts"] = torch.zeros(self.list_rows, **ints)
+        t["pair_order"] = torch.zeros(self.list_rows // 2 + 1, **ints)
         t["rebuild"] = torch.zeros(1, **ints)
         t["rebuild_count"] = torch.zeros(1, **ints)
         t["status"] = torch.zeros(4, **ints)
@@ -162,10 +167,10 @@ class Engine:
     # -- buffers ---------------------------------------------------------------------------
 
     def _size_list(self, width: int, tile_capacity: int) -> None:
-        n = self.num_atoms
         self.width, self.tile_capacity = int(width), int(tile_capacity)
         self.tensors["neighbors"] = torch.zeros(
-            ((n + 31) // 32) * 32 * self.width, dtype=torch.uint16, device=self.device,
+            ((self.list_rows + 31) // 32) * 32 * self.width, dtype=torch.uint16,
+            device=self.device,
         )
         self.system.width = self.width
         self.system.tile_capacity = self.tile_capacity
@@ -177,7 +182,8 @@ class Engine:
             "reference_positions", "shadow_positions", "shadow_velocities",
             "shadow_inverse_masses", "shadow_masses", "shadow_images", "shadow_ids",
             "cell_counts", "cell_offsets", "atom_cell", "slots", "unordered", "order",
-            "scan_temp", "neighbors", "neighbor_counts", "rebuild", "rebuild_count", "status",
+            "scan_temp", "neighbors", "neighbor_counts", "pair_order", "rebuild", "rebuild_count",
+            "status",
             "partials", "totals", "thermostat", "sigma", "epsilon",
         ):
             setattr(s, name, ptr(t[name]))
