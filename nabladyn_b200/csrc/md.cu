@@ -412,25 +412,31 @@ __device__ __forceinline__ int pair_row(int home_first, int brick, int q, int pa
     return 2 * (home_first / 2 + brick + q) + part;
 }
 
-// Whether p lies closer than sqrt(r2max) to center a or to center b.
+// Shifts into `bits` from the right one bit: set when p lies closer than sqrt(r2max) to
+// center a or to center b. The bit is the sign of min(r2) - r2max (negative exactly when
+// r2 < r2max), taken by one funnel shift.
 template <typename T>
-__device__ __forceinline__ bool pair_hit(const Pos4<T>& a, const Pos4<T>& b, const Pos4<T>& p,
-                                         T r2max)
+__device__ __forceinline__ unsigned shift_in_hit(const Pos4<T>& a, const Pos4<T>& b,
+                                                 const Pos4<T>& p, T r2max, unsigned bits)
 {
-    return squared_norm(a.x - p.x, a.y - p.y, a.z - p.z) < r2max ||
-           squared_norm(b.x - p.x, b.y - p.y, b.z - p.z) < r2max;
+    const T ra = squared_norm(a.x - p.x, a.y - p.y, a.z - p.z);
+    const T rb = squared_norm(b.x - p.x, b.y - p.y, b.z - p.z);
+    const T d = (ra < rb ? ra : rb) - r2max;
+    return (bits << 1) | static_cast<unsigned>(d < T(0));
 }
 
 // The same test with the two centers as the halves of packed f32x2 instructions (sm_100):
 // each half rounds as the scalar test, p - x being the exact negative of x - p.
-__device__ __forceinline__ bool pair_hit(const Pos4<float>& a, const Pos4<float>& b,
-                                         const Pos4<float>& p, float r2max)
+__device__ __forceinline__ unsigned shift_in_hit(const Pos4<float>& a, const Pos4<float>& b,
+                                                 const Pos4<float>& p, float r2max,
+                                                 unsigned bits)
 {
     const float2 dx = __fadd2_rn(make_float2(p.x, p.x), make_float2(-a.x, -b.x));
     const float2 dy = __fadd2_rn(make_float2(p.y, p.y), make_float2(-a.y, -b.y));
     const float2 dz = __fadd2_rn(make_float2(p.z, p.z), make_float2(-a.z, -b.z));
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
-    return r2.x < r2max || r2.y < r2max;
+    const float d = fminf(r2.x, r2.y) - r2max;
+    return __funnelshift_l(__float_as_uint(d), bits, 1);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -546,34 +552,39 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
             const int end = start[r * per_row + column_b + 2];
             for (int word = begin; word < end; word += kWarp)
             {
+                // This half's candidates are word + part + 2 jj; candidate jj's hit ends up in
+                // bit 15 - jj.
                 const int size = end - word < kWarp ? end - word : kWarp;
-                unsigned hits = 0;
-                if (size == kWarp)
+                const int tests = (size - part + 1) / 2;
+                const Pos4<T>* candidates = tile + word + part;
+                unsigned bits = 0;
+                if (tests == kWarp / 2)
                 {
 #pragma unroll
-                    for (int j = 0; j < kWarp; j += 2)
+                    for (int jj = 0; jj < kWarp / 2; ++jj)
                     {
-                        hits |= pair_hit(a, b, tile[word + j + part], r2max) ? 1u << (j + part)
-                                                                            : 0u;
+                        bits = shift_in_hit(a, b, candidates[2 * jj], r2max, bits);
                     }
                 }
                 else
                 {
-                    for (int j = part; j < size; j += 2)
+                    for (int jj = 0; jj < tests; ++jj)
                     {
-                        hits |= pair_hit(a, b, tile[word + j], r2max) ? 1u << j : 0u;
+                        bits = shift_in_hit(a, b, candidates[2 * jj], r2max, bits);
                     }
+                    bits <<= kWarp / 2 - tests;
                 }
-                const unsigned off_a = static_cast<unsigned>(self_a - word);
-                const unsigned off_b = static_cast<unsigned>(self_b - word);
-                hits &= off_a < kWarp ? ~(1u << off_a) : ~0u;  // not the centers themselves
-                hits &= off_b < kWarp ? ~(1u << off_b) : ~0u;
-                hits = active ? hits : 0u;
-                while (hits != 0)
+                // Not the centers themselves.
+                const unsigned off_a = static_cast<unsigned>(self_a - word - part);
+                const unsigned off_b = static_cast<unsigned>(self_b - word - part);
+                bits &= off_a < kWarp && !(off_a & 1u) ? ~(0x8000u >> (off_a >> 1)) : ~0u;
+                bits &= off_b < kWarp && !(off_b & 1u) ? ~(0x8000u >> (off_b >> 1)) : ~0u;
+                bits = active ? bits : 0u;
+                while (bits != 0)
                 {
-                    const int j = __ffs(hits) - 1;
-                    hits &= hits - 1;
-                    list.add(word + j);
+                    const int top = 31 - __clz(bits);
+                    bits &= ~(1u << top);
+                    list.add(word + part + 2 * (15 - top));
                 }
             }
         }
