@@ -39,7 +39,11 @@ LENGTH = 36.77
 SIGMA, EPSILON, MASS, CUTOFF, SKIN, TIMESTEP, TEMPERATURE = 0.34, 0.996, 39.948, 1.0, 0.1, 0.004, 120.0
 WORKLOAD = "LJ argon NVE, 1,048,576 atoms (64^3-cell FCC, L=36.77 nm, rho=21.1/nm^3), fp32"
 METRIC = "atom-steps/s, 1M-atom LJ fp32 NVE"
-FORCE_KERNEL_DRAM_BYTES = 342.3e6
+# DRAM bytes (read + write) of one launch of the step's force kernel on this workload, from
+# ncu's dram__bytes_read.sum + dram__bytes_write.sum on a B200 (the pair-list kernel), and what
+# its counters say bounds it.
+FORCE_KERNEL_DRAM_BYTES = 269.7e6
+FORCE_KERNEL_LIMITER = "issue and shared-memory gathers, not HBM (ncu: issue slots and LSU wavefronts)"
 
 # Algorithmic traffic of the force kernel per atom and launch: read x (12 B) and v (12 B),
 # write F (12 B) and v (12 B), and the neighbor indices a half list needs, 58.8 x 4 B.
@@ -960,8 +964,8 @@ def run_ours(args) -> None:
     force_bytes = FORCE_BYTES_PER_ATOM * n
     achieved = force_bytes / (phase_ms[2] / 1e3) / 1e9
     step_roof_s = STEP_BYTES_PER_ATOM / (peaks["hbm_gbs"] * 1e9)
-    # dram__bytes_read.sum + dram__bytes_write.sum of one force launch at this workload
-    # (319.4 + 22.9 MB), from the ncu capture summarised in profiles/force_kernel_lj_1m.md.
+    # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this force kernel (the
+    # pair-list step kernel) at this workload, measured by ncu on a B200; see the constant.
     traffic = FORCE_KERNEL_DRAM_BYTES if n == 1_048_576 else None
 
     # e2e: the public API with host buffers: per call, the frame from pinned host memory,
@@ -1031,6 +1035,7 @@ def run_ours(args) -> None:
             "roofline": {
                 "kernel": "force_kernel (forces, second half kick, float64 tail)",
                 "bound": "hbm",
+                "limiter": FORCE_KERNEL_LIMITER,
                 "achieved": achieved,
                 "peak": peaks["hbm_gbs"],
                 "unit": "GB/s",
