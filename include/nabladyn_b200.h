@@ -244,10 +244,11 @@ typedef struct nd_md_system {
     int32_t* order;          /* [N] */
     void* scan_temp;         /* nd_neighbors_scan_temp_bytes(cells + 1) bytes */
     uint16_t* neighbors;     /* [ceil(rows / 32) * 32 * width]; rows = N when small, else
-                              * N + 2 * bricks + 2 (bricks = bricks_x * dims[1] * dims[2]):
-                              * two rows per center pair, the halves of the pair's list */
+                              * N + 2 * cells + 2: two rows per pair of centers of one cell,
+                              * the halves of the pair's list */
     int32_t* neighbor_counts; /* [rows] */
-    int32_t* pair_order;     /* [rows / 2]: each brick's center pairs, longest lists first */
+    int32_t* pair_order;     /* [2 * (rows / 2 + 1)]: per brick its center pairs, longest
+                              * lists first, as (pair, first center << 1 | has a second) */
     int32_t* rebuild;        /* [1] */
     int32_t* rebuild_count;  /* [1] */
     int32_t* status;         /* [4]: flags, most neighbors needed, largest tile needed, largest tile built */

@@ -7,8 +7,8 @@
 // and the second half kick, plus K for NVT) and programs[2] (the closing chain half step).
 //
 // Layout in HBM. The engine keeps every per-atom array in "cell order": the order of the last
-// rebuild, atoms sorted by cell and by atom id within a cell, so a cell's atoms are one
-// contiguous range. A rebuild re-sorts and permutes the state (positions, velocities, masses,
+// rebuild, atoms sorted by cell, within a cell by their 4 x 4 x 4 sub-cell in Morton order and
+// then by atom id, so a cell's atoms are one contiguous range and neighbours in it are close. A rebuild re-sorts and permutes the state (positions, velocities, masses,
 // images, ids, types); the forces are recomputed in the new order right after it. `ids` maps a
 // slot back to the caller's atom. Positions are
 // [N] x (x, y, z, type) vectors, 16 B in float32, so one load fetches an atom. Between rebuilds
@@ -401,16 +401,48 @@ __device__ __forceinline__ void flag_overflow(index_t* status, int word, int nee
     atomicMax(status + word, needed);
 }
 
-// Center pairs. On the brick path a brick's centers, cell-order slots [home_first, home_end),
-// are taken two at a time: pair q holds slots home_first + 2q and home_first + 2q + 1 (the
-// second missing when the count is odd). Pair q of brick b is P = home_first / 2 + b + q, and
-// its list has two halves, rows 2P and 2P + 1. Bricks come in cell order, so brick b's pairs
-// end at or before the next brick's first (ceil(n / 2) <= n / 2 + 1 makes up for the rounded
-// halves), and the rows of a system are fewer than N + 2 bricks + 2.
-__device__ __forceinline__ int pair_row(int home_first, int brick, int q, int part)
+// Center pairs. On the brick path a cell's atoms, cell-order slots [o, o + n), are taken two
+// at a time: pair q holds slots o + 2q and o + 2q + 1 (the second missing when n is odd), so a
+// pair never spans two cells. Pair q of cell g is P = o / 2 + g + q, and its list has two
+// halves, rows 2P and 2P + 1. Cells come in cell order, so cell g's pairs end at or before
+// cell g + 1's first (ceil(n / 2) <= n / 2 + 1 makes up for the rounded halves), and the rows
+// of a system are fewer than N + 2 cells + 2.
+__device__ __forceinline__ int cell_pair(int offset, int cell, int q)
 {
-    return 2 * (home_first / 2 + brick + q) + part;
+    return offset / 2 + cell + q;
 }
+
+// A brick's pairs: the first home cell's first pair and the count over its home cells. The
+// brick's entries of the pair order start at `first` and never reach the next brick's.
+struct BrickPairs
+{
+    int first;
+    int count;
+};
+
+template <typename T>
+__device__ __forceinline__ BrickPairs brick_pairs(const System<T>& s, const TileShape& shape,
+                                                  const int* start, const int* first)
+{
+    const int per_row = shape.cells_per_row;
+    const int home_row = 4 * per_row;
+    BrickPairs b;
+    b.first = first[home_row + 1] / 2 + shape.x0 + s.dims[0] * (shape.y + s.dims[1] * shape.z);
+    b.count = 0;
+    for (int c = 1; c < per_row - 1; ++c)
+    {
+        b.count += (start[home_row + c + 1] - start[home_row + c] + 1) / 2;
+    }
+    return b;
+}
+
+// One entry of a brick's pair order: the pair's index P and its first center's cell-order
+// slot, shifted left by one, its low bit set when the pair has a second center.
+struct PairEntry
+{
+    int pair;
+    int centers;
+};
 
 // Shifts into `bits` from the right one bit: set when p lies closer than sqrt(r2max) to
 // center a or to center b. The bit is the sign of min(r2) - r2max (negative exactly when
@@ -507,119 +539,140 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
         }
         return;
     }
-    // Pair lists. The brick's centers are taken two at a time in cell order (see pair_row);
-    // a pair's list holds every tile atom closer than the radius to either center, the two
-    // centers themselves excepted, in two halves: candidates at even and at odd offsets of a
-    // 32-candidate word. A warp builds the lists of 16 pairs (32 centers, one or two home
-    // cells): lanes 0-15 the even halves, lanes 16-31 the odd ones. Every candidate row is
-    // the x-run of tile cells around the warp's home cells, so a candidate is one broadcast
-    // read per half-warp (the two half-warps read adjacent slots) and the tests do not
-    // diverge; a lane tests its candidate against both of its centers and keeps one bit per
-    // hit in a word, then appends the word's hits.
+    // Pair lists (see cell_pair). A pair's list holds every tile atom closer than the radius
+    // to either center, the two centers themselves excepted, in two halves: candidates at even
+    // and at odd offsets of a 32-candidate word. One warp per home cell builds the lists of
+    // the cell's pairs, 16 at a time: lanes 0-15 the even halves, lanes 16-31 the odd ones.
+    // Every candidate row is the x-run of three tile cells around the home cell, so a
+    // candidate is one broadcast read per half-warp (the two half-warps read adjacent slots)
+    // and the tests do not diverge; a lane tests its candidate against both of its centers and
+    // keeps one bit per hit, then appends the word's hits.
     const int per_row = shape.cells_per_row;
     const int home_row = 4 * per_row;
-    const int home_first = shape.home_first, home_end = shape.home_end;
-    const int pairs = (home_end - home_first + 1) / 2;
-    const int tile_home = start[home_row + 1];  // the tile slot of center home_first
+    const int row_cell = shape.x0 + s.dims[0] * (shape.y + s.dims[1] * shape.z);
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     const int part = lane >> 4;
     const Pos4<T> far = far_atom<T>();
-    for (int group = warp; group * 16 < pairs; group += kWarpsPerBlock)
+    for (int c = 1 + warp; c < per_row - 1; c += kWarpsPerBlock)
     {
-        const int q = group * 16 + (lane & 15);
-        const bool active = q < pairs;
-        const int first_center = home_first + 2 * q;
-        const bool second = active && first_center + 1 < home_end;
-        const int self_a = active ? tile_home + 2 * q : -1;
-        const int self_b = second ? self_a + 1 : -1;
-        const Pos4<T> a = active ? tile[self_a] : far;
-        const Pos4<T> b = second ? tile[self_b] : far;
-        // The home cells (tile columns) of the group's first and last centers.
-        const int group_first = home_first + 32 * group;
-        const int group_last = min(group_first + 32, home_end) - 1;
-        int column_a = 1, column_b = 1;
-        for (int c = 1; c < per_row - 1; ++c)
+        const int cell = row_cell + c - 1;
+        const int offset = first[home_row + c];
+        const int tile_first = start[home_row + c];
+        const int cell_count = start[home_row + c + 1] - tile_first;
+        const int cell_pairs = (cell_count + 1) / 2;
+        for (int group = 0; group * 16 < cell_pairs; ++group)
         {
-            const int f = first[home_row + c];
-            column_a = f <= group_first ? c : column_a;
-            column_b = f <= group_last ? c : column_b;
-        }
-        const std::int64_t row = pair_row(home_first, blockIdx.x, q, part);
-        StagedListWriter list(s.nbr, lane_slots[threadIdx.x], s.width, row);
-        for (int r = 0; r < 9; ++r)
-        {
-            const int begin = start[r * per_row + column_a - 1];
-            const int end = start[r * per_row + column_b + 2];
-            for (int word = begin; word < end; word += kWarp)
+            const int q = group * 16 + (lane & 15);
+            const bool active = q < cell_pairs;
+            const bool second = active && 2 * q + 1 < cell_count;
+            const int self_a = active ? tile_first + 2 * q : -1;
+            const int self_b = second ? self_a + 1 : -1;
+            const Pos4<T> a = active ? tile[self_a] : far;
+            const Pos4<T> b = second ? tile[self_b] : far;
+            const int row = 2 * cell_pair(offset, cell, q) + part;
+            StagedListWriter list(s.nbr, lane_slots[threadIdx.x], s.width, row);
+            for (int r = 0; r < 9; ++r)
             {
-                // This half's candidates are word + part + 2 jj; candidate jj's hit ends up in
-                // bit 15 - jj.
-                const int size = end - word < kWarp ? end - word : kWarp;
-                const int tests = (size - part + 1) / 2;
-                const Pos4<T>* candidates = tile + word + part;
-                unsigned bits = 0;
-                if (tests == kWarp / 2)
+                const int begin = start[r * per_row + c - 1];
+                const int end = start[r * per_row + c + 2];
+                for (int word = begin; word < end; word += kWarp)
                 {
+                    // This half's candidates are word + part + 2 jj; candidate jj's hit ends
+                    // up in bit 15 - jj.
+                    const int size = end - word < kWarp ? end - word : kWarp;
+                    const int tests = (size - part + 1) / 2;
+                    const Pos4<T>* candidates = tile + word + part;
+                    unsigned bits = 0;
+                    if (tests == kWarp / 2)
+                    {
 #pragma unroll
-                    for (int jj = 0; jj < kWarp / 2; ++jj)
-                    {
-                        bits = shift_in_hit(a, b, candidates[2 * jj], r2max, bits);
+                        for (int jj = 0; jj < kWarp / 2; ++jj)
+                        {
+                            bits = shift_in_hit(a, b, candidates[2 * jj], r2max, bits);
+                        }
                     }
-                }
-                else
-                {
-                    for (int jj = 0; jj < tests; ++jj)
+                    else
                     {
-                        bits = shift_in_hit(a, b, candidates[2 * jj], r2max, bits);
+                        for (int jj = 0; jj < tests; ++jj)
+                        {
+                            bits = shift_in_hit(a, b, candidates[2 * jj], r2max, bits);
+                        }
+                        bits <<= kWarp / 2 - tests;
                     }
-                    bits <<= kWarp / 2 - tests;
-                }
-                // Not the centers themselves.
-                const unsigned off_a = static_cast<unsigned>(self_a - word - part);
-                const unsigned off_b = static_cast<unsigned>(self_b - word - part);
-                bits &= off_a < kWarp && !(off_a & 1u) ? ~(0x8000u >> (off_a >> 1)) : ~0u;
-                bits &= off_b < kWarp && !(off_b & 1u) ? ~(0x8000u >> (off_b >> 1)) : ~0u;
-                bits = active ? bits : 0u;
-                while (bits != 0)
-                {
-                    const int top = 31 - __clz(bits);
-                    bits &= ~(1u << top);
-                    list.add(word + part + 2 * (15 - top));
+                    // Not the centers themselves.
+                    const unsigned off_a = static_cast<unsigned>(self_a - word - part);
+                    const unsigned off_b = static_cast<unsigned>(self_b - word - part);
+                    bits &= off_a < kWarp && !(off_a & 1u) ? ~(0x8000u >> (off_a >> 1)) : ~0u;
+                    bits &= off_b < kWarp && !(off_b & 1u) ? ~(0x8000u >> (off_b >> 1)) : ~0u;
+                    bits = active ? bits : 0u;
+                    while (bits != 0)
+                    {
+                        const int top = 31 - __clz(bits);
+                        bits &= ~(1u << top);
+                        list.add(word + part + 2 * (15 - top));
+                    }
                 }
             }
-        }
-        if (active)
-        {
-            list.finish(s.sentinel);
-            s.nbr_count[row] = list.count;
-            if (list.count > s.width)
+            if (active)
             {
-                flag_overflow(s.status, 1, list.count);
+                list.finish(s.sentinel);
+                s.nbr_count[row] = list.count;
+                if (list.count > s.width)
+                {
+                    flag_overflow(s.status, 1, list.count);
+                }
             }
         }
     }
-    // The order in which the force kernel takes the pairs: longest list first (ties by q), so
-    // the lanes of a warp walk lists of about one length. The tile's memory is free now.
+    // The order in which the force kernel takes the brick's pairs: longest list first (ties
+    // by enumeration order), so the lanes of a warp walk lists of about one length. The tile's
+    // memory is free now; the pairs are enumerated cell by cell.
     __syncthreads();
+    const BrickPairs pairs = brick_pairs(s, shape, start, first);
     auto* lengths = reinterpret_cast<int*>(smem_raw);
-    const int first_pair = home_first / 2 + static_cast<int>(blockIdx.x);
-    for (int q = threadIdx.x; q < pairs; q += blockDim.x)
+    for (int k = threadIdx.x; k < pairs.count; k += blockDim.x)
     {
-        const int row = pair_row(home_first, blockIdx.x, q, 0);
+        int c = 1, q = k;
+        for (int cell_pairs; c < per_row - 1; ++c)
+        {
+            cell_pairs = (start[home_row + c + 1] - start[home_row + c] + 1) / 2;
+            if (q < cell_pairs)
+            {
+                break;
+            }
+            q -= cell_pairs;
+        }
+        const int row = 2 * cell_pair(first[home_row + c], row_cell + c - 1, q);
         const int even = s.nbr_count[row], odd = s.nbr_count[row + 1];
-        lengths[q] = even > odd ? even : odd;
+        lengths[k] = even > odd ? even : odd;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < pairs; q += blockDim.x)
+    auto* order = reinterpret_cast<PairEntry*>(s.pair_order);
+    for (int k = threadIdx.x; k < pairs.count; k += blockDim.x)
     {
-        const int mine = lengths[q];
+        const int mine = lengths[k];
         int rank = 0;
-        for (int other = 0; other < pairs; ++other)
+        for (int other = 0; other < pairs.count; ++other)
         {
             const int length = lengths[other];
-            rank += length > mine || (length == mine && other < q);
+            rank += length > mine || (length == mine && other < k);
         }
-        s.pair_order[first_pair + rank] = q;
+        int c = 1, q = k;
+        int cell_count = 0;
+        for (; c < per_row - 1; ++c)
+        {
+            cell_count = start[home_row + c + 1] - start[home_row + c];
+            if (q < (cell_count + 1) / 2)
+            {
+                break;
+            }
+            q -= (cell_count + 1) / 2;
+        }
+        const int offset = first[home_row + c];
+        PairEntry entry;
+        entry.pair = cell_pair(offset, row_cell + c - 1, q);
+        entry.centers = ((offset + 2 * q) << 1) | (2 * q + 1 < cell_count ? 1 : 0);
+        order[pairs.first + rank] = entry;
     }
 }
 
@@ -866,25 +919,34 @@ __device__ __forceinline__ void finish_center(const System<T>& s, int center,
 // tile, so a CTA's first pass loads it while the tile's copies are in flight.
 struct PairStart
 {
-    int q;
-    bool live;  // the lane has a pair
+    int row;     // this lane's half of the pair's list
+    int center;  // the pair's first center (cell-order slot)
+    bool live;   // the lane has a pair
+    bool has_b;  // the pair has a second center
     int count;
     uint4 first_word, second_word;
 };
 
+// Lane `lane_index` of a brick's CTA takes the half (lane_index & 1) of the brick's pair
+// lane_index / 2 in its longest-first order.
 template <typename T>
-__device__ __forceinline__ PairStart pair_start(const System<T>& s, const TileShape& shape,
+__device__ __forceinline__ PairStart pair_start(const System<T>& s, const BrickPairs& pairs,
                                                 int lane_index)
 {
     PairStart p;
-    const int lanes = (shape.home_end - shape.home_first + 1) & ~1;  // two per pair
-    p.live = lane_index < lanes;
-    p.q = p.live ? s.pair_order[shape.home_first / 2 + blockIdx.x + (lane_index >> 1)] : 0;
-    const int row = pair_row(shape.home_first, blockIdx.x, p.q, lane_index & 1);
-    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(row, 0, s.width);
+    p.live = lane_index < 2 * pairs.count;
+    PairEntry entry{0, 0};
+    if (p.live)
+    {
+        entry = reinterpret_cast<const PairEntry*>(s.pair_order)[pairs.first + (lane_index >> 1)];
+    }
+    p.row = 2 * entry.pair + (lane_index & 1);
+    p.center = entry.centers >> 1;
+    p.has_b = p.live && (entry.centers & 1) != 0;
+    const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(p.row, 0, s.width);
     const uint4 zero = make_uint4(0, 0, 0, 0);
     // A row holds width / 8 >= 1 words; the first two are loaded without waiting for the count.
-    p.count = p.live ? s.nbr_count[row] : 0;
+    p.count = p.live ? s.nbr_count[p.row] : 0;
     p.first_word = p.live ? chunks[0] : zero;
     p.second_word = p.live && s.width > kChunk ? chunks[kWarp] : zero;
     return p;
@@ -902,18 +964,14 @@ __device__ __forceinline__ void force_pair(
     const Pos4<T>* __restrict__ tile,
     const PairParams<T>* __restrict__ params,
     const BrickFrame<T>& frame,
-    int home_first,
-    int home_end,
     const PairStart& start,
     int part,
     double* sums
 )
 {
     constexpr bool kEnergy = !kKickStep;  // a step needs no energy; a frame's evaluation does
-    const bool live = start.live;
-    const int q = start.q;
-    const int center_a = home_first + 2 * q;
-    const bool has_b = live && center_a + 1 < home_end;
+    const bool live = start.live, has_b = start.has_b;
+    const int center_a = start.center;
     // The centers in the brick's frame, by the same additions their tile copies took.
     Pos4<T> a = live ? s.pos[center_a] : absent_center<T>();
     Pos4<T> b = has_b ? s.pos[center_a + 1] : absent_center<T>();
@@ -935,7 +993,7 @@ __device__ __forceinline__ void force_pair(
     CenterSums<T> ca{}, cb{};
     if (live)
     {
-        const int row = pair_row(home_first, blockIdx.x, q, part);
+        const int row = start.row;
         if constexpr (std::is_same_v<T, float> && !kMulti && !kVirial && !kEnergy)
         {
             step_half_list(s, tile, params, a, b, row, start.count, start.first_word,
@@ -1329,14 +1387,16 @@ __global__ void __launch_bounds__(kMDThreads, force_blocks_per_sm<T, kKickStep>(
     else
     {
         PairStart prefetched{};
+        BrickPairs pairs{0, 0};
         const TileShape shape =
             stage_brick(s, blockIdx.x, s.pos, tile, start, first, [&](const TileShape& planned) {
-                prefetched = pair_start(s, planned, threadIdx.x);
+                pairs = brick_pairs(s, planned, start, first);
+                prefetched = pair_start(s, pairs, threadIdx.x);
             });
         if (shape.size <= s.tile_cap)
         {
             const BrickFrame<T> frame = brick_frame(s, shape);
-            const int lanes = (shape.home_end - shape.home_first + 1) & ~1;  // two per pair
+            const int lanes = 2 * pairs.count;
             for (int base = 0; base < lanes; base += blockDim.x)
             {
                 if (base + (threadIdx.x & ~(kWarp - 1)) >= lanes)
@@ -1344,9 +1404,9 @@ __global__ void __launch_bounds__(kMDThreads, force_blocks_per_sm<T, kKickStep>(
                     break;  // the whole warp is past the last pair
                 }
                 const int t = base + threadIdx.x;
-                const PairStart pair = base == 0 ? prefetched : pair_start(s, shape, t);
-                force_pair<T, kMulti, kVirial, kKickStep, kThermostat>(
-                    s, tile, params, frame, shape.home_first, shape.home_end, pair, t & 1, sums);
+                const PairStart pair = base == 0 ? prefetched : pair_start(s, pairs, t);
+                force_pair<T, kMulti, kVirial, kKickStep, kThermostat>(s, tile, params, frame,
+                                                                       pair, t & 1, sums);
             }
         }
         else if (threadIdx.x == 0)
@@ -1494,7 +1554,7 @@ __global__ void place_kernel(System<T> s, int gated)
     s.cell_counts[cell] = 0;
 }
 
-// One warp per cell: rank each atom by its id among the cell's atoms; order[new] = old slot.
+// One warp per cell: rank each atom by its key among the cell's atoms; order[new] = old slot.
 template <typename T>
 __global__ void order_kernel(System<T> s, std::int64_t num_cells, int gated)
 {
@@ -1507,20 +1567,39 @@ __global__ void order_kernel(System<T> s, std::int64_t num_cells, int gated)
     }
     const index_t begin = s.cell_offsets[cell];
     const index_t count = s.cell_offsets[cell + 1] - begin;
+    // The key: the atom's 4 x 4 x 4 sub-cell in Morton order, then its id, so consecutive
+    // atoms of a cell are close and the engine's center pairs are tight.
+    const index_t nx = s.dims[0], ny = s.dims[1];
+    const T origin[3] = {T(cell % nx) * s.widths[0], T((cell / nx) % ny) * s.widths[1],
+                         T(cell / (static_cast<std::int64_t>(nx) * ny)) * s.widths[2]};
+    auto key_of = [&](index_t slot) -> unsigned long long {
+        const Pos4<T> p = s.pos[slot];
+        const T c[3] = {p.x, p.y, p.z};
+        unsigned code = 0;
+        for (int a = 0; a < 3; ++a)
+        {
+            int q = static_cast<int>((c[a] - origin[a]) * (T(4) / s.widths[a]));
+            q = q < 0 ? 0 : (q > 3 ? 3 : q);
+            code |= (q & 1u) << a;
+            code |= ((q >> 1) & 1u) << (3 + a);
+        }
+        return (static_cast<unsigned long long>(code) << 32) |
+               static_cast<unsigned>(s.ids[slot]);
+    };
     for (index_t mine = 0; mine < count; mine += kWarp)
     {
         const bool active = mine + lane < count;
         const index_t old = active ? s.unordered[begin + mine + lane] : 0;
-        const index_t id = active ? s.ids[old] : 0;
+        const unsigned long long key = active ? key_of(old) : 0;
         index_t rank = 0;
         for (index_t base = 0; base < count; base += kWarp)
         {
-            const index_t other =
-                base + lane < count ? s.ids[s.unordered[begin + base + lane]] : 0x7fffffff;
+            const unsigned long long other =
+                base + lane < count ? key_of(s.unordered[begin + base + lane]) : ~0ull;
             const int valid = count - base < kWarp ? count - base : kWarp;
             for (int t = 0; t < valid; ++t)
             {
-                rank += __shfl_sync(kFullMask, other, t) < id;
+                rank += __shfl_sync(kFullMask, other, t) < key;
             }
         }
         if (active)

@@ -129,11 +129,11 @@ class Engine:
              _native.ctypes.cast(scan_bytes.data_ptr(), _native.c_int64_p))
         t["scan_temp"] = torch.zeros(int(scan_bytes), dtype=torch.uint8, device=device)
         # List rows: one per atom on the small-box path; on the brick path two per center pair
-        # (the halves of the pair's list), fewer than N + 2 bricks + 2.
-        bricks = bricks_x * dims[1] * dims[2] if not small else 0
-        self.list_rows = n if small else n + 2 * bricks + 2
+        # (the halves of the pair's list; pairs never span two cells), fewer than
+        # N + 2 cells + 2. The pair order holds two int32 per pair.
+        self.list_rows = n if small else n + 2 * math.prod(dims) + 2
         t["neighbor_counts"] = torch.zeros(self.list_rows, **ints)
-        t["pair_order"] = torch.zeros(self.list_rows // 2 + 1, **ints)
+        t["pair_order"] = torch.zeros(2 * (self.list_rows // 2 + 1), **ints)
         t["rebuild"] = torch.zeros(1, **ints)
         t["rebuild_count"] = torch.zeros(1, **ints)
         t["status"] = torch.zeros(4, **ints)
