@@ -630,6 +630,7 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
     __syncthreads();
     const BrickPairs pairs = brick_pairs(s, shape, start, first);
     auto* lengths = reinterpret_cast<int*>(smem_raw);
+    int longest = 0;
     for (int k = threadIdx.x; k < pairs.count; k += blockDim.x)
     {
         int c = 1, q = k;
@@ -645,6 +646,20 @@ __global__ void __launch_bounds__(kMDThreads) build_list_kernel(System<T> s, int
         const int row = 2 * cell_pair(first[home_row + c], row_cell + c - 1, q);
         const int even = s.nbr_count[row], odd = s.nbr_count[row + 1];
         lengths[k] = even > odd ? even : odd;
+        if (s.width == kChunk)
+        {
+            // The sizing build (the smallest width): status[1] gets the longest whole pair
+            // list, the bound a half can reach once the pair's centers drift apart.
+            longest = even + odd > longest ? even + odd : longest;
+        }
+    }
+    if (s.width == kChunk)
+    {
+        longest = __reduce_max_sync(kFullMask, longest);
+        if (lane == 0 && longest > 0)
+        {
+            atomicMax(s.status + 1, longest);
+        }
     }
     __syncthreads();
     auto* order = reinterpret_cast<PairEntry*>(s.pair_order);

@@ -5,8 +5,10 @@ tensors on the model's device, loads a frame, and launches rebuilds, force evalu
 steps on torch's current stream, so a step can be captured in a CUDA Graph.
 
 Sizing follows the reference's capacity rule (src/nabladyn/neighbors/_neighbor_list.py:
-256-261) with its own units: a first build with the smallest list counts the most neighbors any
-atom has and the largest brick tile; the list then gets ``capacity_multiplier`` times each.
+256-261) with its own units: a first build with the smallest list counts the longest list (on
+the brick path the longest whole list of a pair of centers, which either half of a pair's list
+can approach once the pair's centers drift apart) and the largest brick tile; the list then
+gets ``capacity_multiplier`` times each.
 A later frame that needs more sets the overflow bit, and the run fails at its next status read,
 as the reference's does.
 """
@@ -226,7 +228,8 @@ class Engine:
             width = max(8, -(-width // 8) * 8)
             # A tile sums thousands of atoms over tens of cells, so its count fluctuates by
             # about a percent in a liquid: it gets a quarter of the multiplier's margin plus
-            # 64 slots (the list width, a per-atom count, gets the whole margin).
+            # 64 slots (the list width, a count of a few atoms' neighbours, gets the whole
+            # margin).
             tile_margin = 1.0 + (self.capacity_multiplier - 1.0) / 4
             tile = min(self.tile_limit, math.ceil(tile_margin * needed_tile) + 64)
             self._size_list(width, tile)
@@ -373,7 +376,7 @@ class Engine:
         if flags & OVERFLOW:
             if neighbors > self.width:
                 causes.append(
-                    f"the neighbor capacity {self.width} per atom is too small: an atom has "
+                    f"the neighbor capacity {self.width} per list is too small: a list needs "
                     f"{neighbors} neighbors within {self.radius} nm; raise capacity_multiplier",
                 )
             if tile > self.tile_capacity:
