@@ -270,3 +270,35 @@ def test_run_writes_sample_file(argon, cuda, monkeypatch, tmp_path):
             np.testing.assert_array_equal(data[name], values.numpy(), err_msg=name)
     assert attributes["ensemble"] == "NVT" and attributes["timestep"] == 0.004
     assert attributes["cutoff"] == 1.0 and attributes["schema"] == "nabladyn.samples"
+
+
+def test_melting_lattice_keeps_its_pair_lists(cuda):
+    """A jittered simple-cubic start melting at 150 K on the brick path (the serving workload's
+    kind of replica): the pairs of centers drift apart as the lattice melts, and their lists
+    must keep fitting the capacity sized on the first frame. 500 NVT steps run without a
+    failure, and the last frame's forces match the oracle's."""
+    from nabladyn_b200.serving import serving_requests
+
+    request = next(r for r in serving_requests(64, seed=11) if 3000 <= r.positions.shape[0] <= 9000)
+    n = request.positions.shape[0]
+    model = potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64, device=cuda),
+        sigma=torch.tensor([0.34], device=cuda), epsilon=torch.tensor([0.996], device=cuda),
+        cutoff=1.0,
+    )
+    simulation = md.nvt(
+        model, torch.tensor(request.positions, dtype=torch.float32, device=cuda),
+        torch.tensor(request.velocities, dtype=torch.float32, device=cuda),
+        torch.full((n,), 39.948, device=cuda),
+        torch.tensor(request.cell, dtype=torch.float32, device=cuda), timestep=0.004,
+        temperature=150.0, thermostat_timescale=0.1)
+    assert not simulation._engine.small
+    simulation.run(500)
+    state = simulation.state()
+    assert simulation._rebuild_count >= 5
+    cell = request.cell.astype(np.float64)
+    x = on.wrap(state.positions.cpu().double().numpy(), cell)
+    first, second, _ = on.pairs(x, cell, 1.0)
+    _, f64, _ = lj.energy_force_virial(x, cell, first, second, [0.34], [0.996], 1.0)
+    error = np.linalg.norm(state.forces.cpu().double().numpy() - f64) / np.linalg.norm(f64)
+    assert error < 1e-5
