@@ -268,9 +268,36 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
     __syncthreads();
 }
 
-// Forces at the current positions; with `kick`, also the second half kick, returning the
-// thread's part of K (float64); always the thread's part of E.
-template <bool kKick>
+// One list entry's pair term, added to the center's sums (an exact zero outside the cutoff).
+template <bool kEnergy>
+__device__ __forceinline__ void serve_pair(const ReplicaScalars& r, const Pos4<float>& me,
+                                           const Pos4<float>& p, float& fx, float& fy, float& fz,
+                                           float& esum, float& inside_count)
+{
+    const float dx = min_image(me.x, p.x, r.cell[0]);
+    const float dy = min_image(me.y, p.y, r.cell[1]);
+    const float dz = min_image(me.z, p.z, r.cell[2]);
+    const float r2 = squared_norm(dx, dy, dz);
+    const float mask = r2 < r.cutoff_squared ? 1.0f : 0.0f;
+    const float inv_r2 = fast_reciprocal(r2);
+    const float q = r.lj.s2 * inv_r2;
+    const float p6 = q * q * q;
+    const float fs = mask * (inv_r2 * (p6 * fmaf(2.0f, p6, -1.0f)));
+    if (kEnergy)
+    {
+        esum = fmaf(mask, fmaf(p6, p6, -p6), esum);
+        inside_count += mask;
+    }
+    fx = fmaf(fs, dx, fx);
+    fy = fmaf(fs, dy, fy);
+    fz = fmaf(fs, dz, fz);
+}
+
+// Forces at the current positions; with `kKick`, also the second half kick, returning the
+// thread's part of K (float64); with `kEnergy`, the thread's part of E (a step needs E only
+// when its energy is reported: the last step of a round). Whole chunks of the list go through
+// without a bound check; only the last, partial chunk checks the count.
+template <bool kKick, bool kEnergy>
 __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, float* vel,
                                float* force, const float* mass, const float* inv_mass,
                                const std::uint16_t* nbr, const index_t* nbr_count,
@@ -282,38 +309,39 @@ __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, 
         const int count = nbr_count[i] < r.width ? nbr_count[i] : r.width;
         const uint4* chunks = reinterpret_cast<const uint4*>(nbr) + chunk_index(i, 0, r.width);
         float fx = 0, fy = 0, fz = 0, esum = 0, inside_count = 0;
-        for (int chunk = 0; chunk * kChunk < count; ++chunk)
+        const int full = count / kChunk;
+        for (int chunk = 0; chunk < full; ++chunk)
         {
             const uint4 word = chunks[static_cast<std::int64_t>(chunk) * kWarp];
             const unsigned packed[4] = {word.x, word.y, word.z, word.w};
 #pragma unroll
             for (int k = 0; k < kChunk; ++k)
             {
-                if (chunk * kChunk + k >= count)
-                {
-                    break;
-                }
                 const Pos4<float> p = pos[(packed[k / 2] >> (16 * (k % 2))) & 0xffffu];
-                const float dx = min_image(me.x, p.x, r.cell[0]);
-                const float dy = min_image(me.y, p.y, r.cell[1]);
-                const float dz = min_image(me.z, p.z, r.cell[2]);
-                const float r2 = squared_norm(dx, dy, dz);
-                const float mask = r2 < r.cutoff_squared ? 1.0f : 0.0f;
-                const float inv_r2 = fast_reciprocal(r2);
-                const float q = r.lj.s2 * inv_r2;
-                const float p6 = q * q * q;
-                const float fs = mask * (inv_r2 * (p6 * fmaf(2.0f, p6, -1.0f)));
-                esum = fmaf(mask, fmaf(p6, p6, -p6), esum);
-                inside_count += mask;
-                fx = fmaf(fs, dx, fx);
-                fy = fmaf(fs, dy, fy);
-                fz = fmaf(fs, dz, fz);
+                serve_pair<kEnergy>(r, me, p, fx, fy, fz, esum, inside_count);
+            }
+        }
+        if (full * kChunk < count)
+        {
+            const uint4 word = chunks[static_cast<std::int64_t>(full) * kWarp];
+            const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+            for (int k = 0; k < kChunk; ++k)
+            {
+                if (full * kChunk + k < count)
+                {
+                    const Pos4<float> p = pos[(packed[k / 2] >> (16 * (k % 2))) & 0xffffu];
+                    serve_pair<kEnergy>(r, me, p, fx, fy, fz, esum, inside_count);
+                }
             }
         }
         fx *= r.lj.e24;
         fy *= r.lj.e24;
         fz *= r.lj.e24;
-        energy += 0.5 * (double(r.lj.e4) * esum - double(r.lj.shift) * inside_count);
+        if (kEnergy)
+        {
+            energy += 0.5 * (double(r.lj.e4) * esum - double(r.lj.shift) * inside_count);
+        }
         float* f = force + 3LL * i;
         f[0] = fx;
         f[1] = fy;
@@ -393,7 +421,8 @@ __global__ void __launch_bounds__(kServeThreads) serve_kernel(ServePool p, const
         rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start, counts,
                         warp_totals, &flags);
         double kinetic = 0, energy = 0;
-        replica_forces<false>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, kinetic, energy);
+        replica_forces<false, true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, kinetic,
+                                    energy);
         energy = block_sum(energy, warp_sums);
         if (threadIdx.x == 0)
         {
@@ -475,12 +504,28 @@ __global__ void __launch_bounds__(kServeThreads) serve_kernel(ServePool p, const
             }
         }
         double kinetic = 0, energy = 0;
-        replica_forces<true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, kinetic, energy);
+        const bool reported = done + 1 == budget;  // the round's last step reports its energy
+        if (reported)
+        {
+            replica_forces<true, true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count,
+                                       kinetic, energy);
+        }
+        else
+        {
+            replica_forces<true, false>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count,
+                                        kinetic, energy);
+        }
         kinetic = block_sum(kinetic, warp_sums);
-        energy = block_sum(energy, warp_sums);
+        if (reported)
+        {
+            energy = block_sum(energy, warp_sums);
+        }
         if (threadIdx.x == 0)
         {
-            last_energy = energy;
+            if (reported)
+            {
+                last_energy = energy;
+            }
             // The closing chain half step against this step's K.
             double q[3], pc[3];
             for (int k = 0; k < 3; ++k)
