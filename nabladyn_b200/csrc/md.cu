@@ -353,8 +353,15 @@ __device__ __forceinline__ TileShape stage_brick(
         shape.size = s.tile_cap + 1;
         return shape;
     }
-    // Each cell's image shift plus the brick's frame, one warp per cell that moves.
+    // Each cell's image shift plus the brick's frame, one warp per cell that moves. A brick
+    // whose tile crosses no periodic face has no shift at all (its frame is zero too): it
+    // skips the loop, a block-uniform decision.
     const BrickFrame<T> frame = brick_frame(s, shape);
+    const bool inside = x0 > 0 && x1 < nx && y > 0 && y < ny - 1 && z > 0 && z < nz - 1;
+    if (inside)
+    {
+        return shape;  // no barrier is needed: nothing was written after the copies landed
+    }
     int r = 0, c = warp;  // tile cell t = r * per_row + c, stepped without a division
     while (c >= per_row)
     {
