@@ -261,14 +261,18 @@ __device__ __forceinline__ TileShape stage_brick(
     }
     __syncthreads();
     const int warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    // Exclusive scan of the counts by the first warp.
+    // Exclusive scan of the counts by the first warp, which also counts the home cells' pairs.
+    __shared__ int home_pairs;
+    const int home_row = 4 * per_row;
     if (warp == 0)
     {
         int carry = 0;
+        int pairs = 0;
         for (int base = 0; base < cells; base += kWarp)
         {
             const int t = base + lane;
             const int count = t < cells ? start[t] : 0;
+            pairs += t > home_row && t < home_row + per_row - 1 ? (count + 1) / 2 : 0;
             int inclusive = count;
 #pragma unroll
             for (int offset = 1; offset < kWarp; offset *= 2)
@@ -282,20 +286,22 @@ __device__ __forceinline__ TileShape stage_brick(
             }
             carry += __shfl_sync(kFullMask, inclusive, kWarp - 1);
         }
+        pairs = __reduce_add_sync(kFullMask, pairs);
         if (lane == 0)
         {
             start[cells] = carry;
+            home_pairs = pairs;
         }
     }
     __syncthreads();
     TileShape shape;
     shape.cells_per_row = per_row;
     shape.size = start[cells];
+    shape.pairs = home_pairs;
     shape.x0 = x0;
     shape.x1 = x1;
     shape.y = y;
     shape.z = z;
-    const int home_row = 4 * per_row;
     shape.home_first = first[home_row + 1];
     shape.home_end = first[home_row + per_row - 2] + (start[home_row + per_row - 1] -
                                                       start[home_row + per_row - 2]);
@@ -431,15 +437,10 @@ template <typename T>
 __device__ __forceinline__ BrickPairs brick_pairs(const System<T>& s, const TileShape& shape,
                                                   const int* start, const int* first)
 {
-    const int per_row = shape.cells_per_row;
-    const int home_row = 4 * per_row;
     BrickPairs b;
-    b.first = first[home_row + 1] / 2 + shape.x0 + s.dims[0] * (shape.y + s.dims[1] * shape.z);
-    b.count = 0;
-    for (int c = 1; c < per_row - 1; ++c)
-    {
-        b.count += (start[home_row + c + 1] - start[home_row + c] + 1) / 2;
-    }
+    b.first = first[4 * shape.cells_per_row + 1] / 2 + shape.x0 +
+              s.dims[0] * (shape.y + s.dims[1] * shape.z);
+    b.count = shape.pairs;
     return b;
 }
 

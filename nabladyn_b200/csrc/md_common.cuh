@@ -101,6 +101,7 @@ struct TileShape
     int home_first;  // cell-order slots [home_first, home_end) are the brick's centers
     int home_end;
     int x0, x1, y, z;  // the brick: home cells x0 <= x < x1 of row (y, z)
+    int pairs;         // center pairs of the home cells (two per pair, none across cells)
 };
 
 // The list stores each center's entries in chunks of kChunk uint16 indices, one 16-B word per
