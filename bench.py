@@ -42,7 +42,7 @@ METRIC = "atom-steps/s, 1M-atom LJ fp32 NVE"
 # DRAM bytes (read + write) of one launch of the step's force kernel on this workload, from
 # ncu's dram__bytes_read.sum + dram__bytes_write.sum on a B200 (the pair-list kernel), and what
 # its counters say bounds it.
-FORCE_KERNEL_DRAM_BYTES = 269.7e6
+FORCE_KERNEL_DRAM_BYTES = 275.7e6
 FORCE_KERNEL_LIMITER = "issue and shared-memory gathers, not HBM (ncu: issue slots and LSU wavefronts)"
 
 # Algorithmic traffic of the force kernel per atom and launch: read x (12 B) and v (12 B),
