@@ -262,17 +262,24 @@ __global__ void __launch_bounds__(kTile, 6) pair_forward_kernel(PairPass a)
     float4* m4 = reinterpret_cast<float4*>(a.m);
     __shared__ int tile_first[kTile];
 
+    // Each tile's pair records are loaded one tile ahead, so their latency hides behind the
+    // previous tile's products.
+    int2 next_ab = make_int2(0, 0);
+    float4 next_g = make_float4(0.f, 0.f, 0.f, 1.f);
+    if (blockIdx.x * kTile + static_cast<int>(threadIdx.x) < count)
+    {
+        next_ab = a.pairs[blockIdx.x * kTile + threadIdx.x];
+        next_g = a.geometry[blockIdx.x * kTile + threadIdx.x];
+    }
     for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
     {
         const int p = tile * kTile + threadIdx.x;
         const bool live = p < count;
-        int2 ab = make_int2(0, 0);
-        float4 g = make_float4(0.f, 0.f, 0.f, 1.f);
-        if (live)
-        {
-            ab = a.pairs[p];
-            g = a.geometry[p];
-        }
+        const int2 ab = next_ab;
+        const float4 g = next_g;
+        const int ahead = p + gridDim.x * kTile;
+        next_ab = ahead < count ? a.pairs[ahead] : make_int2(0, 0);
+        next_g = ahead < count ? a.geometry[ahead] : make_float4(0.f, 0.f, 0.f, 1.f);
         const float envelope = live ? 0.5f * (__cosf(g.w * a.phase) + 1.0f) : 0.0f;
         tile_first[threadIdx.x] = live ? ab.x : -1;
         cores.tile_index = tile;
@@ -392,17 +399,23 @@ __global__ void __launch_bounds__(kTile, 4) pair_reverse_kernel(PairPass a)
     __shared__ int tile_first[kTile];
     double w[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
 
+    // Each tile's pair records are loaded one tile ahead (see pair_forward_kernel).
+    int2 next_ab = make_int2(0, 0);
+    float4 next_g = make_float4(0.f, 0.f, 0.f, 1.f);
+    if (blockIdx.x * kTile + static_cast<int>(threadIdx.x) < count)
+    {
+        next_ab = a.pairs[blockIdx.x * kTile + threadIdx.x];
+        next_g = a.geometry[blockIdx.x * kTile + threadIdx.x];
+    }
     for (int tile = blockIdx.x; tile * kTile < count; tile += gridDim.x)
     {
         const int p = tile * kTile + threadIdx.x;
         const bool live = p < count;
-        int2 ab = make_int2(0, 0);
-        float4 g = make_float4(0.f, 0.f, 0.f, 1.f);
-        if (live)
-        {
-            ab = a.pairs[p];
-            g = a.geometry[p];
-        }
+        const int2 ab = next_ab;
+        const float4 g = next_g;
+        const int ahead = p + gridDim.x * kTile;
+        next_ab = ahead < count ? a.pairs[ahead] : make_int2(0, 0);
+        next_g = ahead < count ? a.geometry[ahead] : make_float4(0.f, 0.f, 0.f, 1.f);
         float sine, cosine;
         __sincosf(g.w * a.phase, &sine, &cosine);
         const float envelope = live ? 0.5f * (cosine + 1.0f) : 0.0f;
