@@ -1978,16 +1978,24 @@ std::int64_t step_launches(const nd_md_system* m)
 // A small box's step is a few microseconds of work spread over six launches (drift, the three
 // gated rebuild launches, forces, finalize), so the launches bound it. Here one cluster of up
 // to kRunCluster CTAs runs `steps` steps back to back, each CTA owning a contiguous range of
-// atoms, the phases separated by cluster barriers (release/acquire at cluster scope), on the
-// same arrays and with the same arithmetic as those kernels: the chain's opening half step
-// and the drift with the reuse check; on a rebuild the wrap and each CTA's centers' lists over
-// all atoms; the forces with the second half kick (each atom's list over kSmallLanes lanes);
-// the CTAs' float64 E and K summed in CTA order, then the chain's closing half step. Every CTA
-// keeps the chain's state and closes it from the same sums (CTA 0 stores it), and the reuse
-// flag carries the step's stamp instead of being cleared, so a step needs two cluster barriers
-// (three with a rebuild). Every branch around a cluster barrier is decided from values all
-// CTAs read after the same barrier, so every CTA takes the same barriers. A failure (a status
-// bit) stops the rebuilds, as in the per-step path; the host reads it.
+// atoms, the phases separated by cluster barriers (release/acquire at cluster scope), with the
+// same arithmetic as those kernels: the chain's opening half step and the drift with the reuse
+// check; on a rebuild the wrap and each CTA's centers' lists over all atoms; the forces with
+// the second half kick (each atom's list over kSmallLanes lanes); the CTAs' float64 E and K
+// summed in CTA order, then the chain's closing half step.
+//
+// A step is bound by latency, not by work (a few thousand pair terms per SM), so nothing of it
+// goes through global memory: every CTA holds the whole system's positions in its shared
+// memory and the owner of an atom writes its new position into every CTA's copy (distributed
+// shared memory); the reuse and failure flags and the E and K partials travel the same way,
+// each CTA writing its own slot in every CTA. The CTA's centers' lists live in its shared
+// memory when they fit, else in the global list. The state (positions, velocities, forces,
+// references, lists, chain, totals) is loaded at the start and stored at the end; only the
+// rare events (a wrap's image crossings, a failure's status bits) write global memory on the
+// way. Every CTA keeps the chain's state and closes it from the same sums, so a step needs
+// two cluster barriers (three with a rebuild). Every branch around a cluster barrier is decided
+// from values all CTAs read after the same barrier, so every CTA takes the same barriers. A
+// failure (a status bit) stops the rebuilds, as in the per-step path; the host reads it.
 
 constexpr int kRunThreads = 512;
 constexpr int kRunMaxAtoms = 4096;
@@ -1999,26 +2007,75 @@ __device__ __forceinline__ void cluster_barrier()
                  "barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
+// The address of `local` (this CTA's shared memory) in CTA `rank` of the cluster.
+template <typename V>
+__device__ __forceinline__ V* cluster_peer(V* local, unsigned rank)
+{
+    unsigned long long remote;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(remote) : "l"(local), "r"(rank));
+    return reinterpret_cast<V*>(remote);
+}
+
+// One center's list on the small-box path by a whole warp, 32 candidates a round: the hits of a
+// round are ranked by ballot, so the list holds them in ascending index order, as the per-step
+// build's scan of all atoms stores them; a partial last chunk is padded with the sentinel.
+// `entry(e)` is the list's e-th slot. Returns the count (entries past the width not stored).
+template <typename T, typename Entry>
+__device__ __forceinline__ int warp_center_list(const System<T>& s,
+                                                const Pos4<T>* __restrict__ tile, int center,
+                                                Entry&& entry)
+{
+    const int lane = threadIdx.x % kWarp;
+    const Pos4<T> c = tile[center];
+    const T r2max = s.radius_squared;
+    int count = 0;
+    for (int base = 0; base < s.n; base += kWarp)
+    {
+        const int k = base + lane;
+        bool hit = false;
+        if (k < s.n && k != center)
+        {
+            const Pos4<T> p = tile[k];
+            const T dx = min_image(c.x, p.x, s.length[0]);
+            const T dy = min_image(c.y, p.y, s.length[1]);
+            const T dz = min_image(c.z, p.z, s.length[2]);
+            hit = squared_norm(dx, dy, dz) < r2max;
+        }
+        const unsigned hits = __ballot_sync(kFullMask, hit);
+        const int e = count + __popc(hits & ((1u << lane) - 1u));
+        if (hit && e < s.width)
+        {
+            *entry(e) = static_cast<std::uint16_t>(k);
+        }
+        count += __popc(hits);
+    }
+    const int stored = count < s.width ? count : s.width;
+    const int padded = (stored + kChunk - 1) / kChunk * kChunk;
+    if (stored + lane < padded)
+    {
+        *entry(stored + lane) = static_cast<std::uint16_t>(s.sentinel);
+    }
+    return count;
+}
+
 // One center's pair loop on the small-box path, its lanes' sums met in force_center_split's
-// shuffle tree and with its arithmetic, the list's first word loaded with its length; returns
-// the force (lane `part` 0 only) and adds half the pair energy to `energy`.
+// shuffle tree and with its arithmetic; chunk c of its list is chunks[c * stride], `count` its
+// length. Returns the force (lane `part` 0 only) and adds half the pair energy to `energy`.
 template <typename T, bool kMulti>
 __device__ __forceinline__ void run_center_forces(const System<T>& s,
                                                   const Pos4<T>* __restrict__ tile,
                                                   const PairParams<T>* __restrict__ params,
-                                                  int center, int part, T (&force)[3],
-                                                  double& energy)
+                                                  const uint4* __restrict__ chunks, int stride,
+                                                  int count, int center, int part,
+                                                  T (&force)[3], double& energy)
 {
     CenterSums<T> c{};
     const bool real = center < s.n;
     const Pos4<T> me = real ? tile[center] : far_atom<T>();
     if (real)
     {
-        const uint4* chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
         const int stored_chunks = s.width / kChunk;
-        uint4 next = part < stored_chunks ? chunks[static_cast<std::int64_t>(part) * kWarp]
-                                          : make_uint4(0, 0, 0, 0);
-        const int count = s.nbr_count[center];
+        uint4 next = part < stored_chunks ? chunks[part * stride] : make_uint4(0, 0, 0, 0);
         const int used = count < s.width ? count : s.width;
         const int num_chunks = (used + kChunk - 1) / kChunk;
         const T cutoff_squared = s.cutoff_squared;
@@ -2028,7 +2085,7 @@ __device__ __forceinline__ void run_center_forces(const System<T>& s,
             const uint4 word = next;
             if (chunk + kSmallLanes < num_chunks)
             {
-                next = chunks[static_cast<std::int64_t>(chunk + kSmallLanes) * kWarp];
+                next = chunks[(chunk + kSmallLanes) * stride];
             }
             const unsigned packed[4] = {word.x, word.y, word.z, word.w};
 #pragma unroll
@@ -2098,7 +2155,21 @@ __device__ __forceinline__ void run_center_forces(const System<T>& s,
     energy += 0.5 * e;
 }
 
-template <typename T, bool kMulti, bool kThermostat>
+// The dynamic shared memory of a one-launch run: every atom's position (slots 0 .. sentinel),
+// then, with the lists in shared memory, `centers` lists of `width` entries and their counts.
+template <typename T>
+std::size_t run_shared_bytes(const System<T>& s, int centers, bool shared_lists)
+{
+    std::size_t bytes = static_cast<std::size_t>(s.sentinel + 1) * sizeof(Pos4<T>);
+    if (shared_lists)
+    {
+        bytes += static_cast<std::size_t>(centers) * s.width * sizeof(std::uint16_t);
+        bytes += static_cast<std::size_t>(centers) * sizeof(int);
+    }
+    return bytes;
+}
+
+template <typename T, bool kMulti, bool kThermostat, bool kSharedLists>
 __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int steps)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -2107,7 +2178,12 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     __shared__ double warp_sums[kRunThreads / kWarp][2];
     __shared__ T forces[kRunThreads][3];  // this step's force on each owned atom
     __shared__ T scales[2];
-    __shared__ int rebuild;
+    __shared__ double thermo[kThermoSize];  // the chain's slots, stored at the end
+    // Written by CTA r into slot r of every CTA: its E and K; the stamp (step + 1) of a step in
+    // which one of its atoms moved past the reuse threshold; whether it saw a failure.
+    __shared__ double partials[kRunCluster][2];
+    __shared__ int moved[kRunCluster];
+    __shared__ int failed[kRunCluster];
     const int rows = s.num_types * (s.num_types + 1) / 2;
     for (int k = threadIdx.x; k < rows; k += blockDim.x)
     {
@@ -2118,6 +2194,10 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     const int rank = blockIdx.x;  // the grid is one cluster
     const int first = static_cast<int>(static_cast<std::int64_t>(n) * rank / ctas);
     const int last = static_cast<int>(static_cast<std::int64_t>(n) * (rank + 1) / ctas);
+    const int centers = last - first;
+    const int words = s.width / kChunk;  // chunks per list
+    auto* lists = reinterpret_cast<std::uint16_t*>(tile + s.sentinel + 1);
+    auto* counts = reinterpret_cast<int*>(lists + static_cast<std::size_t>(centers) * s.width);
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     // Thread t owns atom first + t (at most kRunThreads per CTA): its state stays in registers
     // for the whole launch and is stored back at the end.
@@ -2138,39 +2218,70 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         inv_mass = s.inv_mass[mine];
         mass = s.mass[mine];
     }
-    double chain_q[3] = {0, 0, 0}, chain_p[3] = {0, 0, 0}, chain_kinetic = 0, pending = 1;
-    if (kThermostat && threadIdx.x == 0)
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
     {
-        for (int k = 0; k < 3; ++k)
-        {
-            chain_q[k] = s.thermo[kChainA + k];
-            chain_p[k] = s.thermo[kChainA + 3 + k];
-        }
-        chain_kinetic = s.thermo[kKineticA];
-        pending = s.thermo[kPendingScale];
+        tile[i] = s.pos[i];
     }
+    if (kSharedLists)
+    {
+        for (int i = threadIdx.x; i < centers; i += blockDim.x)
+        {
+            counts[i] = s.nbr_count[first + i];
+        }
+        const uint4* stored = reinterpret_cast<const uint4*>(s.nbr);
+        for (int w = threadIdx.x; w < centers * words; w += blockDim.x)
+        {
+            reinterpret_cast<uint4*>(lists)[w] =
+                stored[chunk_index(first + w / words, w % words, s.width)];
+        }
+    }
+    if (threadIdx.x < kRunCluster)
+    {
+        moved[threadIdx.x] = 0;
+        failed[threadIdx.x] = 0;
+    }
+    double chain_q[3] = {0, 0, 0}, chain_p[3] = {0, 0, 0}, chain_kinetic = 0, pending = 1;
+    double energy = 0.0, kinetic = 0.0;  // the last step's totals (thread 0)
+    if (threadIdx.x == 0)
+    {
+        tile[s.sentinel] = far_atom<T>();
+        if (kThermostat)
+        {
+            for (int k = 0; k < kThermoSize; ++k)
+            {
+                thermo[k] = s.thermo[k];
+            }
+            for (int k = 0; k < 3; ++k)
+            {
+                chain_q[k] = thermo[kChainA + k];
+                chain_p[k] = thermo[kChainA + 3 + k];
+            }
+            chain_kinetic = thermo[kKineticA];
+            pending = thermo[kPendingScale];
+        }
+    }
+    const bool failed_before = s.status[0] != 0;  // a latched failure stops the rebuilds
+    int rebuilds = 0;
     const T kick = s.half_dt * inv_mass;
+    // No CTA writes into another before every CTA has set up its shared memory.
+    cluster_barrier();
     for (int step = 0; step < steps; ++step)
     {
-        // The chain's opening half step (as every drift block computes it; CTA 0 stores it).
+        // The chain's opening half step (as every drift block computes it).
         if (kThermostat && threadIdx.x == 0)
         {
-            const double* th = s.thermo;
-            const double factor = chain_half_step(chain_kinetic, chain_q, chain_p, th + kChainMass,
-                                                  th[kDegrees], th[kThermalEnergy], th[kTimestep]);
+            const double factor =
+                chain_half_step(chain_kinetic, chain_q, chain_p, thermo + kChainMass,
+                                thermo[kDegrees], thermo[kThermalEnergy], thermo[kTimestep]);
             scales[0] = static_cast<T>(pending);
             scales[1] = static_cast<T>(factor);
-            if (rank == 0)
+            for (int k = 0; k < 3; ++k)
             {
-                double* out = s.thermo;
-                for (int k = 0; k < 3; ++k)
-                {
-                    out[kChainB + k] = chain_q[k];
-                    out[kChainB + 3 + k] = chain_p[k];
-                }
-                out[kKineticB] = chain_kinetic;
-                out[kOpenScale] = factor;
+                thermo[kChainB + k] = chain_q[k];
+                thermo[kChainB + 3 + k] = chain_p[k];
             }
+            thermo[kKineticB] = chain_kinetic;
+            thermo[kOpenScale] = factor;
         }
         __syncthreads();
         // The drift of the owned atom, from registers and this CTA's forces.
@@ -2192,32 +2303,39 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
             velocity[0] = vx;
             velocity[1] = vy;
             velocity[2] = vz;
-            s.pos[mine] = position;
+            for (int r = 0; r < ctas; ++r)
+            {
+                cluster_peer(tile, r)[mine] = position;
+            }
             if (!(isfinite(position.x) && isfinite(position.y) && isfinite(position.z)))
             {
                 atomicOr(s.status, kNonFinite);
+                for (int r = 0; r < ctas; ++r)
+                {
+                    cluster_peer(failed, r)[rank] = 1;
+                }
             }
             else if (squared_norm(position.x - reference.x, position.y - reference.y,
                                   position.z - reference.z) >= s.threshold_squared)
             {
-                s.rebuild[0] = step + 1;  // this step's stamp; every writer stores the same
+                for (int r = 0; r < ctas; ++r)
+                {
+                    cluster_peer(moved, r)[rank] = step + 1;  // every writer stores the same
+                }
             }
         }
         cluster_barrier();
-        // Every CTA reads the same stamp and status here (this step's writers are all before
-        // the barrier, the next step's all after the next one), the tile beside it.
-        if (threadIdx.x == 0)
+        // Every CTA reads the same flags here: this step's writers are all before the barrier,
+        // the next step's after the next one, which no CTA passes before reading these.
+        bool rebuild = false, stop = failed_before;
+        for (int r = 0; r < ctas; ++r)
         {
-            rebuild = (s.rebuild[0] == step + 1 && s.status[0] == 0) ? 1 : 0;
-            tile[s.sentinel] = far_atom<T>();
+            rebuild |= moved[r] == step + 1;
+            stop |= failed[r] != 0;
         }
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (rebuild && !stop)
         {
-            tile[i] = s.pos[i];
-        }
-        __syncthreads();
-        if (rebuild)
-        {
+            ++rebuilds;
             if (owner)
             {
                 long long cx, cy, cz;
@@ -2232,65 +2350,83 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
                     image[2] += cz;
                 }
                 reference = position;
-                s.pos[mine] = position;
-                s.ref_pos[mine] = position;
-            }
-            if (rank == 0 && threadIdx.x == 0)
-            {
-                ++s.rebuild_count[0];
+                for (int r = 0; r < ctas; ++r)
+                {
+                    cluster_peer(tile, r)[mine] = position;
+                }
             }
             cluster_barrier();
-            for (int i = threadIdx.x; i < n; i += blockDim.x)
+            // A warp per center: the ballot build stores what the per-step build's scan does.
+            for (int local = warp; local < centers; local += kRunThreads / kWarp)
             {
-                tile[i] = s.pos[i];
-            }
-            __syncthreads();
-            const T r2max = s.radius_squared;
-            for (int center = first + threadIdx.x; center < last; center += blockDim.x)
-            {
-                const Pos4<T> c = tile[center];
-                ListWriter list(s.nbr, s.width, center, s.sentinel);
-                for (int k = 0; k < n; ++k)
+                const int center = first + local;
+                int count;
+                if (kSharedLists)
                 {
-                    if (k == center)
+                    std::uint16_t* entries = lists + static_cast<std::size_t>(local) * s.width;
+                    count = warp_center_list(s, tile, center, [&](int e) { return entries + e; });
+                    if (lane == 0)
                     {
-                        continue;
-                    }
-                    const Pos4<T> p = tile[k];
-                    const T dx = min_image(c.x, p.x, s.length[0]);
-                    const T dy = min_image(c.y, p.y, s.length[1]);
-                    const T dz = min_image(c.z, p.z, s.length[2]);
-                    if (squared_norm(dx, dy, dz) < r2max)
-                    {
-                        list.add(k);
+                        counts[local] = count;
                     }
                 }
-                list.finish();
-                s.nbr_count[center] = list.count;
-                if (list.count > s.width)
+                else
                 {
-                    flag_overflow(s.status, 1, list.count);
+                    auto* entries = reinterpret_cast<std::uint16_t*>(s.nbr);
+                    count = warp_center_list(s, tile, center, [&](int e) {
+                        return entries + chunk_index(center, e / kChunk, s.width) * kChunk +
+                               e % kChunk;
+                    });
+                    if (lane == 0)
+                    {
+                        s.nbr_count[center] = count;
+                    }
+                }
+                if (lane == 0 && count > s.width)
+                {
+                    flag_overflow(s.status, 1, count);
+                    for (int r = 0; r < ctas; ++r)
+                    {
+                        cluster_peer(failed, r)[rank] = 1;
+                    }
                 }
             }
             __syncthreads();
         }
         // This CTA's centers over kSmallLanes lanes each; the forces meet in shared memory.
         double sums[2] = {0.0, 0.0};
-        const int tasks = (last - first) * kSmallLanes;
+        const int tasks = centers * kSmallLanes;
         for (int base = 0; base < tasks; base += blockDim.x)
         {
             const int task = base + threadIdx.x;
             const int center = task < tasks ? first + task / kSmallLanes : n;  // n: no center
+            const int local = center - first;
+            const uint4* chunks = nullptr;
+            int stride = 0, count = 0;
+            if (center < n)
+            {
+                if (kSharedLists)
+                {
+                    chunks = reinterpret_cast<const uint4*>(lists) +
+                             static_cast<std::size_t>(local) * words;
+                    stride = 1;
+                    count = counts[local];
+                }
+                else
+                {
+                    chunks = reinterpret_cast<const uint4*>(s.nbr) + chunk_index(center, 0, s.width);
+                    stride = kWarp;
+                    count = s.nbr_count[center];
+                }
+            }
             T force[3];
-            run_center_forces<T, kMulti>(s, tile, params, center, task % kSmallLanes, force,
-                                         sums[0]);
+            run_center_forces<T, kMulti>(s, tile, params, chunks, stride, count, center,
+                                         task % kSmallLanes, force, sums[0]);
             if (center < n && task % kSmallLanes == 0)
             {
-                const int local = center - first;
                 for (int a = 0; a < 3; ++a)
                 {
                     forces[local][a] = force[a];
-                    s.force[3LL * center + a] = force[a];
                 }
             }
         }
@@ -2319,77 +2455,109 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         __syncthreads();
         if (threadIdx.x == 0)
         {
-            double energy = 0.0, kinetic = 0.0;
+            double sum[2] = {0.0, 0.0};
             for (int w = 0; w < kRunThreads / kWarp; ++w)
             {
-                energy += warp_sums[w][0];
-                kinetic += warp_sums[w][1];
+                sum[0] += warp_sums[w][0];
+                sum[1] += warp_sums[w][1];
             }
-            s.partials[2 * rank] = energy;
-            s.partials[2 * rank + 1] = kinetic;
+            for (int r = 0; r < ctas; ++r)
+            {
+                double* slot = cluster_peer(&partials[rank][0], r);
+                slot[0] = sum[0];
+                slot[1] = sum[1];
+            }
         }
         cluster_barrier();
         // Every CTA: the totals in CTA order and the chain's closing half step
-        // (finalize_kernel's); CTA 0 stores them. The next step's partials are written only
-        // after its drift barrier, which every CTA reaches after reading these.
+        // (finalize_kernel's). The next step's partials are written only after its drift
+        // barrier, which every CTA reaches after reading these.
         if (threadIdx.x == 0)
         {
-            double energy = 0.0, kinetic = 0.0;
+            energy = 0.0;
+            kinetic = 0.0;
             for (int c = 0; c < ctas; ++c)
             {
-                energy += s.partials[2 * c];
-                kinetic += s.partials[2 * c + 1];
+                energy += partials[c][0];
+                kinetic += partials[c][1];
             }
             if (kThermostat)
             {
-                const double* th = s.thermo;
                 chain_kinetic = kinetic;
-                pending = chain_half_step(chain_kinetic, chain_q, chain_p, th + kChainMass,
-                                          th[kDegrees], th[kThermalEnergy], th[kTimestep]);
-            }
-            if (rank == 0)
-            {
-                s.totals[0] = energy;
-                s.totals[1] = kinetic;
-                for (int r = 2; r < kReduced; ++r)
+                pending = chain_half_step(chain_kinetic, chain_q, chain_p, thermo + kChainMass,
+                                          thermo[kDegrees], thermo[kThermalEnergy],
+                                          thermo[kTimestep]);
+                for (int r = 0; r < 3; ++r)
                 {
-                    s.totals[r] = 0.0;
+                    thermo[kChainA + r] = chain_q[r];
+                    thermo[kChainA + 3 + r] = chain_p[r];
                 }
-                if (kThermostat)
-                {
-                    double* out = s.thermo;
-                    for (int r = 0; r < 3; ++r)
-                    {
-                        out[kChainA + r] = chain_q[r];
-                        out[kChainA + 3 + r] = chain_p[r];
-                    }
-                    out[kKineticA] = chain_kinetic;
-                    out[kPendingScale] = pending;
-                }
+                thermo[kKineticA] = chain_kinetic;
+                thermo[kPendingScale] = pending;
             }
         }
     }
+    // The state back to global memory; no CTA touches another's shared memory after the last
+    // step's second barrier.
     if (owner)
     {
+        s.pos[mine] = position;
+        s.ref_pos[mine] = reference;
         for (int a = 0; a < 3; ++a)
         {
             s.vel[3LL * mine + a] = velocity[a];
+            s.force[3LL * mine + a] = forces[threadIdx.x][a];
         }
     }
-    // Every CTA read the last stamp before the last barrier: the flag starts clean next time.
+    if (kSharedLists && rebuilds > 0)
+    {
+        for (int i = threadIdx.x; i < centers; i += blockDim.x)
+        {
+            s.nbr_count[first + i] = counts[i];
+        }
+        uint4* stored = reinterpret_cast<uint4*>(s.nbr);
+        for (int w = threadIdx.x; w < centers * words; w += blockDim.x)
+        {
+            const int local = w / words, chunk = w % words;
+            if (chunk * kChunk < counts[local])
+            {
+                stored[chunk_index(first + local, chunk, s.width)] =
+                    reinterpret_cast<const uint4*>(lists)[w];
+            }
+        }
+    }
     if (rank == 0 && threadIdx.x == 0)
     {
-        s.rebuild[0] = 0;
+        s.totals[0] = energy;
+        s.totals[1] = kinetic;
+        for (int r = 2; r < kReduced; ++r)
+        {
+            s.totals[r] = 0.0;
+        }
+        if (kThermostat)
+        {
+            for (int k = 0; k < kChainMass; ++k)
+            {
+                s.thermo[k] = thermo[k];
+            }
+        }
+        s.rebuild_count[0] += rebuilds;
+        s.rebuild[0] = 0;  // the reuse flag starts clean, as after a per-step rebuild
     }
 }
 
 template <typename T>
 int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t stream)
 {
-    const std::size_t bytes = tile_bytes(s);
-    // Up to kRunCluster CTAs, no more than the partial slots hold two sums each.
-    const int slots = static_cast<int>(s.force_blocks) * kReduced;
-    const int ctas = std::max(1, std::min(std::min(kRunCluster, slots / 2), static_cast<int>(s.n)));
+    const int ctas = std::max(1, std::min(kRunCluster, static_cast<int>(s.n)));
+    const int centers = static_cast<int>((s.n + ctas - 1) / ctas);
+    // The CTA's lists in shared memory when they fit beside the positions and the kernel's
+    // static shared memory (about 14 KB in float64), else in the global list. The grant is set
+    // on every launch (a launch runs up to a thousand steps; it is never graph-captured): the
+    // static bytes count against the 48 KB a kernel gets without it.
+    constexpr std::size_t kSharedBudget = 200 * 1024;
+    const bool shared_lists = run_shared_bytes(s, centers, true) <= kSharedBudget;
+    const std::size_t bytes = run_shared_bytes(s, centers, shared_lists);
     cudaLaunchConfig_t config = {};
     config.gridDim = dim3(ctas);
     config.blockDim = dim3(kRunThreads);
@@ -2402,19 +2570,23 @@ int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t
     attribute[0].val.clusterDim.z = 1;
     config.attrs = attribute;
     config.numAttrs = 1;
-#define ND_RUN_CASE(MULTI, THERMO)                                                 \
-    if ((s.num_types > 1) == MULTI && (thermostat != 0) == THERMO)                 \
-    {                                                                              \
-        auto kernel = small_run_kernel<T, MULTI, THERMO>;                          \
-        static DeviceGrant grant;                                                  \
-        ND_CUDA_TRY(grant.allow(kernel, bytes));                                   \
-        ND_CUDA_TRY(cudaLaunchKernelEx(&config, kernel, s, steps));                \
-        return ND_OK;                                                              \
+#define ND_RUN_CASE(MULTI, THERMO, SHARED)                                                     \
+    if ((s.num_types > 1) == MULTI && (thermostat != 0) == THERMO && shared_lists == SHARED)   \
+    {                                                                                          \
+        auto kernel = small_run_kernel<T, MULTI, THERMO, SHARED>;                              \
+        ND_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                         static_cast<int>(bytes)));                            \
+        ND_CUDA_TRY(cudaLaunchKernelEx(&config, kernel, s, steps));                            \
+        return ND_OK;                                                                          \
     }
-    ND_RUN_CASE(false, false)
-    ND_RUN_CASE(false, true)
-    ND_RUN_CASE(true, false)
-    ND_RUN_CASE(true, true)
+    ND_RUN_CASE(false, false, true)
+    ND_RUN_CASE(false, true, true)
+    ND_RUN_CASE(true, false, true)
+    ND_RUN_CASE(true, true, true)
+    ND_RUN_CASE(false, false, false)
+    ND_RUN_CASE(false, true, false)
+    ND_RUN_CASE(true, false, false)
+    ND_RUN_CASE(true, true, false)
 #undef ND_RUN_CASE
     return ND_OK;
 }
