@@ -1999,7 +1999,7 @@ std::int64_t step_launches(const nd_md_system* m)
 
 constexpr int kRunThreads = 512;
 constexpr int kRunMaxAtoms = 4096;
-constexpr int kRunCluster = 8;
+constexpr int kRunCluster = 16;  // CTAs of the largest cluster (past 8: non-portable)
 
 __device__ __forceinline__ void cluster_barrier()
 {
@@ -2179,6 +2179,7 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     __shared__ T forces[kRunThreads][3];  // this step's force on each owned atom
     __shared__ T scales[2];
     __shared__ double thermo[kThermoSize];  // the chain's slots, stored at the end
+    __shared__ double totals[2];            // the last step's E and K, stored at the end
     // Written by CTA r into slot r of every CTA: its E and K; the stamp (step + 1) of a step in
     // which one of its atoms moved past the reuse threshold; whether it saw a failure.
     __shared__ double partials[kRunCluster][2];
@@ -2240,8 +2241,9 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         moved[threadIdx.x] = 0;
         failed[threadIdx.x] = 0;
     }
+    // Thread 0's chain state and constants (1 / Q, g, kT, dt), in registers for the launch.
     double chain_q[3] = {0, 0, 0}, chain_p[3] = {0, 0, 0}, chain_kinetic = 0, pending = 1;
-    double energy = 0.0, kinetic = 0.0;  // the last step's totals (thread 0)
+    double inverse[3] = {0, 0, 0}, degrees = 0, thermal = 0, chain_dt = 0;
     if (threadIdx.x == 0)
     {
         tile[s.sentinel] = far_atom<T>();
@@ -2255,9 +2257,13 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
             {
                 chain_q[k] = thermo[kChainA + k];
                 chain_p[k] = thermo[kChainA + 3 + k];
+                inverse[k] = 1.0 / thermo[kChainMass + k];
             }
             chain_kinetic = thermo[kKineticA];
             pending = thermo[kPendingScale];
+            degrees = thermo[kDegrees];
+            thermal = thermo[kThermalEnergy];
+            chain_dt = thermo[kTimestep];
         }
     }
     const bool failed_before = s.status[0] != 0;  // a latched failure stops the rebuilds
@@ -2271,8 +2277,8 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         if (kThermostat && threadIdx.x == 0)
         {
             const double factor =
-                chain_half_step(chain_kinetic, chain_q, chain_p, thermo + kChainMass,
-                                thermo[kDegrees], thermo[kThermalEnergy], thermo[kTimestep]);
+                chain_half_step_inverse(chain_kinetic, chain_q, chain_p, inverse, degrees,
+                                        thermal, chain_dt);
             scales[0] = static_cast<T>(pending);
             scales[1] = static_cast<T>(factor);
             for (int k = 0; k < 3; ++k)
@@ -2327,8 +2333,10 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         cluster_barrier();
         // Every CTA reads the same flags here: this step's writers are all before the barrier,
         // the next step's after the next one, which no CTA passes before reading these.
+        // (Slots past the cluster's CTAs stay zero.)
         bool rebuild = false, stop = failed_before;
-        for (int r = 0; r < ctas; ++r)
+#pragma unroll
+        for (int r = 0; r < kRunCluster; ++r)
         {
             rebuild |= moved[r] == step + 1;
             stop |= failed[r] != 0;
@@ -2474,19 +2482,19 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         // barrier, which every CTA reaches after reading these.
         if (threadIdx.x == 0)
         {
-            energy = 0.0;
-            kinetic = 0.0;
+            double energy = 0.0, kinetic = 0.0;
             for (int c = 0; c < ctas; ++c)
             {
                 energy += partials[c][0];
                 kinetic += partials[c][1];
             }
+            totals[0] = energy;
+            totals[1] = kinetic;
             if (kThermostat)
             {
                 chain_kinetic = kinetic;
-                pending = chain_half_step(chain_kinetic, chain_q, chain_p, thermo + kChainMass,
-                                          thermo[kDegrees], thermo[kThermalEnergy],
-                                          thermo[kTimestep]);
+                pending = chain_half_step_inverse(chain_kinetic, chain_q, chain_p, inverse,
+                                                  degrees, thermal, chain_dt);
                 for (int r = 0; r < 3; ++r)
                 {
                     thermo[kChainA + r] = chain_q[r];
@@ -2528,8 +2536,8 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     }
     if (rank == 0 && threadIdx.x == 0)
     {
-        s.totals[0] = energy;
-        s.totals[1] = kinetic;
+        s.totals[0] = totals[0];
+        s.totals[1] = totals[1];
         for (int r = 2; r < kReduced; ++r)
         {
             s.totals[r] = 0.0;
@@ -2546,18 +2554,25 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
     }
 }
 
-template <typename T>
-int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t stream)
+// Launches one variant on `ctas` CTAs (one cluster); `placed` false when the GPU cannot hold
+// a cluster that size (sizes past 8 are non-portable), nothing launched.
+template <typename T, bool kMulti, bool kThermostat, bool kSharedLists>
+cudaError_t launch_run_variant(const System<T>& s, int steps, int ctas, std::size_t bytes,
+                               cudaStream_t stream, bool& placed)
 {
-    const int ctas = std::max(1, std::min(kRunCluster, static_cast<int>(s.n)));
-    const int centers = static_cast<int>((s.n + ctas - 1) / ctas);
-    // The CTA's lists in shared memory when they fit beside the positions and the kernel's
-    // static shared memory (about 14 KB in float64), else in the global list. The grant is set
-    // on every launch (a launch runs up to a thousand steps; it is never graph-captured): the
-    // static bytes count against the 48 KB a kernel gets without it.
-    constexpr std::size_t kSharedBudget = 200 * 1024;
-    const bool shared_lists = run_shared_bytes(s, centers, true) <= kSharedBudget;
-    const std::size_t bytes = run_shared_bytes(s, centers, shared_lists);
+    auto kernel = small_run_kernel<T, kMulti, kThermostat, kSharedLists>;
+    // Set on every launch (a launch runs up to a thousand steps and is never graph-captured):
+    // the static bytes count against the 48 KB a kernel gets without the grant.
+    cudaError_t rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(bytes));
+    if (rc == cudaSuccess && ctas > 8)
+    {
+        rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
+    if (rc != cudaSuccess)
+    {
+        return rc;
+    }
     cudaLaunchConfig_t config = {};
     config.gridDim = dim3(ctas);
     config.blockDim = dim3(kRunThreads);
@@ -2570,14 +2585,34 @@ int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t
     attribute[0].val.clusterDim.z = 1;
     config.attrs = attribute;
     config.numAttrs = 1;
-#define ND_RUN_CASE(MULTI, THERMO, SHARED)                                                     \
-    if ((s.num_types > 1) == MULTI && (thermostat != 0) == THERMO && shared_lists == SHARED)   \
-    {                                                                                          \
-        auto kernel = small_run_kernel<T, MULTI, THERMO, SHARED>;                              \
-        ND_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                         static_cast<int>(bytes)));                            \
-        ND_CUDA_TRY(cudaLaunchKernelEx(&config, kernel, s, steps));                            \
-        return ND_OK;                                                                          \
+    if (ctas > 8)
+    {
+        int clusters = 0;
+        rc = cudaOccupancyMaxActiveClusters(&clusters, kernel, &config);
+        if (rc != cudaSuccess)
+        {
+            return rc;
+        }
+        if (clusters < 1)
+        {
+            placed = false;
+            return cudaSuccess;
+        }
+    }
+    placed = true;
+    return cudaLaunchKernelEx(&config, kernel, s, steps);
+}
+
+template <typename T>
+cudaError_t launch_run_dispatch(const System<T>& s, bool multi, bool thermostat,
+                                bool shared_lists, int steps, int ctas, std::size_t bytes,
+                                cudaStream_t stream, bool& placed)
+{
+#define ND_RUN_CASE(MULTI, THERMO, SHARED)                                                   \
+    if (multi == MULTI && thermostat == THERMO && shared_lists == SHARED)                    \
+    {                                                                                        \
+        return launch_run_variant<T, MULTI, THERMO, SHARED>(s, steps, ctas, bytes, stream,   \
+                                                            placed);                         \
     }
     ND_RUN_CASE(false, false, true)
     ND_RUN_CASE(false, true, true)
@@ -2588,7 +2623,33 @@ int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t
     ND_RUN_CASE(true, false, false)
     ND_RUN_CASE(true, true, false)
 #undef ND_RUN_CASE
-    return ND_OK;
+    return cudaErrorInvalidValue;
+}
+
+template <typename T>
+int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t stream)
+{
+    // A CTA per 32 atoms up to the largest cluster, a portable 8 when the GPU cannot place
+    // that; the CTA's lists in shared memory when they fit beside the positions and the
+    // kernel's static shared memory (about 14 KB in float64), else in the global list.
+    constexpr std::size_t kSharedBudget = 200 * 1024;
+    const int wanted = static_cast<int>((s.n + kWarp - 1) / kWarp);
+    for (const int limit : {kRunCluster, 8})
+    {
+        const int ctas = std::max(1, std::min(limit, wanted));
+        const int centers = static_cast<int>((s.n + ctas - 1) / ctas);
+        const bool shared_lists = run_shared_bytes(s, centers, true) <= kSharedBudget;
+        const std::size_t bytes = run_shared_bytes(s, centers, shared_lists);
+        bool placed = false;
+        ND_CUDA_TRY(launch_run_dispatch(s, s.num_types > 1, thermostat != 0, shared_lists, steps,
+                                        ctas, bytes, stream, placed));
+        if (placed)
+        {
+            return ND_OK;
+        }
+    }
+    set_error("no cluster of 8 CTAs fits on this GPU for a one-launch run");
+    return ND_ECUDA;
 }
 
 // Sets the rebuild branch of a step graph from the device flag the drift kernel wrote.

@@ -228,13 +228,16 @@ struct StagedListWriter
 
 // The Nose-Hoover chain of three, advanced by half a step against the kinetic energy K
 // (Martyna, Tuckerman, Tobias and Klein 1996; src/nabladyn/md/_ensembles/_chain.py:36-83).
-// Returns the velocity scale; q and p advance in place and K is scaled.
-__device__ inline double chain_half_step(double& kinetic, double* q, double* p, const double* mass,
-                                         double degrees, double kT, double dt)
+// Returns the velocity scale; q and p advance in place and K is scaled. `inverse` holds 1 / Q
+// of each link: the update is one dependent chain, and a product in place of each quotient
+// p / Q takes the divisions off it (a difference in the last bit of float64).
+__device__ inline double chain_half_step_inverse(double& kinetic, double* q, double* p,
+                                                 const double* inverse, double degrees,
+                                                 double kT, double dt)
 {
     const double quarter = 0.25 * dt, eighth = 0.125 * dt;
     auto driving = [&](int k, double energy) {
-        return k == 0 ? 2.0 * energy - degrees * kT : p[k - 1] * p[k - 1] / mass[k - 1] - kT;
+        return k == 0 ? 2.0 * energy - degrees * kT : p[k - 1] * p[k - 1] * inverse[k - 1] - kT;
     };
     double damping[2];
     for (int k = 2; k >= 0; --k)
@@ -250,14 +253,14 @@ __device__ inline double chain_half_step(double& kinetic, double* q, double* p, 
         }
         if (k > 0)
         {
-            damping[k - 1] = exp(-eighth * p[k] / mass[k]);
+            damping[k - 1] = exp(-eighth * p[k] * inverse[k]);
         }
     }
-    const double factor = exp(-0.5 * dt * p[0] / mass[0]);
+    const double factor = exp(-0.5 * dt * p[0] * inverse[0]);
     double scaled = kinetic * (factor * factor);
     for (int k = 0; k < 3; ++k)
     {
-        q[k] = q[k] + 0.5 * dt * p[k] / mass[k];
+        q[k] = q[k] + 0.5 * dt * p[k] * inverse[k];
     }
     for (int k = 0; k < 3; ++k)
     {
@@ -273,6 +276,14 @@ __device__ inline double chain_half_step(double& kinetic, double* q, double* p, 
     }
     kinetic = scaled;
     return factor;
+}
+
+// The same from the links' masses Q.
+__device__ inline double chain_half_step(double& kinetic, double* q, double* p, const double* mass,
+                                         double degrees, double kT, double dt)
+{
+    const double inverse[3] = {1.0 / mass[0], 1.0 / mass[1], 1.0 / mass[2]};
+    return chain_half_step_inverse(kinetic, q, p, inverse, degrees, kT, dt);
 }
 
 }  // namespace nd
