@@ -57,7 +57,7 @@ constexpr int kMaxBrickCells = 14;                  // home cells per brick, at 
 constexpr int kMaxRowCells = kMaxBrickCells + 2;    // tile cells per row
 constexpr int kTileCells = 9 * kMaxRowCells;        // tile cells, at most
 constexpr int kReduced = 8;                         // E, K, W xx yy zz xy xz yz
-constexpr int kSmallLanes = 8;  // small-box forces: lanes sharing one atom's list
+constexpr int kSmallLanes = 16;  // small-box forces: lanes sharing one atom's list
 
 // The device view of one system, built from nd_md_system.
 template <typename T>
@@ -2000,6 +2000,7 @@ std::int64_t step_launches(const nd_md_system* m)
 constexpr int kRunThreads = 512;
 constexpr int kRunMaxAtoms = 4096;
 constexpr int kRunCluster = 16;  // CTAs of the largest cluster (past 8: non-portable)
+static_assert(kRunCluster <= kWarp, "a warp reads every CTA's flag slot in one vote");
 
 __device__ __forceinline__ void cluster_barrier()
 {
@@ -2170,7 +2171,7 @@ std::size_t run_shared_bytes(const System<T>& s, int centers, bool shared_lists)
 }
 
 template <typename T, bool kMulti, bool kThermostat, bool kSharedLists>
-__global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int steps)
+__global__ void __launch_bounds__(kRunThreads, 1) small_run_kernel(System<T> s, int steps)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     auto* tile = reinterpret_cast<Pos4<T>*>(smem_raw);
@@ -2332,15 +2333,13 @@ __global__ void __launch_bounds__(kRunThreads) small_run_kernel(System<T> s, int
         }
         cluster_barrier();
         // Every CTA reads the same flags here: this step's writers are all before the barrier,
-        // the next step's after the next one, which no CTA passes before reading these.
-        // (Slots past the cluster's CTAs stay zero.)
-        bool rebuild = false, stop = failed_before;
-#pragma unroll
-        for (int r = 0; r < kRunCluster; ++r)
-        {
-            rebuild |= moved[r] == step + 1;
-            stop |= failed[r] != 0;
-        }
+        // the next step's after the next one, which no CTA passes before reading these. Lane
+        // r of each warp reads slot r (slots past the cluster's CTAs stay zero).
+        const bool rebuild =
+            __any_sync(kFullMask, lane < kRunCluster && moved[lane % kRunCluster] == step + 1);
+        const bool stop =
+            failed_before ||
+            __any_sync(kFullMask, lane < kRunCluster && failed[lane % kRunCluster] != 0);
         if (rebuild && !stop)
         {
             ++rebuilds;
