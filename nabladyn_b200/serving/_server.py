@@ -12,7 +12,9 @@ Each request is an independent one-type Lennard-Jones NVT simulation (the refere
   small replicas are not held back by large ones;
 * harvests replicas whose steps are done (their frames read back together, in one copy),
   hands back their frame and frees their room, so requests that arrived meanwhile are
-  admitted in the next round.
+  admitted in the next round;
+* pipelines the rounds: the next round is on the device while the host reads the last one's
+  slot table, harvests and admits, so the device does not wait for the host between rounds.
 
 Replicas never interact on the device: each is advanced by its own CTA, so a replica's result
 does not depend on which others share its rounds.
@@ -95,7 +97,6 @@ class _Active:
     units: int
     admitted: float
     steps_left: int = field(default=0)
-    staged: object = None  # the pinned host frame of its upload, kept until the copy is done
 
 
 @dataclass
@@ -147,6 +148,8 @@ class ReplicaServer:
             setattr(pool, name, tensor.data_ptr())
         self.pool = pool
         self._free_units = [(0, n // _ALIGN)]  # (first unit, units), sorted, merged
+        self._pinned: dict[str, list] = {}  # _upload's areas
+        self._pinned_turn: dict[str, int] = {}
         self._free_slots = list(range(self.max_slots - 1, -1, -1))
 
     # -- room ----------------------------------------------------------------------------
@@ -229,13 +232,11 @@ class ReplicaServer:
         record.thermostat[_TIMESTEP] = request.timestep
         return record, velocities32
 
-    def _stage(self, request: ReplicaRequest, pinned: bool = True) -> _Staged:
-        """The host part of an admission: the record and the frame, in pinned memory when the
-        upload is to overlap a round (staged ahead), else in ordinary memory."""
+    def _stage(self, request: ReplicaRequest) -> _Staged:
+        """The host part of an admission: the record and the frame (uploaded by _place)."""
         record, velocities32 = self._describe(request, 0, 0)
         n = record.num_atoms
         frame = torch.empty((n, 9), dtype=torch.float32)
-        frame = frame.pin_memory() if pinned else frame
         masses = np.asarray(request.masses, dtype=np.float32)
         host = frame.numpy()
         host[:, :3] = np.asarray(request.positions, dtype=np.float32)
@@ -245,43 +246,72 @@ class ReplicaServer:
         host[:, 8] = 1.0 / masses
         return _Staged(record, frame)
 
-    def _place(self, staged: _Staged, slot: int, offset: int) -> None:
-        """The device part: the frame's pinned rows copied into the pool (no host sync) and the
-        slot record written with its offsets."""
-        record = staged.record
-        n = record.num_atoms
-        record.atom_offset = offset
-        record.list_offset = offset * _WIDTH
-        record.cell_offset = slot * (_MAX_CELLS + 1)
-        rows = staged.frame.to(self.device, non_blocking=True)
-        b = self.buffers
-        b["positions"][offset:offset + n].copy_(rows[:, :4])
-        b["velocities"][offset:offset + n].copy_(rows[:, 4:7])
-        b["forces"][offset:offset + n].zero_()
-        b["masses"][offset:offset + n].copy_(rows[:, 7])
-        b["inverse_masses"][offset:offset + n].copy_(rows[:, 8])
-        b["images"][offset:offset + n].zero_()
+    def _upload(self, name: str, values: np.ndarray) -> torch.Tensor:
+        """A host array on the device without a host sync, on the current stream: through one
+        of two pinned areas kept per `name` and grown as needed (a copy from pageable memory
+        would wait for the round running on the stream, and a new pinned block per call costs
+        more than the copy). An area is reused after the copy made from it two calls before,
+        which an earlier round's completion has already finished in the serve loop."""
+        values = np.ascontiguousarray(values)
+        areas = self._pinned.setdefault(name, [[None, None], [None, None]])
+        turn = self._pinned_turn[name] = self._pinned_turn.get(name, 1) ^ 1
+        area, copied = areas[turn]
+        if copied is not None:
+            copied.synchronize()
+        if area is None or area.numel() < values.nbytes:
+            grown = max(values.nbytes, 2 * (area.numel() if area is not None else 0), 1 << 16)
+            area = torch.empty(grown, dtype=torch.uint8, pin_memory=True)
+        host = area[:values.nbytes]
+        host.numpy()[:] = values.reshape(-1).view(np.uint8)
+        device = host.to(self.device, non_blocking=True)
+        copied = torch.cuda.Event()
+        copied.record(torch.cuda.current_stream(self.device))
+        areas[turn] = [area, copied]
+        dtype = torch.from_numpy(np.empty(0, dtype=values.dtype)).dtype
+        return device.view(dtype).reshape(values.shape)
+
+    def _place(self, batch: list[tuple[_Staged, int, int]]) -> None:
+        """The device part of admissions, for a batch at once: the frames' pinned rows copied
+        into one device block and scattered into the pool, the slot records written with their
+        offsets; no host sync."""
+        if not batch:
+            return
         size = ctypes.sizeof(Replica)
-        raw = torch.frombuffer(bytearray(ctypes.string_at(ctypes.addressof(record), size)),
-                               dtype=torch.uint8)
-        raw = raw.pin_memory() if staged.frame.is_pinned() else raw
-        self.table[slot * size:(slot + 1) * size].copy_(raw, non_blocking=True)
-        staged.raw = raw  # the pinned record stays alive with the staged frame
+        records = bytearray()
+        destination = []
+        for staged, slot, offset in batch:
+            record = staged.record
+            n = record.num_atoms
+            record.atom_offset = offset
+            record.list_offset = offset * _WIDTH
+            record.cell_offset = slot * (_MAX_CELLS + 1)
+            records += ctypes.string_at(ctypes.addressof(record), size)
+            destination.append(np.arange(offset, offset + n, dtype=np.int64))
+        frames = np.concatenate([staged.frame.numpy() for staged, _, _ in batch])
+        rows = self._upload("frames", frames)
+        index = self._upload("rows", np.concatenate(destination))
+        b = self.buffers
+        b["positions"].index_copy_(0, index, rows[:, :4])
+        b["velocities"].index_copy_(0, index, rows[:, 4:7])
+        b["forces"].index_fill_(0, index, 0.0)
+        b["masses"].index_copy_(0, index, rows[:, 7])
+        b["inverse_masses"].index_copy_(0, index, rows[:, 8])
+        b["images"].index_fill_(0, index, 0)
+        slots = self._upload("slots", np.array([slot for _, slot, _ in batch], dtype=np.int64))
+        table = self._upload("records",
+                             np.frombuffer(bytes(records), dtype=np.uint8).reshape(-1, size))
+        self.table.view(self.max_slots, size).index_copy_(0, slots, table)
 
     def _launch(self, slots: list[int], budgets: list[int] | None, mode: int) -> None:
         if not slots:
             return
-        slot_tensor = torch.tensor(slots, dtype=torch.int32, device=self.device)
-        budget_tensor = (torch.tensor(budgets, dtype=torch.int32, device=self.device)
+        slot_tensor = self._upload(f"launch_slots_{mode}", np.asarray(slots, dtype=np.int32))
+        budget_tensor = (self._upload("launch_budgets", np.asarray(budgets, dtype=np.int32))
                          if budgets is not None else None)
         with torch.cuda.device(self.device):
             call("nd_serve_run", self.pool, slot_tensor.data_ptr(),
                  budget_tensor.data_ptr() if budget_tensor is not None else None,
                  len(slots), mode, stream_handle(self.device))
-
-    def _records(self) -> np.ndarray:
-        """The slot table on the host, as raw bytes per slot."""
-        return self.table.view(self.max_slots, ctypes.sizeof(Replica)).cpu().numpy()
 
     @staticmethod
     def _int_field(raw: np.ndarray, name: str) -> np.ndarray:
@@ -299,13 +329,13 @@ class ReplicaServer:
         for active, raw in done:
             record = Replica.from_buffer_copy(raw.tobytes())
             n, offset = record.num_atoms, active.offset
-            rows.append(torch.arange(offset, offset + n, device=self.device))
-            cells.append(torch.tensor(list(record.cell), dtype=torch.float32).expand(n, 3))
+            rows.append(np.arange(offset, offset + n, dtype=np.int64))
+            cells.append(np.broadcast_to(np.asarray(record.cell, dtype=np.float32), (n, 3)))
             scales.append(np.full(n, np.float32(record.thermostat[_PENDING]), dtype=np.float32))
             sizes.append((record, n))
-        index = torch.cat(rows)
-        cell = torch.cat(cells).to(self.device, non_blocking=True)
-        scale = torch.from_numpy(np.concatenate(scales)).to(self.device, non_blocking=True)
+        index = self._upload("harvest_rows", np.concatenate(rows))
+        cell = self._upload("harvest_cells", np.concatenate(cells))
+        scale = self._upload("harvest_scales", np.concatenate(scales))
         unwrapped = self.buffers["positions"][index, :3]
         crossings = torch.floor(unwrapped / cell)
         wrapped = unwrapped - crossings * cell
@@ -343,12 +373,18 @@ class ReplicaServer:
 
     # -- the loop ------------------------------------------------------------------------
 
-    def serve(self, requests: list[ReplicaRequest], *, realtime: bool = True) -> list[ReplicaResult]:
+    def serve(self, requests: list[ReplicaRequest], *,
+              realtime: bool = True) -> list[ReplicaResult]:
         """Serve requests by their arrival times; returns the results in completion order.
 
         With ``realtime`` the arrivals follow the wall clock from the call (a request is
         admitted only once its arrival time has passed); without, all are present at once.
-        Syncs with the host once per round.
+
+        The rounds are pipelined: round k+1 is launched before round k's slot table is read,
+        so the device runs a round while the host reads the previous one, harvests the
+        replicas that finished in it (on a side stream) and admits new ones. A slot keeps its
+        replica in every round launched before the host learns that it finished; the kernel
+        clamps each budget to the steps left, so such a replica runs no further step.
         """
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         for request in pending:
@@ -358,6 +394,9 @@ class ReplicaServer:
         active: dict[int, _Active] = {}
         results: list[ReplicaResult] = []
         staged: dict[int, _Staged] = {}  # by id(request): host work done ahead of admission
+        # High priority: the harvest's few small kernels go ahead of the round's waiting CTAs.
+        side = torch.cuda.Stream(self.device, priority=-1)
+        inflight = None  # the last round launched and not yet read: (slots, table copy, event)
         start = time.perf_counter()
 
         def stage_ahead(now: float) -> None:
@@ -370,7 +409,7 @@ class ReplicaServer:
 
         while pending or active:
             now = time.perf_counter() - start
-            admitted = []
+            placing = []
             while pending and (not realtime or pending[0].arrival <= now):
                 request = pending[0]
                 units = -(-request.positions.shape[0] // _ALIGN)
@@ -382,36 +421,72 @@ class ReplicaServer:
                 pending.popleft()
                 slot = self._free_slots.pop()
                 offset = first * _ALIGN
-                ready = staged.pop(id(request), None) or self._stage(request, pinned=False)
-                self._place(ready, slot, offset)
-                active[slot] = _Active(request, slot, offset, units, now, int(request.steps),
-                                       ready)
-                admitted.append(slot)
-            self._launch(admitted, None, 0)
+                ready = staged.pop(id(request), None) or self._stage(request)
+                placing.append((ready, slot, offset))
+                # The pinned frame may go once its copy is queued: the host allocator keeps
+                # the block until the copy has run.
+                active[slot] = _Active(request, slot, offset, units, now, int(request.steps))
+            self._place(placing)
+            self._launch([slot for _, slot, _ in placing], None, 0)
             if not active:
                 if pending and realtime:
                     time.sleep(max(0.0, min(pending[0].arrival - now, 0.001)))
                 continue
-            slots = list(active)
-            budgets = [max(1, min(active[s].steps_left,
-                                  -(-self.round_atom_steps // active[s].request.positions.shape[0])))
-                       for s in slots]
-            self._launch(slots, budgets, 1)
-            # While the round runs: the next admissions' host work.
+            launched = [(slot, active[slot]) for slot in active]
+            budgets = [max(1, min(entry.steps_left,
+                                  -(-self.round_atom_steps // entry.request.positions.shape[0])))
+                       for _, entry in launched]
+            self._launch([slot for slot, _ in launched], budgets, 1)
+            table_copy = self._table_copy()
+            # While the round runs: the next admissions' host work, then the previous round.
             if self.stage_ahead:
                 stage_ahead(time.perf_counter() - start)
-            raw = self._records()
-            now = time.perf_counter() - start
-            steps_left_all = self._int_field(raw, "steps_left")
-            status_all = self._int_field(raw, "status")
-            done = []
-            for slot in slots:
-                steps_left, status = int(steps_left_all[slot]), int(status_all[slot])
-                active[slot].steps_left = steps_left
-                if steps_left == 0 or status != 0:
-                    done.append((active.pop(slot), raw[slot]))
-            results.extend(self._harvest(done, now))
+            if inflight is not None:
+                results.extend(self._collect(inflight, active, side, start))
+            inflight = (launched, *table_copy)
+        torch.cuda.current_stream(self.device).synchronize()
         return results
 
+    def _table_copy(self) -> tuple[torch.Tensor, torch.cuda.Event]:
+        """The slot table after the round just launched, copied to pinned host memory without a
+        host sync (two buffers in turn: a copy is read before the one after next is made)."""
+        if not hasattr(self, "_table_hosts"):
+            self._table_hosts = [torch.empty_like(self.table, device="cpu").pin_memory()
+                                 for _ in range(2)]
+            self._table_turn = 0
+        host = self._table_hosts[self._table_turn]
+        self._table_turn ^= 1
+        host.copy_(self.table, non_blocking=True)
+        event = torch.cuda.Event()
+        event.record(torch.cuda.current_stream(self.device))
+        return host, event
+
+    def _collect(self, round_, active: dict[int, _Active], side: torch.cuda.Stream,
+                 start: float) -> list[ReplicaResult]:
+        """Reads a round's slot table (waiting for that round only) and harvests the replicas
+        it finished. A slot whose replica changed since the round was launched is skipped: its
+        entry in that table still describes the replica that left."""
+        launched, host, event = round_
+        event.synchronize()
+        raw = host.view(self.max_slots, ctypes.sizeof(Replica)).numpy()
+        now = time.perf_counter() - start
+        steps_left_all = self._int_field(raw, "steps_left")
+        status_all = self._int_field(raw, "status")
+        done = []
+        for slot, entry in launched:
+            if active.get(slot) is not entry:
+                continue
+            steps_left, status = int(steps_left_all[slot]), int(status_all[slot])
+            entry.steps_left = steps_left
+            if steps_left == 0 or status != 0:
+                done.append((active.pop(slot), raw[slot].copy()))
+        if not done:
+            return []
+        # The round after this one is running on the main stream; the finished replicas' rows
+        # are not written by it (their budgets clamp to zero steps), so they are read on a side
+        # stream after this round.
+        side.wait_event(event)
+        with torch.cuda.stream(side):
+            return self._harvest(done, now)
 
 __all__ = ("ReplicaRequest", "ReplicaResult", "ReplicaServer")
