@@ -53,7 +53,7 @@ def test_md_rejects_small_box_too_large():
     assert library.nd_md_partial_slots(ctypes.byref(system), ctypes.byref(slots)) == _native.ND_EINVAL
     system.num_atoms = 500
     assert library.nd_md_partial_slots(ctypes.byref(system), ctypes.byref(slots)) == _native.ND_OK
-    assert slots.value == 16 * 8  # ceil(500 x 8 lanes / 256) force blocks x 8 sums
+    assert slots.value == 32 * 8  # ceil(500 x 16 lanes / 256) force blocks x 8 sums
 
 
 def test_neighbor_schemas_match_the_reference():
