@@ -133,6 +133,42 @@ __device__ void block_scan_cells(int* counts, int cells, int* warp_totals)
     __syncthreads();
 }
 
+// Adds to `list` the candidates k = begin .. end - 1 (atom order[k], or k without an order)
+// closer to `me` (atom i) than the list radius, in k order. Four candidates at a time: their
+// indices and positions are loaded before any is tested, so the loads of a group overlap.
+__device__ __forceinline__ void scan_candidates(const ReplicaScalars& r, const Pos4<float>& me,
+                                                int i, const index_t* order, int begin, int end,
+                                                const Pos4<float>* pos, ListWriter& list)
+{
+    constexpr int kGroup = 4;
+    for (int k = begin; k < end; k += kGroup)
+    {
+        int j[kGroup];
+        Pos4<float> p[kGroup];
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u)
+        {
+            j[u] = k + u < end ? (order != nullptr ? order[k + u] : k + u) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u)
+        {
+            p[u] = j[u] >= 0 ? pos[j[u]] : me;
+        }
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u)
+        {
+            const float d2 = squared_norm(min_image(me.x, p[u].x, r.cell[0]),
+                                          min_image(me.y, p[u].y, r.cell[1]),
+                                          min_image(me.z, p[u].z, r.cell[2]));
+            if (j[u] >= 0 && j[u] != i && d2 < r.radius_squared)
+            {
+                list.add(j[u]);
+            }
+        }
+    }
+}
+
 // Wraps the positions (counting crossings into the images), stores the reference frame and
 // rebuilds the list. Called by the whole CTA.
 __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<float>* ref,
@@ -208,11 +244,14 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
     {
         __syncthreads();
     }
-    // The list: every neighbor j != i closer than the list radius, minimum image.
-    for (int i = threadIdx.x; i < n; i += kServeThreads)
+    // The list: every neighbor j != i closer than the list radius, minimum image. Row `row`
+    // holds the list of atom sorted[row] on a grid (the lanes of a warp take atoms of one or
+    // two cells, whose candidates they share), of atom `row` otherwise.
+    for (int row = threadIdx.x; row < n; row += kServeThreads)
     {
+        const int i = grid ? sorted[row] : row;
         const Pos4<float> me = pos[i];
-        ListWriter list(nbr, r.width, i, 0xffffu);
+        ListWriter list(nbr, r.width, row, 0xffffu);
         if (grid)
         {
             const int hx = axis_bin(me.x, r.widths[0], r.dims[0]);
@@ -228,38 +267,18 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
                     {
                         const int cx = (hx + dx + r.dims[0]) % r.dims[0];
                         const int c = cx + r.dims[0] * (cy + r.dims[1] * cz);
-                        for (int k = cell_start[c]; k < cell_start[c + 1]; ++k)
-                        {
-                            const int j = sorted[k];
-                            const Pos4<float> p = pos[j];
-                            const float d2 = squared_norm(min_image(me.x, p.x, r.cell[0]),
-                                                          min_image(me.y, p.y, r.cell[1]),
-                                                          min_image(me.z, p.z, r.cell[2]));
-                            if (j != i && d2 < r.radius_squared)
-                            {
-                                list.add(j);
-                            }
-                        }
+                        scan_candidates(r, me, i, sorted, cell_start[c], cell_start[c + 1], pos,
+                                        list);
                     }
                 }
             }
         }
         else
         {
-            for (int j = 0; j < n; ++j)
-            {
-                const Pos4<float> p = pos[j];
-                const float d2 = squared_norm(min_image(me.x, p.x, r.cell[0]),
-                                              min_image(me.y, p.y, r.cell[1]),
-                                              min_image(me.z, p.z, r.cell[2]));
-                if (j != i && d2 < r.radius_squared)
-                {
-                    list.add(j);
-                }
-            }
+            scan_candidates(r, me, i, nullptr, 0, n, pos, list);
         }
         list.finish();
-        nbr_count[i] = list.count;
+        nbr_count[row] = list.count;
         if (list.count > r.width)
         {
             atomicOr(status_flags, kOverflow);
@@ -301,18 +320,38 @@ template <bool kKick, bool kEnergy>
 __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, float* vel,
                                float* force, const float* mass, const float* inv_mass,
                                const std::uint16_t* nbr, const index_t* nbr_count,
-                               double& kinetic, double& energy)
+                               const index_t* order, double& kinetic, double& energy)
 {
-    for (int i = threadIdx.x; i < r.n; i += kServeThreads)
+    for (int row = threadIdx.x; row < r.n; row += kServeThreads)
     {
+        const int i = order != nullptr ? order[row] : row;  // the list row's atom
         const Pos4<float> me = pos[i];
-        const int count = nbr_count[i] < r.width ? nbr_count[i] : r.width;
-        const uint4* chunks = reinterpret_cast<const uint4*>(nbr) + chunk_index(i, 0, r.width);
+        const int count = nbr_count[row] < r.width ? nbr_count[row] : r.width;
+        const uint4* chunks = reinterpret_cast<const uint4*>(nbr) + chunk_index(row, 0, r.width);
+        // The kick's inputs are loaded before the pairs, so their latency hides behind them.
+        float v[3] = {0.0f, 0.0f, 0.0f}, w = 0.0f, m = 0.0f;
+        if (kKick)
+        {
+            const float* vi = vel + 3LL * i;
+            v[0] = vi[0];
+            v[1] = vi[1];
+            v[2] = vi[2];
+            w = inv_mass[i];
+            m = mass[i];
+        }
         float fx = 0, fy = 0, fz = 0, esum = 0, inside_count = 0;
         const int full = count / kChunk;
+        const int chunk_count = (count + kChunk - 1) / kChunk;
+        // Each chunk's word is loaded one chunk ahead: a pool's lists are far larger than L2,
+        // so a word comes from DRAM, and its latency now overlaps the previous chunk's pairs.
+        uint4 next = chunk_count > 0 ? chunks[0] : make_uint4(0, 0, 0, 0);
         for (int chunk = 0; chunk < full; ++chunk)
         {
-            const uint4 word = chunks[static_cast<std::int64_t>(chunk) * kWarp];
+            const uint4 word = next;
+            if (chunk + 1 < chunk_count)
+            {
+                next = chunks[static_cast<std::int64_t>(chunk + 1) * kWarp];
+            }
             const unsigned packed[4] = {word.x, word.y, word.z, word.w};
 #pragma unroll
             for (int k = 0; k < kChunk; ++k)
@@ -321,10 +360,9 @@ __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, 
                 serve_pair<kEnergy>(r, me, p, fx, fy, fz, esum, inside_count);
             }
         }
-        if (full * kChunk < count)
+        if (full < chunk_count)
         {
-            const uint4 word = chunks[static_cast<std::int64_t>(full) * kWarp];
-            const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+            const unsigned packed[4] = {next.x, next.y, next.z, next.w};
 #pragma unroll
             for (int k = 0; k < kChunk; ++k)
             {
@@ -348,22 +386,23 @@ __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, 
         f[2] = fz;
         if (kKick)
         {
-            const float kick = r.half_dt * inv_mass[i];
-            float* v = vel + 3LL * i;
+            const float kick = r.half_dt * w;
             const float vx = fmaf(kick, fx, v[0]);
             const float vy = fmaf(kick, fy, v[1]);
             const float vz = fmaf(kick, fz, v[2]);
-            v[0] = vx;
-            v[1] = vy;
-            v[2] = vz;
-            kinetic += 0.5 * double(mass[i]) * (double(vx) * vx + double(vy) * vy + double(vz) * vz);
+            float* vi = vel + 3LL * i;
+            vi[0] = vx;
+            vi[1] = vy;
+            vi[2] = vz;
+            kinetic += 0.5 * double(m) * (double(vx) * vx + double(vy) * vy + double(vz) * vz);
         }
     }
 }
 
 // mode 0: wrap, rebuild and the first forces of newly admitted replicas. mode 1: run each
-// listed replica for min(budget, steps left) NVT steps.
-__global__ void __launch_bounds__(kServeThreads) serve_kernel(ServePool p, const int* slots,
+// listed replica for min(budget, steps left) NVT steps. One CTA per SM, up to 128 registers a
+// thread: held to two CTAs (64 registers) the kernel spills, and measured slower.
+__global__ void __launch_bounds__(kServeThreads, 1) serve_kernel(ServePool p, const int* slots,
                                                               const int* budgets, int mode)
 {
     __shared__ ReplicaScalars r;
@@ -415,14 +454,17 @@ __global__ void __launch_bounds__(kServeThreads) serve_kernel(ServePool p, const
     index_t* sorted = p.sorted + a0;
     index_t* scratch = p.scratch + a0;
     index_t* cell_start = p.cell_start + replica->cell_offset;
+    // List rows follow the cell order on a grid (set by every rebuild), else the atoms.
+    const bool grid = r.dims[0] >= 3 && r.dims[1] >= 3 && r.dims[2] >= 3;
+    const index_t* order = grid ? sorted : nullptr;
 
     if (mode == 0)
     {
         rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start, counts,
                         warp_totals, &flags);
         double kinetic = 0, energy = 0;
-        replica_forces<false, true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, kinetic,
-                                    energy);
+        replica_forces<false, true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, order,
+                                    kinetic, energy);
         energy = block_sum(energy, warp_sums);
         if (threadIdx.x == 0)
         {
@@ -508,12 +550,12 @@ __global__ void __launch_bounds__(kServeThreads) serve_kernel(ServePool p, const
         if (reported)
         {
             replica_forces<true, true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count,
-                                       kinetic, energy);
+                                       order, kinetic, energy);
         }
         else
         {
             replica_forces<true, false>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count,
-                                        kinetic, energy);
+                                        order, kinetic, energy);
         }
         kinetic = block_sum(kinetic, warp_sums);
         if (reported)
