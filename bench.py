@@ -327,12 +327,12 @@ def run_reference(args) -> None:
 
 
 def serve_requests(device, ranks, requests: int, rate: float | None, seed: int = 7,
-                   stage_ahead: int = 32) -> dict:
+                   stage_ahead: int = 32, budget_gb: float = 16.0) -> dict:
     """``requests`` independent argon NVT replicas (64-16,384 atoms, 500 steps each) through
-    the replica server, Poisson arrivals at ``rate`` per second (None: all at t = 0). With N
-    ranks each serves its share (replicas.shard_requests by atom-steps) on its own GPU with no
-    collective on the data path; the wall time is the slowest rank's, the latencies are
-    gathered from every rank for p50/p99."""
+    the replica server (a pool of ``budget_gb`` GiB), Poisson arrivals at ``rate`` per second
+    (None: all at t = 0). With N ranks each serves its share (replicas.shard_requests by
+    atom-steps) on its own GPU with no collective on the data path; the wall time is the
+    slowest rank's, the latencies are gathered from every rank for p50/p99."""
     import torch
 
     from nabladyn_b200.replicas import shard_requests
@@ -340,7 +340,7 @@ def serve_requests(device, ranks, requests: int, rate: float | None, seed: int =
 
     work = serving_requests(requests, seed=seed, rate=rate)
     mine = shard_requests([r.steps * r.positions.shape[0] for r in work], ranks.world)[ranks.rank]
-    server = ReplicaServer(device=device, budget_bytes=16 << 30, max_slots=2048,
+    server = ReplicaServer(device=device, budget_bytes=int(budget_gb * (1 << 30)), max_slots=2048,
                            stage_ahead=stage_ahead)
     server.serve(serving_requests(8, seed=99, steps=20), realtime=False)  # warm-up
     torch.cuda.synchronize(device)
@@ -414,10 +414,12 @@ def plain_requests(device, requests: int, sample: int, seed: int = 7) -> dict:
 
 
 def run_serving(device, ranks, requests: int, plain_sample: int,
-                rates: tuple[float | None, ...], stage_ahead: int = 32) -> dict:
+                rates: tuple[float | None, ...], stage_ahead: int = 32,
+                budget_gb: float = 16.0) -> dict:
     """The serving workload at each arrival rate, against the plain path (rank 0 only)."""
     legs = {f"rate_{rate if rate else 'all_at_t0'}": serve_requests(device, ranks, requests, rate,
-                                                                    stage_ahead=stage_ahead)
+                                                                    stage_ahead=stage_ahead,
+                                                                    budget_gb=budget_gb)
             for rate in rates}
     out = {"legs": legs}
     if ranks.rank == 0 and plain_sample:
@@ -1085,6 +1087,8 @@ def main() -> None:
                         help="with --workload serving: Poisson arrivals per second")
     parser.add_argument("--stage-ahead", type=int, default=32,
                         help="serving: arrived requests made ready on the host during a round")
+    parser.add_argument("--serving-budget-gb", type=float, default=16.0,
+                        help="serving: the replica pool's device memory, GiB")
     parser.add_argument("--reference-cuda", choices=("auto", "off"), default="auto",
                         help="auto: time the reference's CUDA path beside ours when installed")
     parser.add_argument("--workload",
@@ -1158,7 +1162,8 @@ def main() -> None:
         ranks = Ranks("nccl", device, timeout_s=300)
         rates = (args.serving_rate,) if args.serving_rate else SERVING_RATES
         result = run_serving(device, ranks, args.serving, plain_sample=16 if ranks.rank == 0 else 0,
-                             rates=rates, stage_ahead=args.stage_ahead)
+                             rates=rates, stage_ahead=args.stage_ahead,
+                             budget_gb=args.serving_budget_gb)
         if ranks.rank == 0:
             print(json.dumps(result), flush=True)
         ranks.close()

@@ -111,14 +111,16 @@ private:
 };
 
 // The dynamic shared memory one kernel may use on each device: raised when a launch needs more
-// than any launch before it on that device (launches up to 48 KB need no raise).
+// than any launch before it on that device. A kernel gets 48 KB of static and dynamic shared
+// memory together without the raise, so the kernel's static bytes (read once per device)
+// count against that limit.
 class DeviceGrant
 {
 public:
     template <typename Kernel>
     cudaError_t allow(Kernel kernel, std::size_t bytes)
     {
-        if (bytes <= 48 * 1024)
+        if (bytes == 0)
         {
             return cudaSuccess;
         }
@@ -137,18 +139,35 @@ public:
         {
             return cudaSuccess;
         }
-        rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(bytes));
-        if (rc == cudaSuccess)
+        if (!static_known_[device])
         {
-            granted_[device] = bytes;
+            cudaFuncAttributes attributes{};
+            rc = cudaFuncGetAttributes(&attributes, kernel);
+            if (rc != cudaSuccess)
+            {
+                return rc;
+            }
+            static_bytes_[device] = attributes.sharedSizeBytes;
+            static_known_[device] = true;
         }
-        return rc;
+        if (bytes + static_bytes_[device] > 48 * 1024)
+        {
+            rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(bytes));
+            if (rc != cudaSuccess)
+            {
+                return rc;
+            }
+        }
+        granted_[device] = bytes;
+        return cudaSuccess;
     }
 
 private:
     std::mutex mutex_;
     std::size_t granted_[kMaxDevices] = {};
+    std::size_t static_bytes_[kMaxDevices] = {};
+    bool static_known_[kMaxDevices] = {};
 };
 
 // The current device's multiprocessor count, looked up once per device.

@@ -302,3 +302,32 @@ def test_melting_lattice_keeps_its_pair_lists(cuda):
     _, f64, _ = lj.energy_force_virial(x, cell, first, second, [0.34], [0.996], 1.0)
     error = np.linalg.norm(state.forces.cpu().double().numpy() - f64) / np.linalg.norm(f64)
     assert error < 1e-5
+
+
+def test_small_box_tile_near_the_default_shared_memory(cuda):
+    """3,040 atoms in a 5.0 nm box with a 1.6 nm cutoff take the small-box path with a
+    48,656-B tile: under 48 KB alone, over it with the force kernel's static shared memory, so
+    the launch needs the raised limit. The first frame's forces and energy match the oracle,
+    and the one-launch run steps on."""
+    positions, cell = lattice.simple_cubic(15, 5.0, 0.01, seed=3040, count=3040)
+    n = positions.shape[0]
+    model = potential.lennard_jones(
+        atom_types=torch.zeros(n, dtype=torch.int64, device=cuda),
+        sigma=torch.tensor([0.34], device=cuda), epsilon=torch.tensor([0.996], device=cuda),
+        cutoff=1.6,
+    )
+    masses = torch.full((n,), 39.948, device=cuda)
+    velocities = md.maxwell_boltzmann(masses, 120.0, seed=3040)
+    simulation = md.nve(model, torch.tensor(positions, dtype=torch.float32, device=cuda),
+                        velocities, masses, torch.tensor(cell, dtype=torch.float32, device=cuda),
+                        timestep=0.002)
+    assert simulation._engine.small and simulation._engine.runs_in_one_launch
+    state = simulation.state()
+    cell64 = np.asarray(cell, dtype=np.float64)
+    x = on.wrap(state.positions.cpu().double().numpy(), cell64)
+    first, second, _ = on.pairs(x, cell64, 1.6)
+    _, f64, _ = lj.energy_force_virial(x, cell64, first, second, [0.34], [0.996], 1.6)
+    error = np.linalg.norm(state.forces.cpu().double().numpy() - f64) / np.linalg.norm(f64)
+    assert error < 1e-5
+    simulation.run(20)
+    assert np.isfinite(simulation.state().positions.cpu().numpy()).all()
