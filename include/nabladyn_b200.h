@@ -346,6 +346,7 @@ typedef struct nd_replica_pool {
     int32_t* sorted;           /* [atoms] */
     int32_t* scratch;          /* [atoms] */
     int32_t* cell_starts;      /* the cell tables */
+    void* ordered_positions;   /* [atoms, 4] float32: the last rebuild's positions in cell order */
 } nd_replica_pool;
 
 /* A CUDA graph of `steps` steps of the system (no virial) whose rebuild kernels run in the body

@@ -203,6 +203,7 @@ class ReplicaPool(ctypes.Structure):
         ("sorted", ctypes.c_void_p),
         ("scratch", ctypes.c_void_p),
         ("cell_starts", ctypes.c_void_p),
+        ("ordered_positions", ctypes.c_void_p),
     ]
 
 

@@ -43,6 +43,7 @@ struct ServePool
     index_t* sorted;
     index_t* scratch;
     index_t* cell_start;
+    Pos4<float>* ordered;
 };
 
 // The scalar fields of one replica, in shared memory for the CTA.
@@ -133,11 +134,11 @@ __device__ void block_scan_cells(int* counts, int cells, int* warp_totals)
     __syncthreads();
 }
 
-// Adds to `list` the candidates k = begin .. end - 1 (atom order[k], or k without an order)
-// closer to `me` (atom i) than the list radius, in k order. Four candidates at a time: their
-// indices and positions are loaded before any is tested, so the loads of a group overlap.
+// Adds to `list` the atoms k = begin .. end - 1 closer to `me` (atom i) than the list radius
+// under the minimum image, in k order (the all-pairs path of a replica with fewer than three
+// cells along an axis). Four candidates at a time, loaded before any is tested.
 __device__ __forceinline__ void scan_candidates(const ReplicaScalars& r, const Pos4<float>& me,
-                                                int i, const index_t* order, int begin, int end,
+                                                int i, int begin, int end,
                                                 const Pos4<float>* pos, ListWriter& list)
 {
     constexpr int kGroup = 4;
@@ -148,7 +149,7 @@ __device__ __forceinline__ void scan_candidates(const ReplicaScalars& r, const P
 #pragma unroll
         for (int u = 0; u < kGroup; ++u)
         {
-            j[u] = k + u < end ? (order != nullptr ? order[k + u] : k + u) : -1;
+            j[u] = k + u < end ? k + u : -1;
         }
 #pragma unroll
         for (int u = 0; u < kGroup; ++u)
@@ -169,12 +170,75 @@ __device__ __forceinline__ void scan_candidates(const ReplicaScalars& r, const P
     }
 }
 
+// The image of one stencil cell along an axis: the cell index h + d wrapped into [0, dims),
+// and which side of the displacement takes the period. Past the upper face the center moves
+// (center - L), past the lower face the candidate does (candidate - L): the two forms the
+// minimum image rounds (min_image), so every candidate within the radius gets the bits the
+// per-candidate minimum image gives it (the radius is below half the period: on a grid every
+// axis has at least three cells at least one radius wide, and a displacement under the radius
+// along an axis has one image within half the period).
+struct AxisImage
+{
+    int cell;
+    float center_shift;
+    float candidate_shift;
+};
+
+__device__ __forceinline__ AxisImage axis_image(int h, int d, int dims, float length)
+{
+    AxisImage a{h + d, 0.0f, 0.0f};
+    if (a.cell < 0)
+    {
+        a.cell += dims;
+        a.candidate_shift = length;
+    }
+    else if (a.cell >= dims)
+    {
+        a.cell -= dims;
+        a.center_shift = length;
+    }
+    return a;
+}
+
+// Adds to `list` the candidates of one stencil cell, k = begin .. end - 1 of the cell-ordered
+// copy (x, y, z, and the atom's index in w), that lie closer than the list radius to the
+// center (cell-order row `self`), in k order: one 16-B load per candidate, no index lookup
+// and no per-candidate image choice. Four candidates at a time, loaded before any is tested.
+__device__ __forceinline__ void scan_cell(const ReplicaScalars& r, float cx, float cy, float cz,
+                                          float sx, float sy, float sz, int self,
+                                          const Pos4<float>* __restrict__ ordered, int begin,
+                                          int end, ListWriter& list)
+{
+    constexpr int kGroup = 4;
+    for (int k = begin; k < end; k += kGroup)
+    {
+        Pos4<float> p[kGroup];
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u)
+        {
+            p[u] = k + u < end ? ordered[k + u] : far_atom<float>();
+        }
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u)
+        {
+            const float d2 = squared_norm(cx - (p[u].x - sx), cy - (p[u].y - sy),
+                                          cz - (p[u].z - sz));
+            if (k + u < end && k + u != self && d2 < r.radius_squared)
+            {
+                list.add(static_cast<unsigned>(__float_as_int(p[u].w)));
+            }
+        }
+    }
+}
+
 // Wraps the positions (counting crossings into the images), stores the reference frame and
-// rebuilds the list. Called by the whole CTA.
+// rebuilds the list. Called by the whole CTA. On a grid, `ordered` receives the wrapped
+// positions in cell order with each atom's index in w, which the candidate scan reads.
 __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<float>* ref,
                                 long long* images, std::uint16_t* nbr, index_t* nbr_count,
                                 index_t* sorted, index_t* scratch, index_t* cell_start,
-                                int* counts, int* warp_totals, int* status_flags)
+                                Pos4<float>* ordered, int* counts, int* warp_totals,
+                                int* status_flags)
 {
     const int n = r.n;
     for (int i = threadIdx.x; i < n; i += kServeThreads)
@@ -239,43 +303,52 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
             }
         }
         __syncthreads();
+        for (int row = threadIdx.x; row < n; row += kServeThreads)
+        {
+            const int atom = sorted[row];
+            Pos4<float> p = pos[atom];
+            p.w = __int_as_float(atom);
+            ordered[row] = p;
+        }
     }
-    else
-    {
-        __syncthreads();
-    }
+    __syncthreads();
     // The list: every neighbor j != i closer than the list radius, minimum image. Row `row`
     // holds the list of atom sorted[row] on a grid (the lanes of a warp take atoms of one or
-    // two cells, whose candidates they share), of atom `row` otherwise.
+    // two cells, whose candidates they share), of atom `row` otherwise. On a grid the 27
+    // stencil cells are scanned in the same order as cells and candidates in cell order, each
+    // cell with its image, so a list holds the same entries in the same order as a scan of
+    // every candidate with its own minimum image.
     for (int row = threadIdx.x; row < n; row += kServeThreads)
     {
-        const int i = grid ? sorted[row] : row;
-        const Pos4<float> me = pos[i];
         ListWriter list(nbr, r.width, row, 0xffffu);
         if (grid)
         {
+            const Pos4<float> me = ordered[row];
             const int hx = axis_bin(me.x, r.widths[0], r.dims[0]);
             const int hy = axis_bin(me.y, r.widths[1], r.dims[1]);
             const int hz = axis_bin(me.z, r.widths[2], r.dims[2]);
             for (int dz = -1; dz <= 1; ++dz)
             {
-                const int cz = (hz + dz + r.dims[2]) % r.dims[2];
+                const AxisImage iz = axis_image(hz, dz, r.dims[2], r.cell[2]);
+                const float cz = me.z - iz.center_shift;
                 for (int dy = -1; dy <= 1; ++dy)
                 {
-                    const int cy = (hy + dy + r.dims[1]) % r.dims[1];
+                    const AxisImage iy = axis_image(hy, dy, r.dims[1], r.cell[1]);
+                    const float cy = me.y - iy.center_shift;
                     for (int dx = -1; dx <= 1; ++dx)
                     {
-                        const int cx = (hx + dx + r.dims[0]) % r.dims[0];
-                        const int c = cx + r.dims[0] * (cy + r.dims[1] * cz);
-                        scan_candidates(r, me, i, sorted, cell_start[c], cell_start[c + 1], pos,
-                                        list);
+                        const AxisImage ix = axis_image(hx, dx, r.dims[0], r.cell[0]);
+                        const int c = ix.cell + r.dims[0] * (iy.cell + r.dims[1] * iz.cell);
+                        scan_cell(r, me.x - ix.center_shift, cy, cz, ix.candidate_shift,
+                                  iy.candidate_shift, iz.candidate_shift, row, ordered, counts[c],
+                                  counts[c + 1], list);
                     }
                 }
             }
         }
         else
         {
-            scan_candidates(r, me, i, nullptr, 0, n, pos, list);
+            scan_candidates(r, pos[row], row, 0, n, pos, list);
         }
         list.finish();
         nbr_count[row] = list.count;
@@ -454,14 +527,15 @@ __global__ void __launch_bounds__(kServeThreads, 1) serve_kernel(ServePool p, co
     index_t* sorted = p.sorted + a0;
     index_t* scratch = p.scratch + a0;
     index_t* cell_start = p.cell_start + replica->cell_offset;
+    Pos4<float>* ordered = p.ordered + a0;
     // List rows follow the cell order on a grid (set by every rebuild), else the atoms.
     const bool grid = r.dims[0] >= 3 && r.dims[1] >= 3 && r.dims[2] >= 3;
     const index_t* order = grid ? sorted : nullptr;
 
     if (mode == 0)
     {
-        rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start, counts,
-                        warp_totals, &flags);
+        rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start, ordered,
+                        counts, warp_totals, &flags);
         double kinetic = 0, energy = 0;
         replica_forces<false, true>(r, pos, vel, force, mass, inv_mass, nbr, nbr_count, order,
                                     kinetic, energy);
@@ -538,7 +612,7 @@ __global__ void __launch_bounds__(kServeThreads, 1) serve_kernel(ServePool p, co
         if (__syncthreads_or(moved))
         {
             rebuild_replica(r, pos, ref, images, nbr, nbr_count, sorted, scratch, cell_start,
-                            counts, warp_totals, &flags);
+                            ordered, counts, warp_totals, &flags);
             if (threadIdx.x == 0)
             {
                 ++r.rebuild_count;
@@ -613,7 +687,8 @@ extern "C" int nd_serve_run(const nd_replica_pool* pool, const int32_t* slots,
     ND_REQUIRE(pool->replicas && pool->positions && pool->velocities && pool->forces &&
                    pool->masses && pool->inverse_masses && pool->images &&
                    pool->reference_positions && pool->neighbors && pool->neighbor_counts &&
-                   pool->sorted && pool->scratch && pool->cell_starts,
+                   pool->sorted && pool->scratch && pool->cell_starts &&
+                   pool->ordered_positions,
                "a pool buffer is null");
     if (count == 0)
     {
@@ -633,6 +708,7 @@ extern "C" int nd_serve_run(const nd_replica_pool* pool, const int32_t* slots,
     p.sorted = pool->sorted;
     p.scratch = pool->scratch;
     p.cell_start = pool->cell_starts;
+    p.ordered = static_cast<nd::Pos4<float>*>(pool->ordered_positions);
     nd::serve_kernel<<<count, nd::kServeThreads, 0, static_cast<cudaStream_t>(stream)>>>(
         p, slots, budgets, mode);
     ND_LAUNCH_CHECK();

@@ -38,7 +38,7 @@ from ..units import BOLTZMANN
 _ALIGN = 32          # atoms per allocation unit (one warp of list chunks)
 _MAX_CELLS = 4096    # kServeMaxCells in serve.cu
 _WIDTH = 192         # list slots per atom: room for ~1.5x the mean count at 22 atoms/nm^3
-_BYTES_PER_ATOM = 16 + 12 + 12 + 4 + 4 + 24 + 16 + 2 * _WIDTH + 4 + 4 + 4
+_BYTES_PER_ATOM = 16 + 12 + 12 + 4 + 4 + 24 + 16 + 2 * _WIDTH + 4 + 4 + 4 + 16
 _CHAIN_A, _KINETIC_A, _PENDING, _CHAIN_MASS, _KT, _DEGREES, _TIMESTEP = 0, 6, 14, 16, 19, 20, 21
 
 
@@ -140,6 +140,7 @@ class ReplicaServer:
             "sorted": torch.zeros(n, **i32),
             "scratch": torch.zeros(n, **i32),
             "cell_starts": torch.zeros(self.max_slots * (_MAX_CELLS + 1), **i32),
+            "ordered_positions": torch.zeros((n, 4), **f32),
         }
         self.table = torch.zeros(self.max_slots * ctypes.sizeof(Replica), dtype=torch.uint8,
                                  device=dev)

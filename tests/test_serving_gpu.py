@@ -6,11 +6,14 @@ Tolerances: float32 replicas against the reference's float32 20-step trajectory 
 2e-3 nm/ps (two float32 summation orders); alone against mixed exactly.
 """
 
+import ctypes
+
 import numpy as np
 import pytest
 import torch
 
 from nabladyn_b200 import lattice
+from nabladyn_b200._native import Replica
 from nabladyn_b200.serving import ReplicaRequest, ReplicaServer, serving_requests
 from oracle import lj
 from oracle import neighbors as on
@@ -66,6 +69,53 @@ def test_grid_replica_energy_against_oracle(cuda):
     first, second, _ = on.pairs(wrapped, cell, 1.0)
     energy, _, _ = lj.energy_force_virial(wrapped, cell, first, second, [0.34], [0.996], 1.0)
     assert result.energy == pytest.approx(energy, rel=1e-5)
+
+
+def _served_lists(server, slot: int):
+    """The replica's lists as of its last rebuild, read from the pool: (atom, neighbor) for
+    every entry, the reference frame (that rebuild's wrapped positions) and its record."""
+    size = ctypes.sizeof(Replica)
+    raw = server.table.view(server.max_slots, size)[slot].cpu().numpy().tobytes()
+    record = Replica.from_buffer_copy(raw)
+    n, width, a0 = record.num_atoms, record.width, record.atom_offset
+    b = server.buffers
+    reference = b["reference_positions"][a0:a0 + n, :3].cpu().numpy()
+    order = b["sorted"][a0:a0 + n].cpu().numpy()
+    counts = b["neighbor_counts"][a0:a0 + n].cpu().numpy()
+    words = b["neighbors"].view(torch.int16).cpu().numpy().view(np.uint16)
+    words = words[record.list_offset:record.list_offset + n * width]
+    assert counts.max() <= width
+    rows = np.repeat(np.arange(n), counts)
+    slots = np.concatenate([np.arange(c) for c in counts])
+    # chunk c of row r is 16-B word ((r / 32) * width / 8 + c) * 32 + r % 32
+    word = ((rows >> 5) * (width // 8) + slots // 8) * 32 + (rows & 31)
+    neighbors = words[word * 8 + slots % 8].astype(np.int64)
+    return order[rows].astype(np.int64), neighbors, reference, record
+
+
+def test_grid_replica_lists_equal_minimum_image_scan(cuda):
+    # The in-CTA rebuild scans each stencil cell with one image per cell; its lists must hold
+    # exactly the pairs a per-candidate minimum image puts within the list radius (the oracle's
+    # all-pairs path, contraction pinned), after rebuilds along a trajectory.
+    positions, cell = lattice.fcc(10, 10 * 0.5745, 0.03, seed=21)  # 4,000 atoms, 5 cells/axis
+    velocities = np.random.default_rng(22).normal(0.0, 0.4, positions.shape)
+    request = ReplicaRequest(positions=positions, velocities=velocities,
+                             masses=np.full(len(positions), 39.948), cell=cell,
+                             temperature=300.0, steps=80, name="grid")
+    server = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=1)
+    result = server.serve([request], realtime=False)[0]
+    assert result.status == 0 and result.rebuilds >= 3
+    atoms, neighbors, reference, record = _served_lists(server, 0)
+    assert min(record.dims) >= 3
+    cell32 = np.asarray(record.cell, dtype=np.float32)
+    first, second, path = on.pairs(reference.astype(np.float32), cell32,
+                                   float(np.float32(record.radius)), dims=(3, 3, 3))
+    assert path == "all"
+    n = record.num_atoms
+    want = np.sort(np.concatenate([first * n + second, second * n + first]).astype(np.int64))
+    got = np.sort(atoms * n + neighbors)
+    assert len(np.unique(got)) == len(got)  # no entry twice
+    np.testing.assert_array_equal(got, want)
 
 
 def test_admission_stays_within_budget(cuda):
