@@ -314,35 +314,52 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
     __syncthreads();
     // The list: every neighbor j != i closer than the list radius, minimum image. Row `row`
     // holds the list of atom sorted[row] on a grid (the lanes of a warp take atoms of one or
-    // two cells, whose candidates they share), of atom `row` otherwise. On a grid the 27
-    // stencil cells are scanned in the same order as cells and candidates in cell order, each
-    // cell with its image, so a list holds the same entries in the same order as a scan of
-    // every candidate with its own minimum image.
+    // two cells, whose candidates they share), of atom `row` otherwise. On a grid the stencil
+    // is scanned in two passes, each in stencil order with candidates in cell order: first the
+    // cells that need no image, whose entries (the "direct" ones) keep the plain difference as
+    // their minimum image until the next rebuild, then the cells across a face. Each cell is
+    // scanned with its image, so the entries are those of a scan of every candidate with its
+    // own minimum image. nbr_count[row] holds the count in its low 16 bits and the direct
+    // entries in its high 16 bits (a count is at most N - 1 < 2^16).
     for (int row = threadIdx.x; row < n; row += kServeThreads)
     {
         ListWriter list(nbr, r.width, row, 0xffffu);
+        int direct = 0;
         if (grid)
         {
             const Pos4<float> me = ordered[row];
             const int hx = axis_bin(me.x, r.widths[0], r.dims[0]);
             const int hy = axis_bin(me.y, r.widths[1], r.dims[1]);
             const int hz = axis_bin(me.z, r.widths[2], r.dims[2]);
-            for (int dz = -1; dz <= 1; ++dz)
+            for (int pass = 0; pass < 2; ++pass)
             {
-                const AxisImage iz = axis_image(hz, dz, r.dims[2], r.cell[2]);
-                const float cz = me.z - iz.center_shift;
-                for (int dy = -1; dy <= 1; ++dy)
+                for (int dz = -1; dz <= 1; ++dz)
                 {
-                    const AxisImage iy = axis_image(hy, dy, r.dims[1], r.cell[1]);
-                    const float cy = me.y - iy.center_shift;
-                    for (int dx = -1; dx <= 1; ++dx)
+                    const AxisImage iz = axis_image(hz, dz, r.dims[2], r.cell[2]);
+                    const float cz = me.z - iz.center_shift;
+                    for (int dy = -1; dy <= 1; ++dy)
                     {
-                        const AxisImage ix = axis_image(hx, dx, r.dims[0], r.cell[0]);
-                        const int c = ix.cell + r.dims[0] * (iy.cell + r.dims[1] * iz.cell);
-                        scan_cell(r, me.x - ix.center_shift, cy, cz, ix.candidate_shift,
-                                  iy.candidate_shift, iz.candidate_shift, row, ordered, counts[c],
-                                  counts[c + 1], list);
+                        const AxisImage iy = axis_image(hy, dy, r.dims[1], r.cell[1]);
+                        const float cy = me.y - iy.center_shift;
+                        for (int dx = -1; dx <= 1; ++dx)
+                        {
+                            const AxisImage ix = axis_image(hx, dx, r.dims[0], r.cell[0]);
+                            const bool imaged = hx + dx != ix.cell || hy + dy != iy.cell ||
+                                                hz + dz != iz.cell;
+                            if (imaged != (pass == 1))
+                            {
+                                continue;
+                            }
+                            const int c = ix.cell + r.dims[0] * (iy.cell + r.dims[1] * iz.cell);
+                            scan_cell(r, me.x - ix.center_shift, cy, cz, ix.candidate_shift,
+                                      iy.candidate_shift, iz.candidate_shift, row, ordered,
+                                      counts[c], counts[c + 1], list);
+                        }
                     }
+                }
+                if (pass == 0)
+                {
+                    direct = list.count;
                 }
             }
         }
@@ -351,7 +368,7 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
             scan_candidates(r, pos[row], row, 0, n, pos, list);
         }
         list.finish();
-        nbr_count[row] = list.count;
+        nbr_count[row] = list.count | (direct << 16);
         if (list.count > r.width)
         {
             atomicOr(status_flags, kOverflow);
@@ -361,14 +378,18 @@ __device__ void rebuild_replica(const ReplicaScalars& r, Pos4<float>* pos, Pos4<
 }
 
 // One list entry's pair term, added to the center's sums (an exact zero outside the cutoff).
-template <bool kEnergy>
+// With kImage the displacement takes the minimum image; without, it is the plain difference,
+// which is what the minimum image gives a direct entry (see rebuild_replica): the entry was
+// within the list radius with no image at the rebuild, neither atom has moved half the skin
+// since, and the period is more than twice the radius plus the skin on a grid.
+template <bool kEnergy, bool kImage>
 __device__ __forceinline__ void serve_pair(const ReplicaScalars& r, const Pos4<float>& me,
                                            const Pos4<float>& p, float& fx, float& fy, float& fz,
                                            float& esum, float& inside_count)
 {
-    const float dx = min_image(me.x, p.x, r.cell[0]);
-    const float dy = min_image(me.y, p.y, r.cell[1]);
-    const float dz = min_image(me.z, p.z, r.cell[2]);
+    const float dx = kImage ? min_image(me.x, p.x, r.cell[0]) : me.x - p.x;
+    const float dy = kImage ? min_image(me.y, p.y, r.cell[1]) : me.y - p.y;
+    const float dz = kImage ? min_image(me.z, p.z, r.cell[2]) : me.z - p.z;
     const float r2 = squared_norm(dx, dy, dz);
     const float mask = r2 < r.cutoff_squared ? 1.0f : 0.0f;
     const float inv_r2 = fast_reciprocal(r2);
@@ -385,6 +406,22 @@ __device__ __forceinline__ void serve_pair(const ReplicaScalars& r, const Pos4<f
     fz = fmaf(fs, dz, fz);
 }
 
+// The eight entries of one list word.
+template <bool kEnergy, bool kImage>
+__device__ __forceinline__ void serve_chunk(const ReplicaScalars& r, const Pos4<float>* pos,
+                                            const Pos4<float>& me, const uint4& word, float& fx,
+                                            float& fy, float& fz, float& esum,
+                                            float& inside_count)
+{
+    const unsigned packed[4] = {word.x, word.y, word.z, word.w};
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k)
+    {
+        const Pos4<float> p = pos[(packed[k / 2] >> (16 * (k % 2))) & 0xffffu];
+        serve_pair<kEnergy, kImage>(r, me, p, fx, fy, fz, esum, inside_count);
+    }
+}
+
 // Forces at the current positions; with `kKick`, also the second half kick, returning the
 // thread's part of K (float64); with `kEnergy`, the thread's part of E (a step needs E only
 // when its energy is reported: the last step of a round). Whole chunks of the list go through
@@ -395,11 +432,18 @@ __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, 
                                const std::uint16_t* nbr, const index_t* nbr_count,
                                const index_t* order, double& kinetic, double& energy)
 {
-    for (int row = threadIdx.x; row < r.n; row += kServeThreads)
+    for (int base = 0; base < r.n; base += kServeThreads)
     {
+        const int row = base + static_cast<int>(threadIdx.x);
+        const unsigned active = __ballot_sync(kFullMask, row < r.n);
+        if (row >= r.n)
+        {
+            break;
+        }
         const int i = order != nullptr ? order[row] : row;  // the list row's atom
         const Pos4<float> me = pos[i];
-        const int count = nbr_count[row] < r.width ? nbr_count[row] : r.width;
+        const int listed = nbr_count[row] & 0xffff;
+        const int count = listed < r.width ? listed : r.width;
         const uint4* chunks = reinterpret_cast<const uint4*>(nbr) + chunk_index(row, 0, r.width);
         // The kick's inputs are loaded before the pairs, so their latency hides behind them.
         float v[3] = {0.0f, 0.0f, 0.0f}, w = 0.0f, m = 0.0f;
@@ -415,22 +459,41 @@ __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, 
         float fx = 0, fy = 0, fz = 0, esum = 0, inside_count = 0;
         const int full = count / kChunk;
         const int chunk_count = (count + kChunk - 1) / kChunk;
+        // The whole words of direct entries come first; the word that holds the last direct
+        // entry and every later one take the minimum image (which gives a direct entry the
+        // same bits as the plain difference).
+        const int direct_words = min((nbr_count[row] >> 16) / kChunk, full);
         // Each chunk's word is loaded one chunk ahead: a pool's lists are far larger than L2,
         // so a word comes from DRAM, and its latency now overlaps the previous chunk's pairs.
         uint4 next = chunk_count > 0 ? chunks[0] : make_uint4(0, 0, 0, 0);
-        for (int chunk = 0; chunk < full; ++chunk)
-        {
+        auto advance = [&](int chunk) {
             const uint4 word = next;
             if (chunk + 1 < chunk_count)
             {
                 next = chunks[static_cast<std::int64_t>(chunk + 1) * kWarp];
             }
-            const unsigned packed[4] = {word.x, word.y, word.z, word.w};
-#pragma unroll
-            for (int k = 0; k < kChunk; ++k)
+            return word;
+        };
+        // One vote per word keeps the choice uniform over the warp, whose rows are the atoms of
+        // one or two cells: the plain difference when every lane's word is direct.
+        const int warp_full = __reduce_max_sync(active, full);
+        for (int chunk = 0; chunk < warp_full; ++chunk)
+        {
+            const bool mine = chunk < full;
+            const bool direct = __all_sync(active, !mine || chunk < direct_words);
+            if (mine)
             {
-                const Pos4<float> p = pos[(packed[k / 2] >> (16 * (k % 2))) & 0xffffu];
-                serve_pair<kEnergy>(r, me, p, fx, fy, fz, esum, inside_count);
+                const uint4 word = advance(chunk);
+                if (direct)
+                {
+                    serve_chunk<kEnergy, false>(r, pos, me, word, fx, fy, fz, esum,
+                                                inside_count);
+                }
+                else
+                {
+                    serve_chunk<kEnergy, true>(r, pos, me, word, fx, fy, fz, esum,
+                                               inside_count);
+                }
             }
         }
         if (full < chunk_count)
@@ -442,7 +505,7 @@ __device__ void replica_forces(const ReplicaScalars& r, const Pos4<float>* pos, 
                 if (full * kChunk + k < count)
                 {
                     const Pos4<float> p = pos[(packed[k / 2] >> (16 * (k % 2))) & 0xffffu];
-                    serve_pair<kEnergy>(r, me, p, fx, fy, fz, esum, inside_count);
+                    serve_pair<kEnergy, true>(r, me, p, fx, fy, fz, esum, inside_count);
                 }
             }
         }

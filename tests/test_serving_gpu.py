@@ -73,7 +73,8 @@ def test_grid_replica_energy_against_oracle(cuda):
 
 def _served_lists(server, slot: int):
     """The replica's lists as of its last rebuild, read from the pool: (atom, neighbor) for
-    every entry, the reference frame (that rebuild's wrapped positions) and its record."""
+    every entry, whether the entry is a direct one (listed before the row's entries that need
+    an image), the reference frame (that rebuild's wrapped positions) and its record."""
     size = ctypes.sizeof(Replica)
     raw = server.table.view(server.max_slots, size)[slot].cpu().numpy().tobytes()
     record = Replica.from_buffer_copy(raw)
@@ -81,7 +82,9 @@ def _served_lists(server, slot: int):
     b = server.buffers
     reference = b["reference_positions"][a0:a0 + n, :3].cpu().numpy()
     order = b["sorted"][a0:a0 + n].cpu().numpy()
-    counts = b["neighbor_counts"][a0:a0 + n].cpu().numpy()
+    packed = b["neighbor_counts"][a0:a0 + n].cpu().numpy()
+    counts, direct = packed & 0xFFFF, packed >> 16
+    assert np.all(direct <= counts)
     words = b["neighbors"].view(torch.int16).cpu().numpy().view(np.uint16)
     words = words[record.list_offset:record.list_offset + n * width]
     assert counts.max() <= width
@@ -90,7 +93,7 @@ def _served_lists(server, slot: int):
     # chunk c of row r is 16-B word ((r / 32) * width / 8 + c) * 32 + r % 32
     word = ((rows >> 5) * (width // 8) + slots // 8) * 32 + (rows & 31)
     neighbors = words[word * 8 + slots % 8].astype(np.int64)
-    return order[rows].astype(np.int64), neighbors, reference, record
+    return order[rows].astype(np.int64), neighbors, slots < direct[rows], reference, record
 
 
 def test_grid_replica_lists_equal_minimum_image_scan(cuda):
@@ -105,7 +108,7 @@ def test_grid_replica_lists_equal_minimum_image_scan(cuda):
     server = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=1)
     result = server.serve([request], realtime=False)[0]
     assert result.status == 0 and result.rebuilds >= 3
-    atoms, neighbors, reference, record = _served_lists(server, 0)
+    atoms, neighbors, direct, reference, record = _served_lists(server, 0)
     assert min(record.dims) >= 3
     cell32 = np.asarray(record.cell, dtype=np.float32)
     first, second, path = on.pairs(reference.astype(np.float32), cell32,
@@ -116,6 +119,16 @@ def test_grid_replica_lists_equal_minimum_image_scan(cuda):
     got = np.sort(atoms * n + neighbors)
     assert len(np.unique(got)) == len(got)  # no entry twice
     np.testing.assert_array_equal(got, want)
+    # Direct entries are evaluated without the minimum image until the next rebuild: at the
+    # rebuild, their plain difference was within the list radius on every axis.
+    plain = np.abs(reference[atoms[direct]] - reference[neighbors[direct]])
+    assert direct.mean() > 0.5 and np.all(plain < np.float32(record.radius))
+    # The last step's energy, from lists reused since that rebuild, against the oracle at the
+    # final positions.
+    final = result.positions.astype(np.float64)
+    first, second, _ = on.pairs(final, cell, 1.0)
+    energy, _, _ = lj.energy_force_virial(final, cell, first, second, [0.34], [0.996], 1.0)
+    assert result.energy == pytest.approx(energy, rel=1e-5)
 
 
 def test_admission_stays_within_budget(cuda):
