@@ -1057,9 +1057,9 @@ def run_ours(args) -> None:
             },
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps_per_call": chunk},
-            # Per step the drift, the rebuild condition, the forces and their finalize; the
+            # Per step the drift (which also sets the rebuild condition) and the forces; the
             # rebuild's kernels only in steps whose conditional node takes the rebuild.
-            "gpu_launches": (4 * args.steps + rebuilds * (engine.step_launches - 3)
+            "gpu_launches": (2 * args.steps + rebuilds * (engine.step_launches - 2)
                              if not engine.small else engine.step_launches * args.steps),
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,

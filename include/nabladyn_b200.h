@@ -249,7 +249,8 @@ typedef struct nd_md_system {
     int32_t* neighbor_counts; /* [rows] */
     int32_t* pair_order;     /* [2 * (rows / 2 + 1)]: per brick its center pairs, longest
                               * lists first, as (pair, first center << 1 | has a second) */
-    int32_t* rebuild;        /* [1] */
+    int32_t* rebuild;        /* [2]: the reuse check's flag; a count the step graph's drift
+                              * kernel keeps (zero between steps) */
     int32_t* rebuild_count;  /* [1] */
     int32_t* status;         /* [4]: flags, most neighbors needed, largest tile needed, largest tile built */
     double* partials;        /* [nd_md_partial_slots]: per-block float64 sums */
@@ -289,7 +290,8 @@ int nd_md_step_phase(const nd_md_system* system, int phase, int thermostat, int 
  * counterpart in the reference (its small-box step is the same graph as any other). */
 int nd_md_run_small(const nd_md_system* system, int thermostat, int steps, nd_stream_t stream);
 
-/* The number of kernels one nd_md_step launches. */
+/* The number of kernels one NVE nd_md_step without the virial launches (the drift, the
+ * rebuild's kernels, the forces); an NVT step or one with the virial adds a finalize. */
 int nd_md_step_launches(const nd_md_system* system, int64_t* launches);
 
 /* Writes the frame in the caller's order; any output may be NULL. */

@@ -1147,22 +1147,12 @@ constexpr int kFinalizeThreads = 1024;
 // One block: the fixed-order sum of the block slots into `totals`, then the scalar tail of a
 // step: the rebuild flag cleared for the next check and, for NVT, the closing half step of the
 // chain against this step's K, whose factor the next drift (or a frame read) applies.
-// kSums false: the force kernel reduced nothing (an NVE step without the virial), so only
-// the rebuild flag is cleared and `totals` keep their last values.
-template <bool kThermostat, bool kStep, bool kSums = true>
+template <bool kThermostat, bool kStep>
 __global__ void __launch_bounds__(kFinalizeThreads) finalize_kernel(const double* partials,
                                                                     int blocks, double* totals,
                                                                     double* thermo,
                                                                     index_t* rebuild)
 {
-    if constexpr (!kSums)
-    {
-        if (threadIdx.x == 0)
-        {
-            rebuild[0] = 0;  // the next step's check starts clean
-        }
-        return;
-    }
     __shared__ double warp_sums[kFinalizeThreads / kWarp][kReduced];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     double mine[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1365,6 +1355,11 @@ __device__ __forceinline__ void force_center_split(const System<T>& s,
 
 // Float32 steps are held to 64 registers, so four CTAs share an SM (as their shared memory
 // allows); the other forms keep the registers they need.
+// Whether a force launch reduces anything (and so has a finalize): a frame evaluation always,
+// a step for the thermostat's K or the virial; an NVE step without the virial does not.
+template <bool kVirial, bool kKickStep, bool kThermostat>
+constexpr bool kStepReduces = !kKickStep || kThermostat || kVirial;
+
 template <typename T, bool kKickStep>
 constexpr int force_blocks_per_sm()
 {
@@ -1390,6 +1385,15 @@ __global__ void __launch_bounds__(kMDThreads, force_blocks_per_sm<T, kKickStep>(
     if (threadIdx.x == 0)
     {
         arrivals = 0;
+    }
+    if constexpr (!kStepReduces<kVirial, kKickStep, kThermostat>)
+    {
+        // A step that reduces nothing launches no finalize, so the reuse flag is cleared here
+        // for the next step's check (no kernel reads it after the step's rebuild).
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+        {
+            s.rebuild[0] = 0;
+        }
     }
     double sums[kReduced] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (kSmall)
@@ -1452,10 +1456,15 @@ __global__ void __launch_bounds__(kMDThreads, force_blocks_per_sm<T, kKickStep>(
 
 // ---------------------------------------------------------------------------------------
 // The first half of a step: the deferred thermostat scales, the half kick, the drift, the
-// finiteness check and the reuse check, per atom.
+// finiteness check and the reuse check, per atom. With kCondition (a step graph's drift), the
+// block that finishes last also sets the graph's rebuild condition from the flag, once every
+// block's reuse check is visible to it: each block's first thread fences and takes a ticket
+// from rebuild[1]; the last ticket fences again, reads the flag and the status, sets the
+// condition and puts the count back to zero for the next step (the fence-and-counter pattern
+// of a last-block reduction).
 
-template <typename T, bool kThermostat>
-__global__ void drift_kernel(System<T> s)
+template <typename T, bool kThermostat, bool kCondition>
+__global__ void drift_kernel(System<T> s, cudaGraphConditionalHandle handle)
 {
     __shared__ T scales[2];
     if (kThermostat)
@@ -1491,40 +1500,58 @@ __global__ void drift_kernel(System<T> s)
         __syncthreads();
     }
     const std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= s.n)
+    if (i < s.n)
     {
-        return;
+        T* v = s.vel + 3 * i;
+        const T* f = s.force + 3 * i;
+        const T kick = s.half_dt * s.inv_mass[i];
+        T vx = v[0], vy = v[1], vz = v[2];
+        if (kThermostat)
+        {
+            vx = (vx * scales[0]) * scales[1];
+            vy = (vy * scales[0]) * scales[1];
+            vz = (vz * scales[0]) * scales[1];
+        }
+        vx = fma(kick, f[0], vx);
+        vy = fma(kick, f[1], vy);
+        vz = fma(kick, f[2], vz);
+        Pos4<T> p = s.pos[i];
+        p.x = fma(s.dt, vx, p.x);
+        p.y = fma(s.dt, vy, p.y);
+        p.z = fma(s.dt, vz, p.z);
+        v[0] = vx;
+        v[1] = vy;
+        v[2] = vz;
+        s.pos[i] = p;
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
+        {
+            atomicOr(s.status, kNonFinite);
+        }
+        else
+        {
+            const Pos4<T> r = s.ref_pos[i];
+            if (squared_norm(p.x - r.x, p.y - r.y, p.z - r.z) >= s.threshold_squared)
+            {
+                s.rebuild[0] = 1;  // every writer stores the same value
+            }
+        }
     }
-    T* v = s.vel + 3 * i;
-    const T* f = s.force + 3 * i;
-    const T kick = s.half_dt * s.inv_mass[i];
-    T vx = v[0], vy = v[1], vz = v[2];
-    if (kThermostat)
+    if constexpr (kCondition)
     {
-        vx = (vx * scales[0]) * scales[1];
-        vy = (vy * scales[0]) * scales[1];
-        vz = (vz * scales[0]) * scales[1];
-    }
-    vx = fma(kick, f[0], vx);
-    vy = fma(kick, f[1], vy);
-    vz = fma(kick, f[2], vz);
-    Pos4<T> p = s.pos[i];
-    p.x = fma(s.dt, vx, p.x);
-    p.y = fma(s.dt, vy, p.y);
-    p.z = fma(s.dt, vz, p.z);
-    v[0] = vx;
-    v[1] = vy;
-    v[2] = vz;
-    s.pos[i] = p;
-    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
-    {
-        atomicOr(s.status, kNonFinite);
-        return;
-    }
-    const Pos4<T> r = s.ref_pos[i];
-    if (squared_norm(p.x - r.x, p.y - r.y, p.z - r.z) >= s.threshold_squared)
-    {
-        s.rebuild[0] = 1;  // every writer stores the same value
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            __threadfence();
+            auto* count = reinterpret_cast<unsigned*>(s.rebuild + 1);
+            if (atomicAdd(count, 1u) == gridDim.x - 1)
+            {
+                __threadfence();
+                const volatile index_t* flag = s.rebuild;
+                const volatile index_t* status = s.status;
+                cudaGraphSetConditional(handle, flag[0] != 0 && status[0] == 0 ? 1u : 0u);
+                *count = 0;
+            }
+        }
     }
 }
 
@@ -1899,10 +1926,12 @@ int launch_force_variant(const System<T>& s, cudaStream_t stream)
         ND_CUDA_TRY(grant.allow(kernel, bytes));                                            \
         kernel<<<s.force_blocks, kMDThreads, bytes, stream>>>(s);                           \
         ND_LAUNCH_CHECK();                                                                  \
-        finalize_kernel<kThermostat, kKickStep, !kKickStep || kThermostat || kVirial>        \
-            <<<1, kFinalizeThreads, 0, stream>>>(                                           \
-            s.partials, s.force_blocks, s.totals, s.thermo, s.rebuild);                     \
-        ND_LAUNCH_CHECK();                                                                  \
+        if constexpr (kStepReduces<kVirial, kKickStep, kThermostat>)                       \
+        {                                                                                   \
+            finalize_kernel<kThermostat, kKickStep><<<1, kFinalizeThreads, 0, stream>>>(     \
+                s.partials, s.force_blocks, s.totals, s.thermo, s.rebuild);                 \
+            ND_LAUNCH_CHECK();                                                              \
+        }                                                                                   \
         return ND_OK;                                                                       \
     }
     ND_FORCE_CASE(1, true)
@@ -1931,11 +1960,11 @@ int launch_step(const System<T>& s, std::int64_t num_cells, int thermostat, int 
         const unsigned atoms = blocks_for(s.n);
         if (thermostat)
         {
-            drift_kernel<T, true><<<atoms, kThreads, 0, stream>>>(s);
+            drift_kernel<T, true, false><<<atoms, kThreads, 0, stream>>>(s, 0);
         }
         else
         {
-            drift_kernel<T, false><<<atoms, kThreads, 0, stream>>>(s);
+            drift_kernel<T, false, false><<<atoms, kThreads, 0, stream>>>(s, 0);
         }
         ND_LAUNCH_CHECK();
     }
@@ -1960,7 +1989,7 @@ int launch_step(const System<T>& s, std::int64_t num_cells, int thermostat, int 
     return ND_OK;
 }
 
-// The kernels one step launches, as launch_step issues them.
+// The kernels one NVE step without the virial launches, as launch_step issues them.
 std::int64_t step_launches(const nd_md_system* m)
 {
     const std::int64_t cells = static_cast<std::int64_t>(m->dims[0]) * m->dims[1] * m->dims[2];
@@ -1969,7 +1998,7 @@ std::int64_t step_launches(const nd_md_system* m)
     {
         rebuild += (scan_tiles(cells + 1) <= 1 ? 1 : 3) + 3;  // scan, place, order, permute
     }
-    return 1 + rebuild + 2;  // drift, rebuild, forces and their finalize
+    return 1 + rebuild + 1;  // drift, rebuild, forces (an NVT step adds the finalize)
 }
 
 // ---------------------------------------------------------------------------------------
@@ -2652,16 +2681,10 @@ int launch_small_run(const System<T>& s, int thermostat, int steps, cudaStream_t
 }
 
 // Sets the rebuild branch of a step graph from the device flag the drift kernel wrote.
-__global__ void rebuild_condition_kernel(cudaGraphConditionalHandle handle,
-                                         const index_t* rebuild, const index_t* status)
-{
-    cudaGraphSetConditional(handle, rebuilding(rebuild, status) ? 1u : 0u);
-}
-
 // A graph of `steps` steps in which each step's rebuild kernels sit in the body of a
-// conditional IF node: a one-thread kernel after the drift sets the condition from the device
-// flag, so steps that reuse the list launch only the drift, that kernel, the forces and their
-// finalize. Built by capture into a graph we own (the body by capture into the node's graph).
+// conditional IF node whose condition the drift kernel sets from the device flag, so a step
+// that reuses the list launches only the drift and the forces (and their finalize, when the
+// step reduces anything). Built by capture into a graph we own (the body by capture into the node's graph).
 template <typename T>
 int build_step_graph(const System<T>& s, std::int64_t num_cells, int thermostat, int steps,
                      cudaGraph_t graph)
@@ -2691,11 +2714,6 @@ int build_step_graph(const System<T>& s, std::int64_t num_cells, int thermostat,
     }
     for (int step = 0; step < steps; ++step)
     {
-        int rc = launch_step(s, num_cells, thermostat, 0, 0, main);
-        if (rc != ND_OK)
-        {
-            return fail(rc);
-        }
         cudaGraphConditionalHandle handle;
         if (cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault) !=
             cudaSuccess)
@@ -2703,7 +2721,20 @@ int build_step_graph(const System<T>& s, std::int64_t num_cells, int thermostat,
             set_error("a step graph could not create its conditional handle");
             return fail(ND_ECUDA);
         }
-        rebuild_condition_kernel<<<1, 1, 0, main>>>(handle, s.rebuild, s.status);
+        const unsigned atoms = blocks_for(s.n);
+        if (thermostat)
+        {
+            drift_kernel<T, true, true><<<atoms, kThreads, 0, main>>>(s, handle);
+        }
+        else
+        {
+            drift_kernel<T, false, true><<<atoms, kThreads, 0, main>>>(s, handle);
+        }
+        if (cudaGetLastError() != cudaSuccess)
+        {
+            set_error("a step graph could not capture its drift");
+            return fail(ND_ECUDA);
+        }
         cudaStreamCaptureStatus capture_status;
         const cudaGraphNode_t* dependencies = nullptr;
         std::size_t count = 0;
@@ -2733,7 +2764,7 @@ int build_step_graph(const System<T>& s, std::int64_t num_cells, int thermostat,
             set_error("a step graph could not capture its rebuild");
             return fail(ND_ECUDA);
         }
-        rc = launch_rebuild(s, num_cells, 1, body_stream);
+        int rc = launch_rebuild(s, num_cells, 1, body_stream);
         if (rc != ND_OK)
         {
             return fail(rc);

@@ -136,7 +136,7 @@ class Engine:
         self.list_rows = n if small else n + 2 * math.prod(dims) + 2
         t["neighbor_counts"] = torch.zeros(self.list_rows, **ints)
         t["pair_order"] = torch.zeros(2 * (self.list_rows // 2 + 1), **ints)
-        t["rebuild"] = torch.zeros(1, **ints)
+        t["rebuild"] = torch.zeros(2, **ints)  # the reuse flag; the step graph's drift count
         t["rebuild_count"] = torch.zeros(1, **ints)
         t["status"] = torch.zeros(4, **ints)
         t["totals"] = torch.zeros(16, **doubles)
