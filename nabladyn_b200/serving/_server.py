@@ -108,6 +108,28 @@ class _Staged:
     frame: torch.Tensor  # [n, 9] float32: x, y, z, 0, vx, vy, vz, m, 1/m
 
 
+@dataclass
+class _Lane:
+    """One stream of rounds: its active replicas by slot, its rounds launched and not yet read
+    (slots, table copy, event), its table copies' host buffers and the room its harvested
+    replicas free once its later rounds have run. ``steps`` is the fixed budget of a round
+    (None: the round's atom-steps divided by the replica's size)."""
+
+    name: str
+    stream: torch.cuda.Stream
+    steps: int | None
+    active: dict = field(default_factory=dict)
+    rounds: deque = field(default_factory=deque)
+    deferred: deque = field(default_factory=deque)
+    table_hosts: list | None = None
+    table_turn: int = 0
+
+    def budget(self, entry: _Active, round_atom_steps: int) -> int:
+        n = entry.request.positions.shape[0]
+        steps = self.steps if self.steps is not None else -(-round_atom_steps // n)
+        return max(1, min(entry.steps_left, steps))
+
+
 class ReplicaServer:
     """Resident replicas in one device pool, advanced in rounds by the replica kernel.
 
@@ -115,12 +137,17 @@ class ReplicaServer:
     resident at once; ``round_atom_steps`` is the work a slot gets per round, in atom-steps;
     ``stage_ahead`` is how many arrived requests the host makes ready (slot record, frame in
     pinned memory) while a round runs on the device (0: each at its admission).
+    ``large_atoms``: replicas of at least this many atoms run in rounds of their own, on a
+    second stream, ``large_round_steps`` steps a round (None: one stream for all).
     """
 
     def __init__(self, *, device: torch.device | str = "cuda", budget_bytes: int = 4 << 30,
-                 max_slots: int = 2048, round_atom_steps: int = 200_000, stage_ahead: int = 32):
+                 max_slots: int = 2048, round_atom_steps: int = 200_000, stage_ahead: int = 32,
+                 large_atoms: int | None = 8192, large_round_steps: int = 25):
         self.device = torch.device(device)
         self.stage_ahead = int(stage_ahead)
+        self.large_atoms = None if large_atoms is None else int(large_atoms)
+        self.large_round_steps = int(large_round_steps)
         self.max_slots = int(max_slots)
         self.round_atom_steps = int(round_atom_steps)
         self.capacity = max(_ALIGN, (int(budget_bytes) // _BYTES_PER_ATOM) // _ALIGN * _ALIGN)
@@ -271,7 +298,7 @@ class ReplicaServer:
         dtype = torch.from_numpy(np.empty(0, dtype=values.dtype)).dtype
         return device.view(dtype).reshape(values.shape)
 
-    def _place(self, batch: list[tuple[_Staged, int, int]]) -> None:
+    def _place(self, batch: list[tuple[_Staged, int, int]], lane: str = "") -> None:
         """The device part of admissions, for a batch at once: the frames' pinned rows copied
         into one device block and scattered into the pool, the slot records written with their
         offsets; no host sync."""
@@ -289,8 +316,8 @@ class ReplicaServer:
             records += ctypes.string_at(ctypes.addressof(record), size)
             destination.append(np.arange(offset, offset + n, dtype=np.int64))
         frames = np.concatenate([staged.frame.numpy() for staged, _, _ in batch])
-        rows = self._upload("frames", frames)
-        index = self._upload("rows", np.concatenate(destination))
+        rows = self._upload("frames" + lane, frames)
+        index = self._upload("rows" + lane, np.concatenate(destination))
         b = self.buffers
         b["positions"].index_copy_(0, index, rows[:, :4])
         b["velocities"].index_copy_(0, index, rows[:, 4:7])
@@ -298,16 +325,20 @@ class ReplicaServer:
         b["masses"].index_copy_(0, index, rows[:, 7])
         b["inverse_masses"].index_copy_(0, index, rows[:, 8])
         b["images"].index_fill_(0, index, 0)
-        slots = self._upload("slots", np.array([slot for _, slot, _ in batch], dtype=np.int64))
-        table = self._upload("records",
+        slots = self._upload("slots" + lane,
+                             np.array([slot for _, slot, _ in batch], dtype=np.int64))
+        table = self._upload("records" + lane,
                              np.frombuffer(bytes(records), dtype=np.uint8).reshape(-1, size))
         self.table.view(self.max_slots, size).index_copy_(0, slots, table)
 
-    def _launch(self, slots: list[int], budgets: list[int] | None, mode: int) -> None:
+    def _launch(self, slots: list[int], budgets: list[int] | None, mode: int,
+                lane: str = "") -> None:
         if not slots:
             return
-        slot_tensor = self._upload(f"launch_slots_{mode}", np.asarray(slots, dtype=np.int32))
-        budget_tensor = (self._upload("launch_budgets", np.asarray(budgets, dtype=np.int32))
+        slot_tensor = self._upload(f"launch_slots_{mode}{lane}",
+                                   np.asarray(slots, dtype=np.int32))
+        budget_tensor = (self._upload("launch_budgets" + lane,
+                                      np.asarray(budgets, dtype=np.int32))
                          if budgets is not None else None)
         with torch.cuda.device(self.device):
             call("nd_serve_run", self.pool, slot_tensor.data_ptr(),
@@ -320,10 +351,12 @@ class ReplicaServer:
         offset = getattr(Replica, name).offset
         return np.ascontiguousarray(raw[:, offset:offset + 4]).view(np.int32)[:, 0]
 
-    def _harvest(self, done: list[tuple[_Active, np.ndarray]], now: float) -> list[ReplicaResult]:
+    def _harvest(self, done: list[tuple[_Active, np.ndarray]], now: float,
+                 freed: list[tuple[int, int, int]]) -> list[ReplicaResult]:
         """Finished replicas' frames (positions wrapped as space.wrap does, pending chain factor
         applied to the velocities, images with the last crossings): computed on the device for
-        all of them together and read back in one copy; their room is freed."""
+        all of them together and read back in one copy; their room and slots go to `freed` as
+        (first unit, units, slot)."""
         if not done:
             return []
         rows, cells, scales, sizes = [], [], [], []
@@ -368,9 +401,13 @@ class ReplicaServer:
                 steps=int(active.request.steps) - int(record.steps_left),
             ))
             begin = end
-            self._give(active.offset // _ALIGN, active.units)
-            self._free_slots.append(active.slot)
+            freed.append((active.offset // _ALIGN, active.units, active.slot))
         return results
+
+    def _release(self, freed: list[tuple[int, int, int]]) -> None:
+        for first, units, slot in freed:
+            self._give(first, units)
+            self._free_slots.append(slot)
 
     # -- the loop ------------------------------------------------------------------------
 
@@ -381,24 +418,37 @@ class ReplicaServer:
         With ``realtime`` the arrivals follow the wall clock from the call (a request is
         admitted only once its arrival time has passed); without, all are present at once.
 
-        The rounds are pipelined: round k+1 is launched before round k's slot table is read,
-        so the device runs a round while the host reads the previous one, harvests the
-        replicas that finished in it (on a side stream) and admits new ones. A slot keeps its
-        replica in every round launched before the host learns that it finished; the kernel
-        clamps each budget to the steps left, so such a replica runs no further step.
+        Replicas run in rounds on one of two lanes, each a stream of its own: replicas of at
+        least ``large_atoms`` atoms ``large_round_steps`` steps a round, the others a budget of
+        steps inversely proportional to their size. A large replica is then not held to a small
+        share of every round while many small ones wait (it would finish last, on a nearly idle
+        GPU), and a round of small replicas does not wait for the large ones' CTAs; the two
+        lanes' CTAs share the SMs.
+
+        The rounds are pipelined: each lane keeps its next round queued behind the running
+        one, and the host polls the lanes, reading a round's slot table once it has run,
+        harvesting the replicas that finished in it (on a side stream) and admitting new ones.
+        A slot keeps its replica in every round launched before the host learns that it
+        finished; the kernel clamps each budget to the steps left, so such a replica runs no
+        further step, and its slot and room are reused only once those rounds have run.
         """
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         for request in pending:
             n = request.positions.shape[0]
             if -(-n // _ALIGN) > self.capacity // _ALIGN:
                 raise ValueError(f"a replica of {n} atoms exceeds the server's budget")
-        active: dict[int, _Active] = {}
+        lanes = [_Lane("", torch.cuda.current_stream(self.device), None)]
+        if self.large_atoms is not None:
+            lanes.append(_Lane("_large", torch.cuda.Stream(self.device), self.large_round_steps))
         results: list[ReplicaResult] = []
         staged: dict[int, _Staged] = {}  # by id(request): host work done ahead of admission
-        # High priority: the harvest's few small kernels go ahead of the round's waiting CTAs.
+        # High priority: the harvest's few small kernels go ahead of the rounds' waiting CTAs.
         side = torch.cuda.Stream(self.device, priority=-1)
-        inflight = None  # the last round launched and not yet read: (slots, table copy, event)
         start = time.perf_counter()
+
+        def lane_of(request: ReplicaRequest) -> _Lane:
+            large = self.large_atoms is not None and request.positions.shape[0] >= self.large_atoms
+            return lanes[-1] if large else lanes[0]
 
         def stage_ahead(now: float) -> None:
             # Host preparation of the requests that have arrived, a bounded number ahead.
@@ -408,9 +458,13 @@ class ReplicaServer:
                 if id(request) not in staged:
                     staged[id(request)] = self._stage(request)
 
-        while pending or active:
+        while pending or any(lane.active or lane.rounds for lane in lanes):
+            for lane in lanes:  # room and slots whose last rounds have run
+                while lane.deferred and (lane.deferred[0][0] is None or
+                                         lane.deferred[0][0].query()):
+                    self._release(lane.deferred.popleft()[1])
             now = time.perf_counter() - start
-            placing = []
+            placing: dict[str, list] = {lane.name: [] for lane in lanes}
             while pending and (not realtime or pending[0].arrival <= now):
                 request = pending[0]
                 units = -(-request.positions.shape[0] // _ALIGN)
@@ -422,48 +476,72 @@ class ReplicaServer:
                 pending.popleft()
                 slot = self._free_slots.pop()
                 offset = first * _ALIGN
-                ready = staged.pop(id(request), None) or self._stage(request)
-                placing.append((ready, slot, offset))
+                ready = staged.pop(id(request)) if id(request) in staged else self._stage(request)
+                lane = lane_of(request)
+                placing[lane.name].append((ready, slot, offset))
                 # The pinned frame may go once its copy is queued: the host allocator keeps
                 # the block until the copy has run.
-                active[slot] = _Active(request, slot, offset, units, now, int(request.steps))
-            self._place(placing)
-            self._launch([slot for _, slot, _ in placing], None, 0)
-            if not active:
-                if pending and realtime:
-                    time.sleep(max(0.0, min(pending[0].arrival - now, 0.001)))
-                continue
-            launched = [(slot, active[slot]) for slot in active]
-            budgets = [max(1, min(entry.steps_left,
-                                  -(-self.round_atom_steps // entry.request.positions.shape[0])))
-                       for _, entry in launched]
-            self._launch([slot for slot, _ in launched], budgets, 1)
-            table_copy = self._table_copy()
-            # While the round runs: the next admissions' host work, then the previous round.
+                lane.active[slot] = _Active(request, slot, offset, units, now,
+                                            int(request.steps))
+            progressed = False
+            for lane in lanes:
+                with torch.cuda.stream(lane.stream):
+                    batch = placing[lane.name]
+                    self._place(batch, lane.name)
+                    self._launch([slot for _, slot, _ in batch], None, 0, lane.name)
+                    if lane.active and len(lane.rounds) < 2:
+                        launched = [(slot, lane.active[slot]) for slot in lane.active]
+                        budgets = [lane.budget(entry, self.round_atom_steps)
+                                   for _, entry in launched]
+                        self._launch([slot for slot, _ in launched], budgets, 1, lane.name)
+                        lane.rounds.append((launched, *self._table_copy(lane)))
+                        progressed = True
+            # While the rounds run: the next admissions' host work, then the finished rounds.
             if self.stage_ahead:
                 stage_ahead(time.perf_counter() - start)
-            if inflight is not None:
-                results.extend(self._collect(inflight, active, side, start))
-            inflight = (launched, *table_copy)
-        torch.cuda.current_stream(self.device).synchronize()
+            for lane in lanes:
+                # A round is read once it has run; with one lane, as soon as the next round is
+                # queued behind it (or none will be), waiting for it.
+                alone = len(lanes) == 1 and (len(lane.rounds) == 2 or not lane.active)
+                if lane.rounds and (alone or lane.rounds[0][2].query()):
+                    freed: list[tuple[int, int, int]] = []
+                    results.extend(self._collect(lane.rounds.popleft(), lane.active, side,
+                                                 start, freed))
+                    if len(lanes) == 1:
+                        self._release(freed)  # the stream's order keeps later rounds apart
+                    elif freed:
+                        last = lane.rounds[-1][2] if lane.rounds else None
+                        lane.deferred.append((last, freed))
+                    progressed = True
+            if not progressed:
+                if not any(lane.active or lane.rounds for lane in lanes) and pending and realtime:
+                    time.sleep(max(0.0, min(pending[0].arrival - now, 0.001)))
+                else:
+                    time.sleep(5e-5)
+        for lane in lanes:
+            lane.stream.synchronize()
+        side.synchronize()
+        for lane in lanes:
+            for _, freed in lane.deferred:
+                self._release(freed)
         return results
 
-    def _table_copy(self) -> tuple[torch.Tensor, torch.cuda.Event]:
-        """The slot table after the round just launched, copied to pinned host memory without a
-        host sync (two buffers in turn: a copy is read before the one after next is made)."""
-        if not hasattr(self, "_table_hosts"):
-            self._table_hosts = [torch.empty_like(self.table, device="cpu").pin_memory()
-                                 for _ in range(2)]
-            self._table_turn = 0
-        host = self._table_hosts[self._table_turn]
-        self._table_turn ^= 1
+    def _table_copy(self, lane: "_Lane") -> tuple[torch.Tensor, torch.cuda.Event]:
+        """The slot table after the round just launched on the lane's stream, copied to pinned
+        host memory without a host sync (two buffers per lane in turn: a lane has at most two
+        rounds outstanding, and a copy is read before the one after next is made)."""
+        if lane.table_hosts is None:
+            lane.table_hosts = [torch.empty_like(self.table, device="cpu").pin_memory()
+                                for _ in range(2)]
+        host = lane.table_hosts[lane.table_turn]
+        lane.table_turn ^= 1
         host.copy_(self.table, non_blocking=True)
         event = torch.cuda.Event()
         event.record(torch.cuda.current_stream(self.device))
         return host, event
 
     def _collect(self, round_, active: dict[int, _Active], side: torch.cuda.Stream,
-                 start: float) -> list[ReplicaResult]:
+                 start: float, freed: list[tuple[int, int, int]]) -> list[ReplicaResult]:
         """Reads a round's slot table (waiting for that round only) and harvests the replicas
         it finished. A slot whose replica changed since the round was launched is skipped: its
         entry in that table still describes the replica that left."""
@@ -488,6 +566,6 @@ class ReplicaServer:
         # stream after this round.
         side.wait_event(event)
         with torch.cuda.stream(side):
-            return self._harvest(done, now)
+            return self._harvest(done, now, freed)
 
 __all__ = ("ReplicaRequest", "ReplicaResult", "ReplicaServer")

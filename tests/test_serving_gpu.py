@@ -58,6 +58,27 @@ def test_alone_equals_mixed(cuda):
         assert a.energy == b.energy
 
 
+def test_two_lanes_equal_one_lane(cuda):
+    # Replicas of at least 1,500 atoms run in the second stream's rounds (9 steps a round),
+    # the rest beside them; every result equals its run on a single lane, bit for bit (a
+    # replica's trajectory does not depend on how its steps are split into rounds).
+    requests = serving_requests(20, seed=13, steps=45, smallest=200, largest=6000, rate=300.0)
+    assert sum(r.positions.shape[0] >= 1500 for r in requests) >= 4
+    one = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=32, large_atoms=None)
+    single = {r.name: r for r in one.serve(requests, realtime=False)}
+    two = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=32, large_atoms=1500,
+                        large_round_steps=9, round_atom_steps=30_000)
+    lanes = {r.name: r for r in two.serve(requests, realtime=True)}
+    assert set(lanes) == set(single)
+    for name, a in single.items():
+        b = lanes[name]
+        assert a.status == b.status == 0 and a.steps == b.steps == 45
+        np.testing.assert_array_equal(a.positions, b.positions)
+        np.testing.assert_array_equal(a.velocities, b.velocities)
+        np.testing.assert_array_equal(a.images, b.images)
+        assert a.energy == b.energy
+
+
 def test_grid_replica_energy_against_oracle(cuda):
     positions, cell = lattice.fcc(10, 10 * 0.5745, 0.03, seed=9)  # 4,000 atoms, >= 3 cells/axis
     request = ReplicaRequest(positions=positions, velocities=np.zeros_like(positions),
