@@ -79,6 +79,26 @@ def test_two_lanes_equal_one_lane(cuda):
         assert a.energy == b.energy
 
 
+def test_two_lanes_reuse_slots_and_room(cuda):
+    # Four slots and room for about 8,000 atoms: harvested slots and room are taken again,
+    # across the lanes, only after the rounds that still named them have run; every result
+    # equals its single-lane run bit for bit.
+    requests = serving_requests(14, seed=17, steps=30, smallest=300, largest=3000, rate=500.0)
+    one = ReplicaServer(device=cuda, budget_bytes=64 << 20, max_slots=16, large_atoms=None)
+    single = {r.name: r for r in one.serve(requests, realtime=False)}
+    two = ReplicaServer(device=cuda, budget_bytes=4 << 20, max_slots=4, large_atoms=1200,
+                        large_round_steps=7, round_atom_steps=20_000)
+    results = two.serve(requests, realtime=True)
+    assert len(results) == len(requests) and len({r.name for r in results}) == len(requests)
+    assert len({r.admitted for r in results}) > 4  # slots and room were reused
+    for b in results:
+        a = single[b.name]
+        assert a.status == b.status == 0 and a.steps == b.steps == 30
+        np.testing.assert_array_equal(a.positions, b.positions)
+        np.testing.assert_array_equal(a.velocities, b.velocities)
+        assert a.energy == b.energy
+
+
 def test_grid_replica_energy_against_oracle(cuda):
     positions, cell = lattice.fcc(10, 10 * 0.5745, 0.03, seed=9)  # 4,000 atoms, >= 3 cells/axis
     request = ReplicaRequest(positions=positions, velocities=np.zeros_like(positions),
