@@ -105,6 +105,33 @@ def test_replica_record_layout_and_pool_allocator():
     server._give(b, 5)
     assert server._free_units == [(0, total)]
     assert server._take(total + 1) is None
+    # Freed room and slots are handed back together, in the order given.
+    server._take(4)
+    server._release([(0, 4, 3)])
+    assert server._free_units == [(0, total)] and server._free_slots[-1] == 3
+
+
+def test_serving_lane_budgets():
+    """A round's budget: the large lane's fixed steps, the other lane's atom-steps over the
+    replica's size (at least one step), both clamped to the steps left (no device needed)."""
+    import numpy as np
+
+    from nabladyn_b200.serving._server import ReplicaRequest, _Active, _Lane
+
+    def entry(n, left):
+        request = ReplicaRequest(positions=np.zeros((n, 3)), velocities=np.zeros((n, 3)),
+                                 masses=np.ones(n), cell=np.full(3, 5.0), temperature=100.0,
+                                 steps=500)
+        return _Active(request, 0, 0, -(-n // 32), 0.0, left)
+
+    small = _Lane("", None, None)  # the stream is not needed for a budget
+    large = _Lane("_large", None, 25)
+    assert small.budget(entry(1000, 500), 200_000) == 200
+    assert small.budget(entry(64, 500), 200_000) == 500  # clamped to the steps left
+    assert small.budget(entry(16384, 500), 200_000) == 13
+    assert small.budget(entry(300_000, 500), 200_000) == 1
+    assert large.budget(entry(16384, 500), 200_000) == 25
+    assert large.budget(entry(16384, 7), 200_000) == 7
 
 
 def test_torch_ops_load_first_in_a_fresh_process():
